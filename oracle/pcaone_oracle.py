@@ -1,0 +1,364 @@
+"""ORACLE -- test infrastructure only.
+
+A CPU restatement, in numpy (FP64), of the reference PCAone v0.6.0 hot path. It is the checker
+for the CUDA path and is imported only by tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` leg of ``bench.py``; the product never calls it.
+
+Every function cites the reference file:line it restates (paths inside the PCAone project).
+Its parity is pinned against the reference binary built by ``oracle/ref.mk`` (golden outputs
+under ``tests/golden/``) and against the reference's own Omega/permutation draws
+(``oracle/_ref/omega_ref``).
+"""
+from __future__ import annotations
+
+import ctypes
+import gzip
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+# src/Common.hpp:57-58  BED2GENO = {1, -9 (missing), 0.5, 0} for codes 00, 01, 10, 11
+BED2GENO = np.array([1.0, -9.0, 0.5, 0.0])
+VAR_TOL = 1e-9  # src/Data.hpp:7
+
+
+# --------------------------------------------------------------------------- RNG draws
+def _rnglib():
+    path = os.path.join(_HERE, "liboracle_rng.so")
+    if not os.path.exists(path):
+        import subprocess
+
+        subprocess.check_call(["g++", "-O2", "-shared", "-fPIC", "-o", path,
+                               os.path.join(_HERE, "rng.cpp")])
+    lib = ctypes.CDLL(path)
+    lib.oracle_omega.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ctypes.c_long,
+                                 ctypes.c_void_p]
+    lib.oracle_shuffle.argtypes = [ctypes.c_long, ctypes.c_void_p]
+    return lib
+
+
+def omega(seed: int, nrow: int, ncol: int, rand: int = 1) -> np.ndarray:
+    """Omega as drawn by RsvdOpData::initOmg (src/Halko.cpp:14-22), column-major fill."""
+    out = np.zeros(nrow * ncol)
+    _rnglib().oracle_omega(seed, rand, nrow, ncol, out.ctypes.data)
+    return out.reshape(ncol, nrow).T.copy()
+
+
+def shuffle_perm(n: int) -> np.ndarray:
+    """In-core SNP permutation of permute_matrix (src/RSVD.hpp:63-79)."""
+    out = np.zeros(n, dtype=np.int32)
+    _rnglib().oracle_shuffle(n, out.ctypes.data)
+    return out
+
+
+# --------------------------------------------------------------------------- PLINK input
+@dataclass
+class Bed:
+    N: int
+    M: int
+    packed: np.ndarray  # (M, bpr) uint8, SNP-major as on disk
+
+    @property
+    def bpr(self) -> int:
+        return (self.N + 3) >> 2
+
+
+def count_lines(path: str) -> int:
+    """count_lines (src/Utils.cpp:94-103)."""
+    with open(path, "rb") as f:
+        return sum(1 for _ in f)
+
+
+def read_bed(prefix: str) -> Bed:
+    """FileBed constructor (src/FilePlink.hpp:10-26): N from .fam, M from .bim, magic check."""
+    N = count_lines(prefix + ".fam")
+    M = count_lines(prefix + ".bim")
+    raw = np.fromfile(prefix + ".bed", dtype=np.uint8)
+    if raw.size < 3 or raw[0] != 0x6C or raw[1] != 0x1B or raw[2] != 0x01:
+        raise ValueError("Incorrect magic number in plink bed file.")
+    bpr = (N + 3) >> 2
+    if raw.size < 3 + M * bpr:
+        raise ValueError("truncated .bed")
+    return Bed(N, M, raw[3:3 + M * bpr].reshape(M, bpr).copy())
+
+
+def decode_codes(bed: Bed) -> np.ndarray:
+    """2-bit codes as an (M, N) uint8 matrix (src/FilePlink.cpp:70-88, LSB-first)."""
+    p = bed.packed
+    codes = np.stack([(p >> (2 * k)) & 3 for k in range(4)], axis=2).reshape(bed.M, -1)
+    return codes[:, :bed.N].copy()
+
+
+def allele_counts(codes: np.ndarray):
+    """Integer per-SNP counts (n_hom_A1, n_het, n_nonmissing) for FileBed::read_all
+    (src/FilePlink.cpp:36-64)."""
+    n00 = (codes == 0).sum(axis=1).astype(np.int64)
+    n10 = (codes == 2).sum(axis=1).astype(np.int64)
+    n01 = (codes == 1).sum(axis=1).astype(np.int64)
+    nonmiss = codes.shape[1] - n01
+    return n00, n10, nonmiss
+
+
+def allele_freq(codes: np.ndarray) -> np.ndarray:
+    """F_j = sum of BED2GENO over non-missing / count (src/FilePlink.cpp:36-57).
+    The FP64 sum of {1, 0.5, 0} is exact, so F = ((2 n00 + n10) * 0.5) / c bit-for-bit."""
+    n00, n10, c = allele_counts(codes)
+    s = (2 * n00 + n10).astype(np.float64) * 0.5
+    with np.errstate(invalid="ignore", divide="ignore"):
+        F = np.where(c == 0, 0.0, s / np.maximum(c, 1))
+    return F
+
+
+def centered_matrix(codes: np.ndarray, F: np.ndarray) -> np.ndarray:
+    """G (N x M) = BED2GENO[code] - F_j, missing -> 0 (src/FilePlink.cpp:70-115)."""
+    G = BED2GENO[codes].T.copy()  # N x M
+    miss = codes.T == 1
+    G -= F[None, :]
+    G[miss] = 0.0
+    return G
+
+
+def standardize(G: np.ndarray, F: np.ndarray, ploidy: int = 2) -> np.ndarray:
+    """Data::standardize_E (src/Data.cpp:290-299): G_ij /= sqrt(ploidy F (1-F)) if > 1e-9."""
+    sd = np.sqrt(float(ploidy) * F * (1 - F))
+    out = G.copy()
+    ok = sd > VAR_TOL
+    out[:, ok] /= sd[ok][None, :]
+    return out
+
+
+def standardized_from_bed(bed: Bed, standardize_geno: bool = True) -> tuple[np.ndarray, np.ndarray]:
+    codes = decode_codes(bed)
+    F = allele_freq(codes)
+    G = centered_matrix(codes, F)
+    if standardize_geno:
+        G = standardize(G, F)
+    return G, F
+
+
+# --------------------------------------------------------------------------- RSVD
+def householder_q(H: np.ndarray) -> np.ndarray:
+    """Thin Q of a Householder QR with R_ii = -sign(x_0)||x|| (Eigen::HouseholderQR and LAPACK
+    dgeqrf share this sign convention)."""
+    q, _ = np.linalg.qr(H, mode="reduced")
+    return q
+
+
+def flip_omg(Omg2: np.ndarray, Omg: np.ndarray) -> np.ndarray:
+    """PCAone::flipOmg (src/RSVD.hpp:81-90). Returns the flipped Omg (also the new Omg2)."""
+    out = Omg.copy()
+    for i in range(out.shape[1]):
+        if np.abs(Omg2[:, i] - out[:, i]).sum() > 2 * np.abs(Omg2[:, i] + out[:, i]).sum():
+            out[:, i] *= -1
+    return out
+
+
+def mev(X: np.ndarray, Y: np.ndarray) -> float:
+    """mev (src/Utils.cpp:192-198)."""
+    return float(np.mean([np.linalg.norm(X.T @ Y[:, i]) for i in range(X.shape[1])]))
+
+
+@dataclass
+class RsvdResult:
+    U: np.ndarray
+    S: np.ndarray
+    V: np.ndarray
+    epochs: int
+    diffs: list = field(default_factory=list)
+
+
+def _usv_step(G, H, k):
+    """One computeUSV epoch tail (src/Halko.cpp:54-69): QR(G) twice, B = R^-T H^T, SVD(B)."""
+    Q1, R1 = np.linalg.qr(G, mode="reduced")
+    Q2, R2 = np.linalg.qr(Q1, mode="reduced")
+    R = R2 @ R1
+    B = np.linalg.solve(R.T, H.T)
+    ub, s, vbt = np.linalg.svd(B, full_matrices=False)
+    return Q2, ub, s, vbt.T
+
+
+class _HalkoState:
+    def __init__(self, N, l, seed, rand):
+        self.N, self.l, self.seed, self.rand = N, l, seed, rand
+        self.init_omg()
+
+    def init_omg(self):
+        self.Omg = omega(self.seed, self.N, self.l, self.rand)
+        self.Omg2 = self.Omg.copy()
+
+
+def compute_usv(Z: np.ndarray, k: int, os_: int, p: int, tol: float, gandh, state,
+                winsvd_bands: int | None = None) -> RsvdResult:
+    """RsvdOpData::computeUSV (src/Halko.cpp:45-95). Z is N x M (samples x SNPs)."""
+    N, M = Z.shape
+    Upre = None
+    diffs = []
+    pi = 0
+    Ucur = None
+    while pi <= p:
+        G, H = gandh(pi)
+        Q2, ub, s, vb = _usv_step(G, H, k)
+        Ucur = vb[:, :k]
+        if pi > 0:
+            diff = 1 - mev(Ucur, Upre)
+            diffs.append(diff)
+            if diff < tol or pi == p:
+                if winsvd_bands is not None and 2 ** pi < winsvd_bands:
+                    p = int(np.log2(winsvd_bands))
+                else:
+                    V = Q2 @ ub[:, :k]
+                    return RsvdResult(Ucur, s[:k], V, pi + 1, diffs)
+            else:
+                Upre = Ucur
+        else:
+            Upre = Ucur
+        pi += 1
+    raise RuntimeError("unreachable")  # the loop always returns at pi == p
+
+
+def halko(Z: np.ndarray, k: int, os_: int, p: int, tol: float, seed: int = 101,
+          rand: int = 1) -> RsvdResult:
+    """sSVD, NormalRsvdOpData::computeGandH in-core (src/Halko.cpp:97-125)."""
+    N, M = Z.shape
+    l = k + os_
+    st = _HalkoState(N, l, seed, rand)
+    last = {}
+
+    def gandh(pi):
+        if pi == 0:
+            st.init_omg()
+        else:
+            st.Omg = flip_omg(st.Omg2, householder_q(last["H"]))
+            st.Omg2 = st.Omg.copy()
+        G = Z.T @ st.Omg
+        H = Z @ G
+        last["H"] = H
+        return G, H
+
+    return compute_usv(Z, k, os_, p, tol, gandh, st)
+
+
+def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed: int = 101,
+           rand: int = 1, update_hook=None) -> RsvdResult:
+    """Window-based RSVD, FancyRsvdOpData::computeGandH in-core (src/Halko.cpp:153-226).
+    Z must already be column-permuted when the reference permutes (src/Halko.cpp:181-184)."""
+    N, M = Z.shape
+    l = k + os_
+    st = _HalkoState(N, l, seed, rand)
+    H1 = np.zeros((N, l))
+    H2 = np.zeros((N, l))
+    sched = {"bandsize": 1}
+    blocksize = int(np.ceil(M / bands))
+
+    def gandh(pi):
+        nonlocal H1, H2
+        if pi == 0:
+            st.init_omg()
+        if 2 ** pi >= bands:
+            H1[:] = 0
+            H2[:] = 0
+        if pi == 0:
+            sched["bandsize"] = 1
+        sched["bandsize"] = min(sched["bandsize"] * 2, bands)
+        bandsize = sched["bandsize"]
+        G = np.zeros((M, l))
+        H = None
+        i = 1
+        for b in range(bands):
+            s0 = b * blocksize
+            s1 = M if (b + 1) * blocksize >= M else (b + 1) * blocksize
+            if s0 < M:
+                Gb = Z[:, s0:s1].T @ st.Omg
+                G[s0:s1] = Gb
+                if i <= bandsize // 2:
+                    H1 += Z[:, s0:s1] @ Gb
+                else:
+                    H2 += Z[:, s0:s1] @ Gb
+            adjacent = pi > 0 and (b + 1) == 2 ** (pi - 1) and 2 ** pi < bands
+            if (b + 1) < bandsize and not adjacent:
+                i += 1
+                continue
+            if not (i == bandsize or i == bandsize // 2 or adjacent):
+                i += 1
+                continue
+            H = H1 + H2
+            st.Omg = flip_omg(st.Omg2, householder_q(H))
+            st.Omg2 = st.Omg.copy()
+            if update_hook is not None:
+                update_hook(pi, b, st.Omg)
+            if i == bandsize:
+                H1[:] = 0
+                i = 0
+            else:
+                H2[:] = 0
+            i += 1
+        return G, H
+
+    return compute_usv(Z, k, os_, p, tol, gandh, st, winsvd_bands=bands)
+
+
+def run_pca(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: int = 10,
+            bands: int = 64, tol: float = 1e-4, seed: int = 101, rand: int = 1,
+            shuffle: bool = True, standardize_geno: bool = True):
+    """Plain (no EM) PLINK PCA, run_pca_with_halko (src/Halko.cpp:272-293, 338-342).
+    Returns (eigvals, sigvals, U, V, F, epochs) with V in original SNP order."""
+    os_ = max(oversamples, k)  # src/Cmd.cpp:190
+    Z, F = standardized_from_bed(bed, standardize_geno)
+    if svd == 1:
+        res = halko(Z, k, os_, maxp, tol, seed, rand)
+        V = res.V
+    elif svd == 2:
+        perm = shuffle_perm(bed.M) if shuffle else np.arange(bed.M, dtype=np.int32)
+        res = winsvd(Z[:, perm], k, os_, maxp, tol, bands, seed, rand)
+        V = np.empty_like(res.V)
+        V[perm] = res.V  # data->perm * V (src/Halko.cpp:340)
+    else:
+        raise ValueError("svd must be 1 or 2")
+    eig = res.S ** 2 / bed.M * 2  # src/Halko.cpp:340, ploidy in src/Data.cpp:186
+    return eig, res.S, res.U, V, F, res.epochs
+
+
+def dense_eig(bed: Bed, k: int, standardize_geno: bool = True):
+    """FP64 dense oracle: eigenvalues sigma^2/M*ploidy and U from the full SVD of Z."""
+    Z, F = standardized_from_bed(bed, standardize_geno)
+    u, s, vt = np.linalg.svd(Z, full_matrices=False)
+    return s[:k] ** 2 / bed.M * 2, s[:k], u[:, :k], vt[:k].T
+
+
+# --------------------------------------------------------------------------- comparisons
+def principal_angles(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    qa, _ = np.linalg.qr(A)
+    qb, _ = np.linalg.qr(B)
+    s = np.linalg.svd(qa.T @ qb, compute_uv=False)
+    return np.arccos(np.clip(s, -1.0, 1.0))
+
+
+def max_col_err_up_to_sign(A: np.ndarray, B: np.ndarray) -> float:
+    err = 0.0
+    for i in range(A.shape[1]):
+        e = min(np.abs(A[:, i] - B[:, i]).max(), np.abs(A[:, i] + B[:, i]).max())
+        err = max(err, e)
+    return err
+
+
+# --------------------------------------------------------------------------- text IO
+def fmt6(x: float) -> str:
+    """One value as Eigen IOFormat(6, DontAlignCols, "\\t", "\\n") prints it (stream precision 6,
+    default float format), i.e. C's %.6g."""
+    return format(float(x), ".6g")
+
+
+def read_table(path: str) -> np.ndarray:
+    with open(path) as f:
+        rows = [[float(t) for t in line.split("\t")] for line in f if line.strip()]
+    return np.array(rows)
+
+
+def read_ld_gz(path: str):
+    with gzip.open(path, "rt") as f:
+        head = f.readline()
+        rows = [line.rstrip("\n").split("\t") for line in f]
+    return head, rows

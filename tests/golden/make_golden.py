@@ -1,0 +1,103 @@
+"""Regenerates the golden fixtures in this folder.
+
+Inputs are small seeded synthetic datasets written by the package's simulator
+(``pcaone_b200/bin/pcaone-sim``); outputs are produced by the unmodified reference PCAone
+v0.6.0 binary built from its own sources by ``oracle/ref.mk`` into ``oracle/_ref/PCAone``.
+Run from the repository root in the container that has the reference sources:
+
+    make -f oracle/ref.mk REF=/root/reference -j8
+    python tests/golden/make_golden.py
+
+Each case in ``CASES`` is (name, dataset, reference arguments, output suffixes kept).
+``cases.json`` records the exact commands so the tests can reproduce them.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+SIM = os.path.join(ROOT, "pcaone_b200", "bin", "pcaone-sim")
+REF = os.path.join(ROOT, "oracle", "_ref", "PCAone")
+
+DATASETS = {
+    # odd N (not a multiple of 4) exercises the padded last byte of every SNP record
+    "g1": ["--n", "203", "--m", "1500", "--pops", "3", "--fst", "0.05", "--pmin", "0.05",
+           "--pmax", "0.5", "--miss", "0.01", "--seed", "11"],
+    # heavy per-sample missingness for EMU
+    "g2": ["--n", "120", "--m", "1200", "--pops", "3", "--fst", "0.08", "--pmin", "0.05",
+           "--pmax", "0.5", "--miss-beta", "2,18", "--admix", "0.5", "--seed", "12"],
+    # genotype likelihoods for PCAngsd
+    "g3": ["--n", "80", "--m", "900", "--pops", "3", "--fst", "0.1", "--pmin", "0.05",
+           "--pmax", "0.5", "--beagle", "4,0.01", "--seed", "13"],
+    # two chromosomes with positions for LD windows
+    "g4": ["--n", "100", "--m", "600", "--pops", "3", "--fst", "0.05", "--pmin", "0.05",
+           "--pmax", "0.5", "--miss", "0.01", "--chroms", "2", "--bp-spacing", "500",
+           "--seed", "14"],
+}
+
+EIG = [".eigvals", ".sigvals", ".eigvecs"]
+CASES = [
+    ("g1_halko", "g1", ["-b", "{d}", "-d", "1", "-k", "4", "--oversamples", "10", "-p", "7",
+                        "--tol-rsvd", "0", "-V"], EIG + [".loadings", ".mbim"]),
+    ("g1_halko_p3", "g1", ["-b", "{d}", "-d", "1", "-k", "3", "-p", "3", "--seed", "7"],
+     EIG),
+    ("g1_win", "g1", ["-b", "{d}", "-d", "2", "-k", "4", "-w", "16", "-V"],
+     EIG + [".loadings"]),
+    ("g1_winS", "g1", ["-b", "{d}", "-d", "2", "-k", "4", "-w", "8", "-S", "-V"],
+     EIG + [".loadings"]),
+    ("g1_win_unif", "g1", ["-b", "{d}", "-d", "2", "-k", "3", "-w", "4", "--rand", "0",
+                           "--seed", "3", "-p", "5"], EIG),
+    ("g1_nostd", "g1", ["-b", "{d}", "-d", "1", "-k", "3", "-p", "5", "--tol-rsvd", "0",
+                        "-C", "0"], EIG),
+    ("g2_emu", "g2", ["-b", "{d}", "--emu", "-k", "3", "-w", "8", "--maxiter", "20",
+                      "--tol-em", "1e-6", "-V"], EIG + [".loadings"]),
+    ("g3_pcangsd", "g3", ["-G", "{d}.beagle.gz", "-k", "3", "-S", "-w", "8", "--maxiter", "30",
+                          "-V"], EIG + [".loadings", ".cov"]),
+    ("g3_pcangsd_shuf", "g3", ["-G", "{d}.beagle.gz", "-k", "3", "-w", "8", "--maxiter", "30"],
+     EIG),
+    ("g4_pcs", "g4", ["-b", "{d}", "-d", "1", "-k", "3", "-p", "7", "--tol-rsvd", "0", "-V"],
+     EIG + [".mbim"]),
+    ("g4_ldA", "g4", ["-b", "{d}", "--read-U", "{g}/ref/g4_pcs.eigvecs", "-f",
+                      "{g}/ref/g4_pcs.mbim", "--ld-bp", "5000", "-R"], [".ld.gz"]),
+    ("g4_adj", "g4", ["-b", "{d}", "-d", "1", "-k", "3", "-p", "7", "--tol-rsvd", "0", "-D"],
+     [".residuals", ".mbim"] + EIG),
+    ("g4_ldB", "g4", ["-B", "{g}/ref/g4_adj.residuals", "-f", "{g}/ref/g4_adj.mbim",
+                      "--ld-bp", "5000", "-R"], [".ld.gz"]),
+]
+
+
+def main() -> int:
+    if not os.path.exists(REF):
+        print("reference binary missing: run make -f oracle/ref.mk first", file=sys.stderr)
+        return 1
+    if not os.path.exists(SIM):
+        print("simulator missing: run the package build first", file=sys.stderr)
+        return 1
+    refdir = os.path.join(HERE, "ref")
+    os.makedirs(refdir, exist_ok=True)
+    for name, args in DATASETS.items():
+        subprocess.check_call([SIM, "--out", os.path.join(HERE, name)] + args)
+    record = {"datasets": DATASETS, "cases": []}
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    for name, ds, args, keep in CASES:
+        with tempfile.TemporaryDirectory() as tmp:
+            argv = [a.format(d=os.path.join(HERE, ds), g=HERE) for a in args]
+            out = os.path.join(tmp, name)
+            subprocess.run([REF] + argv + ["-o", out, "-v", "0"], check=True, env=env,
+                           stdout=subprocess.DEVNULL)
+            for suf in keep:
+                shutil.copy(out + suf, os.path.join(refdir, name + suf))
+        record["cases"].append({"name": name, "dataset": ds, "args": args, "outputs": keep})
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(record, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

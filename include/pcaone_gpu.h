@@ -1,0 +1,123 @@
+/*
+ * pcaone_gpu.h -- C ABI of the B200 (sm_100a) implementation of PCAone's randomized-SVD
+ * hot path.
+ *
+ * The reference PCAone is a C++ command-line tool with no library or FFI; its internal
+ * seams on this path are the Data readers (src/Data.hpp:15-20), the RSVD operators
+ * RsvdOpData::computeGandH / computeUSV (src/Halko.hpp:7-42, src/Halko.cpp:45-270), the EM
+ * updates Data::fit_with_pi / pcangsd_standardize_E (src/Data.cpp:247-343) and the LD r2
+ * loop (src/LD.cpp:419-442). Each entry point below replaces one of those seams; the
+ * comment on each names the reference code it stands in for.
+ *
+ * Conventions
+ *  - Every function returns an int status (pcaone_status); 0 is success. No exception or
+ *    C++ type crosses this boundary. pcaone_gpu_last_error() returns the message of the
+ *    last failure on a context.
+ *  - Host buffers are owned by the caller. Matrices are column-major FP64 (as Eigen's
+ *    Mat2D in the reference). No host pointer is retained after a call returns.
+ *  - The context owns all device memory, streams and CUDA graphs on one GPU. Calls on one
+ *    context must be serialised by the caller (one context per host thread).
+ *  - "SNP order" after pcaone_gpu_permute() is the permuted order: SNP j of the context is
+ *    original SNP perm[j] (as G = G * P in src/RSVD.hpp:63-79).
+ */
+#ifndef PCAONE_GPU_H_
+#define PCAONE_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pcaone_ctx pcaone_ctx;
+
+typedef enum {
+  PCAONE_OK = 0,
+  PCAONE_EBADARG = 1,   /* invalid argument or size (e.g. k + oversamples > samples) */
+  PCAONE_EOOM = 2,      /* device allocation failed */
+  PCAONE_ECUDA = 3,     /* CUDA runtime / launch error */
+  PCAONE_ETIMEOUT = 4,  /* a bounded device wait gave up */
+  PCAONE_ENUMERIC = 5,  /* factorisation failed (non-positive Gram matrix) */
+  PCAONE_ESTATE = 6,    /* call out of order (e.g. rsvd before load_bed) */
+  PCAONE_ENODEV = 7     /* no usable sm_100 device / extension not built for it */
+} pcaone_status;
+
+typedef enum {
+  PCAONE_PREC_FP32 = 0,  /* FP32 SIMT decode-GEMMs (the plain FP32 GPU path) */
+  PCAONE_PREC_MIXED = 1, /* tcgen05 BF16 decode-GEMMs, split BF16 hi+lo sketch, FP32 accum */
+  PCAONE_PREC_FP64 = 2   /* FP64 SIMT decode-GEMMs (algorithm-matched FP64 run) */
+} pcaone_precision;
+
+/* Create / destroy a context on CUDA device `device`. Replaces nothing in the reference
+ * (the reference has no device); errors here map to cao.error (src/Logger.hpp:96-105). */
+int pcaone_gpu_create(int device, pcaone_ctx** out);
+int pcaone_gpu_destroy(pcaone_ctx* ctx);
+const char* pcaone_gpu_last_error(const pcaone_ctx* ctx);
+
+/* Upload the packed SNP-major PLINK records (nsnps x ceil(nsamples/4) bytes, the .bed body
+ * without its 3-byte magic) and compute the integer allele counts on the device.
+ * Replaces FileBed::read_all (src/FilePlink.cpp:29-131) up to the F estimate. */
+int pcaone_gpu_load_bed(pcaone_ctx* ctx, const uint8_t* packed, uint64_t nsnps,
+                        uint32_t nsamples);
+
+/* Per-SNP integer counts in the current SNP order: a1x2[j] = 2*n(00) + n(10) (twice the sum
+ * of BED2GENO over non-missing entries, src/FilePlink.cpp:36-57) and nonmiss[j] = number of
+ * non-missing samples. Bit-exact. */
+int pcaone_gpu_counts(pcaone_ctx* ctx, uint32_t* a1x2, uint32_t* nonmiss);
+
+/* Allele frequencies F_j = (a1x2/2)/nonmiss as FP64 (src/FilePlink.cpp:53-56), bit-exact
+ * with the reference's accumulation. */
+int pcaone_gpu_allele_freq(pcaone_ctx* ctx, double* F);
+
+/* Permute SNP records on the device: new SNP j = old SNP perm[j] (src/RSVD.hpp:63-79 for
+ * the in-core winSVD shuffle). perm is a host array of nsnps int32 indices. */
+int pcaone_gpu_permute(pcaone_ctx* ctx, const int32_t* perm);
+
+/* The reference's in-core SNP shuffle (std::shuffle of 0..n-1 with a default-seeded
+ * std::default_random_engine, src/RSVD.hpp:67-70), written to perm (host, n int32). */
+int pcaone_shuffle_perm(uint64_t n, int32_t* perm);
+
+/* The reference's sketch Omega (nrow x ncol, column-major FP64) drawn from
+ * std::default_random_engine seeded with `seed` through std::normal_distribution (rand=1)
+ * or uniform(-1,1) (rand=0), as RsvdOpData::initOmg (src/Halko.cpp:14-22). */
+int pcaone_omega(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);
+
+typedef struct {
+  int32_t k;            /* -k/--pc */
+  int32_t oversamples;  /* effective oversampling (the reference uses max(--oversamples,k)) */
+  int32_t maxp;         /* -p/--maxp: epochs 0..maxp */
+  int32_t svd;          /* 1 = Halko sSVD (--svd 1), 2 = window-based winSVD (--svd 2) */
+  int32_t bands;        /* -w/--batches (winSVD windows); ignored for svd = 1 */
+  int32_t precision;    /* pcaone_precision */
+  int32_t standardize;  /* divide by sqrt(ploidy F (1-F)) (Data::standardize_E) */
+  int32_t ploidy;       /* 2, or 1 with --haploid */
+  int32_t seed;         /* --seed for Omega */
+  int32_t rand;         /* --rand: 1 Gaussian, 0 uniform */
+  double tol;           /* --tol-rsvd */
+  int32_t verbose;      /* print per-epoch "running of epoch" lines to stdout */
+  int32_t profile;      /* time every decode-GEMM launch with CUDA events (gemm_ms) */
+} pcaone_rsvd_opts;
+
+typedef struct {
+  int32_t epochs;        /* epochs run (the reference's "stops at epoch") */
+  int32_t omega_updates; /* Omega re-orthonormalisations performed */
+  double last_diff;      /* last 1 - mev(U, Upre) */
+  double gpu_ms;         /* device time of the whole call (CUDA events) */
+  double gemm_ms;        /* device time inside the decode-GEMM kernels */
+  int64_t kernel_launches;
+  int64_t gemm_launches;
+} pcaone_rsvd_report;
+
+/* Run Halko (svd=1) or window-based (svd=2) RSVD on the loaded genotypes: the epoch loop of
+ * RsvdOpData::computeUSV (src/Halko.cpp:45-95) with NormalRsvdOpData::computeGandH
+ * (src/Halko.cpp:97-126) or FancyRsvdOpData::computeGandH (src/Halko.cpp:153-226).
+ * Outputs (host, column-major): U (nsamples x k), S (k), V (nsnps x k, current SNP order).
+ * Any output pointer may be NULL. report may be NULL. */
+int pcaone_gpu_rsvd(pcaone_ctx* ctx, const pcaone_rsvd_opts* opts, double* U, double* S,
+                    double* V, pcaone_rsvd_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCAONE_GPU_H_ */

@@ -1,0 +1,203 @@
+"""Python binding of the PCAone B200 C ABI (include/pcaone_gpu.h) over ctypes.
+
+This is the ctypes stub a Python caller binds: it loads the in-tree ``lib/libpcaone_gpu.so``
+and fails loudly when that library is missing. There is no CPU fallback: every compute call
+runs on the GPU through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libpcaone_gpu.so")
+BIN_DIR = os.path.join(_HERE, "bin")
+
+PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
+PRECISIONS = {"fp32": PREC_FP32, "mixed": PREC_MIXED, "bf16": PREC_MIXED, "fp64": PREC_FP64}
+
+STATUS = {0: "OK", 1: "EBADARG", 2: "EOOM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENUMERIC",
+          6: "ESTATE", 7: "ENODEV"}
+
+# C ABI symbols declared in include/pcaone_gpu.h
+EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
+           "pcaone_gpu_load_bed", "pcaone_gpu_counts", "pcaone_gpu_allele_freq",
+           "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd"]
+
+
+class PcaoneError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class RsvdOpts(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int32), ("oversamples", ctypes.c_int32),
+                ("maxp", ctypes.c_int32), ("svd", ctypes.c_int32), ("bands", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("standardize", ctypes.c_int32),
+                ("ploidy", ctypes.c_int32), ("seed", ctypes.c_int32), ("rand", ctypes.c_int32),
+                ("tol", ctypes.c_double), ("verbose", ctypes.c_int32),
+                ("profile", ctypes.c_int32)]
+
+
+class RsvdReport(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("omega_updates", ctypes.c_int32),
+                ("last_diff", ctypes.c_double), ("gpu_ms", ctypes.c_double),
+                ("gemm_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64),
+                ("gemm_launches", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the in-tree C ABI library; raise if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C pcaone_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, u32, u64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint64
+        L.pcaone_gpu_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.pcaone_gpu_destroy.argtypes = [vp]
+        L.pcaone_gpu_last_error.argtypes = [vp]
+        L.pcaone_gpu_last_error.restype = ctypes.c_char_p
+        L.pcaone_gpu_load_bed.argtypes = [vp, vp, u64, u32]
+        L.pcaone_gpu_counts.argtypes = [vp, vp, vp]
+        L.pcaone_gpu_allele_freq.argtypes = [vp, vp]
+        L.pcaone_gpu_permute.argtypes = [vp, vp]
+        L.pcaone_shuffle_perm.argtypes = [u64, vp]
+        L.pcaone_omega.argtypes = [ctypes.c_int, ctypes.c_int, u64, u32, vp]
+        L.pcaone_gpu_rsvd.argtypes = [vp, ctypes.POINTER(RsvdOpts), vp, vp, vp,
+                                      ctypes.POINTER(RsvdReport)]
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def shuffle_perm(n: int) -> np.ndarray:
+    """The reference's in-core SNP shuffle (src/RSVD.hpp:63-79)."""
+    out = np.zeros(n, dtype=np.int32)
+    lib().pcaone_shuffle_perm(n, _ptr(out))
+    return out
+
+
+def omega(seed: int, nrow: int, ncol: int, rand: int = 1) -> np.ndarray:
+    """The reference's sketch Omega (src/Halko.cpp:14-22), nrow x ncol."""
+    out = np.zeros(nrow * ncol)
+    lib().pcaone_omega(seed, rand, nrow, ncol, _ptr(out))
+    return out.reshape(ncol, nrow).T.copy()
+
+
+@dataclass
+class RsvdResult:
+    U: np.ndarray
+    S: np.ndarray
+    V: np.ndarray
+    epochs: int
+    omega_updates: int
+    last_diff: float
+    gpu_ms: float
+    gemm_ms: float
+    kernel_launches: int
+    gemm_launches: int
+
+
+class GpuContext:
+    """One GPU context (device memory, stream) holding one genotype matrix."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().pcaone_gpu_create(device, ctypes.byref(h))
+        if st != 0:
+            raise PcaoneError(st, "pcaone_gpu_create failed")
+        self._h = h
+        self.N = self.M = 0
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = lib().pcaone_gpu_last_error(self._h).decode()
+            raise PcaoneError(st, msg)
+
+    def close(self):
+        if self._h:
+            lib().pcaone_gpu_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_bed(self, packed: np.ndarray, nsamples: int):
+        """packed: (M, ceil(N/4)) uint8 SNP-major records."""
+        packed = np.ascontiguousarray(packed, dtype=np.uint8)
+        M = packed.shape[0]
+        if packed.ndim != 2 or packed.shape[1] != (nsamples + 3) // 4:
+            raise ValueError("packed must be (nsnps, ceil(nsamples/4)) bytes")
+        self._check(lib().pcaone_gpu_load_bed(self._h, _ptr(packed), M, nsamples))
+        self.N, self.M = nsamples, M
+
+    def counts(self):
+        a = np.zeros(self.M, dtype=np.uint32)
+        c = np.zeros(self.M, dtype=np.uint32)
+        self._check(lib().pcaone_gpu_counts(self._h, _ptr(a), _ptr(c)))
+        return a, c
+
+    def allele_freq(self) -> np.ndarray:
+        F = np.zeros(self.M)
+        self._check(lib().pcaone_gpu_allele_freq(self._h, _ptr(F)))
+        return F
+
+    def permute(self, perm: np.ndarray):
+        perm = np.ascontiguousarray(perm, dtype=np.int32)
+        self._check(lib().pcaone_gpu_permute(self._h, _ptr(perm)))
+
+    def rsvd(self, k: int = 10, oversamples: int = 10, maxp: int = 20, svd: int = 2,
+             bands: int = 64, precision: int | str = PREC_FP32, standardize: bool = True,
+             ploidy: int = 2, seed: int = 101, rand: int = 1, tol: float = 1e-4,
+             verbose: bool = False, profile: bool = False, want_v: bool = True) -> RsvdResult:
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        os_ = max(oversamples, k)  # src/Cmd.cpp:190
+        o = RsvdOpts(k, os_, maxp, svd, bands, precision, int(standardize), ploidy, seed,
+                     rand, tol, int(verbose), int(profile))
+        U = np.zeros((k, self.N))
+        S = np.zeros(k)
+        V = np.zeros((k, self.M)) if want_v else None
+        rep = RsvdReport()
+        self._check(lib().pcaone_gpu_rsvd(self._h, ctypes.byref(o), _ptr(U), _ptr(S),
+                                          _ptr(V), ctypes.byref(rep)))
+        return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
+                          rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
+                          rep.kernel_launches, rep.gemm_launches)
+
+
+def read_bed(prefix: str):
+    """Read PLINK .bed/.bim/.fam: returns (packed (M, bpr) uint8, N, M)."""
+    with open(prefix + ".fam", "rb") as f:
+        N = sum(1 for _ in f)
+    with open(prefix + ".bim", "rb") as f:
+        M = sum(1 for _ in f)
+    raw = np.fromfile(prefix + ".bed", dtype=np.uint8)
+    if raw.size < 3 or raw[0] != 0x6C or raw[1] != 0x1B or raw[2] != 0x01:
+        raise ValueError("Incorrect magic number in plink bed file.")
+    bpr = (N + 3) // 4
+    if raw.size < 3 + M * bpr:
+        raise ValueError("truncated .bed file")
+    return raw[3:3 + M * bpr].reshape(M, bpr), N, M

@@ -1,0 +1,213 @@
+// C ABI entry points (include/pcaone_gpu.h). Every call catches pg::Error and returns its
+// status code; the message is kept on the context for pcaone_gpu_last_error().
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <random>
+
+#include "internal.hpp"
+#include "rsvd.hpp"
+
+namespace pg {
+
+void* scratch(pcaone_ctx* c, const std::string& name, size_t bytes) {
+  DevBuf& b = c->bufs[name];
+  if (b.bytes < bytes) {
+    if (b.p) PG_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t alloc = round_up(std::max<size_t>(bytes, 256), 256);
+    PG_CUDA(cudaMalloc(&b.p, alloc));
+    b.bytes = alloc;
+  }
+  return b.p;
+}
+
+static void free_ptr(void* p) {
+  if (p) cudaFree(p);
+}
+
+void free_data(pcaone_ctx* c) {
+  free_ptr(c->d_bed);
+  free_ptr(c->d_a1x2);
+  free_ptr(c->d_nonmiss);
+  free_ptr(c->d_F);
+  free_ptr(c->d_bedT);
+  free_ptr(c->d_miss_snp_ptr);
+  free_ptr(c->d_miss_snp_idx);
+  free_ptr(c->d_miss_ws_ptr);
+  free_ptr(c->d_miss_ws_idx);
+  c->d_bed = c->d_bedT = nullptr;
+  c->d_a1x2 = c->d_nonmiss = nullptr;
+  c->d_F = nullptr;
+  c->d_miss_snp_ptr = c->d_miss_ws_ptr = nullptr;
+  c->d_miss_snp_idx = c->d_miss_ws_idx = nullptr;
+  c->loaded = c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
+}
+
+void free_all(pcaone_ctx* c) {
+  free_data(c);
+  for (auto& kv : c->bufs) free_ptr(kv.second.p);
+  c->bufs.clear();
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+namespace {
+
+template <typename F>
+int guarded(pcaone_ctx* c, F&& f) {
+  if (!c) return PCAONE_EBADARG;
+  try {
+    PG_CUDA(cudaSetDevice(c->device));
+    f();
+    c->err.clear();
+    return PCAONE_OK;
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return PCAONE_ECUDA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pcaone_gpu_create(int device, pcaone_ctx** out) {
+  if (!out) return PCAONE_EBADARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return PCAONE_ENODEV;
+  auto* c = new pcaone_ctx();
+  c->device = device;
+  int st = guarded(c, [&] {
+    cudaDeviceProp prop;
+    PG_CUDA(cudaGetDeviceProperties(&prop, device));
+    c->sm_count = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    PG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PG_CUDA(cudaEventCreate(&c->ev0));
+    PG_CUDA(cudaEventCreate(&c->ev1));
+  });
+  if (st != PCAONE_OK) {
+    delete c;
+    return st;
+  }
+  *out = c;
+  return PCAONE_OK;
+}
+
+int pcaone_gpu_destroy(pcaone_ctx* c) {
+  if (!c) return PCAONE_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PCAONE_OK;
+}
+
+const char* pcaone_gpu_last_error(const pcaone_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int pcaone_gpu_load_bed(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, uint32_t nsamples) {
+  return guarded(c, [&] {
+    PG_REQUIRE(packed && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty genotype matrix");
+    PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 30), PCAONE_EBADARG, "genotype matrix too large");
+    free_data(c);
+    c->N = nsamples;
+    c->M = nsnps;
+    c->bpr = (nsamples + 3) / 4;
+    c->Npad = (uint32_t)round_up(nsamples, kRowPad);
+    c->pitch = c->Npad / 4;  // == round_up(bpr, kPitchAlign)
+    c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
+    const size_t bytes = (size_t)c->Mpad * c->pitch;
+    PG_CUDA(cudaMalloc(&c->d_bed, bytes));
+    PG_CUDA(cudaMalloc(&c->d_a1x2, c->M * 4));
+    PG_CUDA(cudaMalloc(&c->d_nonmiss, c->M * 4));
+    PG_CUDA(cudaMalloc(&c->d_F, c->M * 8));
+    PG_CUDA(cudaMemsetAsync(c->d_bed, 0xFF, bytes, c->stream));
+    PG_CUDA(cudaMemcpy2DAsync(c->d_bed, c->pitch, packed, c->bpr, c->bpr, c->M,
+                              cudaMemcpyHostToDevice, c->stream));
+    launch_fix_padding(c);
+    launch_counts(c);
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    c->loaded = true;
+  });
+}
+
+int pcaone_gpu_counts(pcaone_ctx* c, uint32_t* a1x2, uint32_t* nonmiss) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+    if (a1x2) PG_CUDA(cudaMemcpyAsync(a1x2, c->d_a1x2, c->M * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (nonmiss)
+      PG_CUDA(cudaMemcpyAsync(nonmiss, c->d_nonmiss, c->M * 4, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_allele_freq(pcaone_ctx* c, double* F) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+    PG_REQUIRE(F, PCAONE_EBADARG, "null output");
+    PG_CUDA(cudaMemcpyAsync(F, c->d_F, c->M * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_permute(pcaone_ctx* c, const int32_t* perm) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+    PG_REQUIRE(perm, PCAONE_EBADARG, "null permutation");
+    std::vector<char> seen(c->M, 0);
+    for (uint64_t j = 0; j < c->M; ++j) {
+      PG_REQUIRE(perm[j] >= 0 && (uint64_t)perm[j] < c->M && !seen[perm[j]], PCAONE_EBADARG,
+                 "perm is not a permutation of 0..nsnps-1");
+      seen[perm[j]] = 1;
+    }
+    int32_t* d_perm = (int32_t*)scratch(c, "perm", c->M * 4);
+    PG_CUDA(cudaMemcpyAsync(d_perm, perm, c->M * 4, cudaMemcpyHostToDevice, c->stream));
+    uint8_t* out = nullptr;
+    const size_t bytes = (size_t)c->Mpad * c->pitch;
+    PG_CUDA(cudaMalloc(&out, bytes));
+    PG_CUDA(cudaMemsetAsync(out, 0xFF, bytes, c->stream));
+    launch_permute(c, d_perm, out);
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    PG_CUDA(cudaFree(c->d_bed));
+    c->d_bed = out;
+    launch_counts(c);
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
+  });
+}
+
+int pcaone_shuffle_perm(uint64_t n, int32_t* perm) {
+  if (!perm) return PCAONE_EBADARG;
+  std::iota(perm, perm + n, 0);
+  auto rng = std::default_random_engine{};
+  std::shuffle(perm, perm + n, rng);
+  return PCAONE_OK;
+}
+
+int pcaone_omega(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out) {
+  if (!out) return PCAONE_EBADARG;
+  omega_host(seed, rand, nrow, ncol, out);
+  return PCAONE_OK;
+}
+
+int pcaone_gpu_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts* opts, double* U, double* S, double* V,
+                    pcaone_rsvd_report* report) {
+  return guarded(c, [&] {
+    PG_REQUIRE(opts, PCAONE_EBADARG, "null options");
+    run_rsvd(c, *opts, U, S, V, report);
+  });
+}
+
+}  // extern "C"

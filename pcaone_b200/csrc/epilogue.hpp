@@ -1,0 +1,40 @@
+// Parameters and launchers of the decode-GEMM epilogues (kernels_epilogue.cu).
+#pragma once
+
+#include "internal.hpp"
+
+namespace pg {
+
+struct EpiP1 {          // after the Z^T Omega product of one window
+  int64_t start = 0;    // first SNP of the window (current SNP order)
+  int64_t m = 0;        // SNPs in the window
+  int l = 0, ksplit = 1, standardize = 1, ploidy = 2;
+  const double* F = nullptr;         // M
+  const double* wsum = nullptr;      // l: column sums of Omega
+  const double* omega = nullptr;     // Npad x l
+  const int64_t* miss_ptr = nullptr; // by-SNP CSR
+  const int32_t* miss_idx = nullptr;
+  const double* miss_val = nullptr;  // e_ij per entry (EM-imputed), or null for 0
+  double* G = nullptr;               // M x l (rows start..start+m written)
+};
+
+struct EpiP2 {          // after the Z * G product of one window
+  int window = 0;
+  int64_t n = 0, npad = 0;
+  int l = 0, ksplit = 1, standardize = 1, ploidy = 2;
+  const double* F = nullptr;
+  const double* G = nullptr;         // M x l
+  const double* h0 = nullptr;        // l
+  const int64_t* miss_ptr = nullptr; // by (window, sample) CSR
+  const int32_t* miss_idx = nullptr;
+  const double* miss_val = nullptr;
+  double* H = nullptr;               // Npad x l accumulator
+};
+
+template <typename T>
+void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0);
+template <typename T>
+void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2);
+void zero(pcaone_ctx* c, double* a, int64_t n);
+
+}  // namespace pg

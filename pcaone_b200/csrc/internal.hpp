@@ -1,0 +1,130 @@
+// Internal declarations shared by the CUDA translation units of libpcaone_gpu.so.
+// Nothing here crosses the C ABI (include/pcaone_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pcaone_gpu.h"
+
+namespace pg {
+
+// ---------------------------------------------------------------- errors
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define PG_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      throw ::pg::Error(e_ == cudaErrorMemoryAllocation ? PCAONE_EOOM : PCAONE_ECUDA,     \
+                        std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +     \
+                            __FILE__ + ":" + std::to_string(__LINE__));                   \
+    }                                                                                    \
+  } while (0)
+
+#define PG_CHECK_LAUNCH() PG_CUDA(cudaGetLastError())
+
+#define PG_REQUIRE(cond, code, msg)                 \
+  do {                                              \
+    if (!(cond)) throw ::pg::Error((code), (msg));  \
+  } while (0)
+
+// ---------------------------------------------------------------- device buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+// Layout constants of the device-resident genotype matrices.
+constexpr int kPitchAlign = 64;   // bytes; row pitch of packed matrices (TMA needs 16)
+constexpr int kRowPad = 256;      // rows are padded to a multiple of this (sample / SNP tiles)
+constexpr int kLmax = 64;         // largest sketch width l = k + oversamples supported
+
+inline uint64_t round_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+// Window layout of the transposed (sample-major) packed copy used by the X * G product.
+struct WindowLayout {
+  int bands = 0;           // number of windows (1 for Halko)
+  uint64_t blocksize = 0;  // SNPs per window (last may be shorter)
+  uint32_t pitch = 0;      // bytes per sample row inside one window block
+  std::vector<uint64_t> start, stop;  // [start, stop) SNP range of each window
+};
+
+}  // namespace pg
+
+struct pcaone_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+
+  // genotypes
+  bool loaded = false;
+  uint32_t N = 0;       // samples
+  uint64_t M = 0;       // SNPs
+  uint32_t bpr = 0;     // bytes per SNP record = ceil(N/4)
+  uint32_t pitch = 0;   // device row pitch of the SNP-major copy
+  uint32_t Npad = 0;    // samples rounded up to kRowPad
+  uint64_t Mpad = 0;    // SNPs rounded up to kRowPad
+  uint8_t* d_bed = nullptr;  // Mpad x pitch, SNP-major (current SNP order)
+  uint32_t* d_a1x2 = nullptr;
+  uint32_t* d_nonmiss = nullptr;
+  double* d_F = nullptr;
+
+  // transposed copy for the current window layout
+  pg::WindowLayout win;
+  uint8_t* d_bedT = nullptr;  // bands x Npad x win.pitch
+  bool bedT_valid = false;
+
+  // missing entries: by SNP (CSR over current SNP order) and by (window, sample)
+  int64_t n_missing = 0;
+  int64_t* d_miss_snp_ptr = nullptr;   // M + 1
+  int32_t* d_miss_snp_idx = nullptr;   // sample index per entry
+  int64_t* d_miss_ws_ptr = nullptr;    // bands * N + 1
+  int32_t* d_miss_ws_idx = nullptr;    // SNP index (global, current order) per entry
+  bool miss_snp_valid = false, miss_ws_valid = false;
+
+  // named scratch buffers (grown on demand, freed with the context)
+  std::map<std::string, pg::DevBuf> bufs;
+
+  // timing
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double gemm_ms_accum = 0.0;
+  int64_t launches = 0, gemm_launches = 0;
+};
+
+namespace pg {
+
+void* scratch(pcaone_ctx* c, const std::string& name, size_t bytes);
+void free_all(pcaone_ctx* c);
+
+// ---------------------------------------------------------------- bed kernels (kernels_bed.cu)
+void launch_fix_padding(pcaone_ctx* c);
+void launch_counts(pcaone_ctx* c);
+void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out);
+void build_transposed(pcaone_ctx* c, int bands);
+void build_missing_by_snp(pcaone_ctx* c);
+void build_missing_by_window_sample(pcaone_ctx* c);
+
+// ---------------------------------------------------------------- SIMT decode-GEMM
+// out[s][r][c] = sum_{k in split s} val(code[r][k]) * B[k][c], val(00,01,10,11) = (2,0,1,0)
+// codes: rows x pitch bytes; B: row-major K x ldb (T); out: ksplit x rows x l (T).
+template <typename T>
+void launch_decode_gemm_simt(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows,
+                             int64_t K, const T* B, int ldb, int l, int ksplit, T* out);
+
+// ---------------------------------------------------------------- tcgen05 decode-GEMM
+// Same contract with BF16 hi/lo split of B; see kernels_gemm_tc.cu.
+bool tc_supported(pcaone_ctx* c);
+
+}  // namespace pg

@@ -1,0 +1,126 @@
+// Epilogues of the two decode-GEMMs of one window.
+//
+// The reference multiplies the dense FP64 matrix Z_ij = s_j (x_ij - F_j) (missing -> e_ij,
+// 0 before any EM update) by Omega and by G (src/FilePlink.cpp:106-114, src/Data.cpp:290-299,
+// src/Halko.cpp:193-202). Here x_ij = r_ij / 2 with r the raw A1 count decoded from the packed
+// codes (missing decodes to r = 0), so
+//
+//   Z_ij = (s_j/2) r_ij - s_j F_j + [missing] s_j (e_ij + F_j)
+//
+// and the two products become a raw decode-GEMM plus a rank-1 term plus a sparse term over
+// the missing entries:
+//
+//   G_j = s_j/2 (R^T Omega)_j - s_j F_j sum_i Omega_i + sum_{i miss} s_j (e_ij + F_j) Omega_i
+//   H_i = (R B2)_i - h0 + sum_{j miss} s_j (e_ij + F_j) G_j,  B2_j = s_j/2 G_j,
+//                                                             h0 = sum_j s_j F_j G_j
+#include "epilogue.hpp"
+
+namespace pg {
+
+namespace {
+
+__device__ __forceinline__ double snp_scale(double F, int standardize, int ploidy) {
+  if (!standardize) return 1.0;
+  double sd = sqrt((double)ploidy * F * (1.0 - F));
+  return sd > 1e-9 ? 1.0 / sd : 1.0;
+}
+
+// Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
+// per-CTA partials of h0.
+template <typename T>
+__global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
+                       double* __restrict__ h0_part) {
+  extern __shared__ double sh0[];  // warps x l
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int c = lane; c < p.l; c += 32) sh0[warp * p.l + c] = 0.0;
+  for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < p.m; jl += (int64_t)gridDim.x * nwarps) {
+    const int64_t j = p.start + jl;
+    const double F = p.F[j];
+    const double s = snp_scale(F, p.standardize, p.ploidy);
+    const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
+    for (int c = lane; c < p.l; c += 32) {
+      double d = 0.0;
+      for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * p.m + jl) * p.l + c];
+      double sparse = 0.0;
+      for (int64_t e = e0; e < e1; ++e) {
+        double ev = p.miss_val ? p.miss_val[e] : 0.0;
+        sparse += (ev + F) * p.omega[(int64_t)p.miss_idx[e] * p.l + c];
+      }
+      double g = s * (0.5 * d - F * p.wsum[c] + sparse);
+      p.G[j * p.l + c] = g;
+      B2[jl * p.l + c] = (T)(0.5 * s * g);
+      sh0[warp * p.l + c] += s * F * g;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < p.l; c += blockDim.x) {
+    double acc = 0.0;
+    for (int w = 0; w < nwarps; ++w) acc += sh0[w * p.l + c];
+    h0_part[(int64_t)blockIdx.x * p.l + c] = acc;
+  }
+}
+
+__global__ void k_reduce_cols(const double* __restrict__ part, int nblk, int l, double* __restrict__ out) {
+  int c = threadIdx.x;
+  if (c >= l) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * l + c];
+  out[c] = s;
+}
+
+// Warp per sample: H[i] += sum_split D2 - h0 + sparse.
+template <typename T>
+__global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int64_t i = (int64_t)blockIdx.x * nwarps + warp; i < p.n; i += (int64_t)gridDim.x * nwarps) {
+    const int64_t row = (int64_t)p.window * p.npad + i;
+    const int64_t e0 = p.miss_ptr[row], e1 = p.miss_ptr[row + 1];
+    for (int c = lane; c < p.l; c += 32) {
+      double d = 0.0;
+      for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D2[((int64_t)sp * p.n + i) * p.l + c];
+      double sparse = 0.0;
+      for (int64_t e = e0; e < e1; ++e) {
+        int64_t j = p.miss_idx[e];
+        double F = p.F[j];
+        double s = snp_scale(F, p.standardize, p.ploidy);
+        double ev = p.miss_val ? p.miss_val[e] : 0.0;
+        sparse += s * (ev + F) * p.G[j * p.l + c];
+      }
+      p.H[i * p.l + c] += d - p.h0[c] + sparse;
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) {
+  const int threads = 256, nwarps = threads / 32;
+  int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
+  double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
+  k_prep<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p, D1, B2, part);
+  PG_CHECK_LAUNCH();
+  k_reduce_cols<<<1, 128, 0, c->stream>>>(part, nblk, p.l, h0);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
+
+template <typename T>
+void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
+  const int threads = 256, nwarps = threads / 32;
+  int nblk = (int)std::min<int64_t>(4 * c->sm_count, (p.n + nwarps - 1) / nwarps);
+  k_accum<T><<<nblk, threads, 0, c->stream>>>(p, D2);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void zero(pcaone_ctx* c, double* a, int64_t n) {
+  PG_CUDA(cudaMemsetAsync(a, 0, n * sizeof(double), c->stream));
+}
+
+template void launch_prep<float>(pcaone_ctx*, const EpiP1&, const float*, float*, double*);
+template void launch_prep<double>(pcaone_ctx*, const EpiP1&, const double*, double*, double*);
+template void launch_accum<float>(pcaone_ctx*, const EpiP2&, const float*);
+template void launch_accum<double>(pcaone_ctx*, const EpiP2&, const double*);
+
+}  // namespace pg

@@ -1,0 +1,345 @@
+// FP64 kernels for the (k+p)-wide sketch: Gram matrices, Cholesky, triangular solves
+// (CholeskyQR2), recovery of the Householder-QR column signs, flipOmg, and small products.
+//
+// Tall matrices are row-major n x l (one sample or SNP per row, l <= kLmax columns).
+// All reductions are two-pass (per-CTA partials, then a fixed-order sum) so results are
+// deterministic run to run.
+#include "internal.hpp"
+#include "linalg.hpp"
+
+namespace pg {
+
+namespace {
+
+constexpr int kGramRowsMax = 64;  // rows staged per iteration in the Gram kernels
+constexpr int kGramBlocks = 296;
+
+// Partial cross products P[blk] = A^T B over a slice of rows (A: n x la, B: n x lb).
+__global__ void k_cross_partial(const double* __restrict__ A, int la, const double* __restrict__ Bm,
+                                int lb, int64_t n, int kGramRows, double* __restrict__ part) {
+  extern __shared__ double sm[];
+  double* sa = sm;                       // kGramRows x la
+  double* sb = sm + kGramRows * la;      // kGramRows x lb
+  const int npairs = la * lb;
+  double acc[8];
+  for (int t = 0; t < 8; ++t) acc[t] = 0.0;
+  const int64_t rows_per_blk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t rb = blockIdx.x * rows_per_blk, re = min(n, rb + rows_per_blk);
+  for (int64_t r0 = rb; r0 < re; r0 += kGramRows) {
+    int nr = (int)(re - r0 < kGramRows ? re - r0 : kGramRows);
+    for (int t = threadIdx.x; t < nr * la; t += blockDim.x) sa[t] = A[r0 * la + t];
+    for (int t = threadIdx.x; t < nr * lb; t += blockDim.x) sb[t] = Bm[r0 * lb + t];
+    __syncthreads();
+    for (int q = 0; q < 8; ++q) {
+      int p = threadIdx.x + q * blockDim.x;
+      if (p >= npairs) break;
+      int i = p / lb, j = p - i * lb;
+      double s = acc[q];
+      for (int r = 0; r < nr; ++r) s = fma(sa[r * la + i], sb[r * lb + j], s);
+      acc[q] = s;
+    }
+    __syncthreads();
+  }
+  for (int q = 0; q < 8; ++q) {
+    int p = threadIdx.x + q * blockDim.x;
+    if (p < npairs) part[(int64_t)blockIdx.x * npairs + p] = acc[q];
+  }
+}
+
+__global__ void k_sum_partials(const double* __restrict__ part, int nblk, int npairs,
+                               double* __restrict__ out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * npairs + p];
+  out[p] = s;
+}
+
+// Cholesky W = R^T R (R upper) for l x l; one CTA. status[0] is set to 1 + j on failure.
+// If Rprev != nullptr, also writes Racc = R * Rprev (accumulated R of CholeskyQR2).
+__global__ void k_cholesky(const double* __restrict__ W, int l, double* __restrict__ R,
+                           const double* __restrict__ Rprev, double* __restrict__ Racc,
+                           int* __restrict__ status) {
+  extern __shared__ double s[];  // l x l
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) s[t] = W[t];
+  __syncthreads();
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  // right-looking: s holds the trailing matrix; row j of R is written into row j of s
+  for (int j = 0; j < l; ++j) {
+    if (threadIdx.x == 0) {
+      double d = s[j * l + j];
+      if (!(d > 0.0) || !isfinite(d)) {
+        bad = j + 1;
+        d = 1.0;
+      }
+      s[j * l + j] = sqrt(d);
+    }
+    __syncthreads();
+    double djj = s[j * l + j];
+    for (int i = j + 1 + threadIdx.x; i < l; i += blockDim.x) s[j * l + i] /= djj;
+    __syncthreads();
+    for (int t = threadIdx.x; t < (l - j - 1) * (l - j - 1); t += blockDim.x) {
+      int a = j + 1 + t / (l - j - 1), b = j + 1 + t % (l - j - 1);
+      if (b >= a) s[a * l + b] -= s[j * l + a] * s[j * l + b];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
+    int i = t / l, j = t % l;
+    R[t] = (j >= i) ? s[t] : 0.0;
+  }
+  __syncthreads();
+  if (Rprev) {
+    for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
+      int i = t / l, j = t % l;
+      double acc = 0.0;
+      for (int k = i; k <= j; ++k) acc += R[i * l + k] * Rprev[k * l + j];
+      Racc[t] = (j >= i) ? acc : 0.0;
+    }
+  }
+  if (threadIdx.x == 0 && bad && status) atomicMax(status, bad);
+}
+
+// Q = A R^{-1} (row-wise forward substitution x R = a), R upper l x l. One thread per row.
+__global__ void k_trsm_right_upper(const double* __restrict__ A, const double* __restrict__ R,
+                                   int l, int64_t n, double* __restrict__ Q) {
+  extern __shared__ double sr[];
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) sr[t] = R[t];
+  __syncthreads();
+  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double x[kLmax];
+  const double* a = A + r * l;
+  for (int j = 0; j < l; ++j) {
+    double v = a[j];
+    for (int k = 0; k < j; ++k) v -= x[k] * sr[k * l + j];
+    x[j] = v / sr[j * l + j];
+  }
+  double* q = Q + r * l;
+  for (int j = 0; j < l; ++j) q[j] = x[j];
+}
+
+// Householder column signs of an orthonormal Q from the modified LU of its top l x l block
+// (Ballard et al., "Reconstructing Householder vectors from tall-skinny QR", 2015):
+// at step i the pivot's sign s gives D_ii = -sign(s) (sign(0) = +), matching the stable
+// Householder choice R_ii = -sign(x_0)||x|| of Eigen::HouseholderQR and LAPACK dgeqrf.
+__global__ void k_householder_signs(const double* __restrict__ Q, int l, double* __restrict__ D) {
+  extern __shared__ double a[];  // l x l
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) a[t] = Q[t];
+  __syncthreads();
+  for (int i = 0; i < l; ++i) {
+    double piv = a[i * l + i];
+    double di = piv >= 0.0 ? -1.0 : 1.0;
+    double p = piv - di;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      D[i] = di;
+      a[i * l + i] = p;
+    }
+    // eliminate rows below i
+    for (int r = i + 1 + threadIdx.x; r < l; r += blockDim.x) a[r * l + i] /= p;
+    __syncthreads();
+    for (int t = threadIdx.x; t < (l - i - 1) * (l - i - 1); t += blockDim.x) {
+      int r = i + 1 + t / (l - i - 1), cidx = i + 1 + t % (l - i - 1);
+      a[r * l + cidx] -= a[r * l + i] * a[i * l + cidx];
+    }
+    __syncthreads();
+  }
+}
+
+// flipOmg partials: per column, sum |O2 - Qd| and |O2 + Qd| with Qd = Q * D.
+__global__ void k_flip_partial(const double* __restrict__ O2, const double* __restrict__ Q,
+                               const double* __restrict__ D, int l, int64_t n,
+                               double* __restrict__ part) {
+  __shared__ double sm[2][256];
+  const int col = blockIdx.y;
+  double dm = 0.0, dp = 0.0;
+  const double d = D[col];
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    double o = O2[r * l + col], q = Q[r * l + col] * d;
+    dm += fabs(o - q);
+    dp += fabs(o + q);
+  }
+  sm[0][threadIdx.x] = dm;
+  sm[1][threadIdx.x] = dp;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm[0][threadIdx.x] += sm[0][threadIdx.x + s];
+      sm[1][threadIdx.x] += sm[1][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[((int64_t)col * gridDim.x + blockIdx.x) * 2 + 0] = sm[0][0];
+    part[((int64_t)col * gridDim.x + blockIdx.x) * 2 + 1] = sm[1][0];
+  }
+}
+
+// Final column multipliers: D_c, negated when |O2 - Qd|_1 > 2 |O2 + Qd|_1 (src/RSVD.hpp:85).
+__global__ void k_flip_final(const double* __restrict__ part, int nblk, const double* __restrict__ D,
+                             int l, double* __restrict__ mult) {
+  int col = threadIdx.x;
+  if (col >= l) return;
+  double dm = 0.0, dp = 0.0;
+  for (int b = 0; b < nblk; ++b) {
+    dm += part[((int64_t)col * nblk + b) * 2 + 0];
+    dp += part[((int64_t)col * nblk + b) * 2 + 1];
+  }
+  mult[col] = (dm > 2.0 * dp) ? -D[col] : D[col];
+}
+
+// Omega = Q * diag(mult); Omega2 = Omega; optional FP32 copy (row-major, ld l).
+__global__ void k_apply_cols(const double* __restrict__ Q, const double* __restrict__ mult, int l,
+                             int64_t n, double* __restrict__ O, double* __restrict__ O2,
+                             float* __restrict__ Of) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * l) return;
+  double v = Q[t] * mult[t % l];
+  O[t] = v;
+  if (O2) O2[t] = v;
+  if (Of) Of[t] = (float)v;
+}
+
+// Column sums of A (n x l) into partials (grid.y = column).
+__global__ void k_colsum_partial(const double* __restrict__ A, int l, int64_t n,
+                                 double* __restrict__ part) {
+  __shared__ double sm[256];
+  const int col = blockIdx.y;
+  double s = 0.0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x)
+    s += A[r * l + col];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st; st >>= 1) {
+    if (threadIdx.x < st) sm[threadIdx.x] += sm[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[(int64_t)col * gridDim.x + blockIdx.x] = sm[0];
+}
+
+__global__ void k_colsum_final(const double* __restrict__ part, int nblk, int l,
+                               double* __restrict__ out) {
+  int col = threadIdx.x;
+  if (col >= l) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(int64_t)col * nblk + b];
+  out[col] = s;
+}
+
+// Y (n x kc) = X (n x l) * C (l x ldc, first kc columns), row-major.
+__global__ void k_rowmat(const double* __restrict__ X, int l, const double* __restrict__ C, int ldc,
+                         int kc, int64_t n, double* __restrict__ Y) {
+  extern __shared__ double sc[];
+  for (int t = threadIdx.x; t < l * kc; t += blockDim.x) sc[t] = C[(t / kc) * ldc + t % kc];
+  __syncthreads();
+  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const double* x = X + r * l;
+  double xr[kLmax];
+  for (int j = 0; j < l; ++j) xr[j] = x[j];
+  for (int c = 0; c < kc; ++c) {
+    double s = 0.0;
+    for (int j = 0; j < l; ++j) s = fma(xr[j], sc[j * kc + c], s);
+    Y[r * kc + c] = s;
+  }
+}
+
+__global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                      double* __restrict__ out) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < n) out[t] = a[t] + b[t];
+}
+
+}  // namespace
+
+void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int64_t n, double* out) {
+  const int npairs = la * lb;
+  PG_REQUIRE(npairs <= 8 * 512, PCAONE_EBADARG, "cross product too wide");
+  int threads = std::min(512, std::max(128, (npairs + 7) / 8 + 31) / 32 * 32);
+  while (threads * 8 < npairs) threads += 32;
+  // stage as many rows as fit in 48 KB of shared memory
+  const int rows = std::max(8, std::min(kGramRowsMax, 6144 / (la + lb)));
+  int nblk = (int)std::min<int64_t>(kGramBlocks, std::max<int64_t>(1, (n + rows - 1) / rows));
+  double* part = (double*)scratch(c, "cross_part", (size_t)nblk * npairs * 8);
+  size_t smem = (size_t)rows * (la + lb) * 8;
+  k_cross_partial<<<nblk, threads, smem, c->stream>>>(A, la, B, lb, n, rows, part);
+  PG_CHECK_LAUNCH();
+  k_sum_partials<<<(npairs + 255) / 256, 256, 0, c->stream>>>(part, nblk, npairs, out);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
+
+void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rprev, double* Racc,
+              int* d_status) {
+  k_cholesky<<<1, 256, (size_t)l * l * 8, c->stream>>>(W, l, R, Rprev, Racc, d_status);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q) {
+  k_trsm_right_upper<<<(unsigned)((n + 127) / 128), 128, (size_t)l * l * 8, c->stream>>>(A, R, l, n, Q);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double* R, int* d_status) {
+  double* W = (double*)scratch(c, "cq_W", (size_t)l * l * 8);
+  double* R1 = (double*)scratch(c, "cq_R1", (size_t)l * l * 8);
+  double* R2 = (double*)scratch(c, "cq_R2", (size_t)l * l * 8);
+  cross(c, A, l, A, l, n, W);
+  cholesky(c, W, l, R1, nullptr, nullptr, d_status);
+  trsm_right_upper(c, A, R1, l, n, Q);
+  cross(c, Q, l, Q, l, n, W);
+  cholesky(c, W, l, R2, R1, R, d_status);
+  trsm_right_upper(c, Q, R2, l, n, Q);
+}
+
+void householder_signs(pcaone_ctx* c, const double* Q, int l, double* D) {
+  k_householder_signs<<<1, 128, (size_t)l * l * 8, c->stream>>>(Q, l, D);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void flip_and_apply(pcaone_ctx* c, const double* Q, const double* D, int l, int64_t n, double* O,
+                    double* O2, float* Of) {
+  const int nblk = 64;
+  double* part = (double*)scratch(c, "flip_part", (size_t)l * nblk * 2 * 8);
+  double* mult = (double*)scratch(c, "flip_mult", (size_t)l * 8);
+  k_flip_partial<<<dim3(nblk, l), 256, 0, c->stream>>>(O2, Q, D, l, n, part);
+  PG_CHECK_LAUNCH();
+  k_flip_final<<<1, 128, 0, c->stream>>>(part, nblk, D, l, mult);
+  PG_CHECK_LAUNCH();
+  int64_t tot = n * l;
+  k_apply_cols<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(Q, mult, l, n, O, O2, Of);
+  PG_CHECK_LAUNCH();
+  c->launches += 3;
+}
+
+void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out) {
+  const int nblk = 64;
+  double* part = (double*)scratch(c, "colsum_part", (size_t)l * nblk * 8);
+  k_colsum_partial<<<dim3(nblk, l), 256, 0, c->stream>>>(A, l, n, part);
+  PG_CHECK_LAUNCH();
+  k_colsum_final<<<1, 128, 0, c->stream>>>(part, nblk, l, out);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
+
+void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y) {
+  k_rowmat<<<(unsigned)((n + 127) / 128), 128, (size_t)l * kc * 8, c->stream>>>(X, l, C, ldc, kc, n, Y);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out) {
+  k_add<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a, b, n, out);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+}  // namespace pg

@@ -1,0 +1,28 @@
+// FP64 sketch-width linear algebra launchers (kernels_linalg.cu). Tall matrices are
+// row-major n x l.
+#pragma once
+
+#include "internal.hpp"
+
+namespace pg {
+
+// out (la x lb, row-major) = A^T B for A: n x la, B: n x lb.
+void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int64_t n, double* out);
+// W = R^T R; R upper. When Rprev is given, Racc = R * Rprev. d_status gets 1+j on failure.
+void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rprev, double* Racc,
+              int* d_status);
+// Q = A R^-1 (may alias A == Q).
+void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q);
+// CholeskyQR2: A = Q R with Q orthonormal (Q may alias A).
+void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double* R, int* d_status);
+// D (l) such that Q * diag(D) is the thin Q of a Householder QR of the same matrix.
+void householder_signs(pcaone_ctx* c, const double* Q, int l, double* D);
+// flipOmg against O2 (src/RSVD.hpp:81-90), then O = Q diag(D*flip), O2 = O, Of = float(O).
+void flip_and_apply(pcaone_ctx* c, const double* Q, const double* D, int l, int64_t n, double* O,
+                    double* O2, float* Of);
+void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);
+// Y (n x kc) = X (n x l) * C[:, :kc] with C l x ldc row-major.
+void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y);
+void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out);
+
+}  // namespace pg

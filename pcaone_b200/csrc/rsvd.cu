@@ -1,0 +1,426 @@
+// Randomized SVD driver on device-resident packed genotypes: the epoch loop of
+// RsvdOpData::computeUSV (src/Halko.cpp:45-95) with the Halko schedule of
+// NormalRsvdOpData::computeGandH (src/Halko.cpp:97-125) or the window schedule of
+// FancyRsvdOpData::computeGandH (src/Halko.cpp:153-226).
+//
+// Differences of form (not of result) from the reference:
+//  * thin QR is CholeskyQR2 in FP64 instead of Householder; the Householder column signs,
+//    which steer the winSVD trajectory through flipOmg, are recovered exactly from the
+//    CholeskyQR2 factor (kernels_linalg.cu, k_householder_signs);
+//  * B = R^-T H^T is never formed: its SVD comes from CholeskyQR2 of B^T = H R^-1 and a
+//    one-sided Jacobi SVD of the l x l triangular factor on the host.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <random>
+
+#include "epilogue.hpp"
+#include "linalg.hpp"
+#include "rsvd.hpp"
+
+namespace pg {
+
+// ---------------------------------------------------------------- host helpers
+void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out) {
+  // RsvdOpData::initOmg (src/Halko.cpp:14-22): engine seeded with --seed, column-major fill.
+  std::default_random_engine rng;
+  rng.seed(seed);
+  const uint64_t n = nrow * (uint64_t)ncol;
+  if (rand) {
+    std::normal_distribution<double> d{0, 1};
+    for (uint64_t i = 0; i < n; ++i) out[i] = d(rng);
+  } else {
+    std::uniform_real_distribution<double> d{-1, 1};
+    for (uint64_t i = 0; i < n; ++i) out[i] = d(rng);
+  }
+}
+
+// One-sided Jacobi SVD of a small square matrix A (n x n, row-major): A = U diag(s) V^T,
+// singular values sorted in decreasing order. U, V row-major n x n.
+void jacobi_svd(int n, const double* A, double* U, double* s, double* V) {
+  std::vector<double> a(A, A + (size_t)n * n), v((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < n - 1; ++p) {
+      for (int q = p + 1; q < n; ++q) {
+        double alpha = 0, beta = 0, gamma = 0;
+        for (int i = 0; i < n; ++i) {
+          double ap = a[(size_t)i * n + p], aq = a[(size_t)i * n + q];
+          alpha += ap * ap;
+          beta += aq * aq;
+          gamma += ap * aq;
+        }
+        if (gamma == 0.0) continue;
+        double conv = std::fabs(gamma) / std::sqrt(alpha * beta);
+        off = std::max(off, conv);
+        if (conv < 1e-15) continue;
+        double zeta = (beta - alpha) / (2.0 * gamma);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        double cs = 1.0 / std::sqrt(1.0 + t * t), sn = cs * t;
+        for (int i = 0; i < n; ++i) {
+          double ap = a[(size_t)i * n + p], aq = a[(size_t)i * n + q];
+          a[(size_t)i * n + p] = cs * ap - sn * aq;
+          a[(size_t)i * n + q] = sn * ap + cs * aq;
+          double vp = v[(size_t)i * n + p], vq = v[(size_t)i * n + q];
+          v[(size_t)i * n + p] = cs * vp - sn * vq;
+          v[(size_t)i * n + q] = sn * vp + cs * vq;
+        }
+      }
+    }
+    if (off < 1e-15) break;
+  }
+  std::vector<double> norms(n);
+  for (int j = 0; j < n; ++j) {
+    double acc = 0;
+    for (int i = 0; i < n; ++i) acc += a[(size_t)i * n + j] * a[(size_t)i * n + j];
+    norms[j] = std::sqrt(acc);
+  }
+  std::vector<int> ord(n);
+  for (int j = 0; j < n; ++j) ord[j] = j;
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return norms[x] > norms[y]; });
+  for (int jj = 0; jj < n; ++jj) {
+    int j = ord[jj];
+    s[jj] = norms[j];
+    for (int i = 0; i < n; ++i) {
+      U[(size_t)i * n + jj] = norms[j] > 0 ? a[(size_t)i * n + j] / norms[j] : (i == jj ? 1.0 : 0.0);
+      V[(size_t)i * n + jj] = v[(size_t)i * n + j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- engine
+template <typename T>
+struct Engine {
+  pcaone_ctx* c;
+  pcaone_rsvd_opts o;
+  int N, l, k;
+  int64_t M, Npad;
+  GemmFnT<T> gemm;
+
+  double *Omg, *Omg2, *wsum, *G, *H, *H1, *H2, *Tb, *Rg, *Rb, *Dsig, *Ucur, *Upre, *Ck;
+  T* OmgT;   // Omega as the B operand of the first product (alias of Omg for FP64)
+  int* d_status;
+
+  Engine(pcaone_ctx* c_, const pcaone_rsvd_opts& o_, GemmFnT<T> g) : c(c_), o(o_), gemm(g) {
+    N = (int)c->N;
+    M = (int64_t)c->M;
+    Npad = c->Npad;
+    k = o.k;
+    l = o.k + o.oversamples;
+    auto d = [&](const char* name, size_t n) { return (double*)scratch(c, name, n * sizeof(double)); };
+    Omg = d("r_omg", Npad * l);
+    Omg2 = d("r_omg2", Npad * l);
+    wsum = d("r_wsum", l);
+    G = d("r_G", (size_t)c->Mpad * l);
+    H = d("r_H", Npad * l);
+    H1 = d("r_H1", Npad * l);
+    H2 = d("r_H2", Npad * l);
+    Tb = d("r_Tb", Npad * l);
+    Rg = d("r_Rg", l * l);
+    Rb = d("r_Rb", l * l);
+    Dsig = d("r_D", l);
+    Ucur = d("r_Ucur", Npad * k);
+    Upre = d("r_Upre", Npad * k);
+    Ck = d("r_Ck", (size_t)kLmax * kLmax);
+    d_status = (int*)scratch(c, "r_status", sizeof(int));
+    PG_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), c->stream));
+    if (std::is_same<T, double>::value)
+      OmgT = reinterpret_cast<T*>(Omg);
+    else
+      OmgT = (T*)scratch(c, "r_omgT", Npad * l * sizeof(T));
+  }
+
+  float* omg_float() { return std::is_same<T, float>::value ? reinterpret_cast<float*>(OmgT) : nullptr; }
+
+  void init_omega() {
+    std::vector<double> cm((size_t)N * l), rm((size_t)Npad * l, 0.0);
+    omega_host(o.seed, o.rand, N, l, cm.data());
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = cm[(size_t)j * N + i];
+    PG_CUDA(cudaMemcpyAsync(Omg, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    PG_CUDA(cudaMemcpyAsync(Omg2, Omg, rm.size() * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if (!std::is_same<T, double>::value) {
+      std::vector<float> f(rm.begin(), rm.end());
+      PG_CUDA(cudaMemcpyAsync(OmgT, f.data(), f.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    colsum(c, Omg, l, N, wsum);
+    PG_CUDA(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
+    gemm.omega_changed(c, Omg, l, Npad);
+  }
+
+  // Omega = flipOmg(Omega2, thinQ(Householder QR of Hsrc)); Omega2 = Omega.
+  void update_omega(const double* Hsrc) {
+    double* Q = Tb;
+    double* Rtmp = (double*)scratch(c, "r_Rtmp", (size_t)l * l * 8);
+    cholqr2(c, Hsrc, l, N, Q, Rtmp, d_status);
+    householder_signs(c, Q, l, Dsig);
+    flip_and_apply(c, Q, Dsig, l, N, Omg, Omg2, omg_float());
+    colsum(c, Omg, l, N, wsum);
+    gemm.omega_changed(c, Omg, l, Npad);
+  }
+
+  // G rows of window b and accumulation of Z_b G_b into Ht.
+  void process_window(int b, double* Ht) {
+    const int64_t s = (int64_t)c->win.start[b], e = (int64_t)c->win.stop[b], m = e - s;
+    // product 1: D1 = R_b^T Omega
+    int ks1 = gemm.ksplit(c, m, N);
+    T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * m * l * sizeof(T));
+    timed([&] { gemm.p1(c, c->d_bed + s * (int64_t)c->pitch, c->pitch, m, N, OmgT, l, ks1, D1); });
+    EpiP1 p1;
+    p1.start = s;
+    p1.m = m;
+    p1.l = l;
+    p1.ksplit = ks1;
+    p1.standardize = o.standardize;
+    p1.ploidy = o.ploidy;
+    p1.F = c->d_F;
+    p1.wsum = wsum;
+    p1.omega = Omg;
+    p1.miss_ptr = c->d_miss_snp_ptr;
+    p1.miss_idx = c->d_miss_snp_idx;
+    p1.miss_val = nullptr;
+    p1.G = G;
+    T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
+    double* h0 = (double*)scratch(c, "r_h0", l * 8);
+    launch_prep<T>(c, p1, D1, B2, h0);
+    gemm.b2_ready(c, B2, l, m);
+    // product 2: D2 = R_b B2
+    int ks2 = gemm.ksplit(c, N, m);
+    T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
+    const uint8_t* codesT = c->d_bedT + (int64_t)b * Npad * c->win.pitch;
+    timed([&] { gemm.p2(c, codesT, c->win.pitch, N, m, B2, l, ks2, D2); });
+    EpiP2 p2;
+    p2.window = b;
+    p2.n = N;
+    p2.npad = Npad;
+    p2.l = l;
+    p2.ksplit = ks2;
+    p2.standardize = o.standardize;
+    p2.ploidy = o.ploidy;
+    p2.F = c->d_F;
+    p2.G = G;
+    p2.h0 = h0;
+    p2.miss_ptr = c->d_miss_ws_ptr;
+    p2.miss_idx = c->d_miss_ws_idx;
+    p2.miss_val = nullptr;
+    p2.H = Ht;
+    launch_accum<T>(c, p2, D2);
+  }
+
+  int bandsize = 1;
+  int updates = 0;
+
+  // With opts.profile, bracket each decode-GEMM launch with CUDA events on the launching
+  // stream; the elapsed times are summed into gemm_ms after each epoch.
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+  size_t ev_used = 0;
+  template <typename F>
+  void timed(F&& f) {
+    if (!o.profile) {
+      f();
+      return;
+    }
+    if (ev_used == evs.size()) {
+      cudaEvent_t a, b;
+      PG_CUDA(cudaEventCreate(&a));
+      PG_CUDA(cudaEventCreate(&b));
+      evs.push_back({a, b});
+    }
+    PG_CUDA(cudaEventRecord(evs[ev_used].first, c->stream));
+    f();
+    PG_CUDA(cudaEventRecord(evs[ev_used].second, c->stream));
+    ev_used++;
+  }
+  void collect_times() {
+    if (!ev_used) return;
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < ev_used; ++i) {
+      float ms = 0.f;
+      PG_CUDA(cudaEventElapsedTime(&ms, evs[i].first, evs[i].second));
+      c->gemm_ms_accum += ms;
+    }
+    ev_used = 0;
+  }
+  ~Engine() {
+    for (auto& e : evs) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  }
+
+  void epoch_halko(int pi) {
+    if (pi == 0)
+      init_omega();
+    else {
+      update_omega(H);
+      updates++;
+    }
+    zero(c, H, Npad * l);
+    process_window(0, H);
+  }
+
+  void epoch_winsvd(int pi) {
+    const int bands = o.bands;
+    if (pi == 0) init_omega();
+    if (std::pow(2.0, pi) >= bands) {
+      zero(c, H1, Npad * l);
+      zero(c, H2, Npad * l);
+    }
+    if (pi == 0) bandsize = 1;
+    bandsize = std::min(bandsize * 2, bands);
+    for (int b = 0, i = 1; b < bands; ++b, ++i) {
+      process_window(b, i <= bandsize / 2 ? H1 : H2);
+      const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) && std::pow(2.0, pi) < bands;
+      if ((b + 1) < bandsize && !adjacent) continue;
+      if (!((i == bandsize) || (i == bandsize / 2) || adjacent)) continue;
+      add(c, H1, H2, Npad * l, H);
+      update_omega(H);
+      updates++;
+      if (i == bandsize) {
+        zero(c, H1, Npad * l);
+        i = 0;
+      } else {
+        zero(c, H2, Npad * l);
+      }
+    }
+  }
+
+  void check_status() {
+    int st = 0;
+    PG_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    PG_REQUIRE(st == 0, PCAONE_ENUMERIC,
+               "Cholesky factorisation of a sketch Gram matrix failed at column " + std::to_string(st - 1));
+  }
+
+  void run(double* U, double* S, double* V, pcaone_rsvd_report* rep) {
+    // zero the FP64 work buffers once so padded rows stay zero
+    zero(c, H, Npad * l);
+    zero(c, H1, Npad * l);
+    zero(c, H2, Npad * l);
+    zero(c, Tb, Npad * l);
+    zero(c, Ucur, Npad * k);
+    zero(c, Upre, Npad * k);
+    int p = o.maxp;
+    std::vector<double> rb((size_t)l * l), ur((size_t)l * l), vr((size_t)l * l), sv(l), ck((size_t)k * k);
+    double diff = 0.0;
+    int epochs = 0;
+    bool done = false;
+    for (int pi = 0; pi <= p && !done; ++pi) {
+      if (o.svd == 1)
+        epoch_halko(pi);
+      else
+        epoch_winsvd(pi);
+      // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B)
+      cholqr2(c, G, l, M, G, Rg, d_status);
+      trsm_right_upper(c, H, Rg, l, N, Tb);
+      cholqr2(c, Tb, l, N, Tb, Rb, d_status);
+      PG_CUDA(cudaMemcpyAsync(rb.data(), Rb, rb.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+      check_status();
+      collect_times();
+      jacobi_svd(l, rb.data(), ur.data(), sv.data(), vr.data());
+      // Ucur = Qb Ur[:, :k]
+      PG_CUDA(cudaMemcpyAsync(Ck, ur.data(), ur.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      rowmat(c, Tb, l, Ck, l, k, N, Ucur);
+      epochs = pi + 1;
+      if (pi > 0) {
+        cross(c, Ucur, k, Upre, k, N, Ck);
+        PG_CUDA(cudaMemcpyAsync(ck.data(), Ck, ck.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+        PG_CUDA(cudaStreamSynchronize(c->stream));
+        double acc = 0.0;  // mev (src/Utils.cpp:192-198)
+        for (int j = 0; j < k; ++j) {
+          double nrm = 0.0;
+          for (int i = 0; i < k; ++i) nrm += ck[(size_t)i * k + j] * ck[(size_t)i * k + j];
+          acc += std::sqrt(nrm);
+        }
+        diff = 1.0 - acc / k;
+        if (o.verbose) printf("running of epoch = %d, diff = %g\n", pi, diff);
+        if (diff < o.tol || pi == p) {
+          if (o.svd == 2 && std::pow(2.0, pi) < o.bands) {
+            p = (int)std::log2((double)o.bands);
+          } else {
+            done = true;
+            break;
+          }
+        } else {
+          PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
+        }
+      } else {
+        PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
+      }
+    }
+    // outputs: U = Ucur, S = sigma[:k], V = Q_G Vr[:, :k]
+    if (S)
+      for (int j = 0; j < k; ++j) S[j] = sv[j];
+    std::vector<double> rowm;
+    if (U) {
+      rowm.resize((size_t)N * k);
+      PG_CUDA(cudaMemcpyAsync(rowm.data(), Ucur, rowm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+      for (int i = 0; i < N; ++i)
+        for (int j = 0; j < k; ++j) U[(size_t)j * N + i] = rowm[(size_t)i * k + j];
+    }
+    if (V) {
+      double* Vd = (double*)scratch(c, "r_V", (size_t)c->Mpad * k * 8);
+      PG_CUDA(cudaMemcpyAsync(Ck, vr.data(), vr.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      rowmat(c, G, l, Ck, l, k, M, Vd);
+      rowm.resize((size_t)M * k);
+      PG_CUDA(cudaMemcpyAsync(rowm.data(), Vd, rowm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+      for (int64_t i = 0; i < M; ++i)
+        for (int j = 0; j < k; ++j) V[(size_t)j * M + i] = rowm[(size_t)i * k + j];
+    }
+    if (rep) {
+      rep->epochs = epochs;
+      rep->omega_updates = updates;
+      rep->last_diff = diff;
+    }
+  }
+};
+
+void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, double* V,
+              pcaone_rsvd_report* rep) {
+  PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+  PG_REQUIRE(o.k >= 1 && o.oversamples >= 0, PCAONE_EBADARG, "bad k / oversamples");
+  const int l = o.k + o.oversamples;
+  PG_REQUIRE(l <= kLmax, PCAONE_EBADARG, "k + oversamples must be <= " + std::to_string(kLmax));
+  PG_REQUIRE((uint32_t)l <= c->N, PCAONE_EBADARG, "k + oversamples must not exceed the number of samples");
+  PG_REQUIRE(o.svd == 1 || o.svd == 2, PCAONE_EBADARG, "svd must be 1 (Halko) or 2 (winSVD)");
+  PG_REQUIRE(o.svd == 1 || (o.bands >= 4 && o.bands % 2 == 0), PCAONE_EBADARG,
+             "the -w/--batches must be a power of 2 and the minimun is 4.");
+  PG_REQUIRE(o.maxp >= 0, PCAONE_EBADARG, "maxp must be >= 0");
+  PG_REQUIRE(o.ploidy == 1 || o.ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
+  const int bands = o.svd == 1 ? 1 : o.bands;
+  build_transposed(c, bands);
+  build_missing_by_snp(c);
+  build_missing_by_window_sample(c);
+  c->gemm_ms_accum = 0.0;
+  const int64_t l0 = c->launches, g0 = c->gemm_launches;
+  PG_CUDA(cudaEventRecord(c->ev0, c->stream));
+  if (o.precision == PCAONE_PREC_FP64) {
+    Engine<double> e(c, o, gemm_simt_double());
+    e.run(U, S, V, rep);
+  } else if (o.precision == PCAONE_PREC_FP32) {
+    Engine<float> e(c, o, gemm_simt_float());
+    e.run(U, S, V, rep);
+  } else if (o.precision == PCAONE_PREC_MIXED) {
+    PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
+    Engine<float> e(c, o, gemm_tc());
+    e.run(U, S, V, rep);
+  } else {
+    throw Error(PCAONE_EBADARG, "unknown precision");
+  }
+  PG_CUDA(cudaEventRecord(c->ev1, c->stream));
+  PG_CUDA(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  PG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (rep) {
+    rep->gpu_ms = ms;
+    rep->gemm_ms = c->gemm_ms_accum;
+    rep->kernel_launches = c->launches - l0;
+    rep->gemm_launches = c->gemm_launches - g0;
+  }
+}
+
+}  // namespace pg

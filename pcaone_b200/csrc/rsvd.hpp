@@ -1,0 +1,31 @@
+// RSVD driver and the decode-GEMM back ends it can run on.
+#pragma once
+
+#include "internal.hpp"
+
+namespace pg {
+
+// A decode-GEMM back end. p1/p2 compute out[s][r][c] = sum_k val(code[r][k]) * B[k][c]
+// over K split into `ks` ranges (see kernels_gemm_simt.cu); B is row-major K x l.
+// omega_changed / b2_ready let a back end re-pack the B operands into its own layout.
+template <typename T>
+struct GemmFnT {
+  int (*ksplit)(pcaone_ctx* c, int64_t rows, int64_t K);
+  void (*p1)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K,
+             const T* B, int l, int ks, T* out);
+  void (*p2)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K,
+             const T* B, int l, int ks, T* out);
+  void (*omega_changed)(pcaone_ctx* c, const double* omega, int l, int64_t npad);
+  void (*b2_ready)(pcaone_ctx* c, const T* B2, int l, int64_t m);
+};
+
+GemmFnT<float> gemm_simt_float();
+GemmFnT<double> gemm_simt_double();
+GemmFnT<float> gemm_tc();
+
+void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);
+void jacobi_svd(int n, const double* A, double* U, double* s, double* V);
+void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, double* V,
+              pcaone_rsvd_report* rep);
+
+}  // namespace pg

@@ -1,0 +1,112 @@
+"""GPU parity tests of the RSVD path through the C ABI: counts and F bit-exact against the
+oracle, FP64/FP32 Halko and winSVD against the reference's golden outputs and the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import pcaone_b200 as pb
+from oracle import pcaone_oracle as O
+from tests.helpers import (GOLDEN, assert_cols_close, assert_eig_close, max_angle, ref_eigvals,
+                           ref_table)
+
+pytestmark = pytest.mark.gpu
+
+
+def load(gpu, name):
+    packed, N, M = pb.read_bed(os.path.join(GOLDEN, name))
+    gpu.load_bed(packed, N)
+    return O.read_bed(os.path.join(GOLDEN, name))
+
+
+def random_bed(N, M, seed, miss=0.02):
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(0.05, 0.5, M)
+    d = (rng.random((M, N)) < p[:, None]).astype(np.uint8) + (rng.random((M, N)) < p[:, None])
+    codes = np.where(d == 2, 0, np.where(d == 1, 2, 3)).astype(np.uint8)
+    codes[rng.random((M, N)) < miss] = 1
+    bpr = (N + 3) // 4
+    pad = np.zeros((M, bpr * 4), dtype=np.uint8)
+    pad[:, :N] = codes
+    pad = pad.reshape(M, bpr, 4)
+    packed = (pad[:, :, 0] | (pad[:, :, 1] << 2) | (pad[:, :, 2] << 4) | (pad[:, :, 3] << 6)).astype(np.uint8)
+    return O.Bed(N, M, packed)
+
+
+@pytest.mark.parametrize("N,M", [(203, 1500), (1001, 777), (1002, 300), (1003, 64), (4096, 2000)])
+def test_counts_and_freq_bit_exact(gpu, N, M):
+    bed = random_bed(N, M, seed=N + M)
+    gpu.load_bed(bed.packed, N)
+    a, c = gpu.counts()
+    n00, n10, nonmiss = O.allele_counts(O.decode_codes(bed))
+    np.testing.assert_array_equal(a, 2 * n00 + n10)
+    np.testing.assert_array_equal(c, nonmiss)
+    np.testing.assert_array_equal(gpu.allele_freq(), O.allele_freq(O.decode_codes(bed)))
+
+
+def test_permute_then_counts(gpu):
+    bed = random_bed(555, 1234, seed=9)
+    gpu.load_bed(bed.packed, bed.N)
+    a0, c0 = gpu.counts()
+    perm = pb.shuffle_perm(bed.M)
+    gpu.permute(perm)
+    a1, c1 = gpu.counts()
+    np.testing.assert_array_equal(a1, a0[perm])
+    np.testing.assert_array_equal(c1, c0[perm])
+
+
+def test_bad_permutation_rejected(gpu):
+    bed = random_bed(100, 50, seed=1)
+    gpu.load_bed(bed.packed, bed.N)
+    with pytest.raises(pb.PcaoneError):
+        gpu.permute(np.zeros(50, dtype=np.int32))
+
+
+GOLDEN_CASES = [
+    ("g1_halko", dict(svd=1, k=4, oversamples=10, maxp=7, tol=0.0), False),
+    ("g1_halko_p3", dict(svd=1, k=3, maxp=3, seed=7), False),
+    ("g1_win", dict(svd=2, k=4, bands=16), True),
+    ("g1_winS", dict(svd=2, k=4, bands=8), False),
+    ("g1_win_unif", dict(svd=2, k=3, bands=4, rand=0, seed=3, maxp=5), True),
+    ("g1_nostd", dict(svd=1, k=3, maxp=5, tol=0.0, standardize=False), False),
+]
+
+
+def run_gpu(gpu, bed, shuffle, **kw):
+    gpu.load_bed(bed.packed, bed.N)
+    perm = pb.shuffle_perm(bed.M) if shuffle else None
+    if shuffle:
+        gpu.permute(perm)
+    r = gpu.rsvd(**kw)
+    V = r.V
+    if shuffle:
+        V = np.empty_like(r.V)
+        V[perm] = r.V
+    return r, V
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,kw,shuffle", GOLDEN_CASES)
+def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
+    bed = O.read_bed(os.path.join(GOLDEN, "g1"))
+    r, V = run_gpu(gpu, bed, shuffle, precision=prec, **kw)
+    eig = r.S ** 2 / bed.M * 2
+    # reference prints 6 significant digits; FP32 path also within the 1e-5 parity bar
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(r.U, ref_table(name, ".eigvecs"), 2e-6 if prec == "fp64" else 5e-4)
+    lpath = os.path.join(GOLDEN, "ref", name + ".loadings")
+    if os.path.exists(lpath):
+        assert_cols_close(V, O.read_table(lpath), 2e-6 if prec == "fp64" else 5e-4)
+
+
+@pytest.mark.parametrize("svd,bands", [(1, 0), (2, 16), (2, 64)])
+def test_rsvd_matches_oracle_larger(gpu, svd, bands):
+    bed = random_bed(1502, 9001, seed=5, miss=0.01)
+    kw = dict(k=6, maxp=6, tol=0.0) if svd == 1 else dict(k=6, maxp=8, bands=bands)
+    eig_o, S_o, U_o, V_o, F_o, ep_o = O.run_pca(bed, svd=svd, **kw)
+    for prec, rtol, ang in [("fp64", 1e-9, 1e-7), ("fp32", 1e-5, 1e-3)]:
+        r, V = run_gpu(gpu, bed, svd == 2, precision=prec, svd=svd, **kw)
+        assert r.epochs == ep_o
+        assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, rtol)
+        assert max_angle(r.U, U_o) <= ang
+        assert max_angle(V, V_o) <= ang

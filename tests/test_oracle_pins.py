@@ -1,0 +1,74 @@
+"""CPU tests: the oracle is pinned against the reference's own outputs (golden fixtures
+made by the reference binary, tests/golden/make_golden.py) and the reference's own RNG."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import pcaone_oracle as O
+from tests.helpers import GOLDEN, assert_cols_close, assert_eig_close, ref_eigvals, ref_table
+
+REF_OMEGA = os.path.join(os.path.dirname(O._HERE), "oracle", "_ref", "omega_ref")
+
+
+def g(name):
+    return O.read_bed(os.path.join(GOLDEN, name))
+
+
+def test_allele_freq_matches_reference_mbim():
+    bed = g("g1")
+    F = O.allele_freq(O.decode_codes(bed))
+    mbim = [float(line.split("\t")[6]) for line in open(os.path.join(GOLDEN, "ref", "g1_halko.mbim"))]
+    # the .mbim prints F with 6 significant digits
+    np.testing.assert_allclose(F, mbim, rtol=5e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("name,svd,kw", [
+    ("g1_halko", 1, dict(k=4, oversamples=10, maxp=7, tol=0.0)),
+    ("g1_halko_p3", 1, dict(k=3, maxp=3, seed=7)),
+    ("g1_win", 2, dict(k=4, bands=16)),
+    ("g1_winS", 2, dict(k=4, bands=8, shuffle=False)),
+    ("g1_win_unif", 2, dict(k=3, bands=4, rand=0, seed=3, maxp=5)),
+    ("g1_nostd", 1, dict(k=3, maxp=5, tol=0.0, standardize_geno=False)),
+])
+def test_oracle_rsvd_matches_reference(name, svd, kw):
+    bed = g("g1")
+    eig, S, U, V, F, ep = O.run_pca(bed, svd=svd, **kw)
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(U, ref_table(name, ".eigvecs"), 2e-6)
+    if os.path.exists(os.path.join(GOLDEN, "ref", name + ".loadings")):
+        assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_OMEGA), reason="reference build not present")
+@pytest.mark.parametrize("rand", [0, 1])
+def test_oracle_rng_matches_reference_build(rand):
+    N, l, pn = 777, 13, 3001
+    raw = subprocess.run([REF_OMEGA, "101", str(rand), str(N), str(l), str(pn)],
+                         capture_output=True, check=True).stdout
+    ref = np.frombuffer(raw[:N * l * 8], dtype=np.float64).reshape(l, N).T
+    perm = np.frombuffer(raw[N * l * 8:], dtype=np.int32)
+    assert np.array_equal(O.omega(101, N, l, rand), ref)
+    assert np.array_equal(O.shuffle_perm(pn), perm)
+
+
+def test_oracle_householder_sign_recovery():
+    # CholeskyQR2 + modified-LU signs reproduce the Householder thin Q (LAPACK convention)
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        n, l = int(rng.integers(40, 300)), int(rng.integers(2, 24))
+        H = rng.standard_normal((n, l)) @ rng.standard_normal((l, l))
+        W = H.T @ H
+        R = np.linalg.cholesky(W).T
+        Q = np.linalg.solve(R.T, H.T).T
+        R2 = np.linalg.cholesky(Q.T @ Q).T
+        Q = np.linalg.solve(R2.T, Q.T).T
+        A = Q[:l, :l].copy()
+        D = np.zeros(l)
+        for i in range(l):
+            D[i] = -1.0 if A[i, i] >= 0 else 1.0
+            A[i, i] -= D[i]
+            A[i + 1:, i] /= A[i, i]
+            A[i + 1:, i + 1:] -= np.outer(A[i + 1:, i], A[i, i + 1:])
+        np.testing.assert_allclose(Q * D, O.householder_q(H), atol=1e-8)

@@ -116,6 +116,16 @@ typedef struct {
 int pcaone_gpu_rsvd(pcaone_ctx* ctx, const pcaone_rsvd_opts* opts, double* U, double* S,
                     double* V, pcaone_rsvd_report* report);
 
+/* One standardised product on the loaded genotypes, the blockwise matvec of
+ * ArnoldiOpData::perform_op (src/Arnoldi.cpp:18-46) and each half of
+ * NormalRsvdOpData::computeGandH (src/Halko.cpp:123-124):
+ *   transpose = 0: out (nsnps x ncols)    = Z^T B, B is nsamples x ncols;
+ *   transpose = 1: out (nsamples x ncols) = Z B,   B is nsnps x ncols;
+ * Z_ij = s_j (x_ij - F_j), missing -> 0, s_j = 1/sqrt(ploidy F_j (1-F_j)) when standardize
+ * (src/Data.cpp:290-299) else 1. Column-major FP64 host buffers; ncols <= 64. */
+int pcaone_gpu_product(pcaone_ctx* ctx, int precision, int transpose, int standardize,
+                       int ploidy, const double* B, uint32_t ncols, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,8 @@ STATUS = {0: "OK", 1: "EBADARG", 2: "EOOM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENUME
 # C ABI symbols declared in include/pcaone_gpu.h
 EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_load_bed", "pcaone_gpu_counts", "pcaone_gpu_allele_freq",
-           "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd"]
+           "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
+           "pcaone_gpu_product"]
 
 
 class PcaoneError(RuntimeError):
@@ -73,6 +74,8 @@ def lib() -> ctypes.CDLL:
         L.pcaone_omega.argtypes = [ctypes.c_int, ctypes.c_int, u64, u32, vp]
         L.pcaone_gpu_rsvd.argtypes = [vp, ctypes.POINTER(RsvdOpts), vp, vp, vp,
                                       ctypes.POINTER(RsvdReport)]
+        L.pcaone_gpu_product.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         vp, u32, vp]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
         _lib = L
@@ -186,6 +189,30 @@ class GpuContext:
         return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
                           rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
                           rep.kernel_launches, rep.gemm_launches)
+
+
+def _product(ctx: "GpuContext", B: np.ndarray, transpose: int, precision, standardize, ploidy):
+    if isinstance(precision, str):
+        precision = PRECISIONS[precision]
+    B = np.asarray(B, dtype=np.float64)
+    if B.ndim == 1:
+        B = B[:, None]
+    rows_in, rows_out = (ctx.N, ctx.M) if transpose == 0 else (ctx.M, ctx.N)
+    if B.shape[0] != rows_in:
+        raise ValueError(f"B must have {rows_in} rows")
+    Bc = np.asfortranarray(B)
+    out = np.zeros((rows_out, B.shape[1]), order="F")
+    ctx._check(lib().pcaone_gpu_product(ctx._h, precision, transpose, int(standardize), ploidy,
+                                        _ptr(Bc), B.shape[1], _ptr(out)))
+    return np.ascontiguousarray(out)
+
+
+GpuContext.product_t = lambda self, B, precision=PREC_FP64, standardize=True, ploidy=2: \
+    _product(self, B, 0, precision, standardize, ploidy)
+GpuContext.product_t.__doc__ = "Z^T B (nsnps x ncols) for B nsamples x ncols."
+GpuContext.product = lambda self, B, precision=PREC_FP64, standardize=True, ploidy=2: \
+    _product(self, B, 1, precision, standardize, ploidy)
+GpuContext.product.__doc__ = "Z B (nsamples x ncols) for B nsnps x ncols."
 
 
 def read_bed(prefix: str):

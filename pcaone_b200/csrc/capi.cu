@@ -210,4 +210,9 @@ int pcaone_gpu_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts* opts, double* U, doub
   });
 }
 
+int pcaone_gpu_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
+                       const double* B, uint32_t ncols, double* out) {
+  return guarded(c, [&] { run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out); });
+}
+
 }  // extern "C"

@@ -33,6 +33,9 @@ struct EpiP2 {          // after the Z * G product of one window
 
 template <typename T>
 void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0);
+// B2 = s/2 G and h0 = sum s F G for the rows [start, start+m) of p.G (no product).
+template <typename T>
+void launch_scale_g(pcaone_ctx* c, const EpiP1& p, T* B2, double* h0);
 template <typename T>
 void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2);
 void zero(pcaone_ctx* c, double* a, int64_t n);

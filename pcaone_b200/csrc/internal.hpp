@@ -126,5 +126,7 @@ void launch_decode_gemm_simt(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch
 // ---------------------------------------------------------------- tcgen05 decode-GEMM
 // Same contract with BF16 hi/lo split of B; see kernels_gemm_tc.cu.
 bool tc_supported(pcaone_ctx* c);
+void tc_clear_error(pcaone_ctx* c);
+void tc_check_error(pcaone_ctx* c);
 
 }  // namespace pg

@@ -60,6 +60,31 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
   }
 }
 
+// B2_j = s_j/2 G_j and per-CTA partials of h0 = sum_j s_j F_j G_j, for a given G.
+template <typename T>
+__global__ void k_scale_g(int64_t start, int64_t m, int l, int standardize, int ploidy,
+                          const double* __restrict__ F, const double* __restrict__ G,
+                          T* __restrict__ B2, double* __restrict__ h0_part) {
+  extern __shared__ double sh0[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int c = lane; c < l; c += 32) sh0[warp * l + c] = 0.0;
+  for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < m; jl += (int64_t)gridDim.x * nwarps) {
+    const int64_t j = start + jl;
+    const double f = F[j], s = snp_scale(f, standardize, ploidy);
+    for (int c = lane; c < l; c += 32) {
+      const double g = G[j * l + c];
+      B2[jl * l + c] = (T)(0.5 * s * g);
+      sh0[warp * l + c] += s * f * g;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < l; c += blockDim.x) {
+    double acc = 0.0;
+    for (int w = 0; w < nwarps; ++w) acc += sh0[w * l + c];
+    h0_part[(int64_t)blockIdx.x * l + c] = acc;
+  }
+}
+
 __global__ void k_reduce_cols(const double* __restrict__ part, int nblk, int l, double* __restrict__ out) {
   int c = threadIdx.x;
   if (c >= l) return;
@@ -114,12 +139,27 @@ void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
   c->launches++;
 }
 
+template <typename T>
+void launch_scale_g(pcaone_ctx* c, const EpiP1& p, T* B2, double* h0) {
+  const int threads = 256, nwarps = threads / 32;
+  int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
+  double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
+  k_scale_g<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p.start, p.m, p.l, p.standardize,
+                                                                       p.ploidy, p.F, p.G, B2, part);
+  PG_CHECK_LAUNCH();
+  k_reduce_cols<<<1, 128, 0, c->stream>>>(part, nblk, p.l, h0);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
+
 void zero(pcaone_ctx* c, double* a, int64_t n) {
   PG_CUDA(cudaMemsetAsync(a, 0, n * sizeof(double), c->stream));
 }
 
 template void launch_prep<float>(pcaone_ctx*, const EpiP1&, const float*, float*, double*);
 template void launch_prep<double>(pcaone_ctx*, const EpiP1&, const double*, double*, double*);
+template void launch_scale_g<float>(pcaone_ctx*, const EpiP1&, float*, double*);
+template void launch_scale_g<double>(pcaone_ctx*, const EpiP1&, double*, double*);
 template void launch_accum<float>(pcaone_ctx*, const EpiP2&, const float*);
 template void launch_accum<double>(pcaone_ctx*, const EpiP2&, const double*);
 

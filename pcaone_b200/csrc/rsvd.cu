@@ -287,6 +287,7 @@ struct Engine {
   }
 
   void check_status() {
+    if (o.precision == PCAONE_PREC_MIXED) tc_check_error(c);
     int st = 0;
     PG_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
@@ -379,6 +380,95 @@ struct Engine {
   }
 };
 
+// One standardised product through the same kernels as the RSVD (single window).
+template <typename T>
+void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, int ploidy,
+               const double* B, int l, double* out) {
+  const int N = (int)c->N;
+  const int64_t M = (int64_t)c->M, Npad = c->Npad;
+  auto d = [&](const char* name, size_t n) { return (double*)scratch(c, name, n * sizeof(double)); };
+  double* G = d("r_G", (size_t)c->Mpad * l);
+  double* H = d("r_H", Npad * l);
+  double* Bd = d("r_omg", Npad * l);
+  double* wsum = d("r_wsum", l);
+  double* h0 = d("r_h0", l);
+  T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
+  std::vector<double> rm;
+  if (transpose == 0) {
+    rm.assign((size_t)Npad * l, 0.0);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = B[(size_t)j * N + i];
+    PG_CUDA(cudaMemcpyAsync(Bd, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    T* BT = std::is_same<T, double>::value ? reinterpret_cast<T*>(Bd) : (T*)scratch(c, "r_omgT", Npad * l * sizeof(T));
+    if (!std::is_same<T, double>::value) {
+      std::vector<float> f(rm.begin(), rm.end());
+      PG_CUDA(cudaMemcpyAsync(BT, f.data(), f.size() * 4, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    colsum(c, Bd, l, N, wsum);
+    gemm.omega_changed(c, Bd, l, Npad);
+    const int ks = gemm.ksplit(c, M, N);
+    T* D1 = (T*)scratch(c, "r_D1", (size_t)ks * M * l * sizeof(T));
+    gemm.p1(c, c->d_bed, c->pitch, M, N, BT, l, ks, D1);
+    EpiP1 p1;
+    p1.start = 0; p1.m = M; p1.l = l; p1.ksplit = ks; p1.standardize = standardize; p1.ploidy = ploidy;
+    p1.F = c->d_F; p1.wsum = wsum; p1.omega = Bd; p1.miss_ptr = c->d_miss_snp_ptr;
+    p1.miss_idx = c->d_miss_snp_idx; p1.G = G;
+    launch_prep<T>(c, p1, D1, B2, h0);
+    rm.resize((size_t)M * l);
+    PG_CUDA(cudaMemcpyAsync(rm.data(), G, rm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < M; ++i)
+      for (int j = 0; j < l; ++j) out[(size_t)j * M + i] = rm[(size_t)i * l + j];
+  } else {
+    rm.assign((size_t)M * l, 0.0);
+    for (int64_t i = 0; i < M; ++i)
+      for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = B[(size_t)j * M + i];
+    PG_CUDA(cudaMemcpyAsync(G, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    EpiP1 p1;
+    p1.start = 0; p1.m = M; p1.l = l; p1.standardize = standardize; p1.ploidy = ploidy;
+    p1.F = c->d_F; p1.G = G;
+    launch_scale_g<T>(c, p1, B2, h0);
+    gemm.b2_ready(c, B2, l, M);
+    const int ks = gemm.ksplit(c, N, M);
+    T* D2 = (T*)scratch(c, "r_D2", (size_t)ks * N * l * sizeof(T));
+    gemm.p2(c, c->d_bedT, c->win.pitch, N, M, B2, l, ks, D2);
+    zero(c, H, Npad * l);
+    EpiP2 p2;
+    p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks; p2.standardize = standardize;
+    p2.ploidy = ploidy; p2.F = c->d_F; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
+    p2.miss_idx = c->d_miss_ws_idx; p2.H = H;
+    launch_accum<T>(c, p2, D2);
+    rm.resize((size_t)N * l);
+    PG_CUDA(cudaMemcpyAsync(rm.data(), H, rm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < l; ++j) out[(size_t)j * N + i] = rm[(size_t)i * l + j];
+  }
+}
+
+void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
+                 const double* B, int l, double* out) {
+  PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+  PG_REQUIRE(B && out && l >= 1 && l <= kLmax, PCAONE_EBADARG, "bad product operands");
+  PG_REQUIRE(transpose == 0 || transpose == 1, PCAONE_EBADARG, "transpose must be 0 or 1");
+  build_transposed(c, 1);
+  build_missing_by_snp(c);
+  build_missing_by_window_sample(c);
+  if (precision == PCAONE_PREC_FP64) {
+    product_t<double>(c, gemm_simt_double(), transpose, standardize, ploidy, B, l, out);
+  } else if (precision == PCAONE_PREC_FP32) {
+    product_t<float>(c, gemm_simt_float(), transpose, standardize, ploidy, B, l, out);
+  } else if (precision == PCAONE_PREC_MIXED) {
+    PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
+    tc_clear_error(c);
+    product_t<float>(c, gemm_tc(), transpose, standardize, ploidy, B, l, out);
+    tc_check_error(c);
+  } else {
+    throw Error(PCAONE_EBADARG, "unknown precision");
+  }
+}
+
 void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, double* V,
               pcaone_rsvd_report* rep) {
   PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
@@ -406,6 +496,7 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
     e.run(U, S, V, rep);
   } else if (o.precision == PCAONE_PREC_MIXED) {
     PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
+    tc_clear_error(c);
     Engine<float> e(c, o, gemm_tc());
     e.run(U, S, V, rep);
   } else {

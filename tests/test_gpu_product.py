@@ -1,0 +1,45 @@
+"""GPU tests of the standardised decode-GEMM products through the C ABI, each precision
+against the FP64 numpy restatement of Z (oracle): Z^T B and Z B."""
+import numpy as np
+import pytest
+
+import pcaone_b200 as pb
+from oracle import pcaone_oracle as O
+from tests.test_gpu_rsvd import random_bed
+
+pytestmark = pytest.mark.gpu
+
+# max |err| / max |ref| per output column; the mixed path uses split-BF16 (hi+lo, 16 bits)
+TOL = {"fp64": 1e-12, "fp32": 2e-6, "mixed": 5e-5}
+
+
+def rel_col_err(got, ref):
+    return float((np.abs(got - ref).max(axis=0) / np.abs(ref).max(axis=0)).max())
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("N,M,l", [(1003, 2500, 40), (517, 777, 20), (2048, 1300, 7), (300, 4100, 64)])
+def test_products_match_dense(gpu, prec, N, M, l):
+    bed = random_bed(N, M, seed=N * 7 + l, miss=0.02)
+    Z, F = O.standardized_from_bed(bed)
+    gpu.load_bed(bed.packed, N)
+    rng = np.random.default_rng(l)
+    B1 = rng.standard_normal((N, l))
+    got1 = gpu.product_t(B1, precision=prec)
+    assert rel_col_err(got1, Z.T @ B1) <= TOL[prec]
+    B2 = rng.standard_normal((M, l))
+    got2 = gpu.product(B2, precision=prec)
+    assert rel_col_err(got2, Z @ B2) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_products_unstandardised_haploid(gpu, prec):
+    bed = random_bed(640, 900, seed=3, miss=0.05)
+    codes = O.decode_codes(bed)
+    F = O.allele_freq(codes)
+    Zc = O.centered_matrix(codes, F)
+    gpu.load_bed(bed.packed, bed.N)
+    B = np.random.default_rng(0).standard_normal((bed.N, 12))
+    assert rel_col_err(gpu.product_t(B, precision=prec, standardize=False), Zc.T @ B) <= TOL[prec]
+    Zh = O.standardize(Zc, F, ploidy=1)
+    assert rel_col_err(gpu.product_t(B, precision=prec, ploidy=1), Zh.T @ B) <= TOL[prec]

@@ -85,7 +85,7 @@ def run_gpu(gpu, bed, shuffle, **kw):
     return r, V
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
 @pytest.mark.parametrize("name,kw,shuffle", GOLDEN_CASES)
 def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
     bed = O.read_bed(os.path.join(GOLDEN, "g1"))
@@ -97,6 +97,8 @@ def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
     lpath = os.path.join(GOLDEN, "ref", name + ".loadings")
     if os.path.exists(lpath):
         assert_cols_close(V, O.read_table(lpath), 2e-6 if prec == "fp64" else 5e-4)
+    if prec == "mixed":
+        assert r.gemm_launches > 0
 
 
 @pytest.mark.parametrize("svd,bands", [(1, 0), (2, 16), (2, 64)])
@@ -104,7 +106,7 @@ def test_rsvd_matches_oracle_larger(gpu, svd, bands):
     bed = random_bed(1502, 9001, seed=5, miss=0.01)
     kw = dict(k=6, maxp=6, tol=0.0) if svd == 1 else dict(k=6, maxp=8, bands=bands)
     eig_o, S_o, U_o, V_o, F_o, ep_o = O.run_pca(bed, svd=svd, **kw)
-    for prec, rtol, ang in [("fp64", 1e-9, 1e-7), ("fp32", 1e-5, 1e-3)]:
+    for prec, rtol, ang in [("fp64", 1e-9, 1e-7), ("fp32", 1e-5, 1e-3), ("mixed", 1e-5, 1e-3)]:
         r, V = run_gpu(gpu, bed, svd == 2, precision=prec, svd=svd, **kw)
         assert r.epochs == ep_o
         assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, rtol)

@@ -39,6 +39,10 @@ CONFIGS = {
     "c2": dict(workload="winSVD k=20, 64 windows, 20000 samples x 500000 SNPs, 5 BN pops",
                n=20000, m=500000, pops=5, fst=(0.01, 0.1), pmin=0.01, pmax=0.5, miss=0.005,
                seed=2, k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_sample_snps=8000),
+    # profiling-size case of c2 (packed matrix 250 MB > L2), same shapes per window row/column
+    "c2s": dict(workload="winSVD k=20, 64 windows, 20000 samples x 50000 SNPs, 5 BN pops",
+                n=20000, m=50000, pops=5, fst=(0.01, 0.1), pmin=0.01, pmax=0.5, miss=0.005,
+                seed=2, k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_sample_snps=8000),
     "c1": dict(workload="Halko k=10 p=7, 2000 samples x 50000 SNPs, 3 BN pops",
                n=2000, m=50000, pops=3, fst=(0.05, 0.05), pmin=0.05, pmax=0.5, miss=0.01,
                seed=1, k=10, svd=1, bands=64, maxp=7, tol=0.0, cpu_sample_snps=50000),

@@ -96,6 +96,11 @@ typedef struct {
   double tol;           /* --tol-rsvd */
   int32_t verbose;      /* print per-epoch "running of epoch" lines to stdout */
   int32_t profile;      /* time every decode-GEMM launch with CUDA events (gemm_ms) */
+  int32_t carry_window_state; /* winSVD: keep the window sums H1/H2 of the previous call on
+                                 this context, as successive computeUSV calls on one
+                                 FancyRsvdOpData do (src/Halko.hpp:68, src/Halko.cpp:159-163);
+                                 0 starts from zero like a fresh process */
+  int32_t reserved;
 } pcaone_rsvd_opts;
 
 typedef struct {
@@ -125,6 +130,20 @@ int pcaone_gpu_rsvd(pcaone_ctx* ctx, const pcaone_rsvd_opts* opts, double* U, do
  * (src/Data.cpp:290-299) else 1. Column-major FP64 host buffers; ncols <= 64. */
 int pcaone_gpu_product(pcaone_ctx* ctx, int precision, int transpose, int standardize,
                        int ploidy, const double* B, uint32_t ncols, double* out);
+
+/* EMU imputation step, Data::fit_with_pi EMU branch (src/Data.cpp:272-287): every missing
+ * genotype of the loaded matrix takes the centred value
+ *   e_ij = clip(sum_t U_it S_t V_jt, -F_j, 1 - F_j)
+ * in place of 0 in all later products and RSVD runs, until pcaone_gpu_clear_imputed or a
+ * new load/permutation. U (nsamples x k), S (k), V (nsnps x k, current SNP order) are host
+ * column-major buffers, e.g. the outputs of the previous pcaone_gpu_rsvd call.
+ * reference_index = 1 reproduces the reference's index semantics after the in-core
+ * shuffle: the clip bounds, and the standardisation of later runs while imputation is
+ * active, read F at the SNP's permuted position (F in load order) as src/Data.cpp:283 and
+ * :296 do; 0 uses each SNP's own F. */
+int pcaone_gpu_fit_emu(pcaone_ctx* ctx, const double* U, const double* S, const double* V,
+                       uint32_t k, int reference_index);
+int pcaone_gpu_clear_imputed(pcaone_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -242,14 +242,24 @@ def halko(Z: np.ndarray, k: int, os_: int, p: int, tol: float, seed: int = 101,
 
 
 def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed: int = 101,
-           rand: int = 1, update_hook=None) -> RsvdResult:
+           rand: int = 1, update_hook=None, state: dict | None = None) -> RsvdResult:
     """Window-based RSVD, FancyRsvdOpData::computeGandH in-core (src/Halko.cpp:153-226).
-    Z must already be column-permuted when the reference permutes (src/Halko.cpp:181-184)."""
+    Z must already be column-permuted when the reference permutes (src/Halko.cpp:181-184).
+
+    `state` carries the window sums H1/H2 between successive calls: FancyRsvdOpData keeps
+    them as members (src/Halko.hpp:68) and only zeroes them when 2^pi >= bands
+    (src/Halko.cpp:159-163), so a second computeUSV on the same operator (the EM loops,
+    src/Halko.cpp:301-336) starts from the previous call's leftover H2."""
     N, M = Z.shape
     l = k + os_
     st = _HalkoState(N, l, seed, rand)
-    H1 = np.zeros((N, l))
-    H2 = np.zeros((N, l))
+    if state is not None and "H1" in state:
+        H1, H2 = state["H1"], state["H2"]
+    else:
+        H1 = np.zeros((N, l))
+        H2 = np.zeros((N, l))
+    if state is not None:
+        state["H1"], state["H2"] = H1, H2
     sched = {"bandsize": 1}
     blocksize = int(np.ceil(M / bands))
 
@@ -321,6 +331,69 @@ def run_pca(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: in
     return eig, res.S, res.U, V, F, res.epochs
 
 
+def missing_mask(codes: np.ndarray) -> np.ndarray:
+    """C: N x M boolean, True where the genotype is missing (src/FilePlink.cpp:79-85)."""
+    return (codes == 1).T.copy()
+
+
+def fit_emu(G: np.ndarray, miss: np.ndarray, U, S, V, Fclip) -> None:
+    """Data::fit_with_pi EMU branch (src/Data.cpp:272-287), in place: missing entries of the
+    centred G take clip(U S V^T, -F, 1 - F). G, miss are N x M in the current column order;
+    Fclip[j] is the F the reference reads for column j."""
+    pred = (U * S) @ V.T
+    lo = -Fclip[None, :]
+    hi = 1.0 - Fclip[None, :]
+    G[miss] = np.clip(pred, lo, hi)[miss]
+
+
+def run_emu(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: int = 10,
+            bands: int = 64, tol: float = 1e-4, maxiter: int = 100, tolem: float = 1e-5,
+            seed: int = 101, rand: int = 1, shuffle: bool = True, reference_index: bool = True):
+    """EMU PCA, run_pca_with_halko impute branch with --emu (src/Halko.cpp:294-336, 338-342).
+
+    Reference index semantics (reference_index=True): after the in-core shuffle G's columns
+    are permuted but F stays in input order, so the clip bounds (src/Data.cpp:283) and the
+    final standardize_E (src/Data.cpp:296) read F at the permuted position. The missing mask
+    is read through the permutation (src/Data.cpp:277) and is correct.
+    Returns (eigvals, S, U, V in input order, F, em_iterations, diffs)."""
+    os_ = max(oversamples, k)
+    codes = decode_codes(bed)
+    F = allele_freq(codes)
+    G = centered_matrix(codes, F)
+    miss = missing_mask(codes)
+    M = bed.M
+    perm = shuffle_perm(M) if (svd == 2 and shuffle) else np.arange(M, dtype=np.int32)
+    Gp = G[:, perm].copy()
+    missp = miss[:, perm]
+    Fclip = F if reference_index else F[perm]
+    state = {}
+
+    def rsvd(Z):
+        if svd == 1:
+            return halko(Z, k, os_, maxp, tol, seed, rand)
+        return winsvd(Z, k, os_, maxp, tol, bands, seed, rand, state=state)
+
+    res = rsvd(Gp)
+    diffs = []
+    it = 0
+    for it in range(maxiter):
+        Vpre = res.V
+        fit_emu(Gp, missp, res.U, res.S, res.V, Fclip)
+        res = rsvd(Gp)
+        diff = 1.0 - mev(res.V, Vpre)
+        diffs.append(diff)
+        if diff < tolem:
+            break
+    # final standardised run (src/Halko.cpp:332-336)
+    fit_emu(Gp, missp, res.U, res.S, res.V, Fclip)
+    Gs = standardize(Gp, Fclip)
+    res = rsvd(Gs)
+    V = np.empty_like(res.V)
+    V[perm] = res.V
+    eig = res.S ** 2 / M * 2
+    return eig, res.S, res.U, V, F, it + 1, diffs
+
+
 def dense_eig(bed: Bed, k: int, standardize_geno: bool = True):
     """FP64 dense oracle: eigenvalues sigma^2/M*ploidy and U from the full SVD of Z."""
     Z, F = standardized_from_bed(bed, standardize_geno)
@@ -362,3 +435,108 @@ def read_ld_gz(path: str):
         head = f.readline()
         rows = [line.rstrip("\n").split("\t") for line in f]
     return head, rows
+
+
+# --------------------------------------------------------------------------- LD r2
+@dataclass
+class SnpLD:
+    chr: list
+    pos: np.ndarray
+    end_pos: list
+    bims: list       # "chr\tpos\tid" per SNP (struct BIM, src/LD.hpp:18-28)
+    ws: np.ndarray = None
+    we: np.ndarray = None
+
+
+def read_snp_pos(filebim: str) -> SnpLD:
+    """get_snp_pos_bim (src/LD.cpp:51-74): chromosome runs, positions, and the BIM strings."""
+    chrs, pos, end_pos, bims = [], [], [], []
+    prev = None
+    with open(filebim) as f:
+        for i, line in enumerate(f):
+            tok = [t for t in line.rstrip("\n").replace(" ", "\t").split("\t")]
+            cur = tok[0]
+            if prev is None:
+                chrs.append(cur)
+            elif prev != cur:
+                end_pos.append(i - 1)
+                chrs.append(cur)
+            prev = cur
+            pos.append(int(tok[3]))
+            bims.append(tok[0] + "\t" + tok[3] + "\t" + tok[1])
+    end_pos.append(len(pos) - 1)
+    return SnpLD(chrs, np.array(pos, dtype=np.int64), end_pos, bims)
+
+
+def divide_pos_by_window(snp: SnpLD, ld_bp: int) -> None:
+    """divide_pos_by_window (src/LD.cpp:125-139): for each SNP i that is not at its
+    chromosome's last position, the window holds the SNPs j >= i of that chromosome with
+    pos_j - pos_i <= ld_bp (i included)."""
+    ws, we = [], []
+    c = 0
+    n = len(snp.pos)
+    for i in range(n):
+        if snp.pos[i] == snp.pos[snp.end_pos[c]]:
+            c += 1
+            continue
+        j = i
+        while j <= snp.end_pos[c]:
+            if snp.pos[j] - snp.pos[i] > ld_bp:
+                break
+            j += 1
+        ws.append(i)
+        we.append(j - i)
+    snp.ws, snp.we = np.array(ws, dtype=np.int64), np.array(we, dtype=np.int64)
+
+
+def ld_pairs(G: np.ndarray, snp: SnpLD):
+    """ld_r2_big (src/LD.cpp:419-442): r = G_i.G_k * sds_i sds_k / (N-1), sds = 1/sd."""
+    N = G.shape[0]
+    sds = 1.0 / np.sqrt((G * G).sum(axis=0) / (N - 1))
+    df = 1.0 / (N - 1)
+    out_i, out_k, out_r = [], [], []
+    for i, w in zip(snp.ws, snp.we):
+        if w <= 1:
+            continue
+        ks = np.arange(i + 1, i + w)
+        r = (G[:, ks].T @ G[:, i]) * (sds[i] * sds[ks] * df)
+        out_i.append(np.full(len(ks), i))
+        out_k.append(ks)
+        out_r.append(r)
+    if not out_i:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0)
+    return np.concatenate(out_i), np.concatenate(out_k), np.concatenate(out_r)
+
+
+def ld_flow_a(bed: Bed, U: np.ndarray):
+    """run_ld_stuff with PLINK + --read-U (src/LD.cpp:444-468): centred G (not standardised,
+    pca is off for LD, src/Cmd.cpp:166-169) projected off U: G = (I - U U^T) G."""
+    codes = decode_codes(bed)
+    F = allele_freq(codes)
+    G = centered_matrix(codes, F)
+    return G - U @ (U.T @ G)
+
+
+def read_residuals(path: str) -> np.ndarray:
+    """FileBin::read_all (src/FileBinary.cpp:21-30): int32 nsnps, nsamples, then float32
+    columns; each column re-centred."""
+    with open(path, "rb") as f:
+        hdr = np.frombuffer(f.read(8), dtype=np.uint32)
+        M, N = int(hdr[0]), int(hdr[1])
+        G = np.frombuffer(f.read(4 * M * N), dtype=np.float32).reshape(M, N).T.astype(np.float64)
+    return G - G.mean(axis=0, keepdims=True)
+
+
+def ld_lines(snp: SnpLD, i, k, r) -> list:
+    """Text lines of the .ld.gz output: bims[i] \\t bims[k] \\t std::to_string(r*r)."""
+    return [f"{snp.bims[a]}\t{snp.bims[b]}\t{x * x:.6f}" for a, b, x in zip(i, k, r)]
+
+
+def read_usv(path: str) -> np.ndarray:
+    """read_usv (src/Utils.cpp:255-286): the tab-separated table is read row by row into one
+    vector, which is then viewed as a column-major (rows x cols) matrix
+    (Eigen::Map<Mat2D>(V.data(), j, k)), so the returned U is the file's row-major values
+    laid out column-major. LD flow A uses this U (src/LD.cpp:462)."""
+    T = read_table(path)
+    j, k = T.shape
+    return T.ravel().reshape(k, j).T.copy()

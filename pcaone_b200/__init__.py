@@ -26,7 +26,7 @@ STATUS = {0: "OK", 1: "EBADARG", 2: "EOOM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENUME
 EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_load_bed", "pcaone_gpu_counts", "pcaone_gpu_allele_freq",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
-           "pcaone_gpu_product"]
+           "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed"]
 
 
 class PcaoneError(RuntimeError):
@@ -41,7 +41,8 @@ class RsvdOpts(ctypes.Structure):
                 ("precision", ctypes.c_int32), ("standardize", ctypes.c_int32),
                 ("ploidy", ctypes.c_int32), ("seed", ctypes.c_int32), ("rand", ctypes.c_int32),
                 ("tol", ctypes.c_double), ("verbose", ctypes.c_int32),
-                ("profile", ctypes.c_int32)]
+                ("profile", ctypes.c_int32), ("carry_window_state", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class RsvdReport(ctypes.Structure):
@@ -76,6 +77,8 @@ def lib() -> ctypes.CDLL:
                                       ctypes.POINTER(RsvdReport)]
         L.pcaone_gpu_product.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          vp, u32, vp]
+        L.pcaone_gpu_fit_emu.argtypes = [vp, vp, vp, vp, u32, ctypes.c_int]
+        L.pcaone_gpu_clear_imputed.argtypes = [vp]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
         _lib = L
@@ -174,12 +177,13 @@ class GpuContext:
     def rsvd(self, k: int = 10, oversamples: int = 10, maxp: int = 20, svd: int = 2,
              bands: int = 64, precision: int | str = PREC_FP32, standardize: bool = True,
              ploidy: int = 2, seed: int = 101, rand: int = 1, tol: float = 1e-4,
-             verbose: bool = False, profile: bool = False, want_v: bool = True) -> RsvdResult:
+             verbose: bool = False, profile: bool = False, want_v: bool = True,
+             carry: bool = False) -> RsvdResult:
         if isinstance(precision, str):
             precision = PRECISIONS[precision]
         os_ = max(oversamples, k)  # src/Cmd.cpp:190
         o = RsvdOpts(k, os_, maxp, svd, bands, precision, int(standardize), ploidy, seed,
-                     rand, tol, int(verbose), int(profile))
+                     rand, tol, int(verbose), int(profile), int(carry), 0)
         U = np.zeros((k, self.N))
         S = np.zeros(k)
         V = np.zeros((k, self.M)) if want_v else None
@@ -213,6 +217,61 @@ GpuContext.product_t.__doc__ = "Z^T B (nsnps x ncols) for B nsamples x ncols."
 GpuContext.product = lambda self, B, precision=PREC_FP64, standardize=True, ploidy=2: \
     _product(self, B, 1, precision, standardize, ploidy)
 GpuContext.product.__doc__ = "Z B (nsamples x ncols) for B nsnps x ncols."
+
+
+def _fit_emu(self, U, S, V, reference_index=True):
+    """Data::fit_with_pi EMU step on the device (see pcaone_gpu_fit_emu)."""
+    k = len(S)
+    Uf = np.asfortranarray(U, dtype=np.float64)
+    Vf = np.asfortranarray(V, dtype=np.float64)
+    Sf = np.ascontiguousarray(S, dtype=np.float64)
+    self._check(lib().pcaone_gpu_fit_emu(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), k,
+                                         int(reference_index)))
+
+
+def _clear_imputed(self):
+    self._check(lib().pcaone_gpu_clear_imputed(self._h))
+
+
+GpuContext.fit_emu = _fit_emu
+GpuContext.clear_imputed = _clear_imputed
+
+
+def mev(X: np.ndarray, Y: np.ndarray) -> float:
+    """1/k sum_i ||X^T Y_i|| (src/Utils.cpp:192-198)."""
+    C = X.T @ Y
+    return float(np.mean(np.linalg.norm(C, axis=0)))
+
+
+def run_emu(ctx: "GpuContext", packed: np.ndarray, N: int, k: int = 10, svd: int = 2,
+            bands: int = 64, maxp: int = 20, oversamples: int = 10, tol: float = 1e-4,
+            maxiter: int = 100, tolem: float = 1e-5, seed: int = 101, rand: int = 1,
+            shuffle: bool = True, precision=PREC_MIXED, reference_index: bool = True):
+    """EMU PCA on the GPU: the impute branch of run_pca_with_halko with --emu
+    (src/Halko.cpp:294-336). Returns (eigvals, S, U, V in input SNP order, iterations)."""
+    ctx.load_bed(packed, N)
+    M = packed.shape[0]
+    perm = shuffle_perm(M) if (svd == 2 and shuffle) else None
+    if perm is not None:
+        ctx.permute(perm)
+    kw = dict(k=k, oversamples=oversamples, maxp=maxp, svd=svd, bands=bands, tol=tol,
+              seed=seed, rand=rand, precision=precision)
+    r = ctx.rsvd(standardize=False, carry=False, **kw)
+    it = 0
+    for it in range(maxiter):
+        Vpre = r.V
+        ctx.fit_emu(r.U, r.S, r.V, reference_index)
+        r = ctx.rsvd(standardize=False, carry=True, **kw)
+        if 1.0 - mev(r.V, Vpre) < tolem:
+            break
+    ctx.fit_emu(r.U, r.S, r.V, reference_index)
+    r = ctx.rsvd(standardize=True, carry=True, **kw)
+    ctx.clear_imputed()
+    V = r.V
+    if perm is not None:
+        V = np.empty_like(r.V)
+        V[perm] = r.V
+    return r.S ** 2 / M * 2, r.S, r.U, V, it + 1
 
 
 def read_bed(prefix: str):

@@ -37,6 +37,15 @@ void free_data(pcaone_ctx* c) {
   free_ptr(c->d_miss_snp_idx);
   free_ptr(c->d_miss_ws_ptr);
   free_ptr(c->d_miss_ws_idx);
+  free_ptr(c->d_F_load);
+  free_ptr(c->d_scale);
+  free_ptr(c->d_imp_US);
+  free_ptr(c->d_imp_V);
+  free_ptr(c->d_miss_snp_val);
+  free_ptr(c->d_miss_ws_val);
+  c->d_F_load = c->d_scale = c->d_imp_US = c->d_imp_V = c->d_miss_snp_val = c->d_miss_ws_val = nullptr;
+  c->imputed = false;
+  c->miss_ws_val_valid = false;
   c->d_bed = c->d_bedT = nullptr;
   c->d_a1x2 = c->d_nonmiss = nullptr;
   c->d_F = nullptr;
@@ -122,6 +131,7 @@ int pcaone_gpu_load_bed(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, ui
     PG_REQUIRE(packed && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty genotype matrix");
     PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 30), PCAONE_EBADARG, "genotype matrix too large");
     free_data(c);
+    c->generation++;
     c->N = nsamples;
     c->M = nsnps;
     c->bpr = (nsamples + 3) / 4;
@@ -133,11 +143,14 @@ int pcaone_gpu_load_bed(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, ui
     PG_CUDA(cudaMalloc(&c->d_a1x2, c->M * 4));
     PG_CUDA(cudaMalloc(&c->d_nonmiss, c->M * 4));
     PG_CUDA(cudaMalloc(&c->d_F, c->M * 8));
+    PG_CUDA(cudaMalloc(&c->d_F_load, c->M * 8));
+    PG_CUDA(cudaMalloc(&c->d_scale, c->M * 8));
     PG_CUDA(cudaMemsetAsync(c->d_bed, 0xFF, bytes, c->stream));
     PG_CUDA(cudaMemcpy2DAsync(c->d_bed, c->pitch, packed, c->bpr, c->bpr, c->M,
                               cudaMemcpyHostToDevice, c->stream));
     launch_fix_padding(c);
     launch_counts(c);
+    PG_CUDA(cudaMemcpyAsync(c->d_F_load, c->d_F, c->M * 8, cudaMemcpyDeviceToDevice, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
     c->loaded = true;
   });
@@ -185,6 +198,9 @@ int pcaone_gpu_permute(pcaone_ctx* c, const int32_t* perm) {
     launch_counts(c);
     PG_CUDA(cudaStreamSynchronize(c->stream));
     c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
+    c->generation++;
+    c->imputed = false;  // imputed values are tied to the SNP order of the lists
+    c->miss_ws_val_valid = false;
   });
 }
 
@@ -213,6 +229,39 @@ int pcaone_gpu_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts* opts, double* U, doub
 int pcaone_gpu_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
                        const double* B, uint32_t ncols, double* out) {
   return guarded(c, [&] { run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out); });
+}
+
+int pcaone_gpu_fit_emu(pcaone_ctx* c, const double* U, const double* S, const double* V,
+                       uint32_t k, int reference_index) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+    PG_REQUIRE(U && S && V && k >= 1 && k <= (uint32_t)kLmax, PCAONE_EBADARG, "bad EMU factors");
+    build_missing_by_snp(c);
+    // US = U diag(S), row-major N x k; V row-major M x k
+    std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
+    for (uint32_t i = 0; i < c->N; ++i)
+      for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+    for (uint64_t j = 0; j < c->M; ++j)
+      for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
+    if (c->d_imp_US) cudaFree(c->d_imp_US);
+    if (c->d_imp_V) cudaFree(c->d_imp_V);
+    c->d_imp_US = c->d_imp_V = nullptr;
+    PG_CUDA(cudaMalloc(&c->d_imp_US, us.size() * 8));
+    PG_CUDA(cudaMalloc(&c->d_imp_V, v.size() * 8));
+    PG_CUDA(cudaMemcpyAsync(c->d_imp_US, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    PG_CUDA(cudaMemcpyAsync(c->d_imp_V, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    c->imp_k = (int)k;
+    c->imputed_compat = reference_index != 0;
+    compute_imputed_snp(c);
+    c->miss_ws_val_valid = false;
+    if (c->miss_ws_valid) compute_imputed_ws(c);
+    c->imputed = true;
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_clear_imputed(pcaone_ctx* c) {
+  return guarded(c, [&] { c->imputed = false; });
 }
 
 }  // extern "C"

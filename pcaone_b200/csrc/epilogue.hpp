@@ -8,8 +8,9 @@ namespace pg {
 struct EpiP1 {          // after the Z^T Omega product of one window
   int64_t start = 0;    // first SNP of the window (current SNP order)
   int64_t m = 0;        // SNPs in the window
-  int l = 0, ksplit = 1, standardize = 1, ploidy = 2;
-  const double* F = nullptr;         // M
+  int l = 0, ksplit = 1;
+  const double* F = nullptr;         // M, centring frequencies
+  const double* scale = nullptr;     // M, per-SNP scale s_j
   const double* wsum = nullptr;      // l: column sums of Omega
   const double* omega = nullptr;     // Npad x l
   const int64_t* miss_ptr = nullptr; // by-SNP CSR
@@ -21,8 +22,9 @@ struct EpiP1 {          // after the Z^T Omega product of one window
 struct EpiP2 {          // after the Z * G product of one window
   int window = 0;
   int64_t n = 0, npad = 0;
-  int l = 0, ksplit = 1, standardize = 1, ploidy = 2;
+  int l = 0, ksplit = 1;
   const double* F = nullptr;
+  const double* scale = nullptr;
   const double* G = nullptr;         // M x l
   const double* h0 = nullptr;        // l
   const int64_t* miss_ptr = nullptr; // by (window, sample) CSR

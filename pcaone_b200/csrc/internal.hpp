@@ -80,6 +80,8 @@ struct pcaone_ctx {
   uint32_t* d_a1x2 = nullptr;
   uint32_t* d_nonmiss = nullptr;
   double* d_F = nullptr;
+  double* d_F_load = nullptr;  // F in the SNP order of load time (before any permutation)
+  double* d_scale = nullptr;   // per-SNP multiplier of the centred genotypes (current order)
 
   // transposed copy for the current window layout
   pg::WindowLayout win;
@@ -93,6 +95,21 @@ struct pcaone_ctx {
   int64_t* d_miss_ws_ptr = nullptr;    // bands * N + 1
   int32_t* d_miss_ws_idx = nullptr;    // SNP index (global, current order) per entry
   bool miss_snp_valid = false, miss_ws_valid = false;
+
+  // EM imputation (EMU): centred values e_ij of the missing entries, aligned with the two
+  // lists, computed from factors U diag(S) V^T kept on the device
+  bool imputed = false;        // use e_ij instead of 0 for missing entries
+  bool imputed_compat = true;  // reference index semantics for F after the permutation
+  int imp_k = 0;
+  double* d_imp_US = nullptr;  // N x k (U diag S)
+  double* d_imp_V = nullptr;   // M x k (current SNP order)
+  double* d_miss_snp_val = nullptr;
+  double* d_miss_ws_val = nullptr;
+  bool miss_ws_val_valid = false;
+
+  // key (N, l, bands, data generation) of the winSVD window sums kept between calls
+  uint64_t h12_key = 0;
+  uint64_t generation = 0;  // bumped by every load / permutation
 
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;
@@ -115,6 +132,13 @@ void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out);
 void build_transposed(pcaone_ctx* c, int bands);
 void build_missing_by_snp(pcaone_ctx* c);
 void build_missing_by_window_sample(pcaone_ctx* c);
+// e_ij = clip(sum_k US_ik V_jk, -Fc_j, 1 - Fc_j) for every entry of the by-SNP list (and of
+// the (window, sample) list when it exists); Fc = F at load time under reference index
+// semantics, else the current F (Data::fit_with_pi EMU branch, src/Data.cpp:272-287).
+void compute_imputed_snp(pcaone_ctx* c);
+void compute_imputed_ws(pcaone_ctx* c);
+// d_scale_j = 1/sqrt(ploidy Fs_j (1 - Fs_j)) (or 1 when not standardising / sd <= 1e-9).
+void compute_scale(pcaone_ctx* c, int standardize, int ploidy);
 
 // ---------------------------------------------------------------- SIMT decode-GEMM
 // out[s][r][c] = sum_{k in split s} val(code[r][k]) * B[k][c], val(00,01,10,11) = (2,0,1,0)

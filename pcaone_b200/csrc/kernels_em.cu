@@ -1,0 +1,100 @@
+// EM support kernels: the per-SNP standardisation scale and the EMU imputation of missing
+// entries (Data::fit_with_pi EMU branch, src/Data.cpp:272-287; Data::standardize_E,
+// src/Data.cpp:290-299).
+//
+// Reference index semantics: after the in-core SNP shuffle the reference keeps F in the
+// original SNP order while G's columns are permuted, so the EMU clip bounds and the
+// standardisation of the final EMU run read F at the permuted column's position
+// (F_load[j] for SNP j of the current order) rather than that SNP's own frequency. With
+// imputed_compat the same arrays are used here; without it the SNP's own F is used.
+#include "internal.hpp"
+
+namespace pg {
+
+namespace {
+
+__global__ void k_scale(const double* __restrict__ F, uint64_t M, int standardize, int ploidy,
+                        double* __restrict__ scale) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= M) return;
+  double s = 1.0;
+  if (standardize) {
+    double sd = sqrt((double)ploidy * F[j] * (1.0 - F[j]));
+    if (sd > 1e-9) s = 1.0 / sd;
+  }
+  scale[j] = s;
+}
+
+__device__ __forceinline__ double imputed_value(const double* __restrict__ US, const double* __restrict__ V,
+                                                int k, int64_t i, int64_t j, double Fc) {
+  double g = 0.0;
+  for (int t = 0; t < k; ++t) g += US[i * k + t] * V[j * k + t];  // sum_k U S V^T
+  return fmin(fmax(g, -Fc), 1.0 - Fc);
+}
+
+// by-SNP list: thread per entry, SNP found by the row of a grid-stride over rows (warp/row)
+__global__ void k_impute_snp(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, uint64_t M,
+                             const double* __restrict__ US, const double* __restrict__ V, int k,
+                             const double* __restrict__ Fc, double* __restrict__ val) {
+  uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (j >= M) return;
+  for (int64_t e = ptr[j] + lane; e < ptr[j + 1]; e += 32)
+    val[e] = imputed_value(US, V, k, idx[e], (int64_t)j, Fc[j]);
+}
+
+// (window, sample) list: row r = b * Npad + i holds the SNPs of window b missing in sample i
+__global__ void k_impute_ws(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, uint64_t rows,
+                            uint32_t npad, const double* __restrict__ US, const double* __restrict__ V,
+                            int k, const double* __restrict__ Fc, double* __restrict__ val) {
+  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  const int64_t i = (int64_t)(r % npad);
+  for (int64_t e = ptr[r] + lane; e < ptr[r + 1]; e += 32) {
+    const int64_t j = idx[e];
+    val[e] = imputed_value(US, V, k, i, j, Fc[j]);
+  }
+}
+
+}  // namespace
+
+void compute_scale(pcaone_ctx* c, int standardize, int ploidy) {
+  const double* Fs = (c->imputed && c->imputed_compat) ? c->d_F_load : c->d_F;
+  k_scale<<<(unsigned)((c->M + 255) / 256), 256, 0, c->stream>>>(Fs, c->M, standardize, ploidy, c->d_scale);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+static const double* clip_freq(pcaone_ctx* c) { return c->imputed_compat ? c->d_F_load : c->d_F; }
+
+void compute_imputed_snp(pcaone_ctx* c) {
+  PG_REQUIRE(c->miss_snp_valid, PCAONE_ESTATE, "missing-entry list not built");
+  if (c->d_miss_snp_val) cudaFree(c->d_miss_snp_val);
+  c->d_miss_snp_val = nullptr;
+  PG_CUDA(cudaMalloc(&c->d_miss_snp_val, std::max<int64_t>(c->n_missing, 1) * 8));
+  uint64_t threads = c->M * 32;
+  k_impute_snp<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+      c->d_miss_snp_ptr, c->d_miss_snp_idx, c->M, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
+      c->d_miss_snp_val);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void compute_imputed_ws(pcaone_ctx* c) {
+  if (c->miss_ws_val_valid) return;
+  PG_REQUIRE(c->miss_ws_valid, PCAONE_ESTATE, "missing-entry list not built");
+  if (c->d_miss_ws_val) cudaFree(c->d_miss_ws_val);
+  c->d_miss_ws_val = nullptr;
+  PG_CUDA(cudaMalloc(&c->d_miss_ws_val, std::max<int64_t>(c->n_missing, 1) * 8));
+  const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
+  uint64_t threads = rows * 32;
+  k_impute_ws<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+      c->d_miss_ws_ptr, c->d_miss_ws_idx, rows, c->Npad, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
+      c->d_miss_ws_val);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+  c->miss_ws_val_valid = true;
+}
+
+}  // namespace pg

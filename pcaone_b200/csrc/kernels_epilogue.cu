@@ -19,12 +19,6 @@ namespace pg {
 
 namespace {
 
-__device__ __forceinline__ double snp_scale(double F, int standardize, int ploidy) {
-  if (!standardize) return 1.0;
-  double sd = sqrt((double)ploidy * F * (1.0 - F));
-  return sd > 1e-9 ? 1.0 / sd : 1.0;
-}
-
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
 // per-CTA partials of h0.
 template <typename T>
@@ -36,7 +30,7 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
   for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < p.m; jl += (int64_t)gridDim.x * nwarps) {
     const int64_t j = p.start + jl;
     const double F = p.F[j];
-    const double s = snp_scale(F, p.standardize, p.ploidy);
+    const double s = p.scale[j];
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
@@ -62,7 +56,7 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
 
 // B2_j = s_j/2 G_j and per-CTA partials of h0 = sum_j s_j F_j G_j, for a given G.
 template <typename T>
-__global__ void k_scale_g(int64_t start, int64_t m, int l, int standardize, int ploidy,
+__global__ void k_scale_g(int64_t start, int64_t m, int l, const double* __restrict__ scale,
                           const double* __restrict__ F, const double* __restrict__ G,
                           T* __restrict__ B2, double* __restrict__ h0_part) {
   extern __shared__ double sh0[];
@@ -70,7 +64,7 @@ __global__ void k_scale_g(int64_t start, int64_t m, int l, int standardize, int 
   for (int c = lane; c < l; c += 32) sh0[warp * l + c] = 0.0;
   for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < m; jl += (int64_t)gridDim.x * nwarps) {
     const int64_t j = start + jl;
-    const double f = F[j], s = snp_scale(f, standardize, ploidy);
+    const double f = F[j], s = scale[j];
     for (int c = lane; c < l; c += 32) {
       const double g = G[j * l + c];
       B2[jl * l + c] = (T)(0.5 * s * g);
@@ -106,10 +100,8 @@ __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
       double sparse = 0.0;
       for (int64_t e = e0; e < e1; ++e) {
         int64_t j = p.miss_idx[e];
-        double F = p.F[j];
-        double s = snp_scale(F, p.standardize, p.ploidy);
         double ev = p.miss_val ? p.miss_val[e] : 0.0;
-        sparse += s * (ev + F) * p.G[j * p.l + c];
+        sparse += p.scale[j] * (ev + p.F[j]) * p.G[j * p.l + c];
       }
       p.H[i * p.l + c] += d - p.h0[c] + sparse;
     }
@@ -144,8 +136,8 @@ void launch_scale_g(pcaone_ctx* c, const EpiP1& p, T* B2, double* h0) {
   const int threads = 256, nwarps = threads / 32;
   int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
   double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
-  k_scale_g<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p.start, p.m, p.l, p.standardize,
-                                                                       p.ploidy, p.F, p.G, B2, part);
+  k_scale_g<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p.start, p.m, p.l, p.scale,
+                                                                       p.F, p.G, B2, part);
   PG_CHECK_LAUNCH();
   k_reduce_cols<<<1, 128, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();

@@ -172,14 +172,13 @@ struct Engine {
     p1.m = m;
     p1.l = l;
     p1.ksplit = ks1;
-    p1.standardize = o.standardize;
-    p1.ploidy = o.ploidy;
     p1.F = c->d_F;
+    p1.scale = c->d_scale;
     p1.wsum = wsum;
     p1.omega = Omg;
     p1.miss_ptr = c->d_miss_snp_ptr;
     p1.miss_idx = c->d_miss_snp_idx;
-    p1.miss_val = nullptr;
+    p1.miss_val = c->imputed ? c->d_miss_snp_val : nullptr;
     p1.G = G;
     T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
     double* h0 = (double*)scratch(c, "r_h0", l * 8);
@@ -196,14 +195,13 @@ struct Engine {
     p2.npad = Npad;
     p2.l = l;
     p2.ksplit = ks2;
-    p2.standardize = o.standardize;
-    p2.ploidy = o.ploidy;
     p2.F = c->d_F;
+    p2.scale = c->d_scale;
     p2.G = G;
     p2.h0 = h0;
     p2.miss_ptr = c->d_miss_ws_ptr;
     p2.miss_idx = c->d_miss_ws_idx;
-    p2.miss_val = nullptr;
+    p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
     p2.H = Ht;
     launch_accum<T>(c, p2, D2);
   }
@@ -296,10 +294,15 @@ struct Engine {
   }
 
   void run(double* U, double* S, double* V, pcaone_rsvd_report* rep) {
-    // zero the FP64 work buffers once so padded rows stay zero
+    // zero the FP64 work buffers once so padded rows stay zero; the winSVD window sums are
+    // kept from the previous call when asked to and still valid for this shape and data
+    const uint64_t key = ((uint64_t)N * 131 + (uint64_t)l) * 1031 + (uint64_t)o.bands + (c->generation << 40);
     zero(c, H, Npad * l);
-    zero(c, H1, Npad * l);
-    zero(c, H2, Npad * l);
+    if (!(o.svd == 2 && o.carry_window_state && c->h12_key == key)) {
+      zero(c, H1, Npad * l);
+      zero(c, H2, Npad * l);
+    }
+    c->h12_key = o.svd == 2 ? key : 0;
     zero(c, Tb, Npad * l);
     zero(c, Ucur, Npad * k);
     zero(c, Upre, Npad * k);
@@ -411,9 +414,9 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks * M * l * sizeof(T));
     gemm.p1(c, c->d_bed, c->pitch, M, N, BT, l, ks, D1);
     EpiP1 p1;
-    p1.start = 0; p1.m = M; p1.l = l; p1.ksplit = ks; p1.standardize = standardize; p1.ploidy = ploidy;
-    p1.F = c->d_F; p1.wsum = wsum; p1.omega = Bd; p1.miss_ptr = c->d_miss_snp_ptr;
-    p1.miss_idx = c->d_miss_snp_idx; p1.G = G;
+    p1.start = 0; p1.m = M; p1.l = l; p1.ksplit = ks;
+    p1.F = c->d_F; p1.scale = c->d_scale; p1.wsum = wsum; p1.omega = Bd; p1.miss_ptr = c->d_miss_snp_ptr;
+    p1.miss_idx = c->d_miss_snp_idx; p1.miss_val = c->imputed ? c->d_miss_snp_val : nullptr; p1.G = G;
     launch_prep<T>(c, p1, D1, B2, h0);
     rm.resize((size_t)M * l);
     PG_CUDA(cudaMemcpyAsync(rm.data(), G, rm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -426,8 +429,8 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
       for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = B[(size_t)j * M + i];
     PG_CUDA(cudaMemcpyAsync(G, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
     EpiP1 p1;
-    p1.start = 0; p1.m = M; p1.l = l; p1.standardize = standardize; p1.ploidy = ploidy;
-    p1.F = c->d_F; p1.G = G;
+    p1.start = 0; p1.m = M; p1.l = l;
+    p1.F = c->d_F; p1.scale = c->d_scale; p1.G = G;
     launch_scale_g<T>(c, p1, B2, h0);
     gemm.b2_ready(c, B2, l, M);
     const int ks = gemm.ksplit(c, N, M);
@@ -435,9 +438,9 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     gemm.p2(c, c->d_bedT, c->win.pitch, N, M, B2, l, ks, D2);
     zero(c, H, Npad * l);
     EpiP2 p2;
-    p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks; p2.standardize = standardize;
-    p2.ploidy = ploidy; p2.F = c->d_F; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
-    p2.miss_idx = c->d_miss_ws_idx; p2.H = H;
+    p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks;
+    p2.F = c->d_F; p2.scale = c->d_scale; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
+    p2.miss_idx = c->d_miss_ws_idx; p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr; p2.H = H;
     launch_accum<T>(c, p2, D2);
     rm.resize((size_t)N * l);
     PG_CUDA(cudaMemcpyAsync(rm.data(), H, rm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -452,9 +455,12 @@ void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, i
   PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
   PG_REQUIRE(B && out && l >= 1 && l <= kLmax, PCAONE_EBADARG, "bad product operands");
   PG_REQUIRE(transpose == 0 || transpose == 1, PCAONE_EBADARG, "transpose must be 0 or 1");
+  PG_REQUIRE(ploidy == 1 || ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
   build_transposed(c, 1);
   build_missing_by_snp(c);
   build_missing_by_window_sample(c);
+  if (c->imputed) compute_imputed_ws(c);
+  compute_scale(c, standardize, ploidy);
   if (precision == PCAONE_PREC_FP64) {
     product_t<double>(c, gemm_simt_double(), transpose, standardize, ploidy, B, l, out);
   } else if (precision == PCAONE_PREC_FP32) {
@@ -485,6 +491,8 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
   build_transposed(c, bands);
   build_missing_by_snp(c);
   build_missing_by_window_sample(c);
+  if (c->imputed) compute_imputed_ws(c);
+  compute_scale(c, o.standardize, o.ploidy);
   c->gemm_ms_accum = 0.0;
   const int64_t l0 = c->launches, g0 = c->gemm_launches;
   PG_CUDA(cudaEventRecord(c->ev0, c->stream));

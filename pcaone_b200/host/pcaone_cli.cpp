@@ -1,0 +1,420 @@
+// PCAone command-line front end for the B200 implementation: the same flags and output
+// files as the reference CLI (src/Cmd.cpp:28-111, src/Main.cpp:44-165) for the modes this
+// build covers, with all compute going through the C ABI in include/pcaone_gpu.h.
+//
+// Covered: PLINK input (-b) with --svd 1 (Halko) and --svd 2 (winSVD, in-core shuffle unless
+// -S), -k, -p, -w/--batches/--windows, --oversamples, --seed, --rand, --tol-rsvd, --maf,
+// -C/--scale 0 (no standardisation), --haploid, -V, -o, -v; outputs .sigvals .eigvals
+// .eigvecs [.loadings .mbim] .eigvecs2 and .log. Options of the reference that belong to
+// modes outside this build are recognised and rejected with a clear message and exit 1.
+#include <sys/utsname.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/pcaone_gpu.h"
+
+namespace {
+
+// ------------------------------------------------------------------ logging (src/Logger.hpp)
+struct Log {
+  std::ofstream file;
+  bool screen = true;
+  template <typename... A>
+  void print(const A&... a) {
+    std::ostringstream s;
+    s.precision(6);
+    s.setf(std::ios::fixed, std::ios::floatfield);
+    (..., (s << a << " "));
+    std::string line = s.str();
+    if (!line.empty()) line.pop_back();
+    if (file.is_open()) file << line << "\n" << std::flush;
+    if (screen) std::cout << line << std::endl;
+  }
+};
+Log g_log;
+
+std::string date() {
+  auto now = std::chrono::system_clock::now();
+  auto t = std::chrono::system_clock::to_time_t(now);
+  std::stringstream ss;
+  ss << std::put_time(std::localtime(&t), "[%d/%m/%Y-%X]");
+  return ss.str();
+}
+
+[[noreturn]] void fail(const std::string& msg) {
+  if (g_log.file.is_open()) g_log.file << "error: " << msg << "\n";
+  std::cerr << "error: " << msg << "\n";
+  std::exit(EXIT_FAILURE);
+}
+
+// ------------------------------------------------------------------ options (src/Cmd.cpp)
+struct Params {
+  std::string bfile, fileout = "pcaone";
+  int svd = 2;
+  unsigned k = 10, maxp = 20, bands = 64, oversamples = 10, rand = 1, verbose = 1, threads = 12;
+  int seed = 101, scale = -1;
+  bool noshuffle = false, printv = false, haploid = false, emu = false;
+  double tol = 1e-4, maf = 0.0, memory = 0.0, tolem = 1e-5;
+  unsigned maxiter = 100;
+  bool fix_index = false;
+  int precision = PCAONE_PREC_MIXED;
+  int device = 0;
+  std::string cmdline;
+};
+
+const std::set<std::string> kUnsupported = {
+    "-c", "--csv", "-g", "--bgen", "-G", "--beagle", "-B", "--binary", "--pcangsd",
+    "-D", "--ld", "-R", "--print-r2", "--ld-bp", "--ld-r2", "--ld-stats", "--clump",
+    "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
+    "--inbreed", "--USV", "--read-U", "--read-V", "--read-S", "-f", "--match-bim", "--M", "--N",
+    "--scale-factor", "--buffer", "--imaxiter", "--itol", "--ncv", "--tol-maf"};
+
+void usage() {
+  std::cout << "PCAone (B200 build)\n"
+               "Usage: PCAone -b plink [-k 10] [-d 2] [-w 64] [-p 20] [-o pcaone] [-V] [-S]\n"
+               "  -b, --bfile      prefix of PLINK .bed/.bim/.fam files\n"
+               "  -k, --pc         top k principal components [10]\n"
+               "  -d, --svd        1: single-pass RSVD (Halko), 2: window-based RSVD [2]\n"
+               "  -p, --maxp       maximum number of power iterations [20]\n"
+               "  -w, --batches    number of windows for --svd 2 (alias --windows) [64]\n"
+               "  -S, --no-shuffle do not shuffle SNPs for --svd 2\n"
+               "      --oversamples, --seed, --rand, --tol-rsvd, --maf, --haploid\n"
+               "      --emu        EMU imputation of missing genotypes (--maxiter, --tol-em)\n"
+               "      --fix-perm-index  EM steps read each SNP's own F after the shuffle\n"
+               "  -C, --scale      0: centre only, 1: standardise (default for PLINK)\n"
+               "  -V, --printv     write .loadings and .mbim\n"
+               "  -o, --out        output prefix [pcaone]\n"
+               "  -v, --verbose    0 silent, 1 screen\n"
+               "      --precision  mixed (BF16 tensor cores, default), fp32 or fp64\n"
+               "      --device     CUDA device index [0]\n";
+}
+
+Params parse(int argc, char** argv) {
+  Params p;
+  for (int i = 0; i < argc; ++i) p.cmdline += std::string(argv[i]) + " ";
+  if (argc == 1) {
+    usage();
+    std::exit(EXIT_SUCCESS);
+  }
+  for (int i = 1; i < argc; ++i) {
+    std::string a = argv[i], val;
+    auto eq = a.find('=');
+    bool has_eq = a.rfind("--", 0) == 0 && eq != std::string::npos;
+    if (has_eq) {
+      val = a.substr(eq + 1);
+      a = a.substr(0, eq);
+    }
+    auto next = [&]() -> std::string {
+      if (has_eq) return val;
+      if (i + 1 >= argc) {
+        std::cerr << "Invalid Option Exception: missing_argument\noption: " << a << "\n";
+        std::exit(EXIT_FAILURE);
+      }
+      return argv[++i];
+    };
+    auto num = [&](const std::string& s) -> double {
+      char* end = nullptr;
+      double v = std::strtod(s.c_str(), &end);
+      if (!end || *end) {
+        std::cerr << "Invalid Option Exception: invalid_argument\noption: " << a << "\nvalue:  " << s << "\n";
+        std::exit(EXIT_FAILURE);
+      }
+      return v;
+    };
+    if (a == "-h" || a == "--help") {
+      usage();
+      std::exit(EXIT_SUCCESS);
+    } else if (a == "-b" || a == "--bfile") p.bfile = next();
+    else if (a == "-o" || a == "--out") p.fileout = next();
+    else if (a == "-k" || a == "--pc") p.k = (unsigned)num(next());
+    else if (a == "-d" || a == "--svd") p.svd = (int)num(next());
+    else if (a == "-p" || a == "--maxp") p.maxp = (unsigned)num(next());
+    else if (a == "-w" || a == "--batches" || a == "--windows") p.bands = (unsigned)num(next());
+    else if (a == "-S" || a == "--no-shuffle") p.noshuffle = true;
+    else if (a == "--seed") p.seed = (int)num(next());
+    else if (a == "--oversamples") p.oversamples = (unsigned)num(next());
+    else if (a == "--rand") p.rand = (unsigned)num(next());
+    else if (a == "--tol-rsvd") p.tol = num(next());
+    else if (a == "--maf") p.maf = num(next());
+    else if (a == "-C" || a == "--scale") p.scale = (int)num(next());
+    else if (a == "--haploid") p.haploid = true;
+    else if (a == "--emu") p.emu = true;
+    else if (a == "--maxiter") p.maxiter = (unsigned)num(next());
+    else if (a == "--tol-em") p.tolem = num(next());
+    else if (a == "--fix-perm-index") p.fix_index = true;
+    else if (a == "-V" || a == "--printv") p.printv = true;
+    else if (a == "-v" || a == "--verbose") p.verbose = (unsigned)num(next());
+    else if (a == "-n" || a == "--threads") p.threads = (unsigned)num(next());
+    else if (a == "-m" || a == "--memory") p.memory = num(next());
+    else if (a == "--device") p.device = (int)num(next());
+    else if (a == "--precision") {
+      std::string v = next();
+      if (v == "mixed" || v == "bf16") p.precision = PCAONE_PREC_MIXED;
+      else if (v == "fp32") p.precision = PCAONE_PREC_FP32;
+      else if (v == "fp64") p.precision = PCAONE_PREC_FP64;
+      else fail("--precision must be mixed, fp32 or fp64");
+    } else if (kUnsupported.count(a)) {
+      fail("option " + a + " belongs to a mode this build does not provide");
+    } else {
+      std::cerr << "unknown option: " << a << "\n";  // src/Cmd.cpp:125-128
+      std::exit(EXIT_FAILURE);
+    }
+  }
+  if (p.bfile.empty()) fail("no input: use -b/--bfile");
+  if (p.svd != 1 && p.svd != 2) fail("--svd must be 1 or 2 in this build");
+  if (p.bands < 4 || p.bands % 2 != 0) fail("the -w/--batches must be a power of 2 and the minimun is 4.");
+  if (p.maf > 0.5) {
+    std::cerr << "warning: '--maf' with a value greater than 0.5 will be converted to 1 - maf.\n";
+    p.maf = 1 - p.maf;
+  }
+  p.oversamples = std::max(p.oversamples, p.k);  // src/Cmd.cpp:190
+  if (p.memory > 0) fail("-m/--memory (out-of-core mode) is not provided by this build: inputs are kept in HBM");
+  return p;
+}
+
+size_t count_lines(const std::string& path) {
+  std::ifstream f(path);
+  if (!f.is_open()) fail("can not open " + path);
+  size_t n = 0;
+  std::string line;
+  while (std::getline(f, line)) ++n;
+  return n;
+}
+
+void check(pcaone_ctx* ctx, int st, const char* what) {
+  if (st != PCAONE_OK) fail(std::string(what) + ": " + pcaone_gpu_last_error(ctx));
+}
+
+// Eigen::IOFormat(6, DontAlignCols, "\t", "\n") of a column-major matrix (src/Data.cpp:181).
+void write_matrix(std::ostream& o, const double* a, size_t rows, size_t cols) {
+  std::ostringstream s;
+  s.precision(6);
+  for (size_t i = 0; i < rows; ++i) {
+    for (size_t j = 0; j < cols; ++j) {
+      if (j) s << '\t';
+      s << a[j * rows + i];
+    }
+    if (i + 1 < rows) s << '\n';
+  }
+  o << s.str();
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Params p = parse(argc, argv);
+  auto t_start = std::chrono::steady_clock::now();
+  g_log.file.open(p.fileout + ".log");
+  g_log.screen = p.verbose > 0;
+  {
+    struct utsname u;
+    uname(&u);
+    g_log.print(std::string("Machine name: ") + u.machine + "\nNode name: " + u.nodename +
+                "\nOperating system release: " + u.release + "\n");
+    g_log.print("PCAone (B200 build)\nOptions in effect:\n" + p.cmdline);
+  }
+  g_log.print(date(), "program started");
+  g_log.print(date(), "start parsing PLINK format");
+  const size_t N = count_lines(p.bfile + ".fam"), M0 = count_lines(p.bfile + ".bim");
+  g_log.print(date(), "N (# samples):", N, ", M (# SNPs):", M0);
+  const size_t bpr = (N + 3) >> 2;
+  std::vector<uint8_t> packed;
+  {
+    std::ifstream f(p.bfile + ".bed", std::ios::binary);
+    if (!f.is_open()) fail("Cannot open bed file.");
+    unsigned char h[3] = {0, 0, 0};
+    f.read((char*)h, 3);
+    if (h[0] != 0x6c || h[1] != 0x1b || h[2] != 0x01) fail("Incorrect magic number in plink bed file.");
+    packed.resize(bpr * M0);
+    f.read((char*)packed.data(), (std::streamsize)packed.size());
+    if ((size_t)f.gcount() != packed.size()) fail("the .bed file is shorter than the .bim/.fam imply");
+  }
+  if (p.k + p.oversamples > N) fail("k + oversamples must not exceed the number of samples");
+
+  pcaone_ctx* ctx = nullptr;
+  if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
+  check(ctx, pcaone_gpu_load_bed(ctx, packed.data(), M0, (uint32_t)N), "load_bed");
+  std::vector<double> F(M0);
+  check(ctx, pcaone_gpu_allele_freq(ctx, F.data()), "allele_freq");
+  for (size_t j = 0; j < M0; ++j)
+    if (F[j] == 0.0 || F[j] == 1.0) {
+      std::cout << "\x1B[33m" << "sites with MAF=0 found! remove them first!" << "\033[0m\n";
+      break;
+    }
+  // --maf filter (src/Data.cpp:74-91): keep SNPs with MAF > maf, re-upload the kept records
+  std::vector<int> keep;
+  size_t M = M0;
+  if (p.maf > 0) {
+    for (size_t j = 0; j < M0; ++j) {
+      double maf = F[j] > 0.5 ? 1 - F[j] : F[j];
+      if (maf > p.maf) keep.push_back((int)j);
+    }
+    M = keep.size();
+    g_log.print(date(), "number of SNPs after filtering by MAF >", p.maf, ":", M);
+    if (M < 1) fail("no SNPs left after filtering!");
+    std::vector<uint8_t> kept(bpr * M);
+    std::vector<double> Fk(M);
+    for (size_t i = 0; i < M; ++i) {
+      std::memcpy(&kept[i * bpr], &packed[(size_t)keep[i] * bpr], bpr);
+      Fk[i] = F[keep[i]];
+    }
+    packed.swap(kept);
+    F.swap(Fk);
+    check(ctx, pcaone_gpu_load_bed(ctx, packed.data(), M, (uint32_t)N), "load_bed");
+  }
+  g_log.print(date(), "done reading all data");
+
+  const bool perm_on = p.svd == 2 && !p.noshuffle;  // src/Cmd.cpp:216
+  std::vector<int32_t> perm;
+  if (perm_on) {
+    perm.resize(M);
+    pcaone_shuffle_perm(M, perm.data());
+    g_log.print(date(), "permuting data matrix by columns in place");
+    check(ctx, pcaone_gpu_permute(ctx, perm.data()), "permute");
+  }
+  g_log.print(date(), p.svd == 2 ? "initialize window-based RSVD (winSVD) with in-core"
+                                 : "initialize single-pass RSVD (sSVD) with in-core");
+  pcaone_rsvd_opts o{};
+  o.k = (int)p.k;
+  o.oversamples = (int)p.oversamples;
+  o.maxp = (int)p.maxp;
+  o.svd = p.svd;
+  o.bands = (int)p.bands;
+  o.precision = p.precision;
+  o.standardize = p.scale == 0 ? 0 : 1;
+  o.ploidy = p.haploid ? 1 : 2;
+  o.seed = p.seed;
+  o.rand = (int)p.rand;
+  o.tol = p.tol;
+  o.verbose = p.verbose > 0;
+  std::vector<double> U(N * p.k), S(p.k), V(M * p.k);
+  pcaone_rsvd_report rep{};
+  double gpu_s = 0;
+  if (!p.emu) {
+    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+    gpu_s += rep.gpu_ms / 1e3;
+    g_log.print(date(), "stops at epoch =", rep.epochs);
+  } else {
+    // run_pca_with_halko impute branch with --emu (src/Halko.cpp:294-336)
+    o.standardize = 0;
+    o.carry_window_state = 0;
+    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+    gpu_s += rep.gpu_ms / 1e3;
+    g_log.print(date(), "run EM-PCA. maxiter =", p.maxiter);
+    o.carry_window_state = 1;
+    const int compat = p.fix_index ? 0 : 1;
+    std::vector<double> Vpre;
+    for (unsigned it = 0; it < p.maxiter; ++it) {
+      Vpre = V;
+      check(ctx, pcaone_gpu_fit_emu(ctx, U.data(), S.data(), V.data(), p.k, compat), "fit_emu");
+      check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+      gpu_s += rep.gpu_ms / 1e3;
+      double acc = 0;  // 1 - mev(V, Vpre) (src/Utils.cpp:192-198)
+      for (unsigned b = 0; b < p.k; ++b) {
+        double nrm = 0;
+        for (unsigned a = 0; a < p.k; ++a) {
+          double d = 0;
+          for (size_t j = 0; j < M; ++j) d += V[a * M + j] * Vpre[b * M + j];
+          nrm += d * d;
+        }
+        acc += std::sqrt(nrm);
+      }
+      const double diff = 1.0 - acc / p.k;
+      g_log.print(date(), "individual allele frequencies estimated iter =", it + 1, ", diff =", diff);
+      if (diff < p.tolem) {
+        g_log.print(date(), "come to convergence!");
+        break;
+      }
+    }
+    g_log.print(date(), "standardize the final matrix for EMU");
+    check(ctx, pcaone_gpu_fit_emu(ctx, U.data(), S.data(), V.data(), p.k, compat), "fit_emu");
+    o.standardize = p.scale == 0 ? 0 : 1;
+    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+    gpu_s += rep.gpu_ms / 1e3;
+  }
+  g_log.print(date(), "PCAone - Randomized SVD done; GPU time", gpu_s, "seconds");
+  pcaone_gpu_destroy(ctx);
+
+  // loadings back to the input SNP order (data->perm * V, src/Halko.cpp:340)
+  if (perm_on) {
+    std::vector<double> Vo(V.size());
+    for (size_t j = 0; j < M; ++j)
+      for (unsigned c = 0; c < p.k; ++c) Vo[c * M + perm[j]] = V[c * M + j];
+    V.swap(Vo);
+  }
+  // outputs (src/Data.cpp:177-194)
+  {
+    std::ofstream outs(p.fileout + ".sigvals"), oute(p.fileout + ".eigvals"), outu(p.fileout + ".eigvecs");
+    outs << '#' << N << ',' << M << '\n';
+    write_matrix(outs, S.data(), p.k, 1);
+    outs << '\n';
+    std::vector<double> E(p.k);
+    const int ploidy = p.haploid ? 1 : 2;
+    for (unsigned c = 0; c < p.k; ++c) E[c] = S[c] * S[c] / (double)M * ploidy;
+    write_matrix(oute, E.data(), p.k, 1);
+    oute << '\n';
+    write_matrix(outu, U.data(), N, p.k);
+    outu << '\n';
+  }
+  if (p.printv) {
+    // .mbim: .bim line + tab + F (src/Data.cpp:96-136)
+    g_log.print(date(), "save matched sites in .mbim file and permutation mode is", perm_on ? 1 : 0);
+    std::ifstream ib(p.bfile + ".bim");
+    std::ofstream ob(p.fileout + ".mbim");
+    std::string line;
+    size_t j = 0, i = 0;
+    while (std::getline(ib, line)) {
+      if (!keep.empty()) {
+        if (i < keep.size() && keep[i] == (int)j) {
+          ob << line << "\t" << F[i] << "\n";
+          ++i;
+        }
+      } else {
+        ob << line << "\t" << F[j] << "\n";
+      }
+      ++j;
+    }
+    std::ofstream ov(p.fileout + ".loadings");
+    write_matrix(ov, V.data(), M, p.k);
+    ov << '\n';
+  }
+  g_log.print(date(), "eigen vectors and values saved");
+  {
+    // .eigvecs2 (src/Utils.cpp:223-236)
+    std::ifstream ifam(p.bfile + ".fam"), iev(p.fileout + ".eigvecs");
+    std::ofstream o2(p.fileout + ".eigvecs2");
+    o2 << "#FID\tIID";
+    for (unsigned c = 0; c < p.k; ++c) o2 << "\tPC" << c + 1;
+    o2 << "\n";
+    std::string l1, l2;
+    while (std::getline(ifam, l1)) {
+      std::vector<std::string> tok;
+      size_t b = 0;
+      for (size_t q = 0; q <= l1.size(); ++q)
+        if (q == l1.size() || l1[q] == ' ' || l1[q] == '\t') {
+          tok.push_back(l1.substr(b, q - b));
+          b = q + 1;
+        }
+      std::getline(iev, l2);
+      o2 << tok[0] + "\t" + (tok.size() > 1 ? tok[1] : "") + "\t" << l2 << std::endl;
+    }
+  }
+  double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  g_log.print(date(), "total elapsed wall time:", wall, " seconds");
+  g_log.print(date(), "have a nice day. bye!");
+  return 0;
+}

@@ -1,0 +1,99 @@
+"""The PCAone drop-in CLI (pcaone_b200/bin/PCAone) against the reference's own output files
+for the same flags (golden fixtures), plus its input-error behaviour."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import pcaone_oracle as O
+from tests.helpers import GOLDEN, assert_cols_close, assert_eig_close, case, ref_out, ref_table
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "pcaone_b200", "bin", "PCAone")
+
+
+def run_cli(args, tmp_path, check=True):
+    out = subprocess.run([CLI] + args + ["-v", "0"], capture_output=True, text=True, cwd=tmp_path)
+    if check:
+        assert out.returncode == 0, out.stdout + out.stderr
+    return out
+
+
+def golden_args(name, tmp_path):
+    c = case(name)
+    args = [a.format(d=os.path.join(GOLDEN, c["dataset"]), g=GOLDEN) for a in c["args"]]
+    return args + ["-o", str(tmp_path / name)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+@pytest.mark.parametrize("name", ["g1_halko", "g1_win", "g1_winS", "g1_nostd", "g1_win_unif"])
+def test_cli_matches_reference_outputs(tmp_path, prec, name):
+    run_cli(golden_args(name, tmp_path) + ["--precision", prec], tmp_path)
+    out = str(tmp_path / name)
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table(name, ".eigvals")[:, 0], 1e-5)
+    with open(out + ".sigvals") as f, open(ref_out(name, ".sigvals")) as g:
+        assert f.readline() == g.readline()  # "#N,M"
+    tol = 2e-6 if prec == "fp64" else 5e-4
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table(name, ".eigvecs"), tol)
+    if os.path.exists(ref_out(name, ".loadings")):
+        assert_cols_close(O.read_table(out + ".loadings"), ref_table(name, ".loadings"), tol)
+    if os.path.exists(ref_out(name, ".mbim")):
+        # allele frequencies are bit-exact, so the text is identical
+        assert open(out + ".mbim").read() == open(ref_out(name, ".mbim")).read()
+    lines = open(out + ".eigvecs2").read().splitlines()
+    assert lines[0].startswith("#FID\tIID\tPC1")
+    assert len(lines) == 1 + O.count_lines(os.path.join(GOLDEN, "g1.fam"))
+
+
+@pytest.mark.gpu
+def test_cli_emu_matches_reference_outputs(tmp_path):
+    run_cli(golden_args("g2_emu", tmp_path), tmp_path)
+    out = str(tmp_path / "g2_emu")
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table("g2_emu", ".eigvals")[:, 0], 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table("g2_emu", ".eigvecs"), 5e-4)
+    assert_cols_close(O.read_table(out + ".loadings"), ref_table("g2_emu", ".loadings"), 5e-4)
+
+
+@pytest.mark.gpu
+def test_cli_maf_filter(tmp_path):
+    d = os.path.join(GOLDEN, "g1")
+    run_cli(["-b", d, "-d", "1", "-k", "3", "-p", "4", "--maf", "0.2", "-V", "--precision", "fp64",
+             "-o", str(tmp_path / "maf")], tmp_path)
+    bed = O.read_bed(d)
+    F = O.allele_freq(O.decode_codes(bed))
+    maf = np.minimum(F, 1 - F)
+    keep = np.where(maf > 0.2)[0]
+    assert O.count_lines(str(tmp_path / "maf.mbim")) == len(keep)
+    sub = O.Bed(bed.N, len(keep), bed.packed[keep])
+    eig, *_ = O.run_pca(sub, k=3, svd=1, maxp=4)
+    assert_eig_close(O.read_table(str(tmp_path / "maf.eigvals"))[:, 0], eig, 1e-6)
+
+
+def test_cli_rejects_unknown_option(tmp_path):
+    out = run_cli(["-b", os.path.join(GOLDEN, "g1"), "--no-such-flag"], tmp_path, check=False)
+    assert out.returncode == 1 and "unknown option" in out.stderr
+
+
+def test_cli_rejects_out_of_scope_mode(tmp_path):
+    out = run_cli(["-b", os.path.join(GOLDEN, "g1"), "--project", "1"], tmp_path, check=False)
+    assert out.returncode == 1
+
+
+def test_cli_rejects_bad_magic_and_truncation(tmp_path):
+    for suf in (".bim", ".fam"):
+        shutil.copy(os.path.join(GOLDEN, "g1" + suf), tmp_path / ("bad" + suf))
+    raw = open(os.path.join(GOLDEN, "g1.bed"), "rb").read()
+    (tmp_path / "bad.bed").write_bytes(b"\x6c\x1b\x00" + raw[3:])
+    out = run_cli(["-b", str(tmp_path / "bad")], tmp_path, check=False)
+    assert out.returncode == 1 and "magic" in out.stderr
+    (tmp_path / "bad.bed").write_bytes(raw[: len(raw) // 2])
+    out = run_cli(["-b", str(tmp_path / "bad")], tmp_path, check=False)
+    assert out.returncode == 1 and "shorter" in out.stderr
+
+
+def test_cli_rejects_odd_windows(tmp_path):
+    out = run_cli(["-b", os.path.join(GOLDEN, "g1"), "-w", "5"], tmp_path, check=False)
+    assert out.returncode == 1

@@ -112,3 +112,28 @@ def test_rsvd_matches_oracle_larger(gpu, svd, bands):
         assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, rtol)
         assert max_angle(r.U, U_o) <= ang
         assert max_angle(V, V_o) <= ang
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_emu_matches_reference_golden(gpu, prec):
+    """EMU (--emu -k 3 -w 8 --maxiter 20 --tol-em 1e-6) against the reference's outputs."""
+    packed, N, M = pb.read_bed(os.path.join(GOLDEN, "g2"))
+    eig, S, U, V, iters = pb.run_emu(gpu, packed, N, k=3, bands=8, maxiter=20, tolem=1e-6,
+                                     precision=prec)
+    assert_eig_close(eig, ref_eigvals("g2_emu"), 1e-5)
+    tol = 2e-6 if prec == "fp64" else 5e-4
+    assert_cols_close(U, ref_table("g2_emu", ".eigvecs"), tol)
+    assert_cols_close(V, ref_table("g2_emu", ".loadings"), tol)
+
+
+def test_emu_matches_oracle_other_modes(gpu):
+    """Halko (-d 1) and unshuffled EMU, where the reference itself crashes: oracle only."""
+    bed = O.read_bed(os.path.join(GOLDEN, "g2"))
+    for svd, shuffle in [(1, False), (2, False)]:
+        eig_o, S_o, U_o, V_o, F_o, it_o, _ = O.run_emu(bed, k=3, svd=svd, bands=8, maxiter=10,
+                                                       tolem=1e-6, shuffle=shuffle)
+        eig, S, U, V, it = pb.run_emu(gpu, bed.packed, bed.N, k=3, svd=svd, bands=8, maxiter=10,
+                                      tolem=1e-6, shuffle=shuffle, precision="fp64")
+        assert it == it_o
+        assert_eig_close(eig, eig_o, 1e-9)
+        assert max_angle(U, U_o) < 1e-7

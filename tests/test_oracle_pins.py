@@ -72,3 +72,30 @@ def test_oracle_householder_sign_recovery():
             A[i + 1:, i] /= A[i, i]
             A[i + 1:, i + 1:] -= np.outer(A[i + 1:, i], A[i, i + 1:])
         np.testing.assert_allclose(Q * D, O.householder_q(H), atol=1e-8)
+
+
+def test_oracle_emu_matches_reference():
+    bed = g("g2")
+    eig, S, U, V, F, it, diffs = O.run_emu(bed, k=3, bands=8, maxiter=20, tolem=1e-6)
+    assert_eig_close(eig, ref_eigvals("g2_emu"), 1e-5)
+    assert_cols_close(U, ref_table("g2_emu", ".eigvecs"), 2e-6)
+    assert_cols_close(V, ref_table("g2_emu", ".loadings"), 2e-6)
+
+
+def _ld_check(G, mbim, ref_gz):
+    snp = O.read_snp_pos(os.path.join(GOLDEN, "ref", mbim))
+    O.divide_pos_by_window(snp, 5000)
+    i, k, r = O.ld_pairs(G, snp)
+    head, ref = O.read_ld_gz(os.path.join(GOLDEN, "ref", ref_gz))
+    assert head == "CHR_A\tBP_A\tSNP_A\tCHR_B\tBP_B\tSNP_B\tR2\n"
+    assert O.ld_lines(snp, i, k, r) == ["\t".join(x) for x in ref]
+
+
+def test_oracle_ld_flow_a_matches_reference():
+    U = O.read_usv(os.path.join(GOLDEN, "ref", "g4_pcs.eigvecs"))
+    _ld_check(O.ld_flow_a(g("g4"), U), "g4_pcs.mbim", "g4_ldA.ld.gz")
+
+
+def test_oracle_ld_flow_b_matches_reference():
+    G = O.read_residuals(os.path.join(GOLDEN, "ref", "g4_adj.residuals"))
+    _ld_check(G, "g4_adj.mbim", "g4_ldB.ld.gz")

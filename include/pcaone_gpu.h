@@ -145,6 +145,17 @@ int pcaone_gpu_fit_emu(pcaone_ctx* ctx, const double* U, const double* S, const 
                        uint32_t k, int reference_index);
 int pcaone_gpu_clear_imputed(pcaone_ctx* ctx);
 
+/* Windowed LD r2 on the loaded genotypes (current SNP order, normally unpermuted):
+ * run_ld_stuff flow A (src/LD.cpp:444-468) with ld_r2_big (src/LD.cpp:419-442). The centred
+ * genotypes (missing -> 0) are projected off U when U is given, G = (I - U U^T) G, and for
+ * window w (lead SNP ws[w], we[w] SNPs including the lead) r2[off_w + t - 1] =
+ * (G_i.G_{i+t} / (|G_i| |G_{i+t}|))^2 for t = 1..we[w]-1, off_w = sum_{v<w} (we[v] - 1).
+ * U: nsamples x k column-major host matrix as read by the caller, or NULL (no projection).
+ * r2: host array of sum_w (we[w] - 1) floats. The genotype cross products are exact
+ * integer counts (bit-plane popcounts); the projection is FP64. */
+int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
+                     const int32_t* we, uint64_t nwin, float* r2);
+
 #ifdef __cplusplus
 }
 #endif

@@ -540,3 +540,128 @@ def read_usv(path: str) -> np.ndarray:
     T = read_table(path)
     j, k = T.shape
     return T.ravel().reshape(k, j).T.copy()
+
+
+# --------------------------------------------------------------------------- PCAngsd
+def parse_beagle(path: str):
+    """FileBeagle constructor + parse_beagle_file (src/FileBeagle.hpp:8-40,
+    src/Utils.cpp:377-405): N = columns/3 - 1; P is 2N x M holding the first two of the three
+    genotype likelihoods per sample (the third is implied as 1 - P0 - P1)."""
+    with gzip.open(path, "rt") as f:
+        head = f.readline().split()
+        N = len(head) // 3 - 1
+        rows = [line.split()[3:] for line in f if line.strip()]
+    M = len(rows)
+    gl = np.array(rows, dtype=np.float64).reshape(M, N, 3)
+    P = np.empty((2 * N, M))
+    P[0::2] = gl[:, :, 0].T
+    P[1::2] = gl[:, :, 1].T
+    return P, N, M
+
+
+def _posterior(P, F, pt):
+    """p0 = P0 (1-pt)^2, p1 = P1 2 pt (1-pt), p2 = (1 - P0 - P1) pt^2 (src/Data.cpp:264-266)."""
+    P0, P1 = P[0::2], P[1::2]
+    p0 = P0 * (1.0 - pt) * (1.0 - pt)
+    p1 = P1 * 2 * pt * (1.0 - pt)
+    p2 = (1 - P0 - P1) * pt * pt
+    return p0, p1, p2
+
+
+def em_maf(P: np.ndarray, maxiter: int = 100, tolmaf: float = 1e-6):
+    """emMAF_with_GL (src/Utils.cpp:501-531), F0 = 0.25."""
+    N = P.shape[0] // 2
+    M = P.shape[1]
+    F = np.full(M, 0.25)
+    for it in range(maxiter):
+        Ft = F.copy()
+        p0, p1, p2 = _posterior(P, F[None, :], F[None, :])
+        F = ((p1 + 2.0 * p2) / (p0 + p1 + p2)).sum(axis=0) * (1.0 / (2.0 * N))
+        if np.sqrt(((F - Ft) ** 2).sum() / M) < tolmaf:
+            break
+    return F
+
+
+def pcangsd_e(P: np.ndarray, F: np.ndarray, pred: np.ndarray | None):
+    """Posterior expected genotype minus 2F: FileBeagle::read_all initial E (pt = F,
+    src/FileBeagle.cpp:121-143) or Data::fit_with_pi PCAngsd branch (src/Data.cpp:249-270)
+    with pt = clip((U S V^T + 2F)/2, 1e-4, 1 - 1e-4)."""
+    if pred is None:
+        pt = np.broadcast_to(F[None, :], (P.shape[0] // 2, P.shape[1]))
+    else:
+        pt = np.clip((pred + 2.0 * F[None, :]) / 2.0, 1e-4, 1 - 1e-4)
+    p0, p1, p2 = _posterior(P, F[None, :], pt)
+    return (p1 + 2.0 * p2) / (p0 + p1 + p2) - 2.0 * F[None, :]
+
+
+def pcangsd_standardize(P, F, pred):
+    """Data::pcangsd_standardize_E (src/Data.cpp:301-343): standardised E and the diagonal
+    Dc_i = sum_j sum_g (g - 2F_j)^2 post_g / (2 F_j (1 - F_j))."""
+    pt = np.clip((pred + 2.0 * F[None, :]) / 2.0, 1e-4, 1 - 1e-4)
+    p0, p1, p2 = _posterior(P, F[None, :], pt)
+    s = p0 + p1 + p2
+    E = (p1 + 2 * p2) / s - 2.0 * F[None, :]
+    norm = np.sqrt(2.0 * F * (1.0 - F))
+    ok = norm > VAR_TOL
+    E[:, ok] /= norm[ok][None, :]
+    f2 = 2.0 * F[None, :]
+    tmp = (0 - f2) ** 2 * (p0 / s) + (1 - f2) ** 2 * (p1 / s) + (2 - f2) ** 2 * (p2 / s)
+    Dc = (tmp / (2.0 * F * (1.0 - F))[None, :]).sum(axis=1)
+    return E, Dc
+
+
+def run_pcangsd(beagle: str, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: int = 10,
+                bands: int = 64, tol: float = 1e-4, maxiter: int = 100, tolem: float = 1e-5,
+                tolmaf: float = 1e-6, seed: int = 101, rand: int = 1, shuffle: bool = True,
+                reference_index: bool = True):
+    """PCAngsd, run_pca_with_halko impute branch for Beagle input (src/Halko.cpp:294-331).
+
+    Reference index semantics after the in-core shuffle: every EM step rebuilds E for
+    position j from P[:, j], F[j] and the loading row V[j] of the previous run, then permutes
+    the columns again (src/Halko.cpp:164-184), so position j ends up with SNP perm[j]'s
+    likelihoods and the prediction of loading row perm[j]. Returns
+    (eigvals, S, U, V in input order, F, iterations, C (GRM), Dc)."""
+    P, N, M = parse_beagle(beagle)
+    F = em_maf(P, maxiter, tolmaf)
+    os_ = max(oversamples, k)
+    perm = shuffle_perm(M) if (svd == 2 and shuffle) else np.arange(M, dtype=np.int32)
+    E = pcangsd_e(P, F, None)
+    state = {}
+
+    def rsvd(Z):
+        if svd == 1:
+            return halko(Z, k, os_, maxp, tol, seed, rand)
+        return winsvd(Z, k, os_, maxp, tol, bands, seed, rand, state=state)
+
+    res = rsvd(E[:, perm])
+    it = 0
+    for it in range(maxiter):
+        Vpre = res.V
+        if reference_index:
+            pred = (res.U * res.S) @ res.V.T          # position j <- loading row j
+            Z = pcangsd_e(P, F, pred)[:, perm]
+        else:
+            Vo = np.empty_like(res.V)
+            Vo[perm] = res.V                            # loadings in input order
+            Z = pcangsd_e(P, F, (res.U * res.S) @ Vo.T)[:, perm]
+        res = rsvd(Z)
+        if 1.0 - mev(res.V, Vpre) < tolem:
+            break
+    if reference_index:
+        pred = (res.U * res.S) @ res.V.T
+    else:
+        Vo = np.empty_like(res.V)
+        Vo[perm] = res.V
+        pred = (res.U * res.S) @ Vo.T
+    Es, Dc = pcangsd_standardize(P, F, pred)
+    C = Es @ Es.T / M
+    C[np.diag_indices(N)] = Dc / M
+    V = np.empty_like(res.V)
+    V[perm] = res.V
+    return res.S ** 2 / M * 2, res.S, res.U, V, F, it + 1, C, Dc
+
+
+def read_eigen_matrix(path: str) -> np.ndarray:
+    """A matrix printed by Eigen's default stream format (space separated, aligned)."""
+    with open(path) as f:
+        return np.array([[float(t) for t in line.split()] for line in f if line.strip()])

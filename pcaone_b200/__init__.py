@@ -26,7 +26,8 @@ STATUS = {0: "OK", 1: "EBADARG", 2: "EOOM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENUME
 EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_load_bed", "pcaone_gpu_counts", "pcaone_gpu_allele_freq",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
-           "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed"]
+           "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
+           "pcaone_gpu_ld_r2"]
 
 
 class PcaoneError(RuntimeError):
@@ -79,6 +80,7 @@ def lib() -> ctypes.CDLL:
                                          vp, u32, vp]
         L.pcaone_gpu_fit_emu.argtypes = [vp, vp, vp, vp, u32, ctypes.c_int]
         L.pcaone_gpu_clear_imputed.argtypes = [vp]
+        L.pcaone_gpu_ld_r2.argtypes = [vp, vp, u32, vp, vp, u64, vp]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
         _lib = L
@@ -233,6 +235,19 @@ def _clear_imputed(self):
     self._check(lib().pcaone_gpu_clear_imputed(self._h))
 
 
+def _ld_r2(self, ws, we, U=None):
+    """r2 of every window pair (see pcaone_gpu_ld_r2); ws, we as divide_pos_by_window."""
+    ws = np.ascontiguousarray(ws, dtype=np.int64)
+    we = np.ascontiguousarray(we, dtype=np.int32)
+    out = np.zeros(int(np.maximum(we - 1, 0).sum()), dtype=np.float32)
+    Uf = None if U is None else np.asfortranarray(U, dtype=np.float64)
+    k = 0 if U is None else U.shape[1]
+    self._check(lib().pcaone_gpu_ld_r2(self._h, _ptr(Uf), k, _ptr(ws), _ptr(we), len(ws),
+                                       _ptr(out)))
+    return out
+
+
+GpuContext.ld_r2 = _ld_r2
 GpuContext.fit_emu = _fit_emu
 GpuContext.clear_imputed = _clear_imputed
 

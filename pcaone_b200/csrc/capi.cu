@@ -264,4 +264,57 @@ int pcaone_gpu_clear_imputed(pcaone_ctx* c) {
   return guarded(c, [&] { c->imputed = false; });
 }
 
+int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
+                     uint64_t nwin, float* r2) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+    PG_REQUIRE(ws && we && (r2 || nwin == 0), PCAONE_EBADARG, "null window arrays");
+    PG_REQUIRE(!U || (k >= 1 && k <= (uint32_t)kLmax), PCAONE_EBADARG, "bad U width");
+    PG_REQUIRE(!c->imputed, PCAONE_ESTATE, "clear the EMU imputation before LD");
+    std::vector<int64_t> off(nwin + 1, 0);
+    for (uint64_t w = 0; w < nwin; ++w) {
+      PG_REQUIRE(ws[w] >= 0 && we[w] >= 1 && (uint64_t)ws[w] + we[w] <= c->M, PCAONE_EBADARG,
+                 "window " + std::to_string(w) + " out of range");
+      off[w + 1] = off[w] + (we[w] - 1);
+    }
+    double *dW = nullptr, *dY = nullptr;
+    if (U) {
+      // W = Gc^T U (M x k) through the FP64 product path; Y = (2I - U^T U) W on the host
+      std::vector<double> W((size_t)c->M * k), C((size_t)k * k, 0.0), Wr((size_t)c->M * k), Yr((size_t)c->M * k);
+      run_product(c, PCAONE_PREC_FP64, 0, 0, 2, U, (int)k, W.data());
+      for (uint32_t a = 0; a < k; ++a)
+        for (uint32_t b = 0; b < k; ++b) {
+          double acc = 0;
+          for (uint32_t i = 0; i < c->N; ++i) acc += U[(size_t)a * c->N + i] * U[(size_t)b * c->N + i];
+          C[(size_t)a * k + b] = (a == b ? 2.0 : 0.0) - acc;
+        }
+      for (uint64_t j = 0; j < c->M; ++j)
+        for (uint32_t a = 0; a < k; ++a) {
+          Wr[j * k + a] = W[(size_t)a * c->M + j];
+          double acc = 0;
+          for (uint32_t b = 0; b < k; ++b) acc += C[(size_t)a * k + b] * W[(size_t)b * c->M + j];
+          Yr[j * k + a] = acc;
+        }
+      dW = (double*)scratch(c, "ld_W", Wr.size() * 8);
+      dY = (double*)scratch(c, "ld_Y", Yr.size() * 8);
+      PG_CUDA(cudaMemcpyAsync(dW, Wr.data(), Wr.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(dY, Yr.data(), Yr.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    int64_t* d_ws = (int64_t*)scratch(c, "ld_ws", std::max<uint64_t>(nwin, 1) * 8);
+    int32_t* d_we = (int32_t*)scratch(c, "ld_we", std::max<uint64_t>(nwin, 1) * 4);
+    int64_t* d_off = (int64_t*)scratch(c, "ld_off", (nwin + 1) * 8);
+    float* d_r2 = (float*)scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * 4);
+    if (nwin) {
+      PG_CUDA(cudaMemcpyAsync(d_ws, ws, nwin * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(d_we, we, nwin * 4, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (nwin + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+    }
+    ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2);
+    if (off[nwin] > 0)
+      PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * 4, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 }  // extern "C"

@@ -137,6 +137,9 @@ void build_missing_by_window_sample(pcaone_ctx* c);
 // semantics, else the current F (Data::fit_with_pi EMU branch, src/Data.cpp:272-287).
 void compute_imputed_snp(pcaone_ctx* c);
 void compute_imputed_ws(pcaone_ctx* c);
+// LD r2 of every window pair (kernels_ld.cu). W, Y: M x k row-major device arrays (or null).
+void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,
+           const int32_t* d_we, const int64_t* d_off, int64_t nwin, float* d_r2);
 // d_scale_j = 1/sqrt(ploidy Fs_j (1 - Fs_j)) (or 1 when not standardising / sd <= 1e-9).
 void compute_scale(pcaone_ctx* c, int standardize, int ploidy);
 

@@ -25,6 +25,9 @@
 #include <string>
 #include <vector>
 
+#include <omp.h>
+#include <zlib.h>
+
 #include "../../include/pcaone_gpu.h"
 
 namespace {
@@ -71,6 +74,9 @@ struct Params {
   double tol = 1e-4, maf = 0.0, memory = 0.0, tolem = 1e-5;
   unsigned maxiter = 100;
   bool fix_index = false;
+  bool print_r2 = false, fix_read_u = false;
+  unsigned ld_bp = 0;
+  std::string fileU, filebim;
   int precision = PCAONE_PREC_MIXED;
   int device = 0;
   std::string cmdline;
@@ -78,9 +84,9 @@ struct Params {
 
 const std::set<std::string> kUnsupported = {
     "-c", "--csv", "-g", "--bgen", "-G", "--beagle", "-B", "--binary", "--pcangsd",
-    "-D", "--ld", "-R", "--print-r2", "--ld-bp", "--ld-r2", "--ld-stats", "--clump",
+    "-D", "--ld", "--ld-r2", "--ld-stats", "--clump",
     "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
-    "--inbreed", "--USV", "--read-U", "--read-V", "--read-S", "-f", "--match-bim", "--M", "--N",
+    "--inbreed", "--USV", "--read-V", "--read-S", "--M", "--N",
     "--scale-factor", "--buffer", "--imaxiter", "--itol", "--ncv", "--tol-maf"};
 
 void usage() {
@@ -96,6 +102,8 @@ void usage() {
                "      --emu        EMU imputation of missing genotypes (--maxiter, --tol-em)\n"
                "      --fix-perm-index  EM steps read each SNP's own F after the shuffle\n"
                "  -C, --scale      0: centre only, 1: standardise (default for PLINK)\n"
+               "  LD r2 (flow A): -b plink --read-U pcs.eigvecs -f pcs.mbim --ld-bp BP -R\n"
+               "      --fix-read-u read U row by row (the reference views it column-major)\n"
                "  -V, --printv     write .loadings and .mbim\n"
                "  -o, --out        output prefix [pcaone]\n"
                "  -v, --verbose    0 silent, 1 screen\n"
@@ -156,6 +164,11 @@ Params parse(int argc, char** argv) {
     else if (a == "--maxiter") p.maxiter = (unsigned)num(next());
     else if (a == "--tol-em") p.tolem = num(next());
     else if (a == "--fix-perm-index") p.fix_index = true;
+    else if (a == "-R" || a == "--print-r2") p.print_r2 = true;
+    else if (a == "--ld-bp") p.ld_bp = (unsigned)num(next());
+    else if (a == "--read-U") p.fileU = next();
+    else if (a == "-f" || a == "--match-bim") p.filebim = next();
+    else if (a == "--fix-read-u") p.fix_read_u = true;
     else if (a == "-V" || a == "--printv") p.printv = true;
     else if (a == "-v" || a == "--verbose") p.verbose = (unsigned)num(next());
     else if (a == "-n" || a == "--threads") p.threads = (unsigned)num(next());
@@ -186,6 +199,40 @@ Params parse(int argc, char** argv) {
   return p;
 }
 
+std::vector<std::string> split(const std::string& s, const char* seps) {
+  std::vector<std::string> out;
+  size_t b = 0;
+  for (size_t q = 0; q <= s.size(); ++q)
+    if (q == s.size() || std::strchr(seps, s[q])) {
+      out.push_back(s.substr(b, q - b));
+      b = q + 1;
+    }
+  return out;
+}
+
+// read_usv (src/Utils.cpp:255-286): values are read row by row into one vector that the
+// reference then views as a column-major rows x cols matrix. Returned column-major.
+std::vector<double> read_usv(const std::string& path, size_t& rows, size_t& cols, bool row_major) {
+  std::ifstream f(path);
+  if (!f.is_open()) fail("can not open " + path);
+  std::vector<double> v;
+  std::string line;
+  rows = 0;
+  cols = 0;
+  while (std::getline(f, line)) {
+    auto tok = split(line, "\t");
+    if (rows == 0) cols = tok.size();
+    else if (tok.size() != cols) fail("the columns are not aligned!\n =>" + path);
+    for (auto& t : tok) v.push_back(std::stod(t));
+    ++rows;
+  }
+  if (!row_major) return v;  // reinterpreted column-major, as the reference does
+  std::vector<double> cm(v.size());
+  for (size_t i = 0; i < rows; ++i)
+    for (size_t j = 0; j < cols; ++j) cm[j * rows + i] = v[i * cols + j];
+  return cm;
+}
+
 size_t count_lines(const std::string& path) {
   std::ifstream f(path);
   if (!f.is_open()) fail("can not open " + path);
@@ -214,6 +261,86 @@ void write_matrix(std::ostream& o, const double* a, size_t rows, size_t cols) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- LD r2 output
+// get_snp_pos_bim + divide_pos_by_window (src/LD.cpp:51-74, 125-139) and the .ld.gz text of
+// ld_r2_big (src/LD.cpp:419-442): "chr\tpos\tid" pairs and std::to_string(r2).
+int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M) {
+  const std::string filebim = p.filebim.empty() ? p.bfile + ".bim" : p.filebim;
+  std::ifstream fb(filebim);
+  if (!fb.is_open()) fail("can not open " + filebim);
+  std::vector<long> pos;
+  std::vector<int> end_pos;
+  std::vector<std::string> bims;
+  std::string line, prev;
+  while (std::getline(fb, line)) {
+    auto tok = split(line, " \t");
+    if (tok.size() < 4) fail("the input file is not valid!\n => " + filebim);
+    if (!prev.empty() && prev != tok[0]) end_pos.push_back((int)pos.size() - 1);
+    prev = tok[0];
+    pos.push_back(std::stol(tok[3]));
+    bims.push_back(tok[0] + "\t" + tok[3] + "\t" + tok[1]);
+  }
+  end_pos.push_back((int)pos.size() - 1);
+  if (pos.size() != M) fail("The number of variants is not matching the LD matrix");
+  std::vector<int64_t> ws;
+  std::vector<int32_t> we;
+  for (size_t i = 0, c = 0; i < pos.size(); ++i) {
+    if (pos[i] == pos[end_pos[c]]) {
+      ++c;
+      continue;
+    }
+    size_t j = i;
+    for (; j <= (size_t)end_pos[c]; ++j)
+      if (pos[j] - pos[i] > (long)p.ld_bp) break;
+    ws.push_back((int64_t)i);
+    we.push_back((int32_t)(j - i));
+  }
+  size_t ur = 0, uc = 0;
+  std::vector<double> U = read_usv(p.fileU, ur, uc, p.fix_read_u);
+  if (ur != N) fail("the number of rows of --read-U differs from the samples");
+  std::vector<int64_t> off(ws.size() + 1, 0);
+  for (size_t w = 0; w < ws.size(); ++w) off[w + 1] = off[w] + (we[w] - 1);
+  std::vector<float> r2(std::max<int64_t>(off.back(), 1));
+  auto t0 = std::chrono::steady_clock::now();
+  check(ctx, pcaone_gpu_ld_r2(ctx, U.data(), (uint32_t)uc, ws.data(), we.data(), ws.size(), r2.data()), "ld_r2");
+  double gpu_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  g_log.print(date(), "LD r2 of", off.back(), "pairs computed in", gpu_s, "seconds");
+  // format and deflate chunks of windows in parallel; concatenated gzip members are one file
+  const size_t nw = ws.size(), chunk = 4096;
+  const size_t nchunks = (nw + chunk - 1) / chunk;
+  std::vector<std::string> gz(nchunks);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long q = 0; q < (long)nchunks; ++q) {
+    std::string text;
+    if (q == 0) text = "CHR_A\tBP_A\tSNP_A\tCHR_B\tBP_B\tSNP_B\tR2\n";
+    for (size_t w = q * chunk; w < std::min(nw, (q + 1) * chunk); ++w) {
+      const size_t i = ws[w];
+      for (int t = 1; t < we[w]; ++t) {
+        text += bims[i];
+        text += '\t';
+        text += bims[i + t];
+        text += '\t';
+        text += std::to_string((double)r2[off[w] + t - 1]);
+        text += '\n';
+      }
+    }
+    z_stream zs{};
+    deflateInit2(&zs, Z_DEFAULT_COMPRESSION, Z_DEFLATED, 15 + 16, 8, Z_DEFAULT_STRATEGY);
+    std::string out(deflateBound(&zs, text.size()) + 64, '\0');
+    zs.next_in = (Bytef*)text.data();
+    zs.avail_in = (uInt)text.size();
+    zs.next_out = (Bytef*)&out[0];
+    zs.avail_out = (uInt)out.size();
+    deflate(&zs, Z_FINISH);
+    out.resize(zs.total_out);
+    deflateEnd(&zs);
+    gz[q] = std::move(out);
+  }
+  std::ofstream o(p.fileout + ".ld.gz", std::ios::binary);
+  for (auto& g : gz) o.write(g.data(), (std::streamsize)g.size());
+  return 0;
+}
 
 int main(int argc, char** argv) {
   Params p = parse(argc, argv);
@@ -277,6 +404,16 @@ int main(int argc, char** argv) {
     check(ctx, pcaone_gpu_load_bed(ctx, packed.data(), M, (uint32_t)N), "load_bed");
   }
   g_log.print(date(), "done reading all data");
+
+  if (p.print_r2 || p.ld_bp > 0) {  // LD mode (src/Main.cpp:64-77)
+    if (p.fileU.empty()) fail("LD r2 from PLINK input needs --read-U (flow A)");
+    g_log.print(date(), "run LD stuff");
+    run_ld(p, ctx, N, M);
+    pcaone_gpu_destroy(ctx);
+    double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    g_log.print(date(), "total elapsed wall time:", wall, " seconds");
+    return 0;
+  }
 
   const bool perm_on = p.svd == 2 && !p.noshuffle;  // src/Cmd.cpp:216
   std::vector<int32_t> perm;

@@ -97,3 +97,14 @@ def test_cli_rejects_bad_magic_and_truncation(tmp_path):
 def test_cli_rejects_odd_windows(tmp_path):
     out = run_cli(["-b", os.path.join(GOLDEN, "g1"), "-w", "5"], tmp_path, check=False)
     assert out.returncode == 1
+
+
+@pytest.mark.gpu
+def test_cli_ld_flow_a_matches_reference(tmp_path):
+    run_cli(golden_args("g4_ldA", tmp_path), tmp_path)
+    head, got = O.read_ld_gz(str(tmp_path / "g4_ldA.ld.gz"))
+    rhead, ref = O.read_ld_gz(ref_out("g4_ldA", ".ld.gz"))
+    assert head == rhead and len(got) == len(ref)
+    assert [x[:6] for x in got] == [x[:6] for x in ref]
+    diff = np.abs(np.array([float(x[6]) for x in got]) - np.array([float(x[6]) for x in ref]))
+    assert diff.max() <= 1.01e-6  # 6 printed decimals; the r2 values agree to 1e-5 or better

@@ -99,3 +99,15 @@ def test_oracle_ld_flow_a_matches_reference():
 def test_oracle_ld_flow_b_matches_reference():
     G = O.read_residuals(os.path.join(GOLDEN, "ref", "g4_adj.residuals"))
     _ld_check(G, "g4_adj.mbim", "g4_ldB.ld.gz")
+
+
+@pytest.mark.parametrize("name,shuffle", [("g3_pcangsd", False), ("g3_pcangsd_shuf", True)])
+def test_oracle_pcangsd_matches_reference(name, shuffle):
+    eig, S, U, V, F, it, C, Dc = O.run_pcangsd(os.path.join(GOLDEN, "g3.beagle.gz"), k=3,
+                                               shuffle=shuffle, bands=8, maxiter=30)
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(U, ref_table(name, ".eigvecs"), 2e-6)
+    if not shuffle:
+        assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)
+        Cr = O.read_eigen_matrix(os.path.join(GOLDEN, "ref", name + ".cov"))
+        np.testing.assert_allclose(C, Cr, atol=1e-5)

@@ -156,6 +156,26 @@ int pcaone_gpu_clear_imputed(pcaone_ctx* ctx);
 int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
                      const int32_t* we, uint64_t nwin, float* r2);
 
+/* PCAngsd on genotype likelihoods (Beagle input). Load the likelihood pairs: P is the
+ * reference's 2N x M column-major FP64 matrix of the first two likelihoods per sample and
+ * site (FileBeagle::read_all, src/FileBeagle.cpp:121-143; the third is implied as
+ * 1 - P0 - P1). The context then holds no packed codes; pcaone_gpu_rsvd runs on the dense
+ * posterior matrix E built by pcaone_gpu_gl_update. */
+int pcaone_gpu_load_gl(pcaone_ctx* ctx, const double* P, uint64_t nsnps, uint32_t nsamples);
+
+/* Allele frequencies by EM from the likelihoods, emMAF_with_GL (src/Utils.cpp:501-531):
+ * F0 = 0.25, at most maxiter sweeps, stops when sqrt(mean((F - F_prev)^2)) < tolmaf.
+ * F (host, nsnps) and iters (number of sweeps run) may be NULL. */
+int pcaone_gpu_gl_freq(pcaone_ctx* ctx, int maxiter, double tolmaf, double* F, int* iters);
+
+/* Rebuild E_ij = E[g | likelihoods, pt_ij] - 2 F_j for every sample and site:
+ * pt_ij = F_j when U is NULL (initial E, src/FileBeagle.cpp:121-143), else
+ * pt_ij = clip((sum_t U_it S_t V_jt + 2 F_j) / 2, 1e-4, 1 - 1e-4), Data::fit_with_pi
+ * PCAngsd branch (src/Data.cpp:249-270). V (nsnps x k) row j is the loading used for
+ * site j (the caller applies the reference's index semantics). */
+int pcaone_gpu_gl_update(pcaone_ctx* ctx, const double* U, const double* S, const double* V,
+                         uint32_t k);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,8 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_load_bed", "pcaone_gpu_counts", "pcaone_gpu_allele_freq",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
-           "pcaone_gpu_ld_r2"]
+           "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
+           "pcaone_gpu_gl_update"]
 
 
 class PcaoneError(RuntimeError):
@@ -81,6 +82,9 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_fit_emu.argtypes = [vp, vp, vp, vp, u32, ctypes.c_int]
         L.pcaone_gpu_clear_imputed.argtypes = [vp]
         L.pcaone_gpu_ld_r2.argtypes = [vp, vp, u32, vp, vp, u64, vp]
+        L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
+        L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
+        L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
         _lib = L
@@ -248,6 +252,68 @@ def _ld_r2(self, ws, we, U=None):
 
 
 GpuContext.ld_r2 = _ld_r2
+
+
+def _load_gl(self, P: np.ndarray):
+    """P: 2N x M likelihood pairs (first two of the three per sample and site)."""
+    Pf = np.asfortranarray(P, dtype=np.float64)
+    N, M = P.shape[0] // 2, P.shape[1]
+    self._check(lib().pcaone_gpu_load_gl(self._h, _ptr(Pf), M, N))
+    self.N, self.M = N, M
+
+
+def _gl_freq(self, maxiter=100, tolmaf=1e-6):
+    F = np.zeros(self.M)
+    it = ctypes.c_int(0)
+    self._check(lib().pcaone_gpu_gl_freq(self._h, maxiter, tolmaf, _ptr(F), ctypes.byref(it)))
+    return F, it.value
+
+
+def _gl_update(self, U=None, S=None, V=None):
+    if U is None:
+        self._check(lib().pcaone_gpu_gl_update(self._h, None, None, None, 0))
+        return
+    Uf, Vf = np.asfortranarray(U, dtype=np.float64), np.asfortranarray(V, dtype=np.float64)
+    Sf = np.ascontiguousarray(S, dtype=np.float64)
+    self._check(lib().pcaone_gpu_gl_update(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(S)))
+
+
+GpuContext.load_gl = _load_gl
+GpuContext.gl_freq = _gl_freq
+GpuContext.gl_update = _gl_update
+
+
+def run_pcangsd(ctx: "GpuContext", P: np.ndarray, k: int = 10, svd: int = 2, bands: int = 64,
+                maxp: int = 20, oversamples: int = 10, tol: float = 1e-4, maxiter: int = 100,
+                tolem: float = 1e-5, tolmaf: float = 1e-6, seed: int = 101, rand: int = 1,
+                shuffle: bool = True, reference_index: bool = True):
+    """PCAngsd on the GPU: the impute branch of run_pca_with_halko for Beagle input
+    (src/Halko.cpp:294-316). Returns (eigvals, S, U, V in input order, iterations, F).
+
+    The in-core shuffle is applied by feeding the RSVD the permuted posterior matrix: the
+    likelihood columns are loaded in permuted order, and under the reference's index
+    semantics each EM step predicts position j from loading row perm[j]."""
+    M = P.shape[1]
+    perm = shuffle_perm(M) if (svd == 2 and shuffle) else np.arange(M, dtype=np.int32)
+    ctx.load_gl(P[:, perm])
+    F_perm, _ = ctx.gl_freq(maxiter, tolmaf)
+    ctx.gl_update()
+    kw = dict(k=k, oversamples=oversamples, maxp=maxp, svd=svd, bands=bands, tol=tol,
+              seed=seed, rand=rand, precision=PREC_FP32, standardize=False)
+    r = ctx.rsvd(carry=False, **kw)
+    it = 0
+    for it in range(maxiter):
+        Vpre = r.V
+        Vuse = r.V[perm] if reference_index else r.V
+        ctx.gl_update(r.U, r.S, Vuse)
+        r = ctx.rsvd(carry=True, **kw)
+        if 1.0 - mev(r.V, Vpre) < tolem:
+            break
+    V = np.empty_like(r.V)
+    V[perm] = r.V
+    F = np.empty_like(F_perm)
+    F[perm] = F_perm
+    return r.S ** 2 / M * 2, r.S, r.U, V, it + 1, F
 GpuContext.fit_emu = _fit_emu
 GpuContext.clear_imputed = _clear_imputed
 

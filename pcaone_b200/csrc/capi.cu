@@ -43,6 +43,14 @@ void free_data(pcaone_ctx* c) {
   free_ptr(c->d_imp_V);
   free_ptr(c->d_miss_snp_val);
   free_ptr(c->d_miss_ws_val);
+  free_ptr(c->d_P);
+  free_ptr(c->d_E);
+  free_ptr(c->d_zero);
+  c->d_P = nullptr;
+  c->d_E = nullptr;
+  c->d_zero = nullptr;
+  c->dense = false;
+  c->win = WindowLayout();
   c->d_F_load = c->d_scale = c->d_imp_US = c->d_imp_V = c->d_miss_snp_val = c->d_miss_ws_val = nullptr;
   c->imputed = false;
   c->miss_ws_val_valid = false;
@@ -313,6 +321,69 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
     ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2);
     if (off[nwin] > 0)
       PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * 4, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t nsamples) {
+  return guarded(c, [&] {
+    PG_REQUIRE(P && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty likelihood matrix");
+    PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 29), PCAONE_EBADARG, "likelihood matrix too large");
+    free_data(c);
+    c->generation++;
+    c->dense = true;
+    c->N = nsamples;
+    c->M = nsnps;
+    c->Npad = (uint32_t)round_up(nsamples, kRowPad);
+    c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
+    c->pitch = 1;
+    const size_t np = (size_t)nsnps * 2 * nsamples;
+    std::vector<float> pf(np);
+    for (size_t t = 0; t < np; ++t) pf[t] = (float)P[t];
+    PG_CUDA(cudaMalloc(&c->d_P, np * 4));
+    PG_CUDA(cudaMemcpyAsync(c->d_P, pf.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
+    PG_CUDA(cudaMalloc(&c->d_E, (size_t)c->Mpad * c->Npad * 4));
+    PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
+    PG_CUDA(cudaMalloc(&c->d_F, c->M * 8));
+    PG_CUDA(cudaMalloc(&c->d_F_load, c->M * 8));
+    PG_CUDA(cudaMalloc(&c->d_scale, c->M * 8));
+    PG_CUDA(cudaMalloc(&c->d_zero, c->M * 8));
+    PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
+    std::vector<double> q(c->M, 0.25);
+    PG_CUDA(cudaMemcpyAsync(c->d_F, q.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    c->loaded = true;
+  });
+}
+
+int pcaone_gpu_gl_freq(pcaone_ctx* c, int maxiter, double tolmaf, double* F, int* iters) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");
+    PG_REQUIRE(maxiter >= 1, PCAONE_EBADARG, "maxiter must be >= 1");
+    gl_em_maf(c, maxiter, tolmaf, iters);
+    if (F) PG_CUDA(cudaMemcpyAsync(F, c->d_F, c->M * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_gl_update(pcaone_ctx* c, const double* U, const double* S, const double* V, uint32_t k) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");
+    double *dUS = nullptr, *dV = nullptr;
+    if (U) {
+      PG_REQUIRE(S && V && k >= 1 && k <= (uint32_t)kLmax, PCAONE_EBADARG, "bad factors");
+      std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
+      for (uint32_t i = 0; i < c->N; ++i)
+        for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+      for (uint64_t j = 0; j < c->M; ++j)
+        for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
+      dUS = (double*)scratch(c, "gl_US", us.size() * 8);
+      dV = (double*)scratch(c, "gl_V", v.size() * 8);
+      PG_CUDA(cudaMemcpyAsync(dUS, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(dV, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    gl_posterior(c, dUS, dV, U ? (int)k : 0, false, nullptr);
     PG_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

@@ -83,6 +83,13 @@ struct pcaone_ctx {
   double* d_F_load = nullptr;  // F in the SNP order of load time (before any permutation)
   double* d_scale = nullptr;   // per-SNP multiplier of the centred genotypes (current order)
 
+  // PCAngsd (genotype-likelihood) mode: no packed codes; the RSVD runs on the dense float
+  // posterior matrix E (SNP-major, Npad floats per SNP), rebuilt from the GL pairs P.
+  bool dense = false;
+  float* d_P = nullptr;       // M x 2N floats (P0, P1 per sample)
+  float* d_E = nullptr;       // M x Npad floats
+  double* d_zero = nullptr;   // M zeros (centring frequencies of E, already centred)
+
   // transposed copy for the current window layout
   pg::WindowLayout win;
   uint8_t* d_bedT = nullptr;  // bands x Npad x win.pitch
@@ -130,6 +137,8 @@ void launch_fix_padding(pcaone_ctx* c);
 void launch_counts(pcaone_ctx* c);
 void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out);
 void build_transposed(pcaone_ctx* c, int bands);
+void set_window_layout(pcaone_ctx* c, int bands);  // layout only (dense mode)
+void build_empty_missing(pcaone_ctx* c);           // dense mode: no missing entries
 void build_missing_by_snp(pcaone_ctx* c);
 void build_missing_by_window_sample(pcaone_ctx* c);
 // e_ij = clip(sum_k US_ik V_jk, -Fc_j, 1 - Fc_j) for every entry of the by-SNP list (and of

@@ -179,8 +179,7 @@ void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out) {
   c->launches++;
 }
 
-void build_transposed(pcaone_ctx* c, int bands) {
-  if (c->bedT_valid && c->win.bands == bands) return;
+static WindowLayout make_layout(pcaone_ctx* c, int bands) {
   WindowLayout w;
   w.bands = bands;
   w.blocksize = (uint64_t)std::ceil((double)c->M / bands);  // src/Halko.cpp:178
@@ -194,6 +193,39 @@ void build_transposed(pcaone_ctx* c, int bands) {
     w.start.push_back(s);
     w.stop.push_back(e);
   }
+  return w;
+}
+
+void set_window_layout(pcaone_ctx* c, int bands) {
+  if (c->win.bands == bands && !c->win.start.empty()) return;
+  c->win = make_layout(c, bands);
+  c->miss_ws_valid = false;
+}
+
+void build_empty_missing(pcaone_ctx* c) {
+  const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
+  if (!c->miss_snp_valid) {
+    if (c->d_miss_snp_ptr) cudaFree(c->d_miss_snp_ptr);
+    if (c->d_miss_snp_idx) cudaFree(c->d_miss_snp_idx);
+    PG_CUDA(cudaMalloc(&c->d_miss_snp_ptr, (c->M + 1) * 8));
+    PG_CUDA(cudaMalloc(&c->d_miss_snp_idx, 4));
+    PG_CUDA(cudaMemsetAsync(c->d_miss_snp_ptr, 0, (c->M + 1) * 8, c->stream));
+    c->n_missing = 0;
+    c->miss_snp_valid = true;
+  }
+  if (!c->miss_ws_valid) {
+    if (c->d_miss_ws_ptr) cudaFree(c->d_miss_ws_ptr);
+    if (c->d_miss_ws_idx) cudaFree(c->d_miss_ws_idx);
+    PG_CUDA(cudaMalloc(&c->d_miss_ws_ptr, (rows + 1) * 8));
+    PG_CUDA(cudaMalloc(&c->d_miss_ws_idx, 4));
+    PG_CUDA(cudaMemsetAsync(c->d_miss_ws_ptr, 0, (rows + 1) * 8, c->stream));
+    c->miss_ws_valid = true;
+  }
+}
+
+void build_transposed(pcaone_ctx* c, int bands) {
+  if (c->bedT_valid && c->win.bands == bands) return;
+  WindowLayout w = make_layout(c, bands);
   size_t bytes = (size_t)bands * c->Npad * w.pitch;
   if (c->d_bedT) {
     cudaFree(c->d_bedT);

@@ -145,7 +145,7 @@ void launch_decode_gemm_simt(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch
 
 namespace {
 template <typename T>
-void simt_gemm(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K,
+void simt_gemm(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t, int64_t rows, int64_t K,
                const T* B, int l, int ks, T* out) {
   launch_decode_gemm_simt<T>(c, codes, pitch, rows, K, B, l, l, ks, out);
 }

@@ -464,15 +464,14 @@ void check_err(pcaone_ctx* c) {
   PG_REQUIRE(h == 0, PCAONE_ETIMEOUT, "tensor-core decode-GEMM: bounded wait expired (code " + std::to_string(h) + ")");
 }
 
-void tc_p1(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K, const float*, int l,
-           int ks, float* out) {
-  const int64_t row_off = (codes - c->d_bed) / (int64_t)c->pitch;
+void tc_p1(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t row_off, int64_t rows, int64_t K,
+           const float*, int l, int ks, float* out) {
   auto* Bt = (__nv_bfloat16*)scratch(c, "tc_bt1", (size_t)c->Npad * np_of(l) * 2);
   run_tc(c, codes, pitch, rows, (int64_t)c->Mpad - row_off, K, Bt, c->Npad, l, ks, out);
 }
 
-void tc_p2(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K, const float*, int l,
-           int ks, float* out) {
+void tc_p2(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t, int64_t rows, int64_t K,
+           const float*, int l, int ks, float* out) {
   const int64_t kpad = round_up(c->win.blocksize, 256);
   auto* Bt = (__nv_bfloat16*)scratch(c, "tc_bt2", (size_t)kpad * np_of(l) * 2);
   run_tc(c, codes, pitch, rows, c->Npad, K, Bt, kpad, l, ks, out);

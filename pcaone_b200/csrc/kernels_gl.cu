@@ -1,0 +1,282 @@
+// PCAngsd on genotype likelihoods: allele-frequency EM, posterior expected genotypes and the
+// standardised posterior matrix with its diagonal, plus the dense-matrix decode-GEMM back end
+// the RSVD uses on that matrix.
+//
+//  * emMAF_with_GL (src/Utils.cpp:501-531)
+//  * FileBeagle::read_all initial E (src/FileBeagle.cpp:121-143) and Data::fit_with_pi PCAngsd
+//    branch (src/Data.cpp:249-270): E_ij = (p1 + 2 p2)/(p0 + p1 + p2) - 2 F_j with
+//    p0 = P0 (1-pt)^2, p1 = P1 2 pt (1-pt), p2 = (1 - P0 - P1) pt^2 and pt = F_j initially or
+//    clip((U S V^T + 2F)/2, 1e-4, 1 - 1e-4) in the EM steps
+//  * Data::pcangsd_standardize_E (src/Data.cpp:301-343)
+//
+// Layout: GL pairs are SNP-major floats, P[j][2i + {0,1}] (the reference's 2N x M column-major
+// P); E is SNP-major floats E[j][i] with rows padded to Npad samples (zeros beyond N).
+// Posterior arithmetic is FP64 in registers.
+#include <algorithm>
+#include <cmath>
+
+#include "internal.hpp"
+#include "rsvd.hpp"
+
+namespace pg {
+
+namespace {
+
+__device__ __forceinline__ void posterior(double P0, double P1, double pt, double& p0, double& p1, double& p2) {
+  p0 = P0 * (1.0 - pt) * (1.0 - pt);
+  p1 = P1 * 2 * pt * (1.0 - pt);
+  p2 = (1 - P0 - P1) * pt * pt;
+}
+
+// One EM sweep of the allele frequencies: warp per SNP. diff2[j] = (F_new - F_old)^2.
+__global__ void k_em_maf(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+                         double* __restrict__ F, double* __restrict__ diff2) {
+  const uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= M) return;
+  const double f = F[j];
+  const float* row = P + j * ldp;
+  double acc = 0.0;
+  for (uint32_t i = lane; i < N; i += 32) {
+    double p0, p1, p2;
+    posterior(row[2 * i], row[2 * i + 1], f, p0, p1, p2);
+    acc += (p1 + 2.0 * p2) / (p0 + p1 + p2);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) {
+    const double fn = acc * (1.0 / (2.0 * N));
+    diff2[j] = (fn - f) * (fn - f);
+    F[j] = fn;
+  }
+}
+
+// E (or the standardised E and per-CTA partial Dc) for SNP rows; warp per SNP.
+// US: N x k (U diag S) row-major, V: M x k row-major (row j = the loading used for SNP j).
+template <bool STD>
+__global__ void k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+                              const double* __restrict__ F, const double* __restrict__ US,
+                              const double* __restrict__ V, int k, float* __restrict__ E,
+                              uint32_t lde, double* __restrict__ dc_part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  extern __shared__ double sdc[];  // [nwarps][N] only when STD
+  if (STD)
+    for (uint32_t i = threadIdx.x; i < (uint32_t)nwarps * N; i += blockDim.x) sdc[i] = 0.0;
+  if (STD) __syncthreads();
+  for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
+    const double f = F[j];
+    double v[kLmax];
+    if (V)
+      for (int t = 0; t < k; ++t) v[t] = V[j * k + t];
+    const float* row = P + j * ldp;
+    const double norm = sqrt(2.0 * f * (1.0 - f));
+    for (uint32_t i = lane; i < N; i += 32) {
+      double pt = f;
+      if (V) {
+        double pred = 0.0;
+        for (int t = 0; t < k; ++t) pred += US[(uint64_t)i * k + t] * v[t];
+        pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
+      }
+      double p0, p1, p2;
+      posterior(row[2 * i], row[2 * i + 1], pt, p0, p1, p2);
+      const double s = p0 + p1 + p2;
+      double e = (p1 + 2.0 * p2) / s - 2.0 * f;
+      if (STD) {
+        if (norm > 1e-9) e /= norm;
+        const double f2 = 2.0 * f;
+        double t = (0.0 - f2) * (0.0 - f2) * (p0 / s);
+        t += (1.0 - f2) * (1.0 - f2) * (p1 / s);
+        t += (2.0 - f2) * (2.0 - f2) * (p2 / s);
+        sdc[(uint64_t)warp * N + i] += t / (2.0 * f * (1.0 - f));
+      }
+      E[j * lde + i] = (float)e;
+    }
+  }
+  if (STD) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+      double acc = 0.0;
+      for (int w = 0; w < nwarps; ++w) acc += sdc[(uint64_t)w * N + i];
+      dc_part[(uint64_t)blockIdx.x * N + i] = acc;
+    }
+  }
+}
+
+__global__ void k_sum_rows(const double* __restrict__ part, int nblk, uint32_t n, double* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(uint64_t)b * n + i];
+  out[i] = s;
+}
+
+// Dense SIMT GEMM: out[s][r][c] = sum_{k in split s} A(r, k) * B[k][c]. A(r, k) is
+// A[r * lda + k] when !AT (rows = SNPs, K = samples) and A[k * lda + r] when AT (rows =
+// samples of E's rows, K = SNPs). Same tiling as the decode-GEMM: 128 rows x 8 columns per
+// warp group, 4 rows x 8 columns per thread.
+template <bool AT, int G>
+__global__ void __launch_bounds__(32 * G)
+k_dense_gemm(const float* __restrict__ A, uint64_t lda, int64_t rows, int64_t K, const float* __restrict__ B,
+             int l, int64_t kchunks_per_split, float* __restrict__ out) {
+  constexpr int TR = 128, KC = 32, LDSB = G * 8;
+  __shared__ float as[KC][TR + 1];
+  __shared__ __align__(16) float bs[KC * LDSB];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int64_t r0 = (int64_t)blockIdx.x * TR;
+  const int64_t kc_total = (K + KC - 1) / KC;
+  const int64_t kc0 = (int64_t)blockIdx.y * kchunks_per_split;
+  const int64_t kc1 = min(kc0 + kchunks_per_split, kc_total);
+  float acc[4][8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[q][c] = 0.f;
+  for (int64_t kc = kc0; kc < kc1; ++kc) {
+    const int64_t k0 = kc * KC;
+    for (int t = threadIdx.x; t < KC * TR; t += 32 * G) {
+      int kk, r;
+      if (AT) {
+        kk = t / TR;
+        r = t - kk * TR;
+      } else {
+        r = t / KC;
+        kk = t - r * KC;
+      }
+      const int64_t row = r0 + r, k = k0 + kk;
+      float v = 0.f;
+      if (row < rows && k < K) v = AT ? A[(uint64_t)k * lda + row] : A[(uint64_t)row * lda + k];
+      as[kk][r] = v;
+    }
+    for (int t = threadIdx.x; t < KC * LDSB; t += 32 * G) {
+      int kk = t / LDSB, cc = t - kk * LDSB;
+      int64_t k = k0 + kk;
+      bs[t] = (cc < l && k < K) ? B[k * l + cc] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < KC; ++kk) {
+      float b[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) b[c] = bs[kk * LDSB + g * 8 + c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float a = as[kk][lane + 32 * q];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[q][c] = fmaf(a, b[c], acc[q][c]);
+      }
+    }
+    __syncthreads();
+  }
+  float* o = out + (int64_t)blockIdx.y * rows * l;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int64_t r = r0 + lane + 32 * q;
+    if (r >= rows) continue;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int col = g * 8 + c;
+      if (col < l) o[r * l + col] = acc[q][c];
+    }
+  }
+}
+
+template <bool AT, int G>
+void launch_dense_g(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int64_t K, const float* B, int l,
+                    int ks, float* out) {
+  const int64_t kct = (K + 31) / 32;
+  const int64_t per = (kct + ks - 1) / ks;
+  dim3 grid((unsigned)((rows + 127) / 128), (unsigned)ks);
+  k_dense_gemm<AT, G><<<grid, 32 * G, 0, c->stream>>>(A, lda, rows, K, B, l, per, out);
+  PG_CHECK_LAUNCH();
+}
+
+template <bool AT>
+void launch_dense(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int64_t K, const float* B, int l,
+                  int ks, float* out) {
+  switch ((l + 7) / 8) {
+    case 1: launch_dense_g<AT, 1>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 2: launch_dense_g<AT, 2>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 3: launch_dense_g<AT, 3>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 4: launch_dense_g<AT, 4>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 5: launch_dense_g<AT, 5>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 6: launch_dense_g<AT, 6>(c, A, lda, rows, K, B, l, ks, out); break;
+    case 7: launch_dense_g<AT, 7>(c, A, lda, rows, K, B, l, ks, out); break;
+    default: launch_dense_g<AT, 8>(c, A, lda, rows, K, B, l, ks, out); break;
+  }
+  c->launches++;
+  c->gemm_launches++;
+}
+
+// Back end for the RSVD engine: "codes" are the float rows of E (the engine passes the row
+// offset through the pointer), "pitch" is unused.
+int dense_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) {
+  int64_t tiles = (rows + 127) / 128, chunks = (K + 31) / 32;
+  int64_t want = (2 * (int64_t)c->sm_count + tiles - 1) / tiles;
+  return (int)std::max<int64_t>(1, std::min<int64_t>({want, chunks / 4, 64}));
+}
+void dense_p1(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t row0, int64_t rows, int64_t K, const float* B,
+              int l, int ks, float* out) {
+  launch_dense<false>(c, c->d_E + (uint64_t)row0 * c->Npad, c->Npad, rows, K, B, l, ks, out);
+}
+void dense_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t rows, int64_t K, const float* B,
+              int l, int ks, float* out) {
+  launch_dense<true>(c, c->d_E + c->win.start[window] * (uint64_t)c->Npad, c->Npad, rows, K, B, l, ks, out);
+}
+void dense_none_omega(pcaone_ctx*, const double*, int, int64_t) {}
+void dense_none_b2(pcaone_ctx*, const float*, int, int64_t) {}
+
+}  // namespace
+
+GemmFnT<float> gemm_dense_float() {
+  return GemmFnT<float>{dense_ksplit, dense_p1, dense_p2, dense_none_omega, dense_none_b2};
+}
+
+void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {
+  double* diff2 = (double*)scratch(c, "gl_diff2", c->M * 8);
+  std::vector<double> h(c->M);
+  const double init = 0.25;
+  std::vector<double> f0(c->M, init);
+  PG_CUDA(cudaMemcpyAsync(c->d_F, f0.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+  int it = 0;
+  for (it = 0; it < maxiter; ++it) {
+    k_em_maf<<<(unsigned)((c->M * 32 + 255) / 256), 256, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F,
+                                                                         diff2);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+    PG_CUDA(cudaMemcpyAsync(h.data(), diff2, c->M * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    double sum = 0.0;
+    for (uint64_t j = 0; j < c->M; ++j) sum += h[j];
+    if (std::sqrt(sum / c->M) < tolmaf) break;
+  }
+  if (iters) *iters = std::min(it + 1, maxiter);
+}
+
+void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool standardize, double* Dc) {
+  const int threads = 256, nwarps = threads / 32;
+  if (!standardize) {
+    int nblk = (int)std::min<uint64_t>(8 * c->sm_count, (c->M + nwarps - 1) / nwarps);
+    k_posterior_e<false><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E,
+                                                           c->Npad, nullptr);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+    return;
+  }
+  // per-warp Dc rows in shared memory: keep them within 200 KB
+  const size_t smem = (size_t)nwarps * c->N * 8;
+  PG_REQUIRE(smem <= 200 * 1024, PCAONE_EBADARG, "too many samples for the PCAngsd diagonal kernel");
+  static bool attr = false;
+  if (!attr) {
+    PG_CUDA(cudaFuncSetAttribute(k_posterior_e<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  int nblk = (int)std::min<uint64_t>(2 * c->sm_count, (c->M + nwarps - 1) / nwarps);
+  double* part = (double*)scratch(c, "gl_dc_part", (size_t)nblk * c->N * 8);
+  k_posterior_e<true><<<nblk, threads, smem, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E,
+                                                         c->Npad, part);
+  PG_CHECK_LAUNCH();
+  k_sum_rows<<<(c->N + 255) / 256, 256, 0, c->stream>>>(part, nblk, c->N, Dc);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
+
+}  // namespace pg

@@ -101,11 +101,13 @@ struct Engine {
   double *Omg, *Omg2, *wsum, *G, *H, *H1, *H2, *Tb, *Rg, *Rb, *Dsig, *Ucur, *Upre, *Ck;
   T* OmgT;   // Omega as the B operand of the first product (alias of Omg for FP64)
   int* d_status;
+  const double* Fcent;  // centring frequencies of the epilogues (zeros for the dense E)
 
   Engine(pcaone_ctx* c_, const pcaone_rsvd_opts& o_, GemmFnT<T> g) : c(c_), o(o_), gemm(g) {
     N = (int)c->N;
     M = (int64_t)c->M;
     Npad = c->Npad;
+    Fcent = c->dense ? c->d_zero : c->d_F;
     k = o.k;
     l = o.k + o.oversamples;
     auto d = [&](const char* name, size_t n) { return (double*)scratch(c, name, n * sizeof(double)); };
@@ -166,13 +168,14 @@ struct Engine {
     // product 1: D1 = R_b^T Omega
     int ks1 = gemm.ksplit(c, m, N);
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * m * l * sizeof(T));
-    timed([&] { gemm.p1(c, c->d_bed + s * (int64_t)c->pitch, c->pitch, m, N, OmgT, l, ks1, D1); });
+    const uint8_t* codes = c->dense ? nullptr : c->d_bed + s * (int64_t)c->pitch;
+    timed([&] { gemm.p1(c, codes, c->pitch, s, m, N, OmgT, l, ks1, D1); });
     EpiP1 p1;
     p1.start = s;
     p1.m = m;
     p1.l = l;
     p1.ksplit = ks1;
-    p1.F = c->d_F;
+    p1.F = Fcent;
     p1.scale = c->d_scale;
     p1.wsum = wsum;
     p1.omega = Omg;
@@ -187,15 +190,15 @@ struct Engine {
     // product 2: D2 = R_b B2
     int ks2 = gemm.ksplit(c, N, m);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
-    const uint8_t* codesT = c->d_bedT + (int64_t)b * Npad * c->win.pitch;
-    timed([&] { gemm.p2(c, codesT, c->win.pitch, N, m, B2, l, ks2, D2); });
+    const uint8_t* codesT = c->dense ? nullptr : c->d_bedT + (int64_t)b * Npad * c->win.pitch;
+    timed([&] { gemm.p2(c, codesT, c->win.pitch, b, N, m, B2, l, ks2, D2); });
     EpiP2 p2;
     p2.window = b;
     p2.n = N;
     p2.npad = Npad;
     p2.l = l;
     p2.ksplit = ks2;
-    p2.F = c->d_F;
+    p2.F = Fcent;
     p2.scale = c->d_scale;
     p2.G = G;
     p2.h0 = h0;
@@ -412,7 +415,7 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     gemm.omega_changed(c, Bd, l, Npad);
     const int ks = gemm.ksplit(c, M, N);
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks * M * l * sizeof(T));
-    gemm.p1(c, c->d_bed, c->pitch, M, N, BT, l, ks, D1);
+    gemm.p1(c, c->d_bed, c->pitch, 0, M, N, BT, l, ks, D1);
     EpiP1 p1;
     p1.start = 0; p1.m = M; p1.l = l; p1.ksplit = ks;
     p1.F = c->d_F; p1.scale = c->d_scale; p1.wsum = wsum; p1.omega = Bd; p1.miss_ptr = c->d_miss_snp_ptr;
@@ -435,7 +438,7 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     gemm.b2_ready(c, B2, l, M);
     const int ks = gemm.ksplit(c, N, M);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks * N * l * sizeof(T));
-    gemm.p2(c, c->d_bedT, c->win.pitch, N, M, B2, l, ks, D2);
+    gemm.p2(c, c->d_bedT, c->win.pitch, 0, N, M, B2, l, ks, D2);
     zero(c, H, Npad * l);
     EpiP2 p2;
     p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks;
@@ -456,6 +459,7 @@ void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, i
   PG_REQUIRE(B && out && l >= 1 && l <= kLmax, PCAONE_EBADARG, "bad product operands");
   PG_REQUIRE(transpose == 0 || transpose == 1, PCAONE_EBADARG, "transpose must be 0 or 1");
   PG_REQUIRE(ploidy == 1 || ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
+  PG_REQUIRE(!c->dense, PCAONE_ESTATE, "products need packed genotypes (load_bed)");
   build_transposed(c, 1);
   build_missing_by_snp(c);
   build_missing_by_window_sample(c);
@@ -488,15 +492,29 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
   PG_REQUIRE(o.maxp >= 0, PCAONE_EBADARG, "maxp must be >= 0");
   PG_REQUIRE(o.ploidy == 1 || o.ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
   const int bands = o.svd == 1 ? 1 : o.bands;
-  build_transposed(c, bands);
-  build_missing_by_snp(c);
-  build_missing_by_window_sample(c);
-  if (c->imputed) compute_imputed_ws(c);
-  compute_scale(c, o.standardize, o.ploidy);
+  if (c->dense) {
+    // dense posterior matrix: already centred and not standardised in the EM steps; the
+    // epilogues see F = 0 and s = 2 so that G = E^T Omega and B2 = G exactly
+    set_window_layout(c, bands);
+    build_empty_missing(c);
+    std::vector<double> two(c->M, 2.0);
+    PG_CUDA(cudaMemcpyAsync(c->d_scale, two.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    PG_REQUIRE(o.precision != PCAONE_PREC_FP64, PCAONE_EBADARG, "the PCAngsd matrix is FP32");
+  } else {
+    build_transposed(c, bands);
+    build_missing_by_snp(c);
+    build_missing_by_window_sample(c);
+    if (c->imputed) compute_imputed_ws(c);
+    compute_scale(c, o.standardize, o.ploidy);
+  }
   c->gemm_ms_accum = 0.0;
   const int64_t l0 = c->launches, g0 = c->gemm_launches;
   PG_CUDA(cudaEventRecord(c->ev0, c->stream));
-  if (o.precision == PCAONE_PREC_FP64) {
+  if (c->dense) {
+    Engine<float> e(c, o, gemm_dense_float());
+    e.run(U, S, V, rep);
+  } else if (o.precision == PCAONE_PREC_FP64) {
     Engine<double> e(c, o, gemm_simt_double());
     e.run(U, S, V, rep);
   } else if (o.precision == PCAONE_PREC_FP32) {

@@ -11,10 +11,12 @@ namespace pg {
 template <typename T>
 struct GemmFnT {
   int (*ksplit)(pcaone_ctx* c, int64_t rows, int64_t K);
-  void (*p1)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K,
-             const T* B, int l, int ks, T* out);
-  void (*p2)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t K,
-             const T* B, int l, int ks, T* out);
+  // p1: rows = SNPs row0..row0+rows of the SNP-major matrix; p2: rows = samples of window
+  // `window` of the sample-major copy. `codes` points at the first row of the packed data.
+  void (*p1)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t row0, int64_t rows,
+             int64_t K, const T* B, int l, int ks, T* out);
+  void (*p2)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t window, int64_t rows,
+             int64_t K, const T* B, int l, int ks, T* out);
   void (*omega_changed)(pcaone_ctx* c, const double* omega, int l, int64_t npad);
   void (*b2_ready)(pcaone_ctx* c, const T* B2, int l, int64_t m);
 };
@@ -22,6 +24,11 @@ struct GemmFnT {
 GemmFnT<float> gemm_simt_float();
 GemmFnT<double> gemm_simt_double();
 GemmFnT<float> gemm_tc();
+GemmFnT<float> gemm_dense_float();  // dense float E (PCAngsd), kernels_gl.cu
+
+// PCAngsd device steps (kernels_gl.cu)
+void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters);
+void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool standardize, double* Dc);
 
 void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);
 void jacobi_svd(int n, const double* A, double* U, double* s, double* V);

@@ -137,3 +137,15 @@ def test_emu_matches_oracle_other_modes(gpu):
         assert it == it_o
         assert_eig_close(eig, eig_o, 1e-9)
         assert max_angle(U, U_o) < 1e-7
+
+
+@pytest.mark.parametrize("name,shuffle", [("g3_pcangsd", False), ("g3_pcangsd_shuf", True)])
+def test_pcangsd_matches_reference_golden(gpu, name, shuffle):
+    """PCAngsd (-G g3.beagle.gz -k 3 -w 8 --maxiter 30, with and without -S)."""
+    P, N, M = O.parse_beagle(os.path.join(GOLDEN, "g3.beagle.gz"))
+    eig, S, U, V, iters, F = pb.run_pcangsd(gpu, P, k=3, bands=8, maxiter=30, shuffle=shuffle)
+    np.testing.assert_allclose(F, O.em_maf(P, 30, 1e-6), rtol=1e-6)
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(U, ref_table(name, ".eigvecs"), 5e-4)
+    if not shuffle:
+        assert_cols_close(V, ref_table(name, ".loadings"), 5e-4)

@@ -52,8 +52,11 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
+_T0 = time.time()
+
+
 def log(*a):
-    print(*a, file=sys.stderr, flush=True)
+    print(f"[{time.time() - _T0:8.1f}s]", *a, file=sys.stderr, flush=True)
 
 
 def dist_env():
@@ -226,10 +229,12 @@ def run_ours(args, cfg):
     if rank == 0:
         make_data(cfg, prefix)
     barrier()
+    log("data ready")
     packed, N, M = pb.read_bed(prefix)
     bpr = (N + 3) // 4
     bed_bytes = M * bpr
     perm = pb.shuffle_perm(M) if cfg["svd"] == 2 else None
+    log("bed read into host memory")
     rs_kw = dict(k=cfg["k"], oversamples=10, maxp=cfg["maxp"], svd=cfg["svd"], bands=cfg["bands"],
                  tol=cfg["tol"], seed=101)
 
@@ -238,9 +243,11 @@ def run_ours(args, cfg):
     if perm is not None:
         ctx.permute(perm)
     prec = args.precision
+    log("loaded and permuted on the device")
     # warm-up (also builds the transposed copy and missing-entry lists once)
     for _ in range(args.warmup):
-        ctx.rsvd(precision=prec, **rs_kw)
+        r = ctx.rsvd(precision=prec, **rs_kw)
+        log(f"warm-up step: {r.gpu_ms:.1f} ms, {r.epochs} epochs, {r.kernel_launches} launches")
     barrier()
     with ClockSampler(local) as clk:
         barrier()
@@ -249,6 +256,7 @@ def run_ours(args, cfg):
             res.append(ctx.rsvd(precision=prec, **rs_kw))
         barrier()
     clocks = clk.summary()
+    log(f"timed steps: {[round(r.gpu_ms, 2) for r in res]} ms")
     step_ms = [r.gpu_ms for r in res]
     epochs = res[-1].epochs
     ms_per_step = sum(step_ms) / len(step_ms)
@@ -264,6 +272,7 @@ def run_ours(args, cfg):
 
     # one profiled run: per-launch times of the decode-GEMM kernels (roofline)
     prof = ctx.rsvd(precision=prec, profile=True, **rs_kw)
+    log(f"profiled step: gemm {prof.gemm_ms:.1f} of {prof.gpu_ms:.1f} ms over {prof.gemm_launches} launches")
     l = cfg["k"] + max(10, cfg["k"])
     alg_flops = 4.0 * M * N * l * prof.epochs  # two products per epoch, 2*M*N*l each
     gemm_avg_ms = prof.gemm_ms / max(prof.gemm_launches, 1)
@@ -290,7 +299,9 @@ def run_ours(args, cfg):
     if not args.skip_compare:
         r32 = ctx.rsvd(precision="fp32", **rs_kw)
         fp32_ms = r32.gpu_ms
+        log(f"fp32 path: {r32.gpu_ms:.1f} ms")
         r64 = ctx.rsvd(precision="fp64", **rs_kw)
+        log(f"fp64 path: {r64.gpu_ms:.1f} ms")
         e64 = r64.S ** 2
         for name, r in (("mixed" if prec == "mixed" else prec, res[-1]), ("fp32", r32)):
             e = r.S ** 2
@@ -314,6 +325,7 @@ def run_ours(args, cfg):
         if i > 0:  # first is warm-up (allocations)
             e2e_t.append(t1 - t0)
     e2e_s = sum(e2e_t) / len(e2e_t)
+    log(f"e2e steps: {[round(x, 3) for x in e2e_t]} s")
     if dist:
         import torch
 
@@ -328,6 +340,7 @@ def run_ours(args, cfg):
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu, why = run_reference_sample(cfg, prefix, workdir)
+        log(f"cpu baseline: {cpu}")
         if cpu is None:
             cpu = {"value": None, "unavailable": why}
     ctx.close()

@@ -66,7 +66,8 @@ std::string date() {
 
 // ------------------------------------------------------------------ options (src/Cmd.cpp)
 struct Params {
-  std::string bfile, fileout = "pcaone";
+  std::string bfile, beagle, fileout = "pcaone";
+  double tolmaf = 1e-6;
   int svd = 2;
   unsigned k = 10, maxp = 20, bands = 64, oversamples = 10, rand = 1, verbose = 1, threads = 12;
   int seed = 101, scale = -1;
@@ -83,11 +84,11 @@ struct Params {
 };
 
 const std::set<std::string> kUnsupported = {
-    "-c", "--csv", "-g", "--bgen", "-G", "--beagle", "-B", "--binary", "--pcangsd",
+    "-c", "--csv", "-g", "--bgen", "-B", "--binary",
     "-D", "--ld", "--ld-r2", "--ld-stats", "--clump",
     "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
     "--inbreed", "--USV", "--read-V", "--read-S", "--M", "--N",
-    "--scale-factor", "--buffer", "--imaxiter", "--itol", "--ncv", "--tol-maf"};
+    "--scale-factor", "--buffer", "--imaxiter", "--itol", "--ncv"};
 
 void usage() {
   std::cout << "PCAone (B200 build)\n"
@@ -147,6 +148,9 @@ Params parse(int argc, char** argv) {
       usage();
       std::exit(EXIT_SUCCESS);
     } else if (a == "-b" || a == "--bfile") p.bfile = next();
+    else if (a == "-G" || a == "--beagle") p.beagle = next();
+    else if (a == "--pcangsd") {}  // implied by Beagle input (src/Cmd.cpp:205)
+    else if (a == "--tol-maf") p.tolmaf = num(next());
     else if (a == "-o" || a == "--out") p.fileout = next();
     else if (a == "-k" || a == "--pc") p.k = (unsigned)num(next());
     else if (a == "-d" || a == "--svd") p.svd = (int)num(next());
@@ -187,7 +191,7 @@ Params parse(int argc, char** argv) {
       std::exit(EXIT_FAILURE);
     }
   }
-  if (p.bfile.empty()) fail("no input: use -b/--bfile");
+  if (p.bfile.empty() && p.beagle.empty()) fail("no input: use -b/--bfile or -G/--beagle");
   if (p.svd != 1 && p.svd != 2) fail("--svd must be 1 or 2 in this build");
   if (p.bands < 4 || p.bands % 2 != 0) fail("the -w/--batches must be a power of 2 and the minimun is 4.");
   if (p.maf > 0.5) {
@@ -342,6 +346,153 @@ int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M) {
   return 0;
 }
 
+// ---------------------------------------------------------------- PCAngsd (Beagle input)
+// parse_beagle_file (src/Utils.cpp:377-405): header gives N = columns/3 - 1; each site line
+// holds marker, allele1, allele2 and three likelihoods per sample, of which the first two
+// are used. Lines are parsed in parallel after the whole gz file is inflated.
+std::vector<double> read_beagle(const std::string& path, size_t& N, size_t& M) {
+  gzFile gz = gzopen(path.c_str(), "rb");
+  if (!gz) fail("can not open " + path);
+  std::string text;
+  std::vector<char> buf(1 << 24);
+  int n;
+  while ((n = gzread(gz, buf.data(), (unsigned)buf.size())) > 0) text.append(buf.data(), n);
+  gzclose(gz);
+  std::vector<size_t> starts;
+  size_t b = 0;
+  while (b < text.size()) {
+    starts.push_back(b);
+    size_t e = text.find('\n', b);
+    if (e == std::string::npos) e = text.size();
+    b = e + 1;
+  }
+  if (starts.size() < 2) fail("the Beagle file has no sites");
+  {
+    std::string head = text.substr(starts[0], (starts.size() > 1 ? starts[1] - 1 : text.size()) - starts[0]);
+    size_t cols = 0;
+    std::istringstream hs(head);
+    std::string t;
+    while (hs >> t) ++cols;
+    if (cols % 3) fail("Number of columns should be a multiple of 3.");
+    N = cols / 3 - 1;
+  }
+  M = starts.size() - 1;
+  std::vector<double> P(2 * N * M);
+  bool bad = false;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (long j = 0; j < (long)M; ++j) {
+    const char* q = text.data() + starts[j + 1];
+    char* end = nullptr;
+    for (int f = 0; f < 3; ++f) {  // marker, allele1, allele2
+      while (*q == ' ' || *q == '\t') ++q;
+      while (*q && *q != ' ' && *q != '\t' && *q != '\n') ++q;
+    }
+    for (size_t i = 0; i < N; ++i) {
+      double v[3];
+      for (int f = 0; f < 3; ++f) {
+        v[f] = std::strtod(q, &end);
+        if (end == q) {
+          bad = true;
+          v[f] = 0;
+        }
+        q = end;
+      }
+      P[(size_t)j * 2 * N + 2 * i] = v[0];
+      P[(size_t)j * 2 * N + 2 * i + 1] = v[1];
+    }
+  }
+  if (bad) fail("something wrong parsing beagle");
+  return P;
+}
+
+int run_pcangsd(const Params& p, std::chrono::steady_clock::time_point t_start) {
+  g_log.print(date(), "start parsing BEAGLE format");
+  size_t N = 0, M = 0;
+  std::vector<double> P = read_beagle(p.beagle, N, M);
+  g_log.print(date(), "N (# samples):", N, ", M (# SNPs):", M);
+  if (p.k + p.oversamples > N) fail("k + oversamples must not exceed the number of samples");
+  const bool perm_on = p.svd == 2 && !p.noshuffle;
+  std::vector<int32_t> perm(M);
+  if (perm_on) pcaone_shuffle_perm(M, perm.data());
+  else for (size_t j = 0; j < M; ++j) perm[j] = (int32_t)j;
+  std::vector<double> Pp(P.size());  // sites in the RSVD's column order
+  for (size_t j = 0; j < M; ++j) std::memcpy(&Pp[j * 2 * N], &P[(size_t)perm[j] * 2 * N], 2 * N * sizeof(double));
+  pcaone_ctx* ctx = nullptr;
+  if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
+  check(ctx, pcaone_gpu_load_gl(ctx, Pp.data(), M, (uint32_t)N), "load_gl");
+  g_log.print(date(), "begin to estimate allele frequencies");
+  int fit = 0;
+  check(ctx, pcaone_gpu_gl_freq(ctx, (int)p.maxiter, p.tolmaf, nullptr, &fit), "gl_freq");
+  g_log.print(date(), fit < (int)p.maxiter ? "EM (MAF) converged at iteration:" : "EM (MAF) did not converge", fit);
+  check(ctx, pcaone_gpu_gl_update(ctx, nullptr, nullptr, nullptr, 0), "gl_update");
+  pcaone_rsvd_opts o{};
+  o.k = (int)p.k;
+  o.oversamples = (int)p.oversamples;
+  o.maxp = (int)p.maxp;
+  o.svd = p.svd;
+  o.bands = (int)p.bands;
+  o.precision = PCAONE_PREC_FP32;  // the posterior matrix is dense FP32
+  o.standardize = 0;
+  o.ploidy = 2;
+  o.seed = p.seed;
+  o.rand = (int)p.rand;
+  o.tol = p.tol;
+  o.verbose = p.verbose > 0;
+  std::vector<double> U(N * p.k), S(p.k), V(M * p.k), Vpre, Vuse(M * p.k);
+  pcaone_rsvd_report rep{};
+  check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+  g_log.print(date(), "run EM-PCA. maxiter =", p.maxiter);
+  o.carry_window_state = 1;
+  for (unsigned it = 0; it < p.maxiter; ++it) {
+    Vpre = V;
+    // reference index semantics after the shuffle: position j is predicted from loading row
+    // perm[j] (src/Data.cpp:249-270 indexes P, F and V^T by the permuted column)
+    for (unsigned t = 0; t < p.k; ++t)
+      for (size_t j = 0; j < M; ++j) Vuse[t * M + j] = p.fix_index ? V[t * M + j] : V[t * M + perm[j]];
+    check(ctx, pcaone_gpu_gl_update(ctx, U.data(), S.data(), Vuse.data(), p.k), "gl_update");
+    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+    double acc = 0;
+    for (unsigned b2 = 0; b2 < p.k; ++b2) {
+      double nrm = 0;
+      for (unsigned a = 0; a < p.k; ++a) {
+        double d = 0;
+        for (size_t j = 0; j < M; ++j) d += V[a * M + j] * Vpre[b2 * M + j];
+        nrm += d * d;
+      }
+      acc += std::sqrt(nrm);
+    }
+    const double diff = 1.0 - acc / p.k;
+    g_log.print(date(), "individual allele frequencies estimated iter =", it + 1, ", diff =", diff);
+    if (diff < p.tolem) {
+      g_log.print(date(), "come to convergence!");
+      break;
+    }
+  }
+  pcaone_gpu_destroy(ctx);
+  std::vector<double> Vo(V.size());
+  for (size_t j = 0; j < M; ++j)
+    for (unsigned c = 0; c < p.k; ++c) Vo[c * M + perm[j]] = V[c * M + j];
+  std::ofstream outs(p.fileout + ".sigvals"), oute(p.fileout + ".eigvals"), outu(p.fileout + ".eigvecs");
+  outs << '#' << N << ',' << M << '\n';
+  write_matrix(outs, S.data(), p.k, 1);
+  outs << '\n';
+  std::vector<double> E(p.k);
+  for (unsigned c = 0; c < p.k; ++c) E[c] = S[c] * S[c] / (double)M * 2;
+  write_matrix(oute, E.data(), p.k, 1);
+  oute << '\n';
+  write_matrix(outu, U.data(), N, p.k);
+  outu << '\n';
+  if (p.printv) {
+    std::ofstream ov(p.fileout + ".loadings");
+    write_matrix(ov, Vo.data(), M, p.k);
+    ov << '\n';
+  }
+  g_log.print(date(), "eigen vectors and values saved");
+  double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  g_log.print(date(), "total elapsed wall time:", wall, " seconds");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   Params p = parse(argc, argv);
   auto t_start = std::chrono::steady_clock::now();
@@ -355,6 +506,7 @@ int main(int argc, char** argv) {
     g_log.print("PCAone (B200 build)\nOptions in effect:\n" + p.cmdline);
   }
   g_log.print(date(), "program started");
+  if (!p.beagle.empty()) return run_pcangsd(p, t_start);
   g_log.print(date(), "start parsing PLINK format");
   const size_t N = count_lines(p.bfile + ".fam"), M0 = count_lines(p.bfile + ".bim");
   g_log.print(date(), "N (# samples):", N, ", M (# SNPs):", M0);

@@ -108,3 +108,12 @@ def test_cli_ld_flow_a_matches_reference(tmp_path):
     assert [x[:6] for x in got] == [x[:6] for x in ref]
     diff = np.abs(np.array([float(x[6]) for x in got]) - np.array([float(x[6]) for x in ref]))
     assert diff.max() <= 1.01e-6  # 6 printed decimals; the r2 values agree to 1e-5 or better
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["g3_pcangsd", "g3_pcangsd_shuf"])
+def test_cli_pcangsd_matches_reference_outputs(tmp_path, name):
+    run_cli(golden_args(name, tmp_path), tmp_path)
+    out = str(tmp_path / name)
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table(name, ".eigvals")[:, 0], 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table(name, ".eigvecs"), 5e-4)

@@ -401,6 +401,27 @@ def run_reference_arm(args, cfg):
                 "d2h_bytes_per_step": 0}}), flush=True)
 
 
+def run_profile_kernel(args, cfg):
+    """Smallest command for ncu: one standardised product Z^T Omega through the C ABI on the
+    configured matrix (the mixed path launches the tcgen05 decode-GEMM once), then exit. No
+    child processes, no torch."""
+    import pcaone_b200 as pb
+
+    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
+    os.makedirs(workdir, exist_ok=True)
+    prefix = os.path.join(workdir, args.config)
+    make_data(cfg, prefix)
+    packed, N, M = pb.read_bed(prefix)
+    l = cfg["k"] + max(10, cfg["k"])
+    B = pb.omega(101, N, l)
+    with pb.GpuContext(0) as ctx:
+        ctx.load_bed(packed, N)
+        for _ in range(args.steps):
+            out = ctx.product_t(B, precision=args.precision)
+    print(json.dumps({"profile_kernel": args.precision, "samples": N, "snps": M, "l": l,
+                      "checksum": float(np.abs(out).sum())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,9 +432,13 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-compare", action="store_true")
+    ap.add_argument("--profile-kernel", action="store_true",
+                    help="run --steps products Z^T Omega only (a small command for ncu)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
-    if args.impl == "reference":
+    if args.profile_kernel:
+        run_profile_kernel(args, cfg)
+    elif args.impl == "reference":
         run_reference_arm(args, cfg)
     else:
         run_ours(args, cfg)

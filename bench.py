@@ -272,7 +272,8 @@ def run_ours(args, cfg):
 
     # one profiled run: per-launch times of the decode-GEMM kernels (roofline)
     prof = ctx.rsvd(precision=prec, profile=True, **rs_kw)
-    log(f"profiled step: gemm {prof.gemm_ms:.1f} of {prof.gpu_ms:.1f} ms over {prof.gemm_launches} launches")
+    log(f"profiled step: gemm {prof.gemm_ms:.1f} of {prof.gpu_ms:.1f} ms over {prof.gemm_launches} launches; "
+        f"epilogue {prof.epilogue_ms:.1f}, updates {prof.update_ms:.1f}, epoch tail {prof.tail_ms:.1f}")
     l = cfg["k"] + max(10, cfg["k"])
     alg_flops = 4.0 * M * N * l * prof.epochs  # two products per epoch, 2*M*N*l each
     gemm_avg_ms = prof.gemm_ms / max(prof.gemm_launches, 1)
@@ -291,7 +292,10 @@ def run_ours(args, cfg):
                 "launches": prof.gemm_launches, "avg_launch_ms": round(gemm_avg_ms, 5),
                 "algorithmic_flops_per_launch": alg_flops / max(prof.gemm_launches, 1),
                 "issued_flops_factor": 2.0 if prec == "mixed" else 1.0,
-                "gemm_share_of_step": round(prof.gemm_ms / prof.gpu_ms, 4)}
+                "gemm_share_of_step": round(prof.gemm_ms / prof.gpu_ms, 4),
+                "step_breakdown_ms": {"gemm": round(prof.gemm_ms, 2), "epilogues": round(prof.epilogue_ms, 2),
+                                      "omega_updates": round(prof.update_ms, 2),
+                                      "epoch_tail": round(prof.tail_ms, 2), "total": round(prof.gpu_ms, 2)}}
 
     # comparison runs: the plain FP32 GPU path and the FP64 algorithm-matched path
     acc = {}

@@ -108,9 +108,12 @@ typedef struct {
   int32_t omega_updates; /* Omega re-orthonormalisations performed */
   double last_diff;      /* last 1 - mev(U, Upre) */
   double gpu_ms;         /* device time of the whole call (CUDA events) */
-  double gemm_ms;        /* device time inside the decode-GEMM kernels */
+  double gemm_ms;        /* device time inside the decode-GEMM kernels (with opts.profile) */
   int64_t kernel_launches;
   int64_t gemm_launches;
+  double epilogue_ms;    /* with opts.profile: centring/sparse epilogues and B-operand packing */
+  double update_ms;      /* with opts.profile: Omega re-orthonormalisations (QR, signs, flip) */
+  double tail_ms;        /* with opts.profile: per-epoch QR of G, B, small SVD, mev */
 } pcaone_rsvd_report;
 
 /* Run Halko (svd=1) or window-based (svd=2) RSVD on the loaded genotypes: the epoch loop of

@@ -51,7 +51,8 @@ class RsvdReport(ctypes.Structure):
     _fields_ = [("epochs", ctypes.c_int32), ("omega_updates", ctypes.c_int32),
                 ("last_diff", ctypes.c_double), ("gpu_ms", ctypes.c_double),
                 ("gemm_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64),
-                ("gemm_launches", ctypes.c_int64)]
+                ("gemm_launches", ctypes.c_int64), ("epilogue_ms", ctypes.c_double),
+                ("update_ms", ctypes.c_double), ("tail_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -121,6 +122,9 @@ class RsvdResult:
     gemm_ms: float
     kernel_launches: int
     gemm_launches: int
+    epilogue_ms: float = 0.0
+    update_ms: float = 0.0
+    tail_ms: float = 0.0
 
 
 class GpuContext:
@@ -198,7 +202,8 @@ class GpuContext:
                                           _ptr(V), ctypes.byref(rep)))
         return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
                           rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
-                          rep.kernel_launches, rep.gemm_launches)
+                          rep.kernel_launches, rep.gemm_launches, rep.epilogue_ms,
+                          rep.update_ms, rep.tail_ms)
 
 
 def _product(ctx: "GpuContext", B: np.ndarray, transpose: int, precision, standardize, ploidy):

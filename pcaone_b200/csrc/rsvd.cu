@@ -185,8 +185,10 @@ struct Engine {
     p1.G = G;
     T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
     double* h0 = (double*)scratch(c, "r_h0", l * 8);
-    launch_prep<T>(c, p1, D1, B2, h0);
-    gemm.b2_ready(c, B2, l, m);
+    timed([&] {
+      launch_prep<T>(c, p1, D1, B2, h0);
+      gemm.b2_ready(c, B2, l, m);
+    }, 1);
     // product 2: D2 = R_b B2
     int ks2 = gemm.ksplit(c, N, m);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
@@ -206,7 +208,7 @@ struct Engine {
     p2.miss_idx = c->d_miss_ws_idx;
     p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
     p2.H = Ht;
-    launch_accum<T>(c, p2, D2);
+    timed([&] { launch_accum<T>(c, p2, D2); }, 1);
   }
 
   int bandsize = 1;
@@ -215,13 +217,17 @@ struct Engine {
   // With opts.profile, bracket each decode-GEMM launch with CUDA events on the launching
   // stream; the elapsed times are summed into gemm_ms after each epoch.
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+  std::vector<int> ev_cat;
   size_t ev_used = 0;
+  double cat_ms[4] = {0, 0, 0, 0};
   template <typename F>
-  void timed(F&& f) {
+  void timed(F&& f, int cat = 0) {
     if (!o.profile) {
       f();
       return;
     }
+    if (ev_cat.size() <= ev_used) ev_cat.resize(ev_used + 1);
+    ev_cat[ev_used] = cat;
     if (ev_used == evs.size()) {
       cudaEvent_t a, b;
       PG_CUDA(cudaEventCreate(&a));
@@ -239,7 +245,8 @@ struct Engine {
     for (size_t i = 0; i < ev_used; ++i) {
       float ms = 0.f;
       PG_CUDA(cudaEventElapsedTime(&ms, evs[i].first, evs[i].second));
-      c->gemm_ms_accum += ms;
+      cat_ms[ev_cat[i]] += ms;
+      if (ev_cat[i] == 0) c->gemm_ms_accum += ms;
     }
     ev_used = 0;
   }
@@ -254,7 +261,7 @@ struct Engine {
     if (pi == 0)
       init_omega();
     else {
-      update_omega(H);
+      timed([&] { update_omega(H); }, 2);
       updates++;
     }
     zero(c, H, Npad * l);
@@ -275,8 +282,10 @@ struct Engine {
       const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) && std::pow(2.0, pi) < bands;
       if ((b + 1) < bandsize && !adjacent) continue;
       if (!((i == bandsize) || (i == bandsize / 2) || adjacent)) continue;
-      add(c, H1, H2, Npad * l, H);
-      update_omega(H);
+      timed([&] {
+        add(c, H1, H2, Npad * l, H);
+        update_omega(H);
+      }, 2);
       updates++;
       if (i == bandsize) {
         zero(c, H1, Npad * l);
@@ -320,9 +329,11 @@ struct Engine {
       else
         epoch_winsvd(pi);
       // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B)
-      cholqr2(c, G, l, M, G, Rg, d_status);
-      trsm_right_upper(c, H, Rg, l, N, Tb);
-      cholqr2(c, Tb, l, N, Tb, Rb, d_status);
+      timed([&] {
+        cholqr2(c, G, l, M, G, Rg, d_status);
+        trsm_right_upper(c, H, Rg, l, N, Tb);
+        cholqr2(c, Tb, l, N, Tb, Rb, d_status);
+      }, 3);
       PG_CUDA(cudaMemcpyAsync(rb.data(), Rb, rb.size() * 8, cudaMemcpyDeviceToHost, c->stream));
       check_status();
       collect_times();
@@ -382,6 +393,9 @@ struct Engine {
       rep->epochs = epochs;
       rep->omega_updates = updates;
       rep->last_diff = diff;
+      rep->epilogue_ms = cat_ms[1];
+      rep->update_ms = cat_ms[2];
+      rep->tail_ms = cat_ms[3];
     }
   }
 };

@@ -69,7 +69,7 @@ def test_cli_maf_filter(tmp_path):
     assert O.count_lines(str(tmp_path / "maf.mbim")) == len(keep)
     sub = O.Bed(bed.N, len(keep), bed.packed[keep])
     eig, *_ = O.run_pca(sub, k=3, svd=1, maxp=4)
-    assert_eig_close(O.read_table(str(tmp_path / "maf.eigvals"))[:, 0], eig, 1e-6)
+    assert_eig_close(O.read_table(str(tmp_path / "maf.eigvals"))[:, 0], eig, 1e-5)  # 6 printed digits
 
 
 def test_cli_rejects_unknown_option(tmp_path):

@@ -179,6 +179,23 @@ int pcaone_gpu_gl_freq(pcaone_ctx* ctx, int maxiter, double tolmaf, double* F, i
 int pcaone_gpu_gl_update(pcaone_ctx* ctx, const double* U, const double* S, const double* V,
                          uint32_t k);
 
+/* Allocation-free Z^T B for callers that cannot let a library call cudaMalloc: code running
+ * inside another framework's device memory pool, or an outer solver loop that must not
+ * allocate per call (e.g. an eigensolver using this product as its operator). It has no
+ * counterpart in the reference. Same result as pcaone_gpu_product(ctx, PCAONE_PREC_FP32,
+ * 0, standardize, ploidy, ...) but B (nsamples x ncols) and out (nsnps x ncols) are
+ * column-major FP64 DEVICE buffers owned by the caller, and the call allocates nothing: its
+ * scratch is one fixed 64 MiB device array inside the library (held by every GPU that loads
+ * the library until exit). Problems needing more than that (nsamples*ncols*12 +
+ * nsnps*ncols*4 bytes plus alignment) are rejected with PCAONE_EBADARG. The matrix must be
+ * loaded and pcaone_gpu_product or pcaone_gpu_rsvd must have been called on it once (that
+ * builds the missing-genotype list; PCAONE_ESTATE otherwise). The first call on a device
+ * resolves the array's device address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture. All calls share the array and overwrite what they use; calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int pcaone_gpu_product_t_noalloc(pcaone_ctx* ctx, int standardize, int ploidy, const double* B,
+                                 uint32_t ncols, double* out);
+
 #ifdef __cplusplus
 }
 #endif

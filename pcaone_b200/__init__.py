@@ -28,7 +28,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
-           "pcaone_gpu_gl_update"]
+           "pcaone_gpu_gl_update", "pcaone_gpu_product_t_noalloc"]
 
 
 class PcaoneError(RuntimeError):
@@ -86,6 +86,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
+        L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
         _lib = L
@@ -283,6 +284,14 @@ def _gl_update(self, U=None, S=None, V=None):
     self._check(lib().pcaone_gpu_gl_update(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(S)))
 
 
+def _product_t_noalloc(self, d_B: int, ncols: int, d_out: int, standardize=True, ploidy=2):
+    """Allocation-free Z^T B on caller-owned device buffers (raw device addresses of column-major
+    FP64 nsamples x ncols B and nsnps x ncols out); see pcaone_gpu_product_t_noalloc."""
+    self._check(lib().pcaone_gpu_product_t_noalloc(self._h, int(standardize), ploidy,
+                                                   ctypes.c_void_p(d_B), ncols, ctypes.c_void_p(d_out)))
+
+
+GpuContext.product_t_noalloc = _product_t_noalloc
 GpuContext.load_gl = _load_gl
 GpuContext.gl_freq = _gl_freq
 GpuContext.gl_update = _gl_update

@@ -66,6 +66,8 @@ void free_all(pcaone_ctx* c) {
   free_data(c);
   for (auto& kv : c->bufs) free_ptr(kv.second.p);
   c->bufs.clear();
+  c->bt2_shape = -1;
+  c->bt2_ptr = nullptr;
 }
 
 }  // namespace pg

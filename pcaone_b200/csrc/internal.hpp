@@ -117,6 +117,9 @@ struct pcaone_ctx {
   // key (N, l, bands, data generation) of the winSVD window sums kept between calls
   uint64_t h12_key = 0;
   uint64_t generation = 0;  // bumped by every load / permutation
+  // shape key and address of the zeroed split-BF16 window operand (tensor-core back end)
+  int64_t bt2_shape = -1;
+  void* bt2_ptr = nullptr;
 
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;

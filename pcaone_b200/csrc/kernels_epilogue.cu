@@ -19,6 +19,57 @@ namespace pg {
 
 namespace {
 
+// Position of code index k inside its 64-code chunk in the tcgen05 decode order
+// (kernels_gemm_tc.cu, decode_word): code c -> 2 * (8q + 2p + half) + h.
+__device__ __forceinline__ int64_t tc_pos(int64_t k) {
+  const int c = (int)(k & 63), q = c >> 4, r16 = c & 15;
+  return (k & ~(int64_t)63) + 2 * (8 * q + 2 * (r16 & 3) + (r16 >> 3)) + ((r16 >> 2) & 1);
+}
+
+// Warp-cooperative sparse gather: acc_c += sum_{e in [e0, e1)} w_e * rows[idx_e][c] for the
+// lane's columns c = lane and lane + 32 (l <= 64), summed in entry order. The warp loads 32
+// entries (index and weight) at once, then broadcasts them and keeps four row loads in flight,
+// so the cost is a few L2 latencies per 32 entries instead of two per entry.
+template <typename Wt>
+__device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
+                                            const double* __restrict__ rows, int l, Wt weight,
+                                            double& acc0, double& acc1) {
+  const int lane = threadIdx.x & 31;
+  const bool c0 = lane < l, c1 = lane + 32 < l;
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    int my_i = 0;
+    double my_w = 0.0;
+    if (e < e1) {
+      my_i = idx[e];
+      my_w = weight(e, my_i);
+    }
+    const int cnt = (int)(e1 - base < 32 ? e1 - base : 32);
+    for (int t = 0; t < cnt; t += 4) {
+      int it[4];
+      double wt[4], v0[4], v1[4];
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        it[g] = __shfl_sync(0xffffffffu, my_i, (t + g) & 31);
+        wt[g] = __shfl_sync(0xffffffffu, my_w, (t + g) & 31);
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const double* r = rows + (int64_t)it[g] * l;
+        const bool ok = t + g < cnt;
+        v0[g] = (ok && c0) ? r[lane] : 0.0;
+        v1[g] = (ok && c1) ? r[lane + 32] : 0.0;
+      }
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+        if (t + g < cnt) {
+          acc0 += wt[g] * v0[g];
+          acc1 += wt[g] * v1[g];
+        }
+    }
+  }
+}
+
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
 // per-CTA partials of h0.
 template <typename T>
@@ -32,18 +83,35 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
     const double F = p.F[j];
     const double s = p.scale[j];
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
+    double sp0 = 0.0, sp1 = 0.0;
+    const double* mv = p.miss_val;
+    gather_rows(e0, e1, p.miss_idx, p.omega, p.l,
+                [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; }, sp0, sp1);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * p.m + jl) * p.l + c];
-      double sparse = 0.0;
-      for (int64_t e = e0; e < e1; ++e) {
-        double ev = p.miss_val ? p.miss_val[e] : 0.0;
-        sparse += (ev + F) * p.omega[(int64_t)p.miss_idx[e] * p.l + c];
-      }
+      const double sparse = c < 32 ? sp0 : sp1;
       double g = s * (0.5 * d - F * p.wsum[c] + sparse);
       p.G[j * p.l + c] = g;
-      B2[jl * p.l + c] = (T)(0.5 * s * g);
+      const T b2 = (T)(0.5 * s * g);
+      if (p.bt2) {
+        const float x = (float)b2;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const int64_t kp = tc_pos(jl);
+        p.bt2[(int64_t)c * p.kpad2 + kp] = hi;
+        p.bt2[(int64_t)(p.bt_half + c) * p.kpad2 + kp] = __float2bfloat16_rn(x - __bfloat162float(hi));
+      } else {
+        B2[jl * p.l + c] = b2;
+      }
       sh0[warp * p.l + c] += s * F * g;
+    }
+  }
+  if (p.bt2) {  // positions m..kpad2 of the split operand: zero (a shorter window follows a longer one)
+    const int64_t tail = p.kpad2 - p.m, tot = tail * 2 * p.l;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t r = t / tail, jl = p.m + (t - r * tail);
+      const int64_t row = r < p.l ? r : p.bt_half + (r - p.l);
+      p.bt2[row * p.kpad2 + tc_pos(jl)] = __float2bfloat16_rn(0.0f);
     }
   }
   __syncthreads();
@@ -94,15 +162,15 @@ __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
   for (int64_t i = (int64_t)blockIdx.x * nwarps + warp; i < p.n; i += (int64_t)gridDim.x * nwarps) {
     const int64_t row = (int64_t)p.window * p.npad + i;
     const int64_t e0 = p.miss_ptr[row], e1 = p.miss_ptr[row + 1];
+    double sp0 = 0.0, sp1 = 0.0;
+    const double* mv = p.miss_val;
+    const double *sc = p.scale, *F = p.F;
+    gather_rows(e0, e1, p.miss_idx, p.G, p.l,
+                [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); }, sp0, sp1);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D2[((int64_t)sp * p.n + i) * p.l + c];
-      double sparse = 0.0;
-      for (int64_t e = e0; e < e1; ++e) {
-        int64_t j = p.miss_idx[e];
-        double ev = p.miss_val ? p.miss_val[e] : 0.0;
-        sparse += p.scale[j] * (ev + p.F[j]) * p.G[j * p.l + c];
-      }
+      const double sparse = c < 32 ? sp0 : sp1;
       p.H[i * p.l + c] += d - p.h0[c] + sparse;
     }
   }

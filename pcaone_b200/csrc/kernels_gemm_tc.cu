@@ -7,21 +7,32 @@
 // core accumulates in FP32 in tensor memory. The epilogue kernels (kernels_epilogue.cu) then
 // add the rank-1 centring term and the sparse missing-entry term in FP64.
 //
-// One CTA owns a 128-row tile and one K split. Per 64-code K chunk:
-//   * warp 4 (producer) TMA-loads the packed 2-bit codes of the 128 rows (128 x 16 bytes) and
-//     the B chunk (NP rows x 64 K, BF16, 128B swizzle) into a shared-memory stage;
+// Work split (stream-K): the units are (128-row tile, 64-code K chunk) pairs in tile-major
+// order, and CTA j of G owns units [j U / G, (j+1) U / G). A CTA therefore covers one or more
+// contiguous K ranges ("segments") of one or two tiles; segment q of a tile writes its FP32
+// partial sums to output slot q, and the CTA holding a tile's last chunk zero-fills the slots
+// that tile does not use, so every row has exactly `ks` slots summed by the epilogue in a
+// fixed order (deterministic, no atomics). The grid is two CTAs per SM.
+//
+// Roles (10 warps):
+//   * warp 4 (producer) TMA-loads per unit the packed 2-bit codes of the 128 rows (128 x 16
+//     bytes) and the B chunk (NP rows x 64 K, BF16, 128B swizzle) into a shared-memory ring of
+//     kStages(NP) stages;
 //   * warps 0-3 (decoders) each own 32 rows = the 32 TMEM lanes of their sub-partition: a
 //     thread decodes its row's 64 codes in registers (PRMT table lookup) into 32 BF16 pairs
-//     and writes them with tcgen05.st to the stage's 32 TMEM columns (A operand in TMEM);
-//   * warp 5 (MMA) issues four 128 x NP x 16 tcgen05.mma (A from TMEM, B from shared memory)
-//     accumulating in TMEM, and tcgen05.commit frees the stage.
+//     and writes them with tcgen05.st into one of kAStages TMEM A stages (A operand in TMEM);
+//   * warp 5 (MMA) issues four 128 x NP x 16 tcgen05.mma per unit (A from TMEM, B from shared
+//     memory) into one of two TMEM accumulators (one when NP > 64), and tcgen05.commit frees
+//     the shared-memory stage and the TMEM A stage;
+//   * warps 6-9 (readout) move a finished accumulator to registers with tcgen05.ld, free it
+//     for the next segment and store hi + lo sums to the segment's output slot.
 // B is [B_hi | B_lo] stacked along N (NP = round_up(2l, 16) columns) so each A tile is read
 // by the tensor core once for both halves. The decode emits K pairs in a fixed permuted
 // order inside each 64-code chunk; the B operand is written in the same order.
 //
 // Every mbarrier wait is bounded (about one second of %globaltimer); on timeout the CTA sets
-// an error flag, stops issuing work, waits (bounded) for its copies in flight, frees its
-// tensor memory and returns, and the host reports PCAONE_ETIMEOUT.
+// an error flag, stops issuing work, waits (bounded) for its copies and MMAs in flight, frees
+// its tensor memory and returns, and the host reports PCAONE_ETIMEOUT.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -37,11 +48,20 @@ namespace {
 
 constexpr int kTileRows = 128;
 constexpr int kChunk = 64;        // codes per K chunk (16 packed bytes per row)
-constexpr int kStages = 4;
-constexpr int kThreads = 192;     // 4 decoder warps + producer + MMA
-constexpr int kTmemCols = 256;    // accumulator in [0, NP), A stages from column 128
+constexpr int kAStages = 4;       // decoded A tiles in TMEM
+constexpr int kThreads = 320;     // 4 decoder warps + producer + MMA + 4 readout warps
+constexpr int kTmemCols = 256;    // accumulators in [0, 128), A stages in [128, 256)
 constexpr int kAColBase = 128;
+constexpr int kMinUnitsPerCta = 8;
 constexpr uint64_t kWaitNs = 1000000000ull;  // bounded waits: 1 s
+
+// Shared-memory ring depth for NP accumulator columns: about 104 KB of stages, so two CTAs
+// (and their 2 x 256 TMEM columns) fit on one SM and a third cannot become resident.
+__host__ __device__ constexpr int ring_stages(int np) {
+  return (104 * 1024) / (np * kChunk * 2 + kTileRows * 16) < 16 ? (104 * 1024) / (np * kChunk * 2 + kTileRows * 16)
+                                                                 : 16;
+}
+__host__ __device__ constexpr int acc_bufs(int np) { return np <= 64 ? 2 : 1; }
 
 // ------------------------------------------------------------------ PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -90,6 +110,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
       }
     }
   }
+}
+// Bounded wait that ignores the abort flag: used to drain copies and MMAs in flight.
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = globaltimer();
+  while (!mbar_try(bar, parity))
+    if (globaltimer() - t0 > kWaitNs) return;
 }
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
                                             uint32_t bar) {
@@ -141,6 +167,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr)
       : "memory");
 }
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
+}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -168,46 +200,66 @@ __device__ __forceinline__ void decode_word(uint32_t w, uint32_t* o) {
 }
 
 struct TcArgs {
-  int64_t rows;              // valid rows (outputs written for r < rows)
-  int64_t kchunks_total;     // K chunks of the whole problem
-  int64_t kchunks_per_split;
+  int64_t rows;    // valid rows (outputs written for r < rows)
+  int64_t chunks;  // K chunks (C)
+  int64_t units;   // tiles x C
+  int grid;        // CTAs (G)
+  int ks;          // output slots per row
   int l;
-  float* out;                // [split][rows][l]
+  float* out;      // [ks][rows][l]
   int* err;
 };
+
+__device__ __forceinline__ int64_t unit_begin(int64_t j, const TcArgs& a) { return j * a.units / a.grid; }
+// The CTA whose unit range holds unit x.
+__device__ __forceinline__ int64_t cta_of_unit(int64_t x, const TcArgs& a) {
+  return ((x + 1) * a.grid + a.units - 1) / a.units - 1;
+}
 
 template <int NP>
 __global__ void __launch_bounds__(kThreads, 2)
 k_decode_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  TcArgs args) {
+  constexpr int S = ring_stages(NP);
+  constexpr int T = kAStages;
+  constexpr int NACC = acc_bufs(NP);
   constexpr uint32_t kBStageBytes = NP * kChunk * 2;  // NP rows x 128 bytes
   constexpr uint32_t kAStageBytes = kTileRows * 16;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte alignment for the 128B-swizzled B stages
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sB = smem;                                  // kStages x kBStageBytes
-  uint8_t* sA = smem + kStages * kBStageBytes;         // kStages x kAStageBytes
-  uint64_t* bars = (uint64_t*)(sA + kStages * kAStageBytes);
-  uint64_t* tma_full = bars;                 // [kStages]
-  uint64_t* dec_full = bars + kStages;       // [kStages]
-  uint64_t* empty = bars + 2 * kStages;      // [kStages]
-  uint64_t* acc_full = bars + 3 * kStages;   // [1]
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(bars + 3 * kStages + 1);
-  volatile int* abort_flag = (volatile int*)(bars + 3 * kStages + 2);
+  uint8_t* sB = smem;                          // S x kBStageBytes
+  uint8_t* sA = smem + S * kBStageBytes;       // S x kAStageBytes
+  uint64_t* bars = (uint64_t*)(sA + S * kAStageBytes);
+  uint64_t* tma_full = bars;                   // [S]  TMA landed
+  uint64_t* empty = bars + S;                  // [S]  MMA done with the ring stage
+  uint64_t* dec_full = bars + 2 * S;           // [T]  A tile decoded into TMEM
+  uint64_t* tfree = bars + 2 * S + T;          // [T]  MMA done with the TMEM A stage
+  uint64_t* acc_full = bars + 2 * S + 2 * T;   // [2]  accumulator complete
+  uint64_t* acc_empty = acc_full + 2;          // [2]  accumulator read out
+  uint64_t* done = acc_full + 4;               // [1]  every MMA of this CTA complete
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(acc_full + 5);
+  volatile int* abort_flag = (volatile int*)(acc_full + 6);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t kc0 = (int64_t)blockIdx.y * args.kchunks_per_split;
-  const int64_t kc1 = min(kc0 + args.kchunks_per_split, args.kchunks_total);
-  const int nk = kc1 > kc0 ? (int)(kc1 - kc0) : 0;
-  const int row0 = blockIdx.x * kTileRows;
+  const int64_t u0 = unit_begin(blockIdx.x, args), u1 = unit_begin(blockIdx.x + 1, args);
+  const int n = (int)(u1 - u0);
+  const int64_t C = args.chunks;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < S; ++s) {
       mbar_init(smem_u32(&tma_full[s]), 1);
-      mbar_init(smem_u32(&dec_full[s]), 4);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(acc_full), 1);
+    for (int t = 0; t < T; ++t) {
+      mbar_init(smem_u32(&dec_full[t]), 4);
+      mbar_init(smem_u32(&tfree[t]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), 4);
+    }
+    mbar_init(smem_u32(done), 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -224,23 +276,22 @@ k_decode_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 4) {
-    // ---------------- producer: packed codes + B chunk per stage
+    // ---------------- producer: packed codes + B chunk per unit
     if (lane == 0) {
       int issued = 0;
-      for (int i = 0; i < nk; ++i) {
-        const int s = i % kStages;
-        const uint32_t ph = (i / kStages) & 1;
+      for (int i = 0; i < n; ++i) {
+        const int s = i % S;
+        const uint32_t ph = (i / S) & 1;
         if (!mbar_wait(smem_u32(&empty[s]), ph ^ 1, abort_flag, args.err, 1)) break;
         const uint32_t bar = smem_u32(&tma_full[s]);
         mbar_arrive_tx(bar, kAStageBytes + kBStageBytes);
-        const int kc = (int)(kc0 + i);
-        tma_load_2d(smem_u32(sA + s * kAStageBytes), &tmA, kc * 16, row0, bar);
-        tma_load_2d(smem_u32(sB + s * kBStageBytes), &tmB, kc * kChunk, 0, bar);
+        const int64_t u = u0 + i, tile = u / C, kc = u - tile * C;
+        tma_load_2d(smem_u32(sA + s * kAStageBytes), &tmA, (int)(kc * 16), (int)(tile * kTileRows), bar);
+        tma_load_2d(smem_u32(sB + s * kBStageBytes), &tmB, (int)(kc * kChunk), 0, bar);
         issued = i + 1;
       }
       if (*abort_flag) {  // drain copies in flight before the CTA exits
-        for (int i = max(0, issued - kStages); i < issued; ++i)
-          mbar_wait(smem_u32(&tma_full[i % kStages]), (i / kStages) & 1, abort_flag, args.err, 0);
+        for (int i = max(0, issued - S); i < issued; ++i) mbar_drain(smem_u32(&tma_full[i % S]), (i / S) & 1);
       }
     }
   } else if (warp == 5) {
@@ -249,61 +300,91 @@ k_decode_gemm_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
       constexpr uint32_t idesc = (1u << 4)                 // D: FP32
                                  | (1u << 7) | (1u << 10)  // A, B: BF16
                                  | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(kTileRows >> 4) << 24);
-      bool ok = true;
-      for (int i = 0; i < nk && ok; ++i) {
-        const int s = i % kStages;
-        const uint32_t ph = (i / kStages) & 1;
-        ok = mbar_wait(smem_u32(&tma_full[s]), ph, abort_flag, args.err, 2) &&
-             mbar_wait(smem_u32(&dec_full[s]), ph, abort_flag, args.err, 4);
-        if (!ok) break;
+      int seg = 0;
+      for (int i = 0; i < n; ++i) {
+        const int s = i % S, t = i % T, b = seg % NACC;
+        const int64_t kc = (u0 + i) % C;
+        const bool first = (i == 0 || kc == 0), last = (i == n - 1 || kc == C - 1);
+        if (first) {
+          if (!mbar_wait(smem_u32(&acc_empty[b]), ((seg / NACC) & 1) ^ 1, abort_flag, args.err, 2)) break;
+        }
+        if (!mbar_wait(smem_u32(&tma_full[s]), (i / S) & 1, abort_flag, args.err, 2)) break;
+        if (!mbar_wait(smem_u32(&dec_full[t]), (i / T) & 1, abort_flag, args.err, 4)) break;
         tc_fence_after();
         const uint32_t b_addr = smem_u32(sB + s * kBStageBytes);
-        const uint32_t a_col = tmem + kAColBase + s * 32;
+        const uint32_t a_col = tmem + kAColBase + t * 32;
+        const uint32_t d_col = tmem + b * NP;
 #pragma unroll
         for (int kk = 0; kk < kChunk / 16; ++kk)
-          tc_mma(tmem, a_col + kk * 8, smem_desc_sw128(b_addr + kk * 32), idesc, (i > 0 || kk > 0) ? 1u : 0u);
+          tc_mma(d_col, a_col + kk * 8, smem_desc_sw128(b_addr + kk * 32), idesc, (first && kk == 0) ? 0u : 1u);
         tc_commit(smem_u32(&empty[s]));
+        tc_commit(smem_u32(&tfree[t]));
+        if (last) {
+          tc_commit(smem_u32(&acc_full[b]));
+          ++seg;
+        }
       }
-      tc_commit(smem_u32(acc_full));  // also drains every MMA issued above
+      tc_commit(smem_u32(done));  // tracks every MMA issued above
+      mbar_drain(smem_u32(done), 0);
     }
-  } else {
-    // ---------------- decoders (warps 0-3): row r = 32 * warp + lane, TMEM lanes of this warp
+  } else if (warp < 4) {
+    // ---------------- decoders: row r = 32 * warp + lane, TMEM lanes of this warp
     const int r = warp * 32 + lane;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    for (int i = 0; i < nk; ++i) {
-      const int s = i % kStages;
-      const uint32_t ph = (i / kStages) & 1;
-      if (!mbar_wait(smem_u32(&tma_full[s]), ph, abort_flag, args.err, 8)) break;
+    for (int i = 0; i < n; ++i) {
+      const int s = i % S, t = i % T;
+      if (!mbar_wait(smem_u32(&tma_full[s]), (i / S) & 1, abort_flag, args.err, 8)) break;
+      if (!mbar_wait(smem_u32(&tfree[t]), ((i / T) & 1) ^ 1, abort_flag, args.err, 8)) break;
       const uint4 q = *reinterpret_cast<const uint4*>(sA + s * kAStageBytes + r * 16);
       uint32_t v[32];
       decode_word(q.x, v);
       decode_word(q.y, v + 8);
       decode_word(q.z, v + 16);
       decode_word(q.w, v + 24);
-      tmem_st32(tmem + lane_base + kAColBase + s * 32, v);
+      tc_fence_after();
+      tmem_st32(tmem + lane_base + kAColBase + t * 32, v);
       tmem_wait_st();
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&dec_full[s]));
+      if (lane == 0) mbar_arrive(smem_u32(&dec_full[t]));
     }
-    // ---------------- epilogue: sum hi and lo halves of the accumulator
-    const bool ok = mbar_wait(smem_u32(acc_full), 0, abort_flag, args.err, 16);
-    tc_fence_after();
-    if (ok) {
-      float acc[NP];
+  } else {
+    // ---------------- readout warps 6-9: TMEM lanes 32 * (warp % 4) .. + 31
+    const int q4 = warp & 3;
+    const uint32_t lane_base = (uint32_t)(q4 * 32) << 16;
+    int64_t u = u0;
+    for (int seg = 0; u < u1; ++seg) {
+      const int64_t tile = u / C;
+      const int64_t seg_end = min(u1, (tile + 1) * C);
+      const bool tile_end = seg_end == (tile + 1) * C;
+      const int b = seg % NACC;
+      if (!mbar_wait(smem_u32(&acc_full[b]), (seg / NACC) & 1, abort_flag, args.err, 16)) break;
+      tc_fence_after();
+      const int64_t first_cta = cta_of_unit(tile * C, args);
+      const int slot = (int)(blockIdx.x - first_cta);
+      const int64_t row = tile * kTileRows + q4 * 32 + lane;
+      const bool valid = row < args.rows;
+      float* o = args.out + ((int64_t)slot * args.rows + (valid ? row : 0)) * args.l;
 #pragma unroll
-      for (int c0 = 0; c0 < NP; c0 += 16) {
-        uint32_t t[16];
-        tmem_ld16(tmem + lane_base + c0, t);
+      for (int c0 = 0; c0 < NP / 2; c0 += 8) {  // hi columns c0.., lo columns NP/2 + c0..
+        uint32_t hv[8], lv[8];
+        tmem_ld8(tmem + lane_base + b * NP + c0, hv);
+        tmem_ld8(tmem + lane_base + b * NP + NP / 2 + c0, lv);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc[c0 + j] = nk > 0 ? __uint_as_float(t[j]) : 0.0f;
+        for (int j = 0; j < 8; ++j)
+          if (valid && c0 + j < args.l) o[c0 + j] = __uint_as_float(hv[j]) + __uint_as_float(lv[j]);
       }
-      const int64_t row = row0 + r;
-      if (row < args.rows) {
-        float* o = args.out + ((int64_t)blockIdx.y * args.rows + row) * args.l;
-        for (int c = 0; c < args.l; ++c) o[c] = acc[c] + acc[args.l + c];
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+      if (valid && tile_end) {  // zero the slots this tile does not use
+        for (int sl = slot + 1; sl < args.ks; ++sl) {
+          float* z = args.out + ((int64_t)sl * args.rows + row) * args.l;
+          for (int c = 0; c < args.l; ++c) z[c] = 0.0f;
+        }
       }
+      u = seg_end;
     }
   }
   tc_fence_before();
@@ -323,8 +404,10 @@ __host__ __device__ __forceinline__ int chunk_code_of_pos(int pos) {
   return q * 16 + base[rr] + 4 * h;
 }
 
-// Bt[n][kpos] (NP x kpad, BF16): rows n < l hold bf16(x), rows l..2l-1 hold bf16(x - hi),
-// others zero; x = B[k][n] for the code index k of permuted position kpos (zero past K).
+// Bt[n][kpos] (NP x kpad, BF16): rows n < l hold hi = bf16(x), rows NP/2 .. NP/2 + l - 1 hold
+// bf16(x - hi), others zero; x = B[k][n] for the code index k of permuted position kpos (zero
+// past K). The fixed NP/2 offset of the lo half lets the readout add the halves with
+// compile-time register indices.
 template <typename T>
 __global__ void k_split_bf16(const T* __restrict__ B, int64_t K, int l, int np, int64_t kpad,
                              __nv_bfloat16* __restrict__ Bt) {
@@ -334,11 +417,13 @@ __global__ void k_split_bf16(const T* __restrict__ B, int64_t K, int l, int np, 
   const int64_t kp = t - (int64_t)n * kpad;
   const int64_t k = (kp / kChunk) * kChunk + chunk_code_of_pos((int)(kp % kChunk));
   float v = 0.0f;
-  if (n < 2 * l && k < K) {
-    const int col = n < l ? n : n - l;
+  const int half = np >> 1;
+  const bool is_hi = n < l, is_lo = n >= half && n < half + l;
+  if ((is_hi || is_lo) && k < K) {
+    const int col = is_hi ? n : n - half;
     const float x = (float)B[k * l + col];
     const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    v = n < l ? __bfloat162float(hi) : x - __bfloat162float(hi);
+    v = is_hi ? __bfloat162float(hi) : x - __bfloat162float(hi);
   }
   Bt[t] = __float2bfloat16_rn(v);
 }
@@ -373,56 +458,88 @@ CUtensorMap make_map(CUtensorMapDataType dt, void* base, uint64_t inner, uint64_
 
 int np_of(int l) { return (int)round_up(2 * l, 16); }
 
-// At most two CTAs per SM: each allocates 256 of the SM's 512 TMEM columns, so the
-// shared-memory request is padded to keep a third CTA from becoming resident.
+// At most two CTAs per SM: each allocates 256 of the SM's 512 TMEM columns, so the request is
+// at least 100 KB to keep a third CTA from becoming resident.
 size_t smem_bytes(int np) {
-  size_t need = 1024 + kStages * ((size_t)np * kChunk * 2 + kTileRows * 16) + (3 * kStages + 4) * 8;
+  const int S = ring_stages(np);
+  const size_t need = 1024 + (size_t)S * ((size_t)np * kChunk * 2 + kTileRows * 16) + (2 * S + 2 * kAStages + 8) * 8;
   return std::max<size_t>(need, 100 * 1024);
 }
 
+// Stream-K plan of one product: G CTAs over tiles x C units, and the output slots per row
+// (the largest number of CTAs that share one tile).
+struct TcPlan {
+  int64_t tiles = 0, chunks = 0, units = 0;
+  int grid = 0, ks = 1;
+};
+
+int64_t plan_cta_of_unit(int64_t x, int64_t units, int grid) { return ((x + 1) * grid + units - 1) / units - 1; }
+
+TcPlan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K) {
+  TcPlan p;
+  p.tiles = (rows + kTileRows - 1) / kTileRows;
+  p.chunks = (K + kChunk - 1) / kChunk;
+  p.units = p.tiles * p.chunks;
+  if (p.units == 0) return p;
+  p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(2 * (int64_t)c->sm_count, p.units / kMinUnitsPerCta));
+  int ks = 1;
+  for (int64_t t = 0; t < p.tiles; ++t) {
+    const int64_t a = plan_cta_of_unit(t * p.chunks, p.units, p.grid);
+    const int64_t b = plan_cta_of_unit(t * p.chunks + p.chunks - 1, p.units, p.grid);
+    ks = std::max<int>(ks, (int)(b - a + 1));
+  }
+  p.ks = ks;
+  return p;
+}
+
 template <int NP>
-void launch_np(pcaone_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, const TcArgs& a,
-               dim3 grid) {
+void launch_np(pcaone_ctx* c, const CUtensorMap& ta, const CUtensorMap& tb, const TcArgs& a) {
   static bool attr = false;
   const size_t smem = smem_bytes(NP);
   if (!attr) {
     PG_CUDA(cudaFuncSetAttribute(k_decode_gemm_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
-  k_decode_gemm_tc<NP><<<grid, kThreads, smem, c->stream>>>(ta, tb, a);
+  k_decode_gemm_tc<NP><<<a.grid, kThreads, smem, c->stream>>>(ta, tb, a);
   PG_CHECK_LAUNCH();
 }
 
-// One product: codes (rows_alloc x pitch bytes, rows valid), K codes; Bt (np x kpad BF16).
+// One product: codes (rows_alloc x pitch bytes, rows valid), K codes; Bt (np x kpad BF16);
+// out holds ks = make_plan(rows, K).ks slots of rows x l partial sums.
 void run_tc(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t rows, int64_t rows_alloc,
             int64_t K, const __nv_bfloat16* Bt, int64_t kpad, int l, int ks, float* out) {
   const int np = np_of(l);
   PG_REQUIRE(np <= 128, PCAONE_EBADARG, "sketch width too large for the tensor-core path");
   PG_REQUIRE((int64_t)round_up(rows, kTileRows) <= rows_alloc, PCAONE_EBADARG, "row padding too small");
-  const int64_t nkc = (K + kChunk - 1) / kChunk;
-  PG_REQUIRE(nkc * 16 <= (int64_t)pitch && nkc * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
+  const TcPlan p = make_plan(c, rows, K);
+  PG_REQUIRE(ks == p.ks, PCAONE_EBADARG, "output slot count does not match the product plan");
+  if (p.units == 0) {
+    PG_CUDA(cudaMemsetAsync(out, 0, (size_t)ks * rows * l * sizeof(float), c->stream));
+    return;
+  }
+  PG_REQUIRE(p.chunks * 16 <= (int64_t)pitch && p.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
   CUtensorMap ta = make_map(CU_TENSOR_MAP_DATA_TYPE_UINT8, (void*)codes, pitch, rows_alloc, pitch, 16,
                             kTileRows, CU_TENSOR_MAP_SWIZZLE_NONE);
   CUtensorMap tb = make_map(CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (void*)Bt, kpad, np, kpad * 2, kChunk, np,
                             CU_TENSOR_MAP_SWIZZLE_128B);
-  int* err = (int*)scratch(c, "tc_err", sizeof(int));
   TcArgs a;
   a.rows = rows;
-  a.kchunks_total = nkc;
-  a.kchunks_per_split = (nkc + ks - 1) / ks;
+  a.chunks = p.chunks;
+  a.units = p.units;
+  a.grid = p.grid;
+  a.ks = p.ks;
   a.l = l;
   a.out = out;
-  a.err = err;
-  dim3 grid((unsigned)((rows + kTileRows - 1) / kTileRows), (unsigned)ks);
+  a.err = (int*)scratch(c, "tc_err", sizeof(int));
   switch (np) {
-    case 16: launch_np<16>(c, ta, tb, a, grid); break;
-    case 32: launch_np<32>(c, ta, tb, a, grid); break;
-    case 48: launch_np<48>(c, ta, tb, a, grid); break;
-    case 64: launch_np<64>(c, ta, tb, a, grid); break;
-    case 80: launch_np<80>(c, ta, tb, a, grid); break;
-    case 96: launch_np<96>(c, ta, tb, a, grid); break;
-    case 112: launch_np<112>(c, ta, tb, a, grid); break;
-    default: launch_np<128>(c, ta, tb, a, grid); break;
+    case 16: launch_np<16>(c, ta, tb, a); break;
+    case 32: launch_np<32>(c, ta, tb, a); break;
+    case 48: launch_np<48>(c, ta, tb, a); break;
+    case 64: launch_np<64>(c, ta, tb, a); break;
+    case 80: launch_np<80>(c, ta, tb, a); break;
+    case 96: launch_np<96>(c, ta, tb, a); break;
+    case 112: launch_np<112>(c, ta, tb, a); break;
+    default: launch_np<128>(c, ta, tb, a); break;
   }
   c->launches++;
   c->gemm_launches++;
@@ -438,12 +555,7 @@ void split_bf16(pcaone_ctx* c, const T* B, int64_t K, int l, int64_t kpad, __nv_
 }
 
 // ---- back-end state kept in named scratch buffers
-int tc_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) {
-  const int64_t tiles = (rows + kTileRows - 1) / kTileRows;
-  const int64_t chunks = (K + kChunk - 1) / kChunk;
-  const int64_t want = (2 * (int64_t)c->sm_count + tiles - 1) / tiles;
-  return (int)std::max<int64_t>(1, std::min<int64_t>({want, chunks / 8, 64}));
-}
+int tc_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) { return make_plan(c, rows, K).ks; }
 
 void tc_omega(pcaone_ctx* c, const double* omega, int l, int64_t npad) {
   auto* Bt = (__nv_bfloat16*)scratch(c, "tc_bt1", (size_t)npad * np_of(l) * 2);
@@ -488,6 +600,29 @@ void tc_clear_error(pcaone_ctx* c) {
 
 void tc_check_error(pcaone_ctx* c) { check_err(c); }
 
-GemmFnT<float> gemm_tc() { return GemmFnT<float>{tc_ksplit, tc_p1, tc_p2, tc_omega, tc_b2}; }
+namespace {
+__nv_bfloat16* tc_omega_bt(pcaone_ctx* c, int l, int* half) {
+  *half = np_of(l) / 2;
+  return (__nv_bfloat16*)scratch(c, "tc_bt1", (size_t)c->Npad * np_of(l) * 2);
+}
+// The split window operand written by the first epilogue. Its unused rows stay zero: the
+// buffer is cleared whenever its shape changes.
+__nv_bfloat16* tc_b2_bt(pcaone_ctx* c, int l, int64_t* kpad, int* half) {
+  *kpad = round_up(c->win.blocksize, 256);
+  *half = np_of(l) / 2;
+  const size_t bytes = (size_t)(*kpad) * np_of(l) * 2;
+  auto* p = (__nv_bfloat16*)scratch(c, "tc_bt2", bytes);
+  int64_t& shape = c->bt2_shape;
+  const int64_t key = (*kpad) * 1024 + l;
+  if (shape != key || (void*)p != c->bt2_ptr) {
+    PG_CUDA(cudaMemsetAsync(p, 0, bytes, c->stream));
+    shape = key;
+    c->bt2_ptr = p;
+  }
+  return p;
+}
+}  // namespace
+
+GemmFnT<float> gemm_tc() { return GemmFnT<float>{tc_ksplit, tc_p1, tc_p2, tc_omega, tc_b2, tc_omega_bt, tc_b2_bt}; }
 
 }  // namespace pg

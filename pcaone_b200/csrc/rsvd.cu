@@ -17,6 +17,7 @@
 #include "epilogue.hpp"
 #include "linalg.hpp"
 #include "rsvd.hpp"
+#include "update.hpp"
 
 namespace pg {
 
@@ -101,6 +102,7 @@ struct Engine {
   double *Omg, *Omg2, *wsum, *G, *H, *H1, *H2, *Tb, *Rg, *Rb, *Dsig, *Ucur, *Upre, *Ck;
   T* OmgT;   // Omega as the B operand of the first product (alias of Omg for FP64)
   int* d_status;
+  unsigned* upd_cnt;
   const double* Fcent;  // centring frequencies of the epilogues (zeros for the dense E)
 
   Engine(pcaone_ctx* c_, const pcaone_rsvd_opts& o_, GemmFnT<T> g) : c(c_), o(o_), gemm(g) {
@@ -127,6 +129,8 @@ struct Engine {
     Ck = d("r_Ck", (size_t)kLmax * kLmax);
     d_status = (int*)scratch(c, "r_status", sizeof(int));
     PG_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), c->stream));
+    upd_cnt = (unsigned*)scratch(c, "upd_cnt", 4 * sizeof(unsigned));
+    PG_CUDA(cudaMemsetAsync(upd_cnt, 0, 4 * sizeof(unsigned), c->stream));
     if (std::is_same<T, double>::value)
       OmgT = reinterpret_cast<T*>(Omg);
     else
@@ -151,15 +155,32 @@ struct Engine {
     gemm.omega_changed(c, Omg, l, Npad);
   }
 
-  // Omega = flipOmg(Omega2, thinQ(Householder QR of Hsrc)); Omega2 = Omega.
-  void update_omega(const double* Hsrc) {
-    double* Q = Tb;
-    double* Rtmp = (double*)scratch(c, "r_Rtmp", (size_t)l * l * 8);
-    cholqr2(c, Hsrc, l, N, Q, Rtmp, d_status);
-    householder_signs(c, Q, l, Dsig);
-    flip_and_apply(c, Q, Dsig, l, N, Omg, Omg2, omg_float());
-    colsum(c, Omg, l, N, wsum);
-    gemm.omega_changed(c, Omg, l, Npad);
+  // Omega = flipOmg(Omega2, thinQ(Householder QR of H)); Omega2 = Omega. With H2, the sketch
+  // is H = H1 + H2 (written to H); otherwise H1 is the sketch itself.
+  void update_omega(double* H1in, const double* H2in) {
+    UpdateArgs a;
+    a.H1 = H2in ? H1in : nullptr;
+    a.H2 = H2in;
+    a.H = H2in ? H : H1in;
+    a.Q = Tb;
+    a.Omg = Omg;
+    a.Omg2 = Omg2;
+    a.Omgf = omg_float();
+    a.bt1 = gemm.omega_bt ? gemm.omega_bt(c, l, &a.bt_half) : nullptr;
+    a.kpad = Npad;
+    a.wsum = wsum;
+    a.nblk = 64;
+    a.part = (double*)scratch(c, "upd_part", (size_t)a.nblk * l * l * 8);
+    a.R1 = (double*)scratch(c, "upd_R1", (size_t)l * l * 8);
+    a.R2 = (double*)scratch(c, "upd_R2", (size_t)l * l * 8);
+    a.D = Dsig;
+    a.mult = (double*)scratch(c, "upd_mult", (size_t)l * 8);
+    a.counters = upd_cnt;
+    a.status = d_status;
+    a.N = N;
+    a.l = l;
+    fused_update(c, a);
+    if (!a.bt1) gemm.omega_changed(c, Omg, l, Npad);
   }
 
   // G rows of window b and accumulation of Z_b G_b into Ht.
@@ -185,9 +206,10 @@ struct Engine {
     p1.G = G;
     T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
     double* h0 = (double*)scratch(c, "r_h0", l * 8);
+    if (gemm.b2_bt) p1.bt2 = gemm.b2_bt(c, l, &p1.kpad2, &p1.bt_half);
     timed([&] {
       launch_prep<T>(c, p1, D1, B2, h0);
-      gemm.b2_ready(c, B2, l, m);
+      if (!p1.bt2) gemm.b2_ready(c, B2, l, m);
     }, 1);
     // product 2: D2 = R_b B2
     int ks2 = gemm.ksplit(c, N, m);
@@ -261,7 +283,7 @@ struct Engine {
     if (pi == 0)
       init_omega();
     else {
-      timed([&] { update_omega(H); }, 2);
+      timed([&] { update_omega(H, nullptr); }, 2);
       updates++;
     }
     zero(c, H, Npad * l);
@@ -282,10 +304,7 @@ struct Engine {
       const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) && std::pow(2.0, pi) < bands;
       if ((b + 1) < bandsize && !adjacent) continue;
       if (!((i == bandsize) || (i == bandsize / 2) || adjacent)) continue;
-      timed([&] {
-        add(c, H1, H2, Npad * l, H);
-        update_omega(H);
-      }, 2);
+      timed([&] { update_omega(H1, H2); }, 2);
       updates++;
       if (i == bandsize) {
         zero(c, H1, Npad * l);

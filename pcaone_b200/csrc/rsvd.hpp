@@ -1,6 +1,8 @@
 // RSVD driver and the decode-GEMM back ends it can run on.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "internal.hpp"
 
 namespace pg {
@@ -19,6 +21,11 @@ struct GemmFnT {
              int64_t K, const T* B, int l, int ks, T* out);
   void (*omega_changed)(pcaone_ctx* c, const double* omega, int l, int64_t npad);
   void (*b2_ready)(pcaone_ctx* c, const T* B2, int l, int64_t m);
+  // Split-BF16 operand buffers in the tensor-core layout (nullptr for the SIMT back ends):
+  // when non-null, the fused Omega update and the first epilogue write them directly.
+  // *half receives the row offset of the lo halves.
+  __nv_bfloat16* (*omega_bt)(pcaone_ctx* c, int l, int* half) = nullptr;
+  __nv_bfloat16* (*b2_bt)(pcaone_ctx* c, int l, int64_t* kpad, int* half) = nullptr;
 };
 
 GemmFnT<float> gemm_simt_float();

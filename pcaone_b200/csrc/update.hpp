@@ -1,0 +1,35 @@
+// Fused Omega update (kernels_update.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "internal.hpp"
+
+namespace pg {
+
+struct UpdateArgs {
+  const double* H1 = nullptr;  // winSVD: H = H1 + H2; Halko: H1 = nullptr, H2 = nullptr
+  const double* H2 = nullptr;
+  double* H = nullptr;         // N x l: written when H2 is given, else the input sketch
+  double* Q = nullptr;         // N x l work (Q1 then Q)
+  double* Omg = nullptr;       // N x l outputs
+  double* Omg2 = nullptr;
+  float* Omgf = nullptr;       // FP32 operand copy (SIMT path) or null
+  __nv_bfloat16* bt1 = nullptr;  // split-BF16 operand in the tcgen05 layout (kpad) or null
+  int64_t kpad = 0;
+  int bt_half = 0;               // row offset of the lo half in bt1
+  double* wsum = nullptr;      // l
+  double* part = nullptr;      // nblk * l * l work
+  double* R1 = nullptr;        // l x l work
+  double* R2 = nullptr;
+  double* D = nullptr;         // l
+  double* mult = nullptr;      // l
+  unsigned* counters = nullptr;  // 4 tickets, zero between calls
+  int* status = nullptr;
+  int64_t N = 0;
+  int l = 0, nblk = 64;
+};
+
+void fused_update(pcaone_ctx* c, UpdateArgs a);
+
+}  // namespace pg

@@ -68,6 +68,8 @@ void free_all(pcaone_ctx* c) {
   c->bufs.clear();
   c->bt2_shape = -1;
   c->bt2_ptr = nullptr;
+  c->tiles_valid = false;
+  c->tile1_ptr = c->tile2_ptr = nullptr;
 }
 
 }  // namespace pg

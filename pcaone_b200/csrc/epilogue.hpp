@@ -19,9 +19,9 @@ struct EpiP1 {          // after the Z^T Omega product of one window
   const int32_t* miss_idx = nullptr;
   const double* miss_val = nullptr;  // e_ij per entry (EM-imputed), or null for 0
   double* G = nullptr;               // M x l (rows start..start+m written)
-  __nv_bfloat16* bt2 = nullptr;      // when set: B2 written as split BF16 in the tcgen05 layout
-  int64_t kpad2 = 0;
-  int bt_half = 0;                   // row offset of the lo half in bt2
+  __nv_bfloat16* bt2 = nullptr;      // when set: B2 written as split BF16 (tc_layout.hpp)
+  int64_t kpad2 = 0;                 // K extent of bt2 (multiple of 64)
+  int bt_half = 0;                   // row offset of the lo half in bt2 (= NP / 2)
 };
 
 struct EpiP2 {          // after the Z * G product of one window

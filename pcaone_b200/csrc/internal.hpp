@@ -120,6 +120,11 @@ struct pcaone_ctx {
   // shape key and address of the zeroed split-BF16 window operand (tensor-core back end)
   int64_t bt2_shape = -1;
   void* bt2_ptr = nullptr;
+  // tiled copies of the codes for the tensor-core back end, valid for (generation, windows)
+  bool tiles_valid = false;
+  uint64_t tiles_key = 0;
+  void* tile1_ptr = nullptr;
+  void* tile2_ptr = nullptr;
 
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;

@@ -14,17 +14,11 @@
 //   H_i = (R B2)_i - h0 + sum_{j miss} s_j (e_ij + F_j) G_j,  B2_j = s_j/2 G_j,
 //                                                             h0 = sum_j s_j F_j G_j
 #include "epilogue.hpp"
+#include "tc_layout.hpp"
 
 namespace pg {
 
 namespace {
-
-// Position of code index k inside its 64-code chunk in the tcgen05 decode order
-// (kernels_gemm_tc.cu, decode_word): code c -> 2 * (8q + 2p + half) + h.
-__device__ __forceinline__ int64_t tc_pos(int64_t k) {
-  const int c = (int)(k & 63), q = c >> 4, r16 = c & 15;
-  return (k & ~(int64_t)63) + 2 * (8 * q + 2 * (r16 & 3) + (r16 >> 3)) + ((r16 >> 2) & 1);
-}
 
 // Warp-cooperative sparse gather: acc_c += sum_{e in [e0, e1)} w_e * rows[idx_e][c] for the
 // lane's columns c = lane and lane + 32 (l <= 64), summed in entry order. The warp loads 32
@@ -98,8 +92,9 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
         const float x = (float)b2;
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
         const int64_t kp = tc_pos(jl);
-        p.bt2[(int64_t)c * p.kpad2 + kp] = hi;
-        p.bt2[(int64_t)(p.bt_half + c) * p.kpad2 + kp] = __float2bfloat16_rn(x - __bfloat162float(hi));
+        const int np = 2 * p.bt_half;
+        p.bt2[bt_elem(c, kp, np)] = hi;
+        p.bt2[bt_elem(p.bt_half + c, kp, np)] = __float2bfloat16_rn(x - __bfloat162float(hi));
       } else {
         B2[jl * p.l + c] = b2;
       }
@@ -110,8 +105,8 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
     const int64_t tail = p.kpad2 - p.m, tot = tail * 2 * p.l;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
       const int64_t r = t / tail, jl = p.m + (t - r * tail);
-      const int64_t row = r < p.l ? r : p.bt_half + (r - p.l);
-      p.bt2[row * p.kpad2 + tc_pos(jl)] = __float2bfloat16_rn(0.0f);
+      const int row = (int)(r < p.l ? r : p.bt_half + (r - p.l));
+      p.bt2[bt_elem(row, tc_pos(jl), 2 * p.bt_half)] = __float2bfloat16_rn(0.0f);
     }
   }
   __syncthreads();

@@ -17,6 +17,7 @@
 #include <algorithm>
 
 #include "internal.hpp"
+#include "tc_layout.hpp"
 #include "update.hpp"
 
 namespace pg {
@@ -236,13 +237,6 @@ __global__ void __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
   if (threadIdx.x == 0) a.counters[2] = 0;
 }
 
-__device__ __forceinline__ int64_t chunk_pos_of_code(int64_t i) {
-  // inverse of the decode order of kernels_gemm_tc.cu: code c -> position in its 64-code chunk
-  const int c = (int)(i & 63), q = c >> 4, r16 = c & 15;
-  const int p = r16 & 3, h = (r16 >> 2) & 1, half = r16 >> 3;
-  return (i & ~(int64_t)63) + 2 * (8 * q + 2 * p + half) + h;
-}
-
 __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
@@ -253,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   double cs[kLmax];
   for (int j = 0; j < l; ++j) cs[j] = 0.0;
   for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-    const int64_t kp = a.bt1 ? chunk_pos_of_code(r) : 0;
+    const int64_t kp = tc_pos(r);
     for (int j = 0; j < l; ++j) {
       const double v = a.Q[r * l + j] * a.mult[j];
       a.Omg[r * l + j] = v;
@@ -263,8 +257,8 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
       if (a.bt1) {
         const float x = (float)v;
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-        a.bt1[(int64_t)j * a.kpad + kp] = hi;
-        a.bt1[(int64_t)(a.bt_half + j) * a.kpad + kp] = __float2bfloat16_rn(x - __bfloat162float(hi));
+        a.bt1[bt_elem(j, kp, 2 * a.bt_half)] = hi;
+        a.bt1[bt_elem(a.bt_half + j, kp, 2 * a.bt_half)] = __float2bfloat16_rn(x - __bfloat162float(hi));
       }
     }
   }

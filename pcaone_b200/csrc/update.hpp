@@ -15,9 +15,9 @@ struct UpdateArgs {
   double* Omg = nullptr;       // N x l outputs
   double* Omg2 = nullptr;
   float* Omgf = nullptr;       // FP32 operand copy (SIMT path) or null
-  __nv_bfloat16* bt1 = nullptr;  // split-BF16 operand in the tcgen05 layout (kpad) or null
+  __nv_bfloat16* bt1 = nullptr;  // split-BF16 operand (tc_layout.hpp) or null
   int64_t kpad = 0;
-  int bt_half = 0;               // row offset of the lo half in bt1
+  int bt_half = 0;               // row offset of the lo half in bt1 (= NP / 2)
   double* wsum = nullptr;      // l
   double* part = nullptr;      // nblk * l * l work
   double* R1 = nullptr;        // l x l work

@@ -142,12 +142,17 @@ __global__ void k_scale_g(int64_t start, int64_t m, int l, const double* __restr
   }
 }
 
+// out[c] = sum_b part[b][c]: one warp per column, lanes over b in a fixed order, then a
+// fixed shuffle tree (deterministic).
 __global__ void k_reduce_cols(const double* __restrict__ part, int nblk, int l, double* __restrict__ out) {
-  int c = threadIdx.x;
-  if (c >= l) return;
-  double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * l + c];
-  out[c] = s;
+  const int lane = threadIdx.x & 31;
+  for (int c = threadIdx.x >> 5; c < l; c += blockDim.x >> 5) {
+    double s = 0.0;
+#pragma unroll 4
+    for (int b = lane; b < nblk; b += 32) s += part[(int64_t)b * l + c];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[c] = s;
+  }
 }
 
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse.
@@ -180,7 +185,7 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
   double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
   k_prep<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p, D1, B2, part);
   PG_CHECK_LAUNCH();
-  k_reduce_cols<<<1, 128, 0, c->stream>>>(part, nblk, p.l, h0);
+  k_reduce_cols<<<1, 512, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }
@@ -202,7 +207,7 @@ void launch_scale_g(pcaone_ctx* c, const EpiP1& p, T* B2, double* h0) {
   k_scale_g<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p.start, p.m, p.l, p.scale,
                                                                        p.F, p.G, B2, part);
   PG_CHECK_LAUNCH();
-  k_reduce_cols<<<1, 128, 0, c->stream>>>(part, nblk, p.l, h0);
+  k_reduce_cols<<<1, 512, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }

@@ -14,45 +14,73 @@ namespace {
 constexpr int kGramRowsMax = 64;  // rows staged per iteration in the Gram kernels
 constexpr int kGramBlocks = 296;
 
-// Partial cross products P[blk] = A^T B over a slice of rows (A: n x la, B: n x lb).
+// Partial cross products P[blk] = A^T B over a slice of rows (A: n x la, B: n x lb). Rows
+// are staged in shared memory with widths padded to multiples of 4 (zero columns); each
+// thread accumulates a 4 x 4 block of the la x lb output in registers, so a staged row costs
+// 8 shared-memory loads per 16 FMAs.
 __global__ void k_cross_partial(const double* __restrict__ A, int la, const double* __restrict__ Bm,
                                 int lb, int64_t n, int kGramRows, double* __restrict__ part) {
   extern __shared__ double sm[];
-  double* sa = sm;                       // kGramRows x la
-  double* sb = sm + kGramRows * la;      // kGramRows x lb
-  const int npairs = la * lb;
-  double acc[8];
-  for (int t = 0; t < 8; ++t) acc[t] = 0.0;
+  const int la4 = (la + 3) & ~3, lb4 = (lb + 3) & ~3;
+  double* sa = sm;                        // kGramRows x la4
+  double* sb = sm + kGramRows * la4;      // kGramRows x lb4
+  const int bi = la4 / 4, bj = lb4 / 4;   // 4 x 4 output blocks
+  const int blk = threadIdx.x;
+  const bool active = blk < bi * bj;
+  const int i0 = active ? (blk / bj) * 4 : 0, j0 = active ? (blk % bj) * 4 : 0;
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
   const int64_t rows_per_blk = (n + gridDim.x - 1) / gridDim.x;
   const int64_t rb = blockIdx.x * rows_per_blk, re = min(n, rb + rows_per_blk);
   for (int64_t r0 = rb; r0 < re; r0 += kGramRows) {
-    int nr = (int)(re - r0 < kGramRows ? re - r0 : kGramRows);
-    for (int t = threadIdx.x; t < nr * la; t += blockDim.x) sa[t] = A[r0 * la + t];
-    for (int t = threadIdx.x; t < nr * lb; t += blockDim.x) sb[t] = Bm[r0 * lb + t];
+    const int nr = (int)(re - r0 < kGramRows ? re - r0 : kGramRows);
     __syncthreads();
-    for (int q = 0; q < 8; ++q) {
-      int p = threadIdx.x + q * blockDim.x;
-      if (p >= npairs) break;
-      int i = p / lb, j = p - i * lb;
-      double s = acc[q];
-      for (int r = 0; r < nr; ++r) s = fma(sa[r * la + i], sb[r * lb + j], s);
-      acc[q] = s;
+    for (int t = threadIdx.x; t < nr * la4; t += blockDim.x) {
+      const int r = t / la4, cidx = t - r * la4;
+      sa[t] = cidx < la ? A[(r0 + r) * la + cidx] : 0.0;
+    }
+    for (int t = threadIdx.x; t < nr * lb4; t += blockDim.x) {
+      const int r = t / lb4, cidx = t - r * lb4;
+      sb[t] = cidx < lb ? Bm[(r0 + r) * lb + cidx] : 0.0;
     }
     __syncthreads();
+    if (active) {
+      for (int r = 0; r < nr; ++r) {
+        const double2 a01 = *reinterpret_cast<const double2*>(sa + r * la4 + i0);
+        const double2 a23 = *reinterpret_cast<const double2*>(sa + r * la4 + i0 + 2);
+        const double2 b01 = *reinterpret_cast<const double2*>(sb + r * lb4 + j0);
+        const double2 b23 = *reinterpret_cast<const double2*>(sb + r * lb4 + j0 + 2);
+        const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+      }
+    }
   }
-  for (int q = 0; q < 8; ++q) {
-    int p = threadIdx.x + q * blockDim.x;
-    if (p < npairs) part[(int64_t)blockIdx.x * npairs + p] = acc[q];
+  if (active) {
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+        if (i0 + x < la && j0 + y < lb) part[(int64_t)blockIdx.x * la * lb + (i0 + x) * lb + j0 + y] = acc[x][y];
   }
 }
 
+// out[p] = sum_b part[b][p]: one warp per pair, lanes over b in a fixed order, then a fixed
+// shuffle tree (deterministic).
 __global__ void k_sum_partials(const double* __restrict__ part, int nblk, int npairs,
                                double* __restrict__ out) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (p >= npairs) return;
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * npairs + p];
-  out[p] = s;
+#pragma unroll 4
+  for (int b = lane; b < nblk; b += 32) s += part[(int64_t)b * npairs + p];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[p] = s;
 }
 
 // Cholesky W = R^T R (R upper) for l x l; one CTA. status[0] is set to 1 + j on failure.
@@ -102,23 +130,17 @@ __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restri
   if (threadIdx.x == 0 && bad && status) atomicMax(status, bad);
 }
 
-// Q = A R^{-1} (row-wise forward substitution x R = a), R upper l x l. One thread per row.
-__global__ void k_trsm_right_upper(const double* __restrict__ A, const double* __restrict__ R,
-                                   int l, int64_t n, double* __restrict__ Q) {
-  extern __shared__ double sr[];
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) sr[t] = R[t];
+// Q = A R^{-1} (row-wise forward substitution x R = a), R upper l x l. One thread per row;
+// the row's unknowns stay in registers (LMAX >= l, loops unrolled over LMAX).
+template <int LMAX>
+__global__ void __launch_bounds__(128) k_trsm_right_upper(const double* A, const double* __restrict__ R, int l,
+                                                          int64_t n, double* Q) {  // A may alias Q
+  extern __shared__ double sr[];  // LMAX x LMAX
+  stage_r<LMAX>(R, l, sr);
   __syncthreads();
-  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
-  double x[kLmax];
-  const double* a = A + r * l;
-  for (int j = 0; j < l; ++j) {
-    double v = a[j];
-    for (int k = 0; k < j; ++k) v -= x[k] * sr[k * l + j];
-    x[j] = v / sr[j * l + j];
-  }
-  double* q = Q + r * l;
-  for (int j = 0; j < l; ++j) q[j] = x[j];
+  solve_row_upper<LMAX>(A + r * l, sr, l, Q + r * l);
 }
 
 // Householder column signs of an orthonormal Q from the modified LU of its top l x l block
@@ -231,20 +253,24 @@ __global__ void k_colsum_final(const double* __restrict__ part, int nblk, int l,
   out[col] = s;
 }
 
-// Y (n x kc) = X (n x l) * C (l x ldc, first kc columns), row-major.
-__global__ void k_rowmat(const double* __restrict__ X, int l, const double* __restrict__ C, int ldc,
-                         int kc, int64_t n, double* __restrict__ Y) {
+// Y (n x kc) = X (n x l) * C (l x ldc, first kc columns), row-major; X row in registers.
+template <int LMAX>
+__global__ void __launch_bounds__(128) k_rowmat(const double* __restrict__ X, int l, const double* __restrict__ C,
+                                                int ldc, int kc, int64_t n, double* __restrict__ Y) {
   extern __shared__ double sc[];
   for (int t = threadIdx.x; t < l * kc; t += blockDim.x) sc[t] = C[(t / kc) * ldc + t % kc];
   __syncthreads();
-  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   const double* x = X + r * l;
-  double xr[kLmax];
-  for (int j = 0; j < l; ++j) xr[j] = x[j];
+  double xr[LMAX];
+#pragma unroll
+  for (int j = 0; j < LMAX; ++j) xr[j] = j < l ? x[j] : 0.0;
   for (int c = 0; c < kc; ++c) {
     double s = 0.0;
-    for (int j = 0; j < l; ++j) s = fma(xr[j], sc[j * kc + c], s);
+#pragma unroll
+    for (int j = 0; j < LMAX; ++j)
+      if (j < l) s = fma(xr[j], sc[j * kc + c], s);
     Y[r * kc + c] = s;
   }
 }
@@ -259,17 +285,17 @@ __global__ void k_add(const double* __restrict__ a, const double* __restrict__ b
 
 void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int64_t n, double* out) {
   const int npairs = la * lb;
-  PG_REQUIRE(npairs <= 8 * 512, PCAONE_EBADARG, "cross product too wide");
-  int threads = std::min(512, std::max(128, (npairs + 7) / 8 + 31) / 32 * 32);
-  while (threads * 8 < npairs) threads += 32;
+  PG_REQUIRE(la <= kLmax && lb <= kLmax, PCAONE_EBADARG, "cross product too wide");
+  const int la4 = (la + 3) & ~3, lb4 = (lb + 3) & ~3;
+  const int threads = std::max(32, ((la4 / 4) * (lb4 / 4) + 31) / 32 * 32);
   // stage as many rows as fit in 48 KB of shared memory
-  const int rows = std::max(8, std::min(kGramRowsMax, 6144 / (la + lb)));
+  const int rows = std::max(8, std::min(kGramRowsMax, 6144 / (la4 + lb4)));
   int nblk = (int)std::min<int64_t>(kGramBlocks, std::max<int64_t>(1, (n + rows - 1) / rows));
   double* part = (double*)scratch(c, "cross_part", (size_t)nblk * npairs * 8);
-  size_t smem = (size_t)rows * (la + lb) * 8;
+  size_t smem = (size_t)rows * (la4 + lb4) * 8;
   k_cross_partial<<<nblk, threads, smem, c->stream>>>(A, la, B, lb, n, rows, part);
   PG_CHECK_LAUNCH();
-  k_sum_partials<<<(npairs + 255) / 256, 256, 0, c->stream>>>(part, nblk, npairs, out);
+  k_sum_partials<<<(npairs + 7) / 8, 256, 0, c->stream>>>(part, nblk, npairs, out);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }
@@ -282,7 +308,15 @@ void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rp
 }
 
 void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q) {
-  k_trsm_right_upper<<<(unsigned)((n + 127) / 128), 128, (size_t)l * l * 8, c->stream>>>(A, R, l, n, Q);
+  const dim3 grid((unsigned)((n + 127) / 128));
+  if (l <= 16)
+    k_trsm_right_upper<16><<<grid, 128, 16 * 16 * 8, c->stream>>>(A, R, l, n, Q);
+  else if (l <= 32)
+    k_trsm_right_upper<32><<<grid, 128, 32 * 32 * 8, c->stream>>>(A, R, l, n, Q);
+  else if (l <= 48)
+    k_trsm_right_upper<48><<<grid, 128, 48 * 48 * 8, c->stream>>>(A, R, l, n, Q);
+  else
+    k_trsm_right_upper<64><<<grid, 128, 64 * 64 * 8, c->stream>>>(A, R, l, n, Q);
   PG_CHECK_LAUNCH();
   c->launches++;
 }
@@ -331,7 +365,16 @@ void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out) {
 }
 
 void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y) {
-  k_rowmat<<<(unsigned)((n + 127) / 128), 128, (size_t)l * kc * 8, c->stream>>>(X, l, C, ldc, kc, n, Y);
+  const dim3 grid((unsigned)((n + 127) / 128));
+  const size_t smem = (size_t)l * kc * 8;
+  if (l <= 16)
+    k_rowmat<16><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
+  else if (l <= 32)
+    k_rowmat<32><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
+  else if (l <= 48)
+    k_rowmat<48><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
+  else
+    k_rowmat<64><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
   PG_CHECK_LAUNCH();
   c->launches++;
 }

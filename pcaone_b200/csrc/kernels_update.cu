@@ -12,11 +12,14 @@
 // finishes last (atomic ticket after a __threadfence) reduces the partials in CTA order, so
 // the result is deterministic. The Householder column signs D come from the modified LU of
 // the top l x l block of Q (Ballard et al. 2015): pivot s -> D = -sign(s), sign(0) = +.
+// Row solves keep the row in registers (kernels templated on LMAX >= l); Gram matrices use
+// 4 x 4 register tiles; column sums use a column-strided thread layout.
 #include <cuda_bf16.h>
 
 #include <algorithm>
 
 #include "internal.hpp"
+#include "linalg.hpp"
 #include "tc_layout.hpp"
 #include "update.hpp"
 
@@ -24,7 +27,7 @@ namespace pg {
 
 namespace {
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 256;
 constexpr int kStageRows = 32;
 
 // Shared-memory Cholesky of an l x l SPD matrix (upper R, W = R^T R), in place in s.
@@ -54,23 +57,45 @@ __device__ void chol_smem(double* s, int l, int* status) {
   __syncthreads();
 }
 
-// Accumulate this CTA's rows of A^T A into per-thread pairs (staging rows in shared memory).
-__device__ void gram_rows(const double* A, int l, int64_t r0, int64_t r1, double* stage, double (&acc)[8]) {
-  const int npairs = l * l;
+// This CTA's rows [r0, r1) of A^T A (A: n x l row-major) added into a 4 x 4 register tile per
+// thread; stage holds kStageRows x l4 doubles. Threads past the (l4/4)^2 tiles only stage.
+__device__ void gram_rows(const double* A, int l, int64_t r0, int64_t r1, double* stage, double (&acc)[4][4]) {
+  const int l4 = (l + 3) & ~3, nb = l4 / 4;
+  const bool active = threadIdx.x < nb * nb;
+  const int i0 = active ? (threadIdx.x / nb) * 4 : 0, j0 = active ? (threadIdx.x % nb) * 4 : 0;
   for (int64_t b = r0; b < r1; b += kStageRows) {
     const int nr = (int)(r1 - b < kStageRows ? r1 - b : kStageRows);
     __syncthreads();
-    for (int t = threadIdx.x; t < nr * l; t += blockDim.x) stage[t] = A[b * l + t];
+    for (int t = threadIdx.x; t < nr * l4; t += blockDim.x) {
+      const int r = t / l4, c = t - r * l4;
+      stage[t] = c < l ? A[(b + r) * l + c] : 0.0;
+    }
     __syncthreads();
-    for (int q = 0; q < 8; ++q) {
-      const int p = threadIdx.x + q * blockDim.x;
-      if (p >= npairs) break;
-      const int i = p / l, j = p - i * l;
-      double s = acc[q];
-      for (int r = 0; r < nr; ++r) s = fma(stage[r * l + i], stage[r * l + j], s);
-      acc[q] = s;
+    if (active) {
+      for (int r = 0; r < nr; ++r) {
+        const double2 a01 = *reinterpret_cast<const double2*>(stage + r * l4 + i0);
+        const double2 a23 = *reinterpret_cast<const double2*>(stage + r * l4 + i0 + 2);
+        const double2 b01 = *reinterpret_cast<const double2*>(stage + r * l4 + j0);
+        const double2 b23 = *reinterpret_cast<const double2*>(stage + r * l4 + j0 + 2);
+        const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+      }
     }
   }
+}
+
+__device__ void store_gram_part(const double (&acc)[4][4], int l, double* part) {
+  const int l4 = (l + 3) & ~3, nb = l4 / 4;
+  if (threadIdx.x >= nb * nb) return;
+  const int i0 = (threadIdx.x / nb) * 4, j0 = (threadIdx.x % nb) * 4;
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+      if (i0 + x < l && j0 + y < l) part[(int64_t)blockIdx.x * l * l + (i0 + x) * l + j0 + y] = acc[x][y];
 }
 
 __device__ bool last_cta(unsigned* counter) {
@@ -95,31 +120,30 @@ __device__ void reduce_pairs(const double* part, int nblk, int npairs, double* o
   __syncthreads();
 }
 
-__device__ void trsm_row(const double* a, const double* R, int l, double* x) {
-  for (int j = 0; j < l; ++j) {
-    double v = a[j];
-    for (int k = 0; k < j; ++k) v -= x[k] * R[k * l + j];
-    x[j] = v / R[j * l + j];
-  }
+__device__ __forceinline__ void row_range(int64_t N, int64_t& r0, int64_t& r1) {
+  const int64_t rpb = (N + gridDim.x - 1) / gridDim.x;
+  r0 = blockIdx.x * rpb;
+  r1 = (N < r0 + rpb ? N : r0 + rpb);
+  if (r0 > r1) r0 = r1;
 }
+
+// Column-strided pass over this CTA's rows: thread t owns column t % l of rows
+// r0 + t / l, r0 + t / l + T / l, ... with T = l * (blockDim / l) threads.
+__device__ __forceinline__ int col_threads(int l) { return l * (blockDim.x / l); }
 
 __global__ void __launch_bounds__(kThreads) k_upd1(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* stage = sm;  // kStageRows * l (also reused for the l*l reduction)
-  const int64_t rpb = (a.N + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * rpb, r1 = (a.N < r0 + rpb ? a.N : r0 + rpb);
+  double* stage = sm;  // max(kStageRows, l) x l4
+  int64_t r0, r1;
+  row_range(a.N, r0, r1);
   if (a.H2) {
     for (int64_t t = r0 * l + threadIdx.x; t < r1 * l; t += blockDim.x) a.H[t] = a.H1[t] + a.H2[t];
     __syncthreads();
-    __threadfence_block();
   }
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[4][4] = {};
   gram_rows(a.H, l, r0, r1, stage, acc);
-  for (int q = 0; q < 8; ++q) {
-    const int p = threadIdx.x + q * blockDim.x;
-    if (p < l * l) a.part[(int64_t)blockIdx.x * l * l + p] = acc[q];
-  }
+  store_gram_part(acc, l, a.part);
   if (!last_cta(&a.counters[0])) return;
   reduce_pairs(a.part, gridDim.x, l * l, stage);
   chol_smem(stage, l, a.status);
@@ -127,40 +151,37 @@ __global__ void __launch_bounds__(kThreads) k_upd1(UpdateArgs a) {
   if (threadIdx.x == 0) a.counters[0] = 0;
 }
 
+template <int LMAX>
 __global__ void __launch_bounds__(kThreads) k_upd2(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* R = sm;            // l*l
-  double* stage = sm + l * l;  // kStageRows * l
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) R[t] = a.R1[t];
+  double* R = sm;                    // LMAX x LMAX (row stride LMAX)
+  double* stage = sm + LMAX * LMAX;  // max(kStageRows, l) x l4
+  stage_r<LMAX>(a.R1, l, R);
   __syncthreads();
-  const int64_t rpb = (a.N + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * rpb, r1 = (a.N < r0 + rpb ? a.N : r0 + rpb);
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-    double x[kLmax];
-    trsm_row(a.H + r * l, R, l, x);
-    for (int j = 0; j < l; ++j) a.Q[r * l + j] = x[j];
-  }
+  int64_t r0, r1;
+  row_range(a.N, r0, r1);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) solve_row_upper<LMAX>(a.H + r * l, R, l, a.Q + r * l);
   __syncthreads();
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[4][4] = {};
   gram_rows(a.Q, l, r0, r1, stage, acc);
-  for (int q = 0; q < 8; ++q) {
-    const int p = threadIdx.x + q * blockDim.x;
-    if (p < l * l) a.part[(int64_t)blockIdx.x * l * l + p] = acc[q];
-  }
+  store_gram_part(acc, l, a.part);
   if (!last_cta(&a.counters[1])) return;
-  double* W = stage;  // the stage area holds max(kStageRows, l) * l doubles
   double* Rn = R;
-  reduce_pairs(a.part, gridDim.x, l * l, Rn);  // Rn <- W2 (R1 no longer needed)
+  reduce_pairs(a.part, gridDim.x, l * l, Rn);  // Rn <- W2 (row stride l; R1 no longer needed)
   chol_smem(Rn, l, a.status);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R2[t] = Rn[t];
   __syncthreads();
-  // top l x l block of Q = Q1[0:l] R2^-1, then the modified LU for the Householder signs
-  double* top = W;  // l*l doubles in the stage area
+  // top l x l block of Q = Q1[0:l] R2^-1 (substitution in shared memory), then the modified
+  // LU for the Householder signs
+  double* top = stage;
   for (int r = threadIdx.x; r < l; r += blockDim.x) {
-    double x[kLmax];
-    trsm_row(a.Q + (int64_t)r * l, Rn, l, x);
-    for (int j = 0; j < l; ++j) top[r * l + j] = x[j];
+    const double* q = a.Q + (int64_t)r * l;
+    for (int j = 0; j < l; ++j) {
+      double v = q[j];
+      for (int k = 0; k < j; ++k) v -= top[r * l + k] * Rn[k * l + j];
+      top[r * l + j] = v / Rn[j * l + j];
+    }
   }
   __syncthreads();
   for (int i = 0; i < l; ++i) {
@@ -184,46 +205,40 @@ __global__ void __launch_bounds__(kThreads) k_upd2(UpdateArgs a) {
   if (threadIdx.x == 0) a.counters[1] = 0;
 }
 
+template <int LMAX>
 __global__ void __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* R = sm;                // l*l
-  double* red = sm + l * l;      // 2 * l sums per warp slot: [nwarps][2l]
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) R[t] = a.R2[t];
-  const int nwarps = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x & 31;
-  for (int t = threadIdx.x; t < nwarps * 2 * l; t += blockDim.x) red[t] = 0.0;
+  double* R = sm;                  // LMAX x LMAX (row stride LMAX)
+  double* red = sm + LMAX * LMAX;  // kThreads x 2
+  stage_r<LMAX>(a.R2, l, R);
   __syncthreads();
-  const int64_t rpb = (a.N + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * rpb, r1 = (a.N < r0 + rpb ? a.N : r0 + rpb);
-  double dm[kLmax], dp[kLmax];
-  for (int j = 0; j < l; ++j) dm[j] = dp[j] = 0.0;
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-    double x[kLmax];
-    trsm_row(a.Q + r * l, R, l, x);
-    for (int j = 0; j < l; ++j) {
-      a.Q[r * l + j] = x[j];
-      const double o = a.Omg2[r * l + j], q = x[j] * a.D[j];
-      dm[j] += fabs(o - q);
-      dp[j] += fabs(o + q);
+  int64_t r0, r1;
+  row_range(a.N, r0, r1);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) solve_row_upper<LMAX>(a.Q + r * l, R, l, a.Q + r * l);
+  __syncthreads();  // this CTA's rows of Q are written
+  const int T = col_threads(l);
+  double dm = 0.0, dp = 0.0;
+  if (threadIdx.x < T) {
+    const int c = threadIdx.x % l;
+    const double d = a.D[c];
+    for (int64_t r = r0 + threadIdx.x / l; r < r1; r += T / l) {
+      const double o = a.Omg2[r * l + c], q = a.Q[r * l + c] * d;
+      dm += fabs(o - q);
+      dp += fabs(o + q);
     }
   }
-  // block reduction of dm, dp (warp shuffle, then fixed-order sum over warps)
-  for (int j = 0; j < l; ++j) {
-    double u = dm[j], v = dp[j];
-    for (int o = 16; o; o >>= 1) {
-      u += __shfl_xor_sync(0xffffffffu, u, o);
-      v += __shfl_xor_sync(0xffffffffu, v, o);
-    }
-    if (lane == 0) {
-      red[warp * 2 * l + j] = u;
-      red[warp * 2 * l + l + j] = v;
-    }
-  }
+  red[threadIdx.x * 2] = dm;
+  red[threadIdx.x * 2 + 1] = dp;
   __syncthreads();
-  for (int t = threadIdx.x; t < 2 * l; t += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < nwarps; ++w) s += red[w * 2 * l + t];
-    a.part[(int64_t)blockIdx.x * 2 * l + t] = s;
+  for (int c = threadIdx.x; c < l; c += blockDim.x) {  // fixed-order sum over this column's threads
+    double m = 0.0, p = 0.0;
+    for (int t = c; t < T; t += l) {
+      m += red[t * 2];
+      p += red[t * 2 + 1];
+    }
+    a.part[(int64_t)blockIdx.x * 2 * l + c] = m;
+    a.part[(int64_t)blockIdx.x * 2 * l + l + c] = p;
   }
   if (!last_cta(&a.counters[2])) return;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
@@ -240,21 +255,22 @@ __global__ void __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
 __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  const int nwarps = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x & 31;
-  double* red = sm;  // [nwarps][l]
-  const int64_t rpb = (a.N + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = blockIdx.x * rpb, r1 = (a.N < r0 + rpb ? a.N : r0 + rpb);
-  double cs[kLmax];
-  for (int j = 0; j < l; ++j) cs[j] = 0.0;
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-    const int64_t kp = tc_pos(r);
-    for (int j = 0; j < l; ++j) {
-      const double v = a.Q[r * l + j] * a.mult[j];
+  double* red = sm;  // kThreads
+  int64_t r0, r1;
+  row_range(a.N, r0, r1);
+  const int T = col_threads(l);
+  double cs = 0.0;
+  if (threadIdx.x < T) {
+    const int j = threadIdx.x % l;
+    const double mj = a.mult[j];
+    for (int64_t r = r0 + threadIdx.x / l; r < r1; r += T / l) {
+      const double v = a.Q[r * l + j] * mj;
       a.Omg[r * l + j] = v;
       a.Omg2[r * l + j] = v;
-      cs[j] += v;
+      cs += v;
       if (a.Omgf) a.Omgf[r * l + j] = (float)v;
       if (a.bt1) {
+        const int64_t kp = tc_pos(r);
         const float x = (float)v;
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
         a.bt1[bt_elem(j, kp, 2 * a.bt_half)] = hi;
@@ -262,16 +278,12 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
       }
     }
   }
-  for (int j = 0; j < l; ++j) {
-    double u = cs[j];
-    for (int o = 16; o; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
-    if (lane == 0) red[warp * l + j] = u;
-  }
+  red[threadIdx.x] = cs;
   __syncthreads();
-  for (int t = threadIdx.x; t < l; t += blockDim.x) {
+  for (int c = threadIdx.x; c < l; c += blockDim.x) {
     double s = 0.0;
-    for (int w = 0; w < nwarps; ++w) s += red[w * l + t];
-    a.part[(int64_t)blockIdx.x * l + t] = s;
+    for (int t = c; t < T; t += l) s += red[t];
+    a.part[(int64_t)blockIdx.x * l + c] = s;
   }
   if (!last_cta(&a.counters[3])) return;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
@@ -282,23 +294,43 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   if (threadIdx.x == 0) a.counters[3] = 0;
 }
 
+template <int LMAX>
+void launch_all(pcaone_ctx* c, const UpdateArgs& a) {
+  const int l4 = (a.l + 3) & ~3;
+  const size_t sstage = (size_t)std::max(kStageRows, a.l) * l4 * 8;  // staged rows or an l x l matrix
+  const size_t s1 = sstage;
+  const size_t s2 = (size_t)LMAX * LMAX * 8 + sstage;
+  const size_t s3 = (size_t)LMAX * LMAX * 8 + (size_t)kThreads * 2 * 8;
+  const size_t s4 = (size_t)kThreads * 8;
+  static bool attr = false;  // shared memory above 48 KB for the widest sketches
+  if (!attr) {
+    PG_CUDA(cudaFuncSetAttribute(k_upd2<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)((size_t)LMAX * LMAX * 8 + (size_t)std::max(kStageRows, LMAX) * LMAX * 8)));
+    attr = true;
+  }
+  k_upd1<<<a.nblk, kThreads, s1, c->stream>>>(a);
+  PG_CHECK_LAUNCH();
+  k_upd2<LMAX><<<a.nblk, kThreads, s2, c->stream>>>(a);
+  PG_CHECK_LAUNCH();
+  k_upd3<LMAX><<<a.nblk, kThreads, s3, c->stream>>>(a);
+  PG_CHECK_LAUNCH();
+  k_upd4<<<a.nblk, kThreads, s4, c->stream>>>(a);
+  PG_CHECK_LAUNCH();
+}
+
 }  // namespace
 
 void fused_update(pcaone_ctx* c, UpdateArgs a) {
   PG_REQUIRE(a.l >= 1 && a.l <= kLmax, PCAONE_EBADARG, "sketch width out of range");
-  const int nblk = a.nblk;
-  const size_t s1 = (size_t)std::max(kStageRows, a.l) * a.l * 8;  // staged rows or an l x l matrix
-  const size_t s2 = (size_t)a.l * a.l * 8 + s1;
-  const size_t s3 = (size_t)a.l * a.l * 8 + (size_t)(kThreads / 32) * 2 * a.l * 8;
-  const size_t s4 = (size_t)(kThreads / 32) * a.l * 8;
-  k_upd1<<<nblk, kThreads, s1, c->stream>>>(a);
-  PG_CHECK_LAUNCH();
-  k_upd2<<<nblk, kThreads, s2, c->stream>>>(a);
-  PG_CHECK_LAUNCH();
-  k_upd3<<<nblk, kThreads, s3, c->stream>>>(a);
-  PG_CHECK_LAUNCH();
-  k_upd4<<<nblk, kThreads, s4, c->stream>>>(a);
-  PG_CHECK_LAUNCH();
+  PG_REQUIRE(((a.l + 3) / 4) * ((a.l + 3) / 4) <= kThreads, PCAONE_EBADARG, "sketch width too large for the update");
+  if (a.l <= 16)
+    launch_all<16>(c, a);
+  else if (a.l <= 32)
+    launch_all<32>(c, a);
+  else if (a.l <= 48)
+    launch_all<48>(c, a);
+  else
+    launch_all<64>(c, a);
   c->launches += 4;
 }
 

@@ -25,4 +25,33 @@ void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);
 void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y);
 void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out);
 
+// Forward substitution for one row: x R = a with R upper l x l stored row-major with the
+// compile-time row stride LMAX (so every R address is a constant offset), x kept in registers
+// (LMAX >= l; the loops unroll over LMAX and skip j >= l). Every element of a is read before
+// out is written, so out may alias a.
+template <int LMAX>
+__device__ __forceinline__ void solve_row_upper(const double* a, const double* Rs, int l, double* out) {
+  double x[LMAX];
+#pragma unroll
+  for (int j = 0; j < LMAX; ++j) {
+    if (j < l) {
+      double v = a[j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v -= x[k] * Rs[k * LMAX + j];
+      x[j] = v / Rs[j * LMAX + j];
+    } else {
+      x[j] = 0.0;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < LMAX; ++j)
+    if (j < l) out[j] = x[j];
+}
+
+// Copy R (l x l row-major) into shared memory with row stride LMAX.
+template <int LMAX>
+__device__ __forceinline__ void stage_r(const double* R, int l, double* Rs) {
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) Rs[(t / l) * LMAX + t % l] = R[t];
+}
+
 }  // namespace pg

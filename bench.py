@@ -426,6 +426,28 @@ def run_profile_kernel(args, cfg):
                       "checksum": float(np.abs(out).sum())}))
 
 
+def run_profile_step(args, cfg):
+    """Small command for ncu: --steps RSVD runs of the configured workload through the C ABI
+    (load, shuffle, then the full power iteration), then exit. No child processes, no torch."""
+    import pcaone_b200 as pb
+
+    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
+    os.makedirs(workdir, exist_ok=True)
+    prefix = os.path.join(workdir, args.config)
+    make_data(cfg, prefix)
+    packed, N, M = pb.read_bed(prefix)
+    rs_kw = dict(k=cfg["k"], oversamples=10, maxp=cfg["maxp"], svd=cfg["svd"], bands=cfg["bands"],
+                 tol=cfg["tol"], seed=101)
+    with pb.GpuContext(0) as ctx:
+        ctx.load_bed(packed, N)
+        if cfg["svd"] == 2:
+            ctx.permute(pb.shuffle_perm(M))
+        for _ in range(args.steps):
+            r = ctx.rsvd(precision=args.precision, **rs_kw)
+    print(json.dumps({"profile_step": args.precision, "samples": N, "snps": M, "epochs": r.epochs,
+                      "launches": r.kernel_launches, "gpu_ms": r.gpu_ms}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -438,10 +460,14 @@ def main():
     ap.add_argument("--skip-compare", action="store_true")
     ap.add_argument("--profile-kernel", action="store_true",
                     help="run --steps products Z^T Omega only (a small command for ncu)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="run --steps RSVDs of the config only (a small command for ncu)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.profile_kernel:
         run_profile_kernel(args, cfg)
+    elif args.profile_step:
+        run_profile_step(args, cfg)
     elif args.impl == "reference":
         run_reference_arm(args, cfg)
     else:

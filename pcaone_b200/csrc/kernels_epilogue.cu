@@ -20,16 +20,21 @@ namespace pg {
 
 namespace {
 
-// Warp-cooperative sparse gather: acc_c += sum_{e in [e0, e1)} w_e * rows[idx_e][c] for the
-// lane's columns c = lane and lane + 32 (l <= 64), summed in entry order. The warp loads 32
-// entries (index and weight) at once, then broadcasts them and keeps four row loads in flight,
-// so the cost is a few L2 latencies per 32 entries instead of two per entry.
-template <typename Wt>
+// Warp-cooperative sparse gather: out[c] = sum_{e in [e0, e1)} w_e * rows[idx_e][c] for all
+// c < l. The warp loads 32 entries (index and weight) at once; then four 8-lane groups each
+// take one entry per step (two steps unrolled, so eight rows are in flight), and lane q of a
+// group owns the CPL = ceil(l/8) consecutive columns q*CPL.., so one row is one coalesced
+// segment per group and each entry costs about five warp instructions. The groups' sums are
+// combined with two shuffle levels in a fixed order (deterministic) and written to out
+// (shared memory of this warp).
+template <int CPL, typename Wt>
 __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                             const double* __restrict__ rows, int l, Wt weight,
-                                            double& acc0, double& acc1) {
-  const int lane = threadIdx.x & 31;
-  const bool c0 = lane < l, c1 = lane + 32 < l;
+                                            double* out) {
+  const int lane = threadIdx.x & 31, grp = lane >> 3, c0 = (lane & 7) * CPL;
+  double acc[CPL];
+#pragma unroll
+  for (int k = 0; k < CPL; ++k) acc[k] = 0.0;
   for (int64_t base = e0; base < e1; base += 32) {
     const int64_t e = base + lane;
     int my_i = 0;
@@ -39,52 +44,63 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
       my_w = weight(e, my_i);
     }
     const int cnt = (int)(e1 - base < 32 ? e1 - base : 32);
-    for (int t = 0; t < cnt; t += 4) {
-      int it[4];
-      double wt[4], v0[4], v1[4];
+    for (int t = 0; t < cnt; t += 8) {
+      int it[2];
+      double wt[2], v[2][CPL];
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        it[g] = __shfl_sync(0xffffffffu, my_i, (t + g) & 31);
-        wt[g] = __shfl_sync(0xffffffffu, my_w, (t + g) & 31);
+      for (int h = 0; h < 2; ++h) {
+        const int src = t + 4 * h + grp;
+        it[h] = __shfl_sync(0xffffffffu, my_i, src & 31);
+        wt[h] = __shfl_sync(0xffffffffu, my_w, src & 31);
+        if (src >= cnt) wt[h] = 0.0;
       }
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const double* r = rows + (int64_t)it[g] * l;
-        const bool ok = t + g < cnt;
-        v0[g] = (ok && c0) ? r[lane] : 0.0;
-        v1[g] = (ok && c1) ? r[lane + 32] : 0.0;
+      for (int h = 0; h < 2; ++h) {
+        const double* r = rows + (int64_t)it[h] * l + c0;
+        const bool ok = t + 4 * h + grp < cnt;
+#pragma unroll
+        for (int k = 0; k < CPL; ++k) v[h][k] = (ok && c0 + k < l) ? r[k] : 0.0;
       }
 #pragma unroll
-      for (int g = 0; g < 4; ++g)
-        if (t + g < cnt) {
-          acc0 += wt[g] * v0[g];
-          acc1 += wt[g] * v1[g];
-        }
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < CPL; ++k) acc[k] = fma(wt[h], v[h][k], acc[k]);
     }
   }
+#pragma unroll
+  for (int k = 0; k < CPL; ++k) {
+    acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], 8);
+    acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], 16);
+  }
+  if (grp == 0) {
+#pragma unroll
+    for (int k = 0; k < CPL; ++k)
+      if (c0 + k < l) out[c0 + k] = acc[k];
+  }
+  __syncwarp();
 }
 
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
 // per-CTA partials of h0.
-template <typename T>
+template <typename T, int CPL>
 __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
-  extern __shared__ double sh0[];  // warps x l
+  extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  double* ssp = sh0 + nwarps * p.l + warp * p.l;
   for (int c = lane; c < p.l; c += 32) sh0[warp * p.l + c] = 0.0;
   for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < p.m; jl += (int64_t)gridDim.x * nwarps) {
     const int64_t j = p.start + jl;
     const double F = p.F[j];
     const double s = p.scale[j];
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
-    double sp0 = 0.0, sp1 = 0.0;
     const double* mv = p.miss_val;
-    gather_rows(e0, e1, p.miss_idx, p.omega, p.l,
-                [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; }, sp0, sp1);
+    gather_rows<CPL>(e0, e1, p.miss_idx, p.omega, p.l, [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; },
+                     ssp);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * p.m + jl) * p.l + c];
-      const double sparse = c < 32 ? sp0 : sp1;
+      const double sparse = ssp[c];
       double g = s * (0.5 * d - F * p.wsum[c] + sparse);
       p.G[j * p.l + c] = g;
       const T b2 = (T)(0.5 * s * g);
@@ -100,6 +116,7 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
       }
       sh0[warp * p.l + c] += s * F * g;
     }
+    __syncwarp();  // ssp is rewritten for the next SNP
   }
   if (p.bt2) {  // positions m..kpad2 of the split operand: zero (a shorter window follows a longer one)
     const int64_t tail = p.kpad2 - p.m, tot = tail * 2 * p.l;
@@ -156,23 +173,25 @@ __global__ void k_reduce_cols(const double* __restrict__ part, int nblk, int l, 
 }
 
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse.
-template <typename T>
+template <typename T, int CPL>
 __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
+  extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  double* ssp = ssm + warp * p.l;
   for (int64_t i = (int64_t)blockIdx.x * nwarps + warp; i < p.n; i += (int64_t)gridDim.x * nwarps) {
     const int64_t row = (int64_t)p.window * p.npad + i;
     const int64_t e0 = p.miss_ptr[row], e1 = p.miss_ptr[row + 1];
-    double sp0 = 0.0, sp1 = 0.0;
     const double* mv = p.miss_val;
     const double *sc = p.scale, *F = p.F;
-    gather_rows(e0, e1, p.miss_idx, p.G, p.l,
-                [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); }, sp0, sp1);
+    gather_rows<CPL>(e0, e1, p.miss_idx, p.G, p.l,
+                     [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); }, ssp);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D2[((int64_t)sp * p.n + i) * p.l + c];
-      const double sparse = c < 32 ? sp0 : sp1;
+      const double sparse = ssp[c];
       p.H[i * p.l + c] += d - p.h0[c] + sparse;
     }
+    __syncwarp();  // ssp is rewritten for the next row
   }
 }
 
@@ -183,7 +202,17 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
   const int threads = 256, nwarps = threads / 32;
   int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
   double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
-  k_prep<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p, D1, B2, part);
+  const size_t smem = (size_t)2 * nwarps * p.l * 8;
+  switch ((p.l + 7) / 8) {
+    case 1: k_prep<T, 1><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 2: k_prep<T, 2><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 3: k_prep<T, 3><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 4: k_prep<T, 4><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 5: k_prep<T, 5><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 6: k_prep<T, 6><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 7: k_prep<T, 7><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    default: k_prep<T, 8><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+  }
   PG_CHECK_LAUNCH();
   k_reduce_cols<<<1, 512, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
@@ -194,7 +223,17 @@ template <typename T>
 void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
   const int threads = 256, nwarps = threads / 32;
   int nblk = (int)std::min<int64_t>(4 * c->sm_count, (p.n + nwarps - 1) / nwarps);
-  k_accum<T><<<nblk, threads, 0, c->stream>>>(p, D2);
+  const size_t smem = (size_t)nwarps * p.l * 8;
+  switch ((p.l + 7) / 8) {
+    case 1: k_accum<T, 1><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 2: k_accum<T, 2><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 3: k_accum<T, 3><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 4: k_accum<T, 4><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 5: k_accum<T, 5><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 6: k_accum<T, 6><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 7: k_accum<T, 7><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    default: k_accum<T, 8><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+  }
   PG_CHECK_LAUNCH();
   c->launches++;
 }

@@ -20,6 +20,7 @@ on the host cores, on a bounded sample of the same workload (all samples, a slic
 from __future__ import annotations
 
 import argparse
+import re
 import json
 import os
 import shutil
@@ -280,11 +281,12 @@ def run_ours(args, cfg):
     achieved_tflops = alg_flops / (prof.gemm_ms / 1e3) / 1e12
     pk, pk_kind = peaks()
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "decode_gemm_tc_traffic.json")
-    if os.path.exists(tpath):
+    traffic = None  # DRAM bytes per launch from the committed ncu summary of this kernel
+    tpath = os.path.join(ROOT, "profiles", "k_decode_gemm_tc_c2.md")
+    if prec == "mixed" and args.config == "c2" and os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_launch_scaled")
+            mt = re.search(r"^traffic_bytes_per_launch:\s*([0-9]+)", f.read(), re.M)
+        traffic = int(mt.group(1)) if mt else None
     roofline = {"bound": "tensor", "achieved": round(achieved_tflops, 2), "peak": peak,
                 "unit": "TFLOP/s", "frac": round(achieved_tflops / peak, 4), "traffic": traffic,
                 "peak_source": f"{pk_kind} bf16_tflops_sustained",

@@ -22,16 +22,17 @@ namespace {
 
 // Warp-cooperative sparse gather: out[c] = sum_{e in [e0, e1)} w_e * rows[idx_e][c] for all
 // c < l. The warp loads 32 entries (index and weight) at once; then four 8-lane groups each
-// take one entry per step (two steps unrolled, so eight rows are in flight), and lane q of a
-// group owns the CPL = ceil(l/8) consecutive columns q*CPL.., so one row is one coalesced
-// segment per group and each entry costs about five warp instructions. The groups' sums are
-// combined with two shuffle levels in a fixed order (deterministic) and written to out
-// (shared memory of this warp).
+// take one entry per step (two steps unrolled, so eight rows are in flight), and lane q of
+// a group owns the columns q, q + 8, ..., so each load instruction reads one contiguous
+// 64-byte segment of a row per group and each entry costs a few warp instructions. The
+// groups' sums are combined with two shuffle levels in a fixed order (deterministic) and
+// written to out (shared memory of this warp). CPL = ceil(l / 8).
 template <int CPL, typename Wt>
 __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                             const double* __restrict__ rows, int l, Wt weight,
                                             double* out) {
-  const int lane = threadIdx.x & 31, grp = lane >> 3, c0 = (lane & 7) * CPL;
+  constexpr int kSteps = 2;
+  const int lane = threadIdx.x & 31, grp = lane >> 3, q = lane & 7;
   double acc[CPL];
 #pragma unroll
   for (int k = 0; k < CPL; ++k) acc[k] = 0.0;
@@ -44,25 +45,25 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
       my_w = weight(e, my_i);
     }
     const int cnt = (int)(e1 - base < 32 ? e1 - base : 32);
-    for (int t = 0; t < cnt; t += 8) {
-      int it[2];
-      double wt[2], v[2][CPL];
+    for (int t = 0; t < cnt; t += 4 * kSteps) {
+      int it[kSteps];
+      double wt[kSteps], v[kSteps][CPL];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < kSteps; ++h) {
         const int src = t + 4 * h + grp;
         it[h] = __shfl_sync(0xffffffffu, my_i, src & 31);
         wt[h] = __shfl_sync(0xffffffffu, my_w, src & 31);
         if (src >= cnt) wt[h] = 0.0;
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double* r = rows + (int64_t)it[h] * l + c0;
+      for (int h = 0; h < kSteps; ++h) {
+        const double* r = rows + (int64_t)it[h] * l + q;
         const bool ok = t + 4 * h + grp < cnt;
 #pragma unroll
-        for (int k = 0; k < CPL; ++k) v[h][k] = (ok && c0 + k < l) ? r[k] : 0.0;
+        for (int k = 0; k < CPL; ++k) v[h][k] = (ok && q + 8 * k < l) ? r[8 * k] : 0.0;
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+      for (int h = 0; h < kSteps; ++h)
 #pragma unroll
         for (int k = 0; k < CPL; ++k) acc[k] = fma(wt[h], v[h][k], acc[k]);
     }
@@ -75,7 +76,7 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
   if (grp == 0) {
 #pragma unroll
     for (int k = 0; k < CPL; ++k)
-      if (c0 + k < l) out[c0 + k] = acc[k];
+      if (q + 8 * k < l) out[q + 8 * k] = acc[k];
   }
   __syncwarp();
 }

@@ -111,12 +111,25 @@ __device__ bool last_cta(unsigned* counter) {
   return last;
 }
 
-__device__ void reduce_pairs(const double* part, int nblk, int npairs, double* out_smem) {
-  for (int p = threadIdx.x; p < npairs; p += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * npairs + p];
-    out_smem[p] = s;
+// sum_{b < n} x[b * stride], added in b order (the same result as the plain loop); the loads
+// of eight terms are issued before their adds, so they overlap instead of paying one L2
+// round trip per term.
+__device__ __forceinline__ double sum_strided(const double* x, int n, int64_t stride) {
+  double s = 0.0;
+  int b = 0;
+  for (; b + 8 <= n; b += 8) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = x[(int64_t)(b + k) * stride];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += v[k];
   }
+  for (; b < n; ++b) s += x[(int64_t)b * stride];
+  return s;
+}
+
+__device__ void reduce_pairs(const double* part, int nblk, int npairs, double* out_smem) {
+  for (int p = threadIdx.x; p < npairs; p += blockDim.x) out_smem[p] = sum_strided(part + p, nblk, npairs);
   __syncthreads();
 }
 
@@ -242,11 +255,8 @@ __global__ void __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
   }
   if (!last_cta(&a.counters[2])) return;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
-    double m = 0.0, p = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      m += a.part[(int64_t)b * 2 * l + j];
-      p += a.part[(int64_t)b * 2 * l + l + j];
-    }
+    const double m = sum_strided(a.part + j, gridDim.x, 2 * l);
+    const double p = sum_strided(a.part + l + j, gridDim.x, 2 * l);
     a.mult[j] = (m > 2.0 * p) ? -a.D[j] : a.D[j];  // src/RSVD.hpp:85
   }
   if (threadIdx.x == 0) a.counters[2] = 0;
@@ -286,11 +296,7 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
     a.part[(int64_t)blockIdx.x * l + c] = s;
   }
   if (!last_cta(&a.counters[3])) return;
-  for (int j = threadIdx.x; j < l; j += blockDim.x) {
-    double s = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) s += a.part[(int64_t)b * l + j];
-    a.wsum[j] = s;
-  }
+  for (int j = threadIdx.x; j < l; j += blockDim.x) a.wsum[j] = sum_strided(a.part + j, gridDim.x, l);
   if (threadIdx.x == 0) a.counters[3] = 0;
 }
 

@@ -240,6 +240,7 @@ k_decode_gemm_tc(const __grid_constant__ TcArgs args) {
   uint64_t* done = acc_full + 4;               // [1]  every MMA of this CTA complete
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(acc_full + 5);
   volatile int* abort_flag = (volatile int*)(acc_full + 6);
+  float* stg_all = (float*)(acc_full + 8);       // [4 readout warps][32 rows][9] output staging
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t u0 = unit_begin(blockIdx.x, args), u1 = unit_begin(blockIdx.x + 1, args);
@@ -383,9 +384,11 @@ k_decode_gemm_tc(const __grid_constant__ TcArgs args) {
       tc_fence_after();
       const int64_t first_cta = cta_of_unit(tile * P, args);
       const int slot = (int)(blockIdx.x - first_cta);
-      const int64_t row = tile * kTileRows + q4 * 32 + lane;
-      const bool valid = row < args.rows;
-      float* o = args.out + ((int64_t)slot * args.rows + (valid ? row : 0)) * args.l;
+      // rows row0 .. row0 + nvalid - 1 of this warp are contiguous in the output slot
+      const int64_t row0 = tile * kTileRows + q4 * 32;
+      const int nvalid = (int)(args.rows - row0 < 32 ? (args.rows - row0 > 0 ? args.rows - row0 : 0) : 32);
+      float* stg = stg_all + q4 * 32 * 9;
+      float* o = args.out + ((int64_t)slot * args.rows + row0) * args.l;
 #pragma unroll
       for (int c0 = 0; c0 < NP / 2; c0 += 8) {  // hi columns c0.., lo columns NP/2 + c0..
         uint32_t hv[8], lv[8];
@@ -393,16 +396,23 @@ k_decode_gemm_tc(const __grid_constant__ TcArgs args) {
         tmem_ld8(tmem + lane_base + b * NP + NP / 2 + c0, lv);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (valid && c0 + j < args.l) o[c0 + j] = __uint_as_float(hv[j]) + __uint_as_float(lv[j]);
+        for (int j = 0; j < 8; ++j) stg[lane * 9 + j] = __uint_as_float(hv[j]) + __uint_as_float(lv[j]);
+        __syncwarp();
+        // each store instruction writes 4 rows x 8 columns = four full 32-byte sectors
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int rr = 4 * k + (lane >> 3), e = lane & 7;
+          if (rr < nvalid && c0 + e < args.l) o[(int64_t)rr * args.l + c0 + e] = stg[rr * 9 + e];
+        }
+        __syncwarp();
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
-      if (valid && tile_end) {  // zero the slots this tile does not use
+      if (tile_end) {  // zero the slots this tile does not use: nvalid contiguous rows each
         for (int sl = slot + 1; sl < args.ks; ++sl) {
-          float* z = args.out + ((int64_t)sl * args.rows + row) * args.l;
-          for (int c = 0; c < args.l; ++c) z[c] = 0.0f;
+          float* z = args.out + ((int64_t)sl * args.rows + row0) * args.l;
+          for (int t = lane; t < nvalid * args.l; t += 32) z[t] = 0.0f;
         }
       }
       u = seg_end;
@@ -470,7 +480,7 @@ int np_of(int l) { return (int)round_up(2 * l, 16); }
 // at least 100 KB to keep a third CTA from becoming resident.
 size_t smem_bytes(int np) {
   const int S = ring_stages(np);
-  const size_t need = 1024 + (size_t)S * stage_bytes(np) + (2 * S + 16) * 8;
+  const size_t need = 1024 + (size_t)S * stage_bytes(np) + (2 * S + 16) * 8 + 4 * 32 * 9 * sizeof(float);
   return std::max<size_t>(need, 100 * 1024);
 }
 

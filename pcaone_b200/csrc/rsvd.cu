@@ -21,37 +21,54 @@
 
 namespace pg {
 
-// ---------------------------------------------------------------- host helpers
-void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out) {
-  // RsvdOpData::initOmg (src/Halko.cpp:14-22): engine seeded with --seed, column-major fill.
-  std::default_random_engine rng;
-  rng.seed(seed);
-  const uint64_t n = nrow * (uint64_t)ncol;
-  if (rand) {
-    std::normal_distribution<double> d{0, 1};
-    for (uint64_t i = 0; i < n; ++i) out[i] = d(rng);
-  } else {
-    std::uniform_real_distribution<double> d{-1, 1};
-    for (uint64_t i = 0; i < n; ++i) out[i] = d(rng);
-  }
+namespace {
+// Omega column-major N x l (host layout of the reference) -> row-major Npad x l FP64 copies
+// (padding rows zero) and an optional FP32 copy.
+__global__ void k_omega_layout(const double* __restrict__ cm, int64_t N, int l, int64_t npad, double* __restrict__ O,
+                               double* __restrict__ O2, float* __restrict__ Of) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= npad * l) return;
+  const int64_t i = t / l, j = t - i * l;
+  const double v = i < N ? cm[j * N + i] : 0.0;
+  O[t] = v;
+  O2[t] = v;
+  if (Of) Of[t] = (float)v;
 }
+}  // namespace
 
+// ---------------------------------------------------------------- host helpers
 // One-sided Jacobi SVD of a small square matrix A (n x n, row-major): A = U diag(s) V^T,
 // singular values sorted in decreasing order. U, V row-major n x n.
 void jacobi_svd(int n, const double* A, double* U, double* s, double* V) {
-  std::vector<double> a(A, A + (size_t)n * n), v((size_t)n * n, 0.0);
+  // work on column-major copies so every column is contiguous; the three dot products of a
+  // pair use four partial sums each, which breaks the add-latency chains
+  std::vector<double> a((size_t)n * n), v((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) a[(size_t)j * n + i] = A[(size_t)i * n + j];
   for (int i = 0; i < n; ++i) v[(size_t)i * n + i] = 1.0;
   for (int sweep = 0; sweep < 60; ++sweep) {
     double off = 0.0;
     for (int p = 0; p < n - 1; ++p) {
+      double* ap = a.data() + (size_t)p * n;
+      double* vp = v.data() + (size_t)p * n;
       for (int q = p + 1; q < n; ++q) {
-        double alpha = 0, beta = 0, gamma = 0;
-        for (int i = 0; i < n; ++i) {
-          double ap = a[(size_t)i * n + p], aq = a[(size_t)i * n + q];
-          alpha += ap * ap;
-          beta += aq * aq;
-          gamma += ap * aq;
+        double* aq = a.data() + (size_t)q * n;
+        double* vq = v.data() + (size_t)q * n;
+        double al[4] = {0, 0, 0, 0}, be[4] = {0, 0, 0, 0}, ga[4] = {0, 0, 0, 0};
+        int i = 0;
+        for (; i + 4 <= n; i += 4)
+          for (int u = 0; u < 4; ++u) {
+            al[u] += ap[i + u] * ap[i + u];
+            be[u] += aq[i + u] * aq[i + u];
+            ga[u] += ap[i + u] * aq[i + u];
+          }
+        for (; i < n; ++i) {
+          al[0] += ap[i] * ap[i];
+          be[0] += aq[i] * aq[i];
+          ga[0] += ap[i] * aq[i];
         }
+        const double alpha = (al[0] + al[1]) + (al[2] + al[3]), beta = (be[0] + be[1]) + (be[2] + be[3]);
+        const double gamma = (ga[0] + ga[1]) + (ga[2] + ga[3]);
         if (gamma == 0.0) continue;
         double conv = std::fabs(gamma) / std::sqrt(alpha * beta);
         off = std::max(off, conv);
@@ -59,13 +76,13 @@ void jacobi_svd(int n, const double* A, double* U, double* s, double* V) {
         double zeta = (beta - alpha) / (2.0 * gamma);
         double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
         double cs = 1.0 / std::sqrt(1.0 + t * t), sn = cs * t;
-        for (int i = 0; i < n; ++i) {
-          double ap = a[(size_t)i * n + p], aq = a[(size_t)i * n + q];
-          a[(size_t)i * n + p] = cs * ap - sn * aq;
-          a[(size_t)i * n + q] = sn * ap + cs * aq;
-          double vp = v[(size_t)i * n + p], vq = v[(size_t)i * n + q];
-          v[(size_t)i * n + p] = cs * vp - sn * vq;
-          v[(size_t)i * n + q] = sn * vp + cs * vq;
+        for (int r = 0; r < n; ++r) {
+          const double x = ap[r], y = aq[r];
+          ap[r] = cs * x - sn * y;
+          aq[r] = sn * x + cs * y;
+          const double xv = vp[r], yv = vq[r];
+          vp[r] = cs * xv - sn * yv;
+          vq[r] = sn * xv + cs * yv;
         }
       }
     }
@@ -74,7 +91,7 @@ void jacobi_svd(int n, const double* A, double* U, double* s, double* V) {
   std::vector<double> norms(n);
   for (int j = 0; j < n; ++j) {
     double acc = 0;
-    for (int i = 0; i < n; ++i) acc += a[(size_t)i * n + j] * a[(size_t)i * n + j];
+    for (int i = 0; i < n; ++i) acc += a[(size_t)j * n + i] * a[(size_t)j * n + i];
     norms[j] = std::sqrt(acc);
   }
   std::vector<int> ord(n);
@@ -84,8 +101,8 @@ void jacobi_svd(int n, const double* A, double* U, double* s, double* V) {
     int j = ord[jj];
     s[jj] = norms[j];
     for (int i = 0; i < n; ++i) {
-      U[(size_t)i * n + jj] = norms[j] > 0 ? a[(size_t)i * n + j] / norms[j] : (i == jj ? 1.0 : 0.0);
-      V[(size_t)i * n + jj] = v[(size_t)i * n + j];
+      U[(size_t)i * n + jj] = norms[j] > 0 ? a[(size_t)j * n + i] / norms[j] : (i == jj ? 1.0 : 0.0);
+      V[(size_t)i * n + jj] = v[(size_t)j * n + i];
     }
   }
 }
@@ -140,18 +157,16 @@ struct Engine {
   float* omg_float() { return std::is_same<T, float>::value ? reinterpret_cast<float*>(OmgT) : nullptr; }
 
   void init_omega() {
-    std::vector<double> cm((size_t)N * l), rm((size_t)Npad * l, 0.0);
+    std::vector<double> cm((size_t)N * l);
     omega_host(o.seed, o.rand, N, l, cm.data());
-    for (int i = 0; i < N; ++i)
-      for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = cm[(size_t)j * N + i];
-    PG_CUDA(cudaMemcpyAsync(Omg, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
-    PG_CUDA(cudaMemcpyAsync(Omg2, Omg, rm.size() * 8, cudaMemcpyDeviceToDevice, c->stream));
-    if (!std::is_same<T, double>::value) {
-      std::vector<float> f(rm.begin(), rm.end());
-      PG_CUDA(cudaMemcpyAsync(OmgT, f.data(), f.size() * 4, cudaMemcpyHostToDevice, c->stream));
-    }
+    double* d_cm = (double*)scratch(c, "r_omg_cm", cm.size() * 8);
+    PG_CUDA(cudaMemcpyAsync(d_cm, cm.data(), cm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    const int64_t tot = Npad * l;
+    k_omega_layout<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(d_cm, N, l, Npad, Omg, Omg2, omg_float());
+    PG_CHECK_LAUNCH();
+    c->launches++;
     colsum(c, Omg, l, N, wsum);
-    PG_CUDA(cudaStreamSynchronize(c->stream));  // host vectors go out of scope
+    PG_CUDA(cudaStreamSynchronize(c->stream));  // the host vector goes out of scope
     gemm.omega_changed(c, Omg, l, Npad);
   }
 

@@ -27,25 +27,9 @@ static void free_ptr(void* p) {
   if (p) cudaFree(p);
 }
 
+// Forget the loaded data. Every data buffer is a named scratch buffer of the context (kept,
+// with its capacity, for the next load of the same or a smaller problem; freed by free_all).
 void free_data(pcaone_ctx* c) {
-  free_ptr(c->d_bed);
-  free_ptr(c->d_a1x2);
-  free_ptr(c->d_nonmiss);
-  free_ptr(c->d_F);
-  free_ptr(c->d_bedT);
-  free_ptr(c->d_miss_snp_ptr);
-  free_ptr(c->d_miss_snp_idx);
-  free_ptr(c->d_miss_ws_ptr);
-  free_ptr(c->d_miss_ws_idx);
-  free_ptr(c->d_F_load);
-  free_ptr(c->d_scale);
-  free_ptr(c->d_imp_US);
-  free_ptr(c->d_imp_V);
-  free_ptr(c->d_miss_snp_val);
-  free_ptr(c->d_miss_ws_val);
-  free_ptr(c->d_P);
-  free_ptr(c->d_E);
-  free_ptr(c->d_zero);
   c->d_P = nullptr;
   c->d_E = nullptr;
   c->d_zero = nullptr;
@@ -151,12 +135,13 @@ int pcaone_gpu_load_bed(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, ui
     c->pitch = c->Npad / 4;  // == round_up(bpr, kPitchAlign)
     c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
     const size_t bytes = (size_t)c->Mpad * c->pitch;
-    PG_CUDA(cudaMalloc(&c->d_bed, bytes));
-    PG_CUDA(cudaMalloc(&c->d_a1x2, c->M * 4));
-    PG_CUDA(cudaMalloc(&c->d_nonmiss, c->M * 4));
-    PG_CUDA(cudaMalloc(&c->d_F, c->M * 8));
-    PG_CUDA(cudaMalloc(&c->d_F_load, c->M * 8));
-    PG_CUDA(cudaMalloc(&c->d_scale, c->M * 8));
+    c->bed_slot = 0;
+    c->d_bed = (uint8_t*)scratch(c, "d_bed_0", bytes);
+    c->d_a1x2 = (uint32_t*)scratch(c, "d_a1x2", c->M * 4);
+    c->d_nonmiss = (uint32_t*)scratch(c, "d_nonmiss", c->M * 4);
+    c->d_F = (double*)scratch(c, "d_F", c->M * 8);
+    c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
+    c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
     PG_CUDA(cudaMemsetAsync(c->d_bed, 0xFF, bytes, c->stream));
     PG_CUDA(cudaMemcpy2DAsync(c->d_bed, c->pitch, packed, c->bpr, c->bpr, c->M,
                               cudaMemcpyHostToDevice, c->stream));
@@ -199,14 +184,14 @@ int pcaone_gpu_permute(pcaone_ctx* c, const int32_t* perm) {
     }
     int32_t* d_perm = (int32_t*)scratch(c, "perm", c->M * 4);
     PG_CUDA(cudaMemcpyAsync(d_perm, perm, c->M * 4, cudaMemcpyHostToDevice, c->stream));
-    uint8_t* out = nullptr;
+    // permute into the other of the two packed-matrix slots, then swap
     const size_t bytes = (size_t)c->Mpad * c->pitch;
-    PG_CUDA(cudaMalloc(&out, bytes));
+    uint8_t* out = (uint8_t*)scratch(c, c->bed_slot ? "d_bed_0" : "d_bed_1", bytes);
     PG_CUDA(cudaMemsetAsync(out, 0xFF, bytes, c->stream));
     launch_permute(c, d_perm, out);
     PG_CUDA(cudaStreamSynchronize(c->stream));
-    PG_CUDA(cudaFree(c->d_bed));
     c->d_bed = out;
+    c->bed_slot ^= 1;
     launch_counts(c);
     PG_CUDA(cudaStreamSynchronize(c->stream));
     c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
@@ -255,11 +240,8 @@ int pcaone_gpu_fit_emu(pcaone_ctx* c, const double* U, const double* S, const do
       for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
     for (uint64_t j = 0; j < c->M; ++j)
       for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
-    if (c->d_imp_US) cudaFree(c->d_imp_US);
-    if (c->d_imp_V) cudaFree(c->d_imp_V);
-    c->d_imp_US = c->d_imp_V = nullptr;
-    PG_CUDA(cudaMalloc(&c->d_imp_US, us.size() * 8));
-    PG_CUDA(cudaMalloc(&c->d_imp_V, v.size() * 8));
+    c->d_imp_US = (double*)scratch(c, "d_imp_US", us.size() * 8);
+    c->d_imp_V = (double*)scratch(c, "d_imp_V", v.size() * 8);
     PG_CUDA(cudaMemcpyAsync(c->d_imp_US, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
     PG_CUDA(cudaMemcpyAsync(c->d_imp_V, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
     c->imp_k = (int)k;
@@ -344,14 +326,14 @@ int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t 
     const size_t np = (size_t)nsnps * 2 * nsamples;
     std::vector<float> pf(np);
     for (size_t t = 0; t < np; ++t) pf[t] = (float)P[t];
-    PG_CUDA(cudaMalloc(&c->d_P, np * 4));
+    c->d_P = (float*)scratch(c, "d_P", np * 4);
     PG_CUDA(cudaMemcpyAsync(c->d_P, pf.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
-    PG_CUDA(cudaMalloc(&c->d_E, (size_t)c->Mpad * c->Npad * 4));
+    c->d_E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
     PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
-    PG_CUDA(cudaMalloc(&c->d_F, c->M * 8));
-    PG_CUDA(cudaMalloc(&c->d_F_load, c->M * 8));
-    PG_CUDA(cudaMalloc(&c->d_scale, c->M * 8));
-    PG_CUDA(cudaMalloc(&c->d_zero, c->M * 8));
+    c->d_F = (double*)scratch(c, "d_F", c->M * 8);
+    c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
+    c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
+    c->d_zero = (double*)scratch(c, "d_zero", c->M * 8);
     PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
     std::vector<double> q(c->M, 0.25);
     PG_CUDA(cudaMemcpyAsync(c->d_F, q.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));

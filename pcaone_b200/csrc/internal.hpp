@@ -117,6 +117,7 @@ struct pcaone_ctx {
   // key (N, l, bands, data generation) of the winSVD window sums kept between calls
   uint64_t h12_key = 0;
   uint64_t generation = 0;  // bumped by every load / permutation
+  int bed_slot = 0;         // which of the scratch buffers "d_bed_0" / "d_bed_1" holds d_bed
   // shape key and address of the zeroed split-BF16 window operand (tensor-core back end)
   int64_t bt2_shape = -1;
   void* bt2_ptr = nullptr;

@@ -205,19 +205,15 @@ void set_window_layout(pcaone_ctx* c, int bands) {
 void build_empty_missing(pcaone_ctx* c) {
   const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
   if (!c->miss_snp_valid) {
-    if (c->d_miss_snp_ptr) cudaFree(c->d_miss_snp_ptr);
-    if (c->d_miss_snp_idx) cudaFree(c->d_miss_snp_idx);
-    PG_CUDA(cudaMalloc(&c->d_miss_snp_ptr, (c->M + 1) * 8));
-    PG_CUDA(cudaMalloc(&c->d_miss_snp_idx, 4));
+    c->d_miss_snp_ptr = (int64_t*)scratch(c, "d_miss_snp_ptr", (c->M + 1) * 8);
+    c->d_miss_snp_idx = (int32_t*)scratch(c, "d_miss_snp_idx", 4);
     PG_CUDA(cudaMemsetAsync(c->d_miss_snp_ptr, 0, (c->M + 1) * 8, c->stream));
     c->n_missing = 0;
     c->miss_snp_valid = true;
   }
   if (!c->miss_ws_valid) {
-    if (c->d_miss_ws_ptr) cudaFree(c->d_miss_ws_ptr);
-    if (c->d_miss_ws_idx) cudaFree(c->d_miss_ws_idx);
-    PG_CUDA(cudaMalloc(&c->d_miss_ws_ptr, (rows + 1) * 8));
-    PG_CUDA(cudaMalloc(&c->d_miss_ws_idx, 4));
+    c->d_miss_ws_ptr = (int64_t*)scratch(c, "d_miss_ws_ptr", (rows + 1) * 8);
+    c->d_miss_ws_idx = (int32_t*)scratch(c, "d_miss_ws_idx", 4);
     PG_CUDA(cudaMemsetAsync(c->d_miss_ws_ptr, 0, (rows + 1) * 8, c->stream));
     c->miss_ws_valid = true;
   }
@@ -227,11 +223,7 @@ void build_transposed(pcaone_ctx* c, int bands) {
   if (c->bedT_valid && c->win.bands == bands) return;
   WindowLayout w = make_layout(c, bands);
   size_t bytes = (size_t)bands * c->Npad * w.pitch;
-  if (c->d_bedT) {
-    cudaFree(c->d_bedT);
-    c->d_bedT = nullptr;
-  }
-  PG_CUDA(cudaMalloc(&c->d_bedT, bytes));
+  c->d_bedT = (uint8_t*)scratch(c, "d_bedT", bytes);
   PG_CUDA(cudaMemsetAsync(c->d_bedT, 0xFF, bytes, c->stream));
   dim3 grid((unsigned)((w.blocksize + 63) / 64), c->Npad / 64, bands);
   k_transpose<<<grid, 256, 0, c->stream>>>(c->d_bed, c->pitch, c->M, w.blocksize, c->d_bedT,
@@ -251,12 +243,8 @@ void build_missing_by_snp(pcaone_ctx* c) {
   std::vector<int64_t> ptr(c->M + 1, 0);
   for (uint64_t j = 0; j < c->M; ++j) ptr[j + 1] = ptr[j] + (int64_t)(c->N - nonmiss[j]);
   c->n_missing = ptr[c->M];
-  if (c->d_miss_snp_ptr) cudaFree(c->d_miss_snp_ptr);
-  if (c->d_miss_snp_idx) cudaFree(c->d_miss_snp_idx);
-  c->d_miss_snp_ptr = nullptr;
-  c->d_miss_snp_idx = nullptr;
-  PG_CUDA(cudaMalloc(&c->d_miss_snp_ptr, (c->M + 1) * 8));
-  PG_CUDA(cudaMalloc(&c->d_miss_snp_idx, std::max<int64_t>(c->n_missing, 1) * 4));
+  c->d_miss_snp_ptr = (int64_t*)scratch(c, "d_miss_snp_ptr", (c->M + 1) * 8);
+  c->d_miss_snp_idx = (int32_t*)scratch(c, "d_miss_snp_idx", std::max<int64_t>(c->n_missing, 1) * 4);
   PG_CUDA(cudaMemcpyAsync(c->d_miss_snp_ptr, ptr.data(), (c->M + 1) * 8, cudaMemcpyHostToDevice,
                           c->stream));
   uint64_t threads = c->M * 32;
@@ -281,12 +269,8 @@ void build_missing_by_window_sample(pcaone_ctx* c) {
   PG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, rows * 8, cudaMemcpyDeviceToHost, c->stream));
   PG_CUDA(cudaStreamSynchronize(c->stream));
   for (uint64_t r = 0; r < rows; ++r) ptr[r + 1] = ptr[r] + cnt[r];
-  if (c->d_miss_ws_ptr) cudaFree(c->d_miss_ws_ptr);
-  if (c->d_miss_ws_idx) cudaFree(c->d_miss_ws_idx);
-  c->d_miss_ws_ptr = nullptr;
-  c->d_miss_ws_idx = nullptr;
-  PG_CUDA(cudaMalloc(&c->d_miss_ws_ptr, (rows + 1) * 8));
-  PG_CUDA(cudaMalloc(&c->d_miss_ws_idx, std::max<int64_t>(ptr[rows], 1) * 4));
+  c->d_miss_ws_ptr = (int64_t*)scratch(c, "d_miss_ws_ptr", (rows + 1) * 8);
+  c->d_miss_ws_idx = (int32_t*)scratch(c, "d_miss_ws_idx", std::max<int64_t>(ptr[rows], 1) * 4);
   PG_CUDA(cudaMemcpyAsync(c->d_miss_ws_ptr, ptr.data(), (rows + 1) * 8, cudaMemcpyHostToDevice,
                           c->stream));
   uint64_t* d_base = (uint64_t*)scratch(c, "miss_ws_base", c->win.bands * 8);

@@ -70,9 +70,7 @@ static const double* clip_freq(pcaone_ctx* c) { return c->imputed_compat ? c->d_
 
 void compute_imputed_snp(pcaone_ctx* c) {
   PG_REQUIRE(c->miss_snp_valid, PCAONE_ESTATE, "missing-entry list not built");
-  if (c->d_miss_snp_val) cudaFree(c->d_miss_snp_val);
-  c->d_miss_snp_val = nullptr;
-  PG_CUDA(cudaMalloc(&c->d_miss_snp_val, std::max<int64_t>(c->n_missing, 1) * 8));
+  c->d_miss_snp_val = (double*)scratch(c, "d_miss_snp_val", std::max<int64_t>(c->n_missing, 1) * 8);
   uint64_t threads = c->M * 32;
   k_impute_snp<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
       c->d_miss_snp_ptr, c->d_miss_snp_idx, c->M, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
@@ -84,9 +82,7 @@ void compute_imputed_snp(pcaone_ctx* c) {
 void compute_imputed_ws(pcaone_ctx* c) {
   if (c->miss_ws_val_valid) return;
   PG_REQUIRE(c->miss_ws_valid, PCAONE_ESTATE, "missing-entry list not built");
-  if (c->d_miss_ws_val) cudaFree(c->d_miss_ws_val);
-  c->d_miss_ws_val = nullptr;
-  PG_CUDA(cudaMalloc(&c->d_miss_ws_val, std::max<int64_t>(c->n_missing, 1) * 8));
+  c->d_miss_ws_val = (double*)scratch(c, "d_miss_ws_val", std::max<int64_t>(c->n_missing, 1) * 8);
   const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
   uint64_t threads = rows * 32;
   k_impute_ws<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(

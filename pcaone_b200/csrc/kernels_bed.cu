@@ -115,6 +115,77 @@ __global__ void k_count_missing_rows(const uint8_t* __restrict__ base, uint32_t 
   if (lane == 0) cnt[r] = n;
 }
 
+// ---- exclusive prefix sum of int64 counts on the device (CSR row pointers): per 1024-element
+// block a shuffle scan, then one block scans the block totals, then the offsets are added.
+constexpr int kScanBlock = 1024;
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_local(const int64_t* __restrict__ cnt, uint64_t n,
+                                                           int64_t* __restrict__ ptr, int64_t* __restrict__ bsum) {
+  __shared__ int64_t wsum[32];
+  const uint64_t i = (uint64_t)blockIdx.x * kScanBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t v = i < n ? cnt[i] : 0;
+  int64_t x = v;  // inclusive scan within the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int64_t t = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    wsum[lane] = t;
+  }
+  __syncthreads();
+  const int64_t excl = (w > 0 ? wsum[w - 1] : 0) + x - v;
+  if (i < n) ptr[i] = excl;
+  if (threadIdx.x == kScanBlock - 1) bsum[blockIdx.x] = excl + v;
+}
+
+// In place exclusive scan of nb block totals (one block); bsum[nb] = the grand total.
+__global__ void __launch_bounds__(kScanBlock) k_scan_bsums(int64_t* bsum, int64_t nb) {
+  __shared__ int64_t part[kScanBlock];
+  const int64_t per = (nb + kScanBlock - 1) / kScanBlock;
+  const int64_t b0 = threadIdx.x * per, b1 = b0 + per < nb ? b0 + per : nb;
+  int64_t s = 0;
+  for (int64_t b = b0; b < b1; ++b) s += bsum[b];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t run = 0;
+    for (int t = 0; t < kScanBlock; ++t) {
+      const int64_t v = part[t];
+      part[t] = run;
+      run += v;
+    }
+    bsum[nb] = run;
+  }
+  __syncthreads();
+  int64_t run = part[threadIdx.x];
+  for (int64_t b = b0; b < b1; ++b) {
+    const int64_t v = bsum[b];
+    bsum[b] = run;
+    run += v;
+  }
+}
+
+__global__ void k_scan_add(int64_t* __restrict__ ptr, uint64_t n, const int64_t* __restrict__ bsum, int64_t nb) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ptr[i] += bsum[i / kScanBlock];
+  if (i == 0) ptr[n] = bsum[nb];
+}
+
+// counts of missing codes per SNP from the non-missing counts
+__global__ void k_missing_counts(const uint32_t* __restrict__ nonmiss, uint64_t M, uint32_t N,
+                                 int64_t* __restrict__ cnt) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < M) cnt[j] = (int64_t)(N - nonmiss[j]);
+}
+
 // Warp per packed row: write the positions of missing codes in increasing order.
 // idx_out[ptr[r] + t] = pos_offset(r) + position. pos_base is added to every position;
 // for the (window, sample) lists, row r = b * Npad + i and pos_base = window start of b.
@@ -235,24 +306,36 @@ void build_transposed(pcaone_ctx* c, int bands) {
   c->miss_ws_valid = false;
 }
 
+// ptr[0..n] = exclusive prefix sum of cnt[0..n) on the device; returns ptr[n].
+static int64_t device_exclusive_scan(pcaone_ctx* c, const int64_t* cnt, uint64_t n, int64_t* ptr) {
+  const int64_t nb = (int64_t)((n + kScanBlock - 1) / kScanBlock);
+  int64_t* bsum = (int64_t*)scratch(c, "scan_bsum", (size_t)(nb + 1) * 8);
+  k_scan_local<<<(unsigned)std::max<int64_t>(nb, 1), kScanBlock, 0, c->stream>>>(cnt, n, ptr, bsum);
+  PG_CHECK_LAUNCH();
+  k_scan_bsums<<<1, kScanBlock, 0, c->stream>>>(bsum, nb);
+  PG_CHECK_LAUNCH();
+  k_scan_add<<<(unsigned)((n + 255) / 256 + 1), 256, 0, c->stream>>>(ptr, n, bsum, nb);
+  PG_CHECK_LAUNCH();
+  c->launches += 3;
+  int64_t total = 0;
+  PG_CUDA(cudaMemcpyAsync(&total, ptr + n, 8, cudaMemcpyDeviceToHost, c->stream));
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+  return total;
+}
+
 void build_missing_by_snp(pcaone_ctx* c) {
   if (c->miss_snp_valid) return;
-  std::vector<uint32_t> nonmiss(c->M);
-  PG_CUDA(cudaMemcpyAsync(nonmiss.data(), c->d_nonmiss, c->M * 4, cudaMemcpyDeviceToHost, c->stream));
-  PG_CUDA(cudaStreamSynchronize(c->stream));
-  std::vector<int64_t> ptr(c->M + 1, 0);
-  for (uint64_t j = 0; j < c->M; ++j) ptr[j + 1] = ptr[j] + (int64_t)(c->N - nonmiss[j]);
-  c->n_missing = ptr[c->M];
+  int64_t* d_cnt = (int64_t*)scratch(c, "miss_snp_cnt", c->M * 8);
+  k_missing_counts<<<(unsigned)((c->M + 255) / 256), 256, 0, c->stream>>>(c->d_nonmiss, c->M, c->N, d_cnt);
+  PG_CHECK_LAUNCH();
   c->d_miss_snp_ptr = (int64_t*)scratch(c, "d_miss_snp_ptr", (c->M + 1) * 8);
+  c->n_missing = device_exclusive_scan(c, d_cnt, c->M, c->d_miss_snp_ptr);
   c->d_miss_snp_idx = (int32_t*)scratch(c, "d_miss_snp_idx", std::max<int64_t>(c->n_missing, 1) * 4);
-  PG_CUDA(cudaMemcpyAsync(c->d_miss_snp_ptr, ptr.data(), (c->M + 1) * 8, cudaMemcpyHostToDevice,
-                          c->stream));
   uint64_t threads = c->M * 32;
   k_fill_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
       c->d_bed, c->pitch, c->M, c->pitch / 4, c->d_miss_snp_ptr, c->d_miss_snp_idx, nullptr, 1);
   PG_CHECK_LAUNCH();
-  PG_CUDA(cudaStreamSynchronize(c->stream));  // ptr host vector goes out of scope
-  c->launches++;
+  c->launches += 2;
   c->miss_snp_valid = true;
 }
 
@@ -265,14 +348,9 @@ void build_missing_by_window_sample(pcaone_ctx* c) {
   k_count_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
       c->d_bedT, c->win.pitch, rows, c->win.pitch / 4, d_cnt);
   PG_CHECK_LAUNCH();
-  std::vector<int64_t> cnt(rows), ptr(rows + 1, 0);
-  PG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, rows * 8, cudaMemcpyDeviceToHost, c->stream));
-  PG_CUDA(cudaStreamSynchronize(c->stream));
-  for (uint64_t r = 0; r < rows; ++r) ptr[r + 1] = ptr[r] + cnt[r];
   c->d_miss_ws_ptr = (int64_t*)scratch(c, "d_miss_ws_ptr", (rows + 1) * 8);
-  c->d_miss_ws_idx = (int32_t*)scratch(c, "d_miss_ws_idx", std::max<int64_t>(ptr[rows], 1) * 4);
-  PG_CUDA(cudaMemcpyAsync(c->d_miss_ws_ptr, ptr.data(), (rows + 1) * 8, cudaMemcpyHostToDevice,
-                          c->stream));
+  const int64_t total = device_exclusive_scan(c, d_cnt, rows, c->d_miss_ws_ptr);
+  c->d_miss_ws_idx = (int32_t*)scratch(c, "d_miss_ws_idx", std::max<int64_t>(total, 1) * 4);
   uint64_t* d_base = (uint64_t*)scratch(c, "miss_ws_base", c->win.bands * 8);
   PG_CUDA(cudaMemcpyAsync(d_base, c->win.start.data(), c->win.bands * 8, cudaMemcpyHostToDevice,
                           c->stream));

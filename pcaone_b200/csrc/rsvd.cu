@@ -34,6 +34,14 @@ __global__ void k_omega_layout(const double* __restrict__ cm, int64_t N, int l, 
   O2[t] = v;
   if (Of) Of[t] = (float)v;
 }
+
+// Row-major n x k (row stride ld) -> column-major n x k.
+__global__ void k_to_colmajor(const double* __restrict__ X, int64_t n, int k, int ld, double* __restrict__ Y) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * k) return;
+  const int64_t j = t / n, i = t - j * n;
+  Y[t] = X[i * ld + j];
+}
 }  // namespace
 
 // ---------------------------------------------------------------- host helpers
@@ -405,23 +413,22 @@ struct Engine {
     // outputs: U = Ucur, S = sigma[:k], V = Q_G Vr[:, :k]
     if (S)
       for (int j = 0; j < k; ++j) S[j] = sv[j];
-    std::vector<double> rowm;
+    // U and V leave the device already column-major (the host layout of the outputs)
+    double* cmaj = (double*)scratch(c, "r_out_cm", (size_t)std::max<int64_t>(M, N) * k * 8);
     if (U) {
-      rowm.resize((size_t)N * k);
-      PG_CUDA(cudaMemcpyAsync(rowm.data(), Ucur, rowm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+      k_to_colmajor<<<(unsigned)(((int64_t)N * k + 255) / 256), 256, 0, c->stream>>>(Ucur, N, k, k, cmaj);
+      PG_CHECK_LAUNCH();
+      PG_CUDA(cudaMemcpyAsync(U, cmaj, (size_t)N * k * 8, cudaMemcpyDeviceToHost, c->stream));
       PG_CUDA(cudaStreamSynchronize(c->stream));
-      for (int i = 0; i < N; ++i)
-        for (int j = 0; j < k; ++j) U[(size_t)j * N + i] = rowm[(size_t)i * k + j];
     }
     if (V) {
       double* Vd = (double*)scratch(c, "r_V", (size_t)c->Mpad * k * 8);
       PG_CUDA(cudaMemcpyAsync(Ck, vr.data(), vr.size() * 8, cudaMemcpyHostToDevice, c->stream));
       rowmat(c, G, l, Ck, l, k, M, Vd);
-      rowm.resize((size_t)M * k);
-      PG_CUDA(cudaMemcpyAsync(rowm.data(), Vd, rowm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+      k_to_colmajor<<<(unsigned)((M * k + 255) / 256), 256, 0, c->stream>>>(Vd, M, k, k, cmaj);
+      PG_CHECK_LAUNCH();
+      PG_CUDA(cudaMemcpyAsync(V, cmaj, (size_t)M * k * 8, cudaMemcpyDeviceToHost, c->stream));
       PG_CUDA(cudaStreamSynchronize(c->stream));
-      for (int64_t i = 0; i < M; ++i)
-        for (int j = 0; j < k; ++j) V[(size_t)j * M + i] = rowm[(size_t)i * k + j];
     }
     if (rep) {
       rep->epochs = epochs;

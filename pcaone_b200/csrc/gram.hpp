@@ -1,0 +1,200 @@
+// Gram products of tall row-major matrices (A^T B, n x la and n x lb, or the symmetric A^T A)
+// for the sketch-width kernels: register tiles, thread groups over rows, and a deterministic
+// two-level reduction (8-CTA clusters through distributed shared memory, then one CTA over
+// the cluster sums).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "internal.hpp"
+
+namespace pg {
+
+namespace cg = cooperative_groups;
+
+constexpr int kGramCluster = 8;  // CTAs per cluster of the Gram kernels
+
+// The la4 x lb4 output (widths rounded up to 4) is cut into 4 x 4 tiles; a symmetric product
+// keeps the tiles on and above the diagonal. The CTA's threads form ngrp groups of ntiles
+// threads; group g adds the staged rows g, g + ngrp, ... into its tiles.
+struct GramTiling {
+  int la4, lb4, nbi, nbj, ntiles, ngrp;
+  bool sym;
+};
+
+__host__ __device__ inline GramTiling gram_tiling(int la, int lb, bool sym, int threads) {
+  GramTiling g;
+  g.la4 = (la + 3) & ~3;
+  g.lb4 = (lb + 3) & ~3;
+  g.nbi = g.la4 / 4;
+  g.nbj = g.lb4 / 4;
+  g.sym = sym;
+  g.ntiles = sym ? g.nbi * (g.nbi + 1) / 2 : g.nbi * g.nbj;
+  g.ngrp = threads / g.ntiles > 0 ? threads / g.ntiles : 1;
+  return g;
+}
+
+// Tile index -> first row / column of the tile.
+__device__ __forceinline__ void gram_tile_origin(const GramTiling& g, int tile, int& i0, int& j0) {
+  int bi = 0, bj;
+  if (g.sym) {
+    int t = tile;
+    while (t >= g.nbi - bi) {
+      t -= g.nbi - bi;
+      ++bi;
+    }
+    bj = bi + t;
+  } else {
+    bi = tile / g.nbj;
+    bj = tile - bi * g.nbj;
+  }
+  i0 = bi * 4;
+  j0 = bj * 4;
+}
+
+// Shared-memory doubles the Gram helpers need beside the staged rows: group sums and the
+// CTA sum.
+__host__ __device__ inline int gram_smem_doubles(const GramTiling& g) { return (g.ngrp + 1) * g.ntiles * 16; }
+
+struct GramThread {
+  int i0 = 0, j0 = 0, grp = 0, tile = 0;
+  bool active = false;
+  double acc[4][4];
+
+  __device__ void init(const GramTiling& g) {
+    tile = threadIdx.x % g.ntiles;
+    grp = threadIdx.x / g.ntiles;
+    active = grp < g.ngrp;
+    gram_tile_origin(g, tile, i0, j0);
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+  }
+
+  // sa: nr x la4, sb: nr x lb4 staged rows (columns past la / lb zero)
+  __device__ void add_rows(const double* sa, const double* sb, int nr, const GramTiling& g) {
+    if (!active) return;
+    for (int r = grp; r < nr; r += g.ngrp) {
+      const double2 a01 = *reinterpret_cast<const double2*>(sa + r * g.la4 + i0);
+      const double2 a23 = *reinterpret_cast<const double2*>(sa + r * g.la4 + i0 + 2);
+      const double2 b01 = *reinterpret_cast<const double2*>(sb + r * g.lb4 + j0);
+      const double2 b23 = *reinterpret_cast<const double2*>(sb + r * g.lb4 + j0 + 2);
+      const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+    }
+  }
+
+  // Keeping the tile in red (ngrp * ntiles * 16 doubles of shared memory) between batches
+  // frees its registers for other work of the kernel: park() stores it, unpark() reloads it.
+  __device__ void park(const GramTiling& g, double* red) const {
+    if (!active) return;
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) red[(grp * g.ntiles + tile) * 16 + x * 4 + y] = acc[x][y];
+  }
+  __device__ void unpark(const GramTiling& g, const double* red) {
+    if (!active) return;
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = red[(grp * g.ntiles + tile) * 16 + x * 4 + y];
+  }
+
+  // CTA sum of the groups' tiles (fixed group order) into out[ntiles * 16] (shared memory);
+  // red holds ngrp * ntiles * 16 doubles.
+  __device__ void finish(const GramTiling& g, double* red, double* out) {
+    park(g, red);
+    __syncthreads();
+    const int n = g.ntiles * 16;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      double s = 0.0;
+      for (int q = 0; q < g.ngrp; ++q) s += red[q * n + e];
+      out[e] = s;
+    }
+    __syncthreads();
+  }
+};
+
+// sum_{b < n} x[b * stride] in b order; W loads are issued before their adds.
+template <int W = 8>
+__device__ __forceinline__ double sum_strided(const double* x, int n, int64_t stride) {
+  double s = 0.0;
+  int b = 0;
+  for (; b + W <= n; b += W) {
+    double v[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) v[k] = x[(int64_t)(b + k) * stride];
+#pragma unroll
+    for (int k = 0; k < W; ++k) s += v[k];
+  }
+  for (; b < n; ++b) s += x[(int64_t)b * stride];
+  return s;
+}
+
+// Cluster sum of the CTAs' part[n] (shared memory), in rank order, written to
+// gout[cluster index * n + e]. Every CTA of the cluster calls it; the rank-r CTA sums the
+// elements r * blockDim + t, ... through distributed shared memory. The second cluster barrier
+// keeps each CTA's shared memory alive until the others have read it.
+__device__ __forceinline__ void cluster_sum(const double* part, int n, double* gout) {
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();
+  const int rank = (int)cl.block_rank();
+  const int64_t cid = blockIdx.x / kGramCluster;
+  for (int e = rank * blockDim.x + threadIdx.x; e < n; e += kGramCluster * blockDim.x) {
+    double v[kGramCluster];
+#pragma unroll
+    for (int q = 0; q < kGramCluster; ++q) v[q] = cl.map_shared_rank(part, q)[e];
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < kGramCluster; ++q) s += v[q];
+    gout[cid * n + e] = s;
+  }
+  cl.sync();
+}
+
+// W (la x lb row-major, shared or global memory) = sum over nparts cluster sums of the tile
+// layout in gpart; a symmetric product is mirrored below the diagonal.
+__device__ __forceinline__ void gram_final(const GramTiling& g, const double* gpart, int nparts, int la, int lb,
+                                           double* W) {
+  const int n = g.ntiles * 16;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const double v = sum_strided<16>(gpart + e, nparts, n);
+    int i0, j0;
+    gram_tile_origin(g, e / 16, i0, j0);
+    const int i = i0 + (e % 16) / 4, j = j0 + e % 4;
+    if (i < la && j < lb) {
+      W[i * lb + j] = v;
+      if (g.sym) W[j * lb + i] = v;
+    }
+  }
+  __syncthreads();
+}
+
+// Ticket: true in the CTA that finishes last (after a fence, so it sees every CTA's writes).
+__device__ __forceinline__ bool last_cta(unsigned* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Row range of this CTA when n rows are split over the grid in contiguous blocks.
+__device__ __forceinline__ void row_range(int64_t n, int64_t& r0, int64_t& r1) {
+  const int64_t rpb = (n + gridDim.x - 1) / gridDim.x;
+  r0 = blockIdx.x * rpb;
+  r1 = (n < r0 + rpb ? n : r0 + rpb);
+  if (r0 > r1) r0 = r1;
+}
+
+}  // namespace pg

@@ -160,16 +160,31 @@ __global__ void k_scale_g(int64_t start, int64_t m, int l, const double* __restr
   }
 }
 
-// out[c] = sum_b part[b][c]: one warp per column, lanes over b in a fixed order, then a
-// fixed shuffle tree (deterministic).
-__global__ void k_reduce_cols(const double* __restrict__ part, int nblk, int l, double* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  for (int c = threadIdx.x >> 5; c < l; c += blockDim.x >> 5) {
-    double s = 0.0;
-#pragma unroll 4
-    for (int b = lane; b < nblk; b += 32) s += part[(int64_t)b * l + c];
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) out[c] = s;
+// out[c] = sum_b part[b][c]: one CTA of kRedThreads per column; thread t sums the rows
+// t, t + kRedThreads, ... (eight loads in flight), then a fixed shuffle tree and a fixed
+// combination of the warps' sums (deterministic).
+constexpr int kRedThreads = 128;
+__global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __restrict__ part, int nblk, int l,
+                                                             double* __restrict__ out) {
+  __shared__ double ws[kRedThreads / 32];
+  const int c = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int b = threadIdx.x + u * kRedThreads;
+    v[u] = b < nblk ? part[(int64_t)b * l + c] : 0.0;
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) t += v[u];
+  for (int b = threadIdx.x + 8 * kRedThreads; b < nblk; b += kRedThreads) t += part[(int64_t)b * l + c];
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) ws[warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) acc += ws[w];
+    out[c] = acc;
   }
 }
 
@@ -215,7 +230,7 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
     default: k_prep<T, 8><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
   }
   PG_CHECK_LAUNCH();
-  k_reduce_cols<<<1, 512, 0, c->stream>>>(part, nblk, p.l, h0);
+  k_reduce_cols<<<p.l, kRedThreads, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }
@@ -247,7 +262,7 @@ void launch_scale_g(pcaone_ctx* c, const EpiP1& p, T* B2, double* h0) {
   k_scale_g<T><<<nblk, threads, (size_t)nwarps * p.l * 8, c->stream>>>(p.start, p.m, p.l, p.scale,
                                                                        p.F, p.G, B2, part);
   PG_CHECK_LAUNCH();
-  k_reduce_cols<<<1, 512, 0, c->stream>>>(part, nblk, p.l, h0);
+  k_reduce_cols<<<p.l, kRedThreads, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }

@@ -4,6 +4,7 @@
 // Tall matrices are row-major n x l (one sample or SNP per row, l <= kLmax columns).
 // All reductions are two-pass (per-CTA partials, then a fixed-order sum) so results are
 // deterministic run to run.
+#include "gram.hpp"
 #include "internal.hpp"
 #include "linalg.hpp"
 
@@ -11,80 +12,80 @@ namespace pg {
 
 namespace {
 
-constexpr int kGramRowsMax = 64;  // rows staged per iteration in the Gram kernels
-constexpr int kGramBlocks = 296;
+// A^T B over rows: each CTA of a cluster streams its contiguous row block through two
+// shared-memory stages (cp.async, the next batch in flight while the current one is summed
+// into 4 x 4 register tiles, gram.hpp), sums its thread groups, and the cluster adds its CTAs'
+// sums through distributed shared memory into gpart[cluster] (ntiles * 16 values in tile
+// layout). SYM (A == B): only the tiles on and above the diagonal, one staged copy.
+constexpr int kCrossThreads = 256;
+constexpr int kCrossMaxClusters = 36;
+constexpr int kCrossSmemBudget = 96 * 1024;  // two CTAs an SM
 
-// Partial cross products P[blk] = A^T B over a slice of rows (A: n x la, B: n x lb). Rows
-// are staged in shared memory with widths padded to multiples of 4 (zero columns); each
-// thread accumulates a 4 x 4 block of the la x lb output in registers, so a staged row costs
-// 8 shared-memory loads per 16 FMAs.
-__global__ void k_cross_partial(const double* __restrict__ A, int la, const double* __restrict__ Bm,
-                                int lb, int64_t n, int kGramRows, double* __restrict__ part) {
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+template <bool SYM>
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThreads)
+    k_cross(const double* __restrict__ A, int la, const double* __restrict__ Bm, int lb, int64_t n, int rows,
+            double* __restrict__ gpart) {
   extern __shared__ double sm[];
-  const int la4 = (la + 3) & ~3, lb4 = (lb + 3) & ~3;
-  double* sa = sm;                        // kGramRows x la4
-  double* sb = sm + kGramRows * la4;      // kGramRows x lb4
-  const int bi = la4 / 4, bj = lb4 / 4;   // 4 x 4 output blocks
-  const int blk = threadIdx.x;
-  const bool active = blk < bi * bj;
-  const int i0 = active ? (blk / bj) * 4 : 0, j0 = active ? (blk % bj) * 4 : 0;
-  double acc[4][4];
-#pragma unroll
-  for (int x = 0; x < 4; ++x)
-#pragma unroll
-    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
-  const int64_t rows_per_blk = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t rb = blockIdx.x * rows_per_blk, re = min(n, rb + rows_per_blk);
-  for (int64_t r0 = rb; r0 < re; r0 += kGramRows) {
-    const int nr = (int)(re - r0 < kGramRows ? re - r0 : kGramRows);
-    __syncthreads();
-    for (int t = threadIdx.x; t < nr * la4; t += blockDim.x) {
-      const int r = t / la4, cidx = t - r * la4;
-      sa[t] = cidx < la ? A[(r0 + r) * la + cidx] : 0.0;
+  const GramTiling g = gram_tiling(la, lb, SYM, blockDim.x);
+  const int w = g.la4 + (SYM ? 0 : g.lb4);  // staged doubles per row: A rows (la4), then B rows (lb4)
+  double* red = sm + 2 * rows * w;  // stages: sm and sm + rows * w
+  double* cpart = red + g.ngrp * g.ntiles * 16;
+  for (int t = threadIdx.x; t < 2 * rows; t += blockDim.x) {  // zero padding columns, never copied
+    double* base = sm + (t / rows) * rows * w;
+    const int r = t % rows;
+    for (int cc = la; cc < g.la4; ++cc) base[r * g.la4 + cc] = 0.0;
+    if (!SYM)
+      for (int cc = lb; cc < g.lb4; ++cc) base[rows * g.la4 + r * g.lb4 + cc] = 0.0;
+  }
+  int64_t r0, r1;
+  row_range(n, r0, r1);
+  auto issue = [&](int64_t b, double* dst) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    for (int t = threadIdx.x; t < nr * la; t += blockDim.x) {
+      const int r = t / la;
+      cp_async8(dst + r * g.la4 + (t - r * la), A + b * la + t);
     }
-    for (int t = threadIdx.x; t < nr * lb4; t += blockDim.x) {
-      const int r = t / lb4, cidx = t - r * lb4;
-      sb[t] = cidx < lb ? Bm[(r0 + r) * lb + cidx] : 0.0;
-    }
-    __syncthreads();
-    if (active) {
-      for (int r = 0; r < nr; ++r) {
-        const double2 a01 = *reinterpret_cast<const double2*>(sa + r * la4 + i0);
-        const double2 a23 = *reinterpret_cast<const double2*>(sa + r * la4 + i0 + 2);
-        const double2 b01 = *reinterpret_cast<const double2*>(sb + r * lb4 + j0);
-        const double2 b23 = *reinterpret_cast<const double2*>(sb + r * lb4 + j0 + 2);
-        const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+    if (!SYM)
+      for (int t = threadIdx.x; t < nr * lb; t += blockDim.x) {
+        const int r = t / lb;
+        cp_async8(dst + rows * g.la4 + r * g.lb4 + (t - r * lb), Bm + b * lb + t);
       }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  GramThread gt;
+  gt.init(g);
+  int s = 0;
+  if (r0 < r1) issue(r0, sm);
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    if (b + rows < r1) {
+      issue(b + rows, sm + (s ^ 1) * rows * w);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
+    __syncthreads();  // stage s complete (and the padding zeroed) for every thread
+    const double* sa = sm + s * rows * w;
+    gt.add_rows(sa, SYM ? sa : sa + rows * g.la4, nr, g);
+    __syncthreads();  // stage s is consumed before it is refilled
+    s ^= 1;
   }
-  if (active) {
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y)
-        if (i0 + x < la && j0 + y < lb) part[(int64_t)blockIdx.x * la * lb + (i0 + x) * lb + j0 + y] = acc[x][y];
-  }
+  gt.finish(g, red, cpart);
+  cluster_sum(cpart, g.ntiles * 16, gpart);
 }
 
-// out[p] = sum_b part[b][p]: one warp per pair, lanes over b in a fixed order, then a fixed
-// shuffle tree (deterministic).
-__global__ void k_sum_partials(const double* __restrict__ part, int nblk, int npairs,
-                               double* __restrict__ out) {
-  const int p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (p >= npairs) return;
-  double s = 0.0;
-#pragma unroll 4
-  for (int b = lane; b < nblk; b += 32) s += part[(int64_t)b * npairs + p];
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) out[p] = s;
+// out (la x lb, global) = sum of the nparts cluster sums of k_cross.
+__global__ void __launch_bounds__(kCrossThreads) k_cross_final(const double* __restrict__ gpart, int nparts, int la,
+                                                               int lb, int sym, double* __restrict__ out) {
+  const GramTiling g = gram_tiling(la, lb, sym != 0, kCrossThreads);
+  gram_final(g, gpart, nparts, la, lb, out);
 }
 
-// Cholesky W = R^T R (R upper) for l x l; one CTA. status[0] is set to 1 + j on failure.
-// If Rprev != nullptr, also writes Racc = R * Rprev (accumulated R of CholeskyQR2).
 __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restrict__ R,
                            const double* __restrict__ Rprev, double* __restrict__ Racc,
                            int* __restrict__ status) {
@@ -284,18 +285,26 @@ __global__ void k_add(const double* __restrict__ a, const double* __restrict__ b
 }  // namespace
 
 void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int64_t n, double* out) {
-  const int npairs = la * lb;
-  PG_REQUIRE(la <= kLmax && lb <= kLmax, PCAONE_EBADARG, "cross product too wide");
-  const int la4 = (la + 3) & ~3, lb4 = (lb + 3) & ~3;
-  const int threads = std::max(32, ((la4 / 4) * (lb4 / 4) + 31) / 32 * 32);
-  // stage as many rows as fit in 48 KB of shared memory
-  const int rows = std::max(8, std::min(kGramRowsMax, 6144 / (la4 + lb4)));
-  int nblk = (int)std::min<int64_t>(kGramBlocks, std::max<int64_t>(1, (n + rows - 1) / rows));
-  double* part = (double*)scratch(c, "cross_part", (size_t)nblk * npairs * 8);
-  size_t smem = (size_t)rows * (la4 + lb4) * 8;
-  k_cross_partial<<<nblk, threads, smem, c->stream>>>(A, la, B, lb, n, rows, part);
+  PG_REQUIRE(la >= 1 && lb >= 1 && la <= kLmax && lb <= kLmax, PCAONE_EBADARG, "cross product too wide");
+  const bool sym = A == B && la == lb;
+  const GramTiling g = gram_tiling(la, lb, sym, kCrossThreads);
+  const int w = g.la4 + (sym ? 0 : g.lb4);
+  const int fixed = gram_smem_doubles(g) * 8;
+  const int rows = std::max(8, std::min(128, (kCrossSmemBudget - fixed) / (2 * w * 8)));
+  const size_t smem = (size_t)fixed + (size_t)2 * rows * w * 8;
+  const int64_t want = (n + (int64_t)kGramCluster * 4 * rows - 1) / ((int64_t)kGramCluster * 4 * rows);
+  const int cap = std::max(1, std::min(kCrossMaxClusters, 2 * c->sm_count / kGramCluster));
+  const int ncl = (int)std::max<int64_t>(1, std::min<int64_t>(cap, want));
+  double* gpart = (double*)scratch(c, "cross_part", (size_t)ncl * g.ntiles * 16 * 8);
+  if (sym) {
+    PG_CUDA(cudaFuncSetAttribute(k_cross<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_cross<true><<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, la, A, lb, n, rows, gpart);
+  } else {
+    PG_CUDA(cudaFuncSetAttribute(k_cross<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_cross<false><<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, la, B, lb, n, rows, gpart);
+  }
   PG_CHECK_LAUNCH();
-  k_sum_partials<<<(npairs + 7) / 8, 256, 0, c->stream>>>(part, nblk, npairs, out);
+  k_cross_final<<<1, kCrossThreads, 0, c->stream>>>(gpart, ncl, la, lb, sym ? 1 : 0, out);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }

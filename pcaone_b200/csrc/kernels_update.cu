@@ -8,16 +8,19 @@
 //   K3  Q = Q1 R2^-1, flip sums |O2 - Q D|, |O2 + Q D|      last CTA: multipliers m = +-D
 //   K4  Omega = Q m, Omega2 = Omega, operand copies, column sums  last CTA: sum of Omega
 //
-// Each kernel's CTAs own fixed row ranges and write per-CTA partial sums; the CTA that
-// finishes last (atomic ticket after a __threadfence) reduces the partials in CTA order, so
-// the result is deterministic. The Householder column signs D come from the modified LU of
-// the top l x l block of Q (Ballard et al. 2015): pivot s -> D = -sign(s), sign(0) = +.
-// Row solves keep the row in registers (kernels templated on LMAX >= l); Gram matrices use
-// 4 x 4 register tiles; column sums use a column-strided thread layout.
+// Each kernel runs as clusters of kGramCluster CTAs that own fixed row ranges. A CTA stages
+// its rows in shared memory and sums them into a CTA partial (Gram matrices: 4 x 4 register
+// tiles of the upper triangle, thread groups over rows, gram.hpp); the cluster adds its CTAs'
+// partials through distributed shared memory, and the CTA that finishes last (atomic ticket
+// after a __threadfence) adds the cluster sums in cluster order, so the result is
+// deterministic. The Householder column signs D come from the modified LU of the top l x l
+// block of Q (Ballard et al. 2015): pivot s -> D = -sign(s), sign(0) = +. Row solves keep the
+// row in registers (kernels templated on LMAX >= l).
 #include <cuda_bf16.h>
 
 #include <algorithm>
 
+#include "gram.hpp"
 #include "internal.hpp"
 #include "linalg.hpp"
 #include "tc_layout.hpp"
@@ -28,7 +31,10 @@ namespace pg {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kStageRows = 32;
+
+// rows staged per batch: a batch of rows, the group sums and R fit in about 100 KB, so two
+// CTAs (two clusters' worth per 8 SMs) fit on an SM
+__host__ __device__ constexpr int stage_rows(int l) { return l <= 48 ? 128 : 64; }
 
 // Shared-memory Cholesky of an l x l SPD matrix (upper R, W = R^T R), in place in s.
 __device__ void chol_smem(double* s, int l, int* status) {
@@ -57,137 +63,119 @@ __device__ void chol_smem(double* s, int l, int* status) {
   __syncthreads();
 }
 
-// This CTA's rows [r0, r1) of A^T A (A: n x l row-major) added into a 4 x 4 register tile per
-// thread; stage holds kStageRows x l4 doubles. Threads past the (l4/4)^2 tiles only stage.
-__device__ void gram_rows(const double* A, int l, int64_t r0, int64_t r1, double* stage, double (&acc)[4][4]) {
-  const int l4 = (l + 3) & ~3, nb = l4 / 4;
-  const bool active = threadIdx.x < nb * nb;
-  const int i0 = active ? (threadIdx.x / nb) * 4 : 0, j0 = active ? (threadIdx.x % nb) * 4 : 0;
-  for (int64_t b = r0; b < r1; b += kStageRows) {
-    const int nr = (int)(r1 - b < kStageRows ? r1 - b : kStageRows);
-    __syncthreads();
-    for (int t = threadIdx.x; t < nr * l4; t += blockDim.x) {
-      const int r = t / l4, c = t - r * l4;
-      stage[t] = c < l ? A[(b + r) * l + c] : 0.0;
-    }
-    __syncthreads();
-    if (active) {
-      for (int r = 0; r < nr; ++r) {
-        const double2 a01 = *reinterpret_cast<const double2*>(stage + r * l4 + i0);
-        const double2 a23 = *reinterpret_cast<const double2*>(stage + r * l4 + i0 + 2);
-        const double2 b01 = *reinterpret_cast<const double2*>(stage + r * l4 + j0);
-        const double2 b23 = *reinterpret_cast<const double2*>(stage + r * l4 + j0 + 2);
-        const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-        for (int x = 0; x < 4; ++x)
-#pragma unroll
-          for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
-      }
-    }
-  }
-}
-
-__device__ void store_gram_part(const double (&acc)[4][4], int l, double* part) {
-  const int l4 = (l + 3) & ~3, nb = l4 / 4;
-  if (threadIdx.x >= nb * nb) return;
-  const int i0 = (threadIdx.x / nb) * 4, j0 = (threadIdx.x % nb) * 4;
-#pragma unroll
-  for (int x = 0; x < 4; ++x)
-#pragma unroll
-    for (int y = 0; y < 4; ++y)
-      if (i0 + x < l && j0 + y < l) part[(int64_t)blockIdx.x * l * l + (i0 + x) * l + j0 + y] = acc[x][y];
-}
-
-__device__ bool last_cta(unsigned* counter) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned t = atomicAdd(counter, 1u);
-    last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (last) __threadfence();
-  return last;
-}
-
-// sum_{b < n} x[b * stride], added in b order (the same result as the plain loop); the loads
-// of eight terms are issued before their adds, so they overlap instead of paying one L2
-// round trip per term.
-__device__ __forceinline__ double sum_strided(const double* x, int n, int64_t stride) {
-  double s = 0.0;
-  int b = 0;
-  for (; b + 8 <= n; b += 8) {
-    double v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = x[(int64_t)(b + k) * stride];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s += v[k];
-  }
-  for (; b < n; ++b) s += x[(int64_t)b * stride];
-  return s;
-}
-
-__device__ void reduce_pairs(const double* part, int nblk, int npairs, double* out_smem) {
-  for (int p = threadIdx.x; p < npairs; p += blockDim.x) out_smem[p] = sum_strided(part + p, nblk, npairs);
-  __syncthreads();
-}
-
-__device__ __forceinline__ void row_range(int64_t N, int64_t& r0, int64_t& r1) {
-  const int64_t rpb = (N + gridDim.x - 1) / gridDim.x;
-  r0 = blockIdx.x * rpb;
-  r1 = (N < r0 + rpb ? N : r0 + rpb);
-  if (r0 > r1) r0 = r1;
-}
-
 // Column-strided pass over this CTA's rows: thread t owns column t % l of rows
 // r0 + t / l, r0 + t / l + T / l, ... with T = l * (blockDim / l) threads.
 __device__ __forceinline__ int col_threads(int l) { return l * (blockDim.x / l); }
 
-__global__ void __launch_bounds__(kThreads) k_upd1(UpdateArgs a) {
+// Shared memory of the Gram kernels: [LMAX x LMAX R] | group sums | CTA sum | staged rows
+// (stage_rows(l) x l4, at least l x l).
+__host__ __device__ inline int upd_gram_smem_doubles(int l, int rmax) {
+  const GramTiling g = gram_tiling(l, l, true, kThreads);
+  const int l4 = (l + 3) & ~3;
+  return rmax * rmax + gram_smem_doubles(g) + std::max(stage_rows(l) * l4, l * l);
+}
+
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd1(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* stage = sm;  // max(kStageRows, l) x l4
+  const GramTiling g = gram_tiling(l, l, true, blockDim.x);
+  double* red = sm;
+  double* cpart = red + g.ngrp * g.ntiles * 16;
+  double* stage = cpart + g.ntiles * 16;
+  const int rows = stage_rows(l);
+  GramThread gt;
+  gt.init(g);
   int64_t r0, r1;
   row_range(a.N, r0, r1);
-  if (a.H2) {
-    for (int64_t t = r0 * l + threadIdx.x; t < r1 * l; t += blockDim.x) a.H[t] = a.H1[t] + a.H2[t];
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
     __syncthreads();
+#pragma unroll 4
+    for (int t = threadIdx.x; t < nr * g.la4; t += blockDim.x) {
+      const int r = t / g.la4, cc = t - r * g.la4;
+      double v = 0.0;
+      if (cc < l) {
+        const int64_t o = (b + r) * l + cc;
+        if (a.H2) {
+          v = a.H1[o] + a.H2[o];
+          a.H[o] = v;
+        } else {
+          v = a.H[o];
+        }
+      }
+      stage[t] = v;
+    }
+    __syncthreads();
+    gt.add_rows(stage, stage, nr, g);
   }
-  double acc[4][4] = {};
-  gram_rows(a.H, l, r0, r1, stage, acc);
-  store_gram_part(acc, l, a.part);
+  gt.finish(g, red, cpart);
+  cluster_sum(cpart, g.ntiles * 16, a.part);
   if (!last_cta(&a.counters[0])) return;
-  reduce_pairs(a.part, gridDim.x, l * l, stage);
+  gram_final(g, a.part, gridDim.x / kGramCluster, l, l, stage);
   chol_smem(stage, l, a.status);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R1[t] = stage[t];
   if (threadIdx.x == 0) a.counters[0] = 0;
 }
 
 template <int LMAX>
-__global__ void __launch_bounds__(kThreads) k_upd2(UpdateArgs a) {
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd2(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* R = sm;                    // LMAX x LMAX (row stride LMAX)
-  double* stage = sm + LMAX * LMAX;  // max(kStageRows, l) x l4
+  const GramTiling g = gram_tiling(l, l, true, blockDim.x);
+  double* R = sm;  // LMAX x LMAX (row stride LMAX)
+  double* red = R + LMAX * LMAX;
+  double* cpart = red + g.ngrp * g.ntiles * 16;
+  double* stage = cpart + g.ntiles * 16;
+  const int rows = stage_rows(l);
   stage_r<LMAX>(a.R1, l, R);
-  __syncthreads();
+  {
+    GramThread gt;
+    gt.init(g);
+    gt.park(g, red);  // the tiles live in red between batches (registers go to the row solves)
+  }
   int64_t r0, r1;
   row_range(a.N, r0, r1);
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) solve_row_upper<LMAX>(a.H + r * l, R, l, a.Q + r * l);
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    __syncthreads();  // R staged; the previous batch's rows are consumed
+    for (int r = threadIdx.x; r < nr; r += blockDim.x)
+      solve_row_upper<LMAX>(a.H + (b + r) * l, R, l, stage + r * g.la4);
+    __syncthreads();
+#pragma unroll 4
+    for (int t = threadIdx.x; t < nr * g.la4; t += blockDim.x) {
+      const int r = t / g.la4, cc = t - r * g.la4;
+      if (cc < l)
+        a.Q[(b + r) * l + cc] = stage[t];
+      else
+        stage[t] = 0.0;
+    }
+    __syncthreads();
+    GramThread gt;
+    gt.init(g);
+    gt.unpark(g, red);
+    gt.add_rows(stage, stage, nr, g);
+    gt.park(g, red);
+  }
   __syncthreads();
-  double acc[4][4] = {};
-  gram_rows(a.Q, l, r0, r1, stage, acc);
-  store_gram_part(acc, l, a.part);
+  {
+    const int n = g.ntiles * 16;  // CTA sum of the groups' tiles, fixed group order
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      double s = 0.0;
+      for (int q = 0; q < g.ngrp; ++q) s += red[q * n + e];
+      cpart[e] = s;
+    }
+    __syncthreads();
+  }
+  cluster_sum(cpart, g.ntiles * 16, a.part);
   if (!last_cta(&a.counters[1])) return;
-  double* Rn = R;
-  reduce_pairs(a.part, gridDim.x, l * l, Rn);  // Rn <- W2 (row stride l; R1 no longer needed)
+  double* Rn = stage;  // W2, then R2 (row stride l)
+  gram_final(g, a.part, gridDim.x / kGramCluster, l, l, Rn);
   chol_smem(Rn, l, a.status);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R2[t] = Rn[t];
   __syncthreads();
   // top l x l block of Q = Q1[0:l] R2^-1 (substitution in shared memory), then the modified
   // LU for the Householder signs
-  double* top = stage;
+  double* top = R;  // R1 is no longer needed
   for (int r = threadIdx.x; r < l; r += blockDim.x) {
     const double* q = a.Q + (int64_t)r * l;
     for (int j = 0; j < l; ++j) {
@@ -219,53 +207,67 @@ __global__ void __launch_bounds__(kThreads) k_upd2(UpdateArgs a) {
 }
 
 template <int LMAX>
-__global__ void __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* R = sm;                  // LMAX x LMAX (row stride LMAX)
-  double* red = sm + LMAX * LMAX;  // kThreads x 2
+  const int rows = stage_rows(l);
+  double* R = sm;                      // LMAX x LMAX (row stride LMAX)
+  double* sq = R + LMAX * LMAX;        // rows x l: Q
+  double* so = sq + rows * l;          // rows x l: Omega2
+  double* red = so + rows * l;         // kThreads x 2
+  double* cpart = red + kThreads * 2;  // 2 l
   stage_r<LMAX>(a.R2, l, R);
-  __syncthreads();
   int64_t r0, r1;
   row_range(a.N, r0, r1);
-  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) solve_row_upper<LMAX>(a.Q + r * l, R, l, a.Q + r * l);
-  __syncthreads();  // this CTA's rows of Q are written
   const int T = col_threads(l);
+  const int c = threadIdx.x % l;
+  const double d = threadIdx.x < T ? a.D[c] : 0.0;
   double dm = 0.0, dp = 0.0;
-  if (threadIdx.x < T) {
-    const int c = threadIdx.x % l;
-    const double d = a.D[c];
-    for (int64_t r = r0 + threadIdx.x / l; r < r1; r += T / l) {
-      const double o = a.Omg2[r * l + c], q = a.Q[r * l + c] * d;
-      dm += fabs(o - q);
-      dp += fabs(o + q);
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    __syncthreads();  // R staged; the previous batch is consumed
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) solve_row_upper<LMAX>(a.Q + (b + r) * l, R, l, sq + r * l);
+#pragma unroll 4
+    for (int t = threadIdx.x; t < nr * l; t += blockDim.x) so[t] = a.Omg2[b * l + t];
+    __syncthreads();
+#pragma unroll 4
+    for (int t = threadIdx.x; t < nr * l; t += blockDim.x) a.Q[b * l + t] = sq[t];
+    if (threadIdx.x < T) {
+      for (int r = threadIdx.x / l; r < nr; r += T / l) {
+        const double o = so[r * l + c], q = sq[r * l + c] * d;
+        dm += fabs(o - q);
+        dp += fabs(o + q);
+      }
     }
   }
   red[threadIdx.x * 2] = dm;
   red[threadIdx.x * 2 + 1] = dp;
   __syncthreads();
-  for (int c = threadIdx.x; c < l; c += blockDim.x) {  // fixed-order sum over this column's threads
+  for (int j = threadIdx.x; j < l; j += blockDim.x) {  // fixed-order sum over this column's threads
     double m = 0.0, p = 0.0;
-    for (int t = c; t < T; t += l) {
+    for (int t = j; t < T; t += l) {
       m += red[t * 2];
       p += red[t * 2 + 1];
     }
-    a.part[(int64_t)blockIdx.x * 2 * l + c] = m;
-    a.part[(int64_t)blockIdx.x * 2 * l + l + c] = p;
+    cpart[j] = m;
+    cpart[l + j] = p;
   }
+  cluster_sum(cpart, 2 * l, a.part);
   if (!last_cta(&a.counters[2])) return;
+  const int ncl = gridDim.x / kGramCluster;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
-    const double m = sum_strided(a.part + j, gridDim.x, 2 * l);
-    const double p = sum_strided(a.part + l + j, gridDim.x, 2 * l);
+    const double m = sum_strided<16>(a.part + j, ncl, 2 * l);
+    const double p = sum_strided<16>(a.part + l + j, ncl, 2 * l);
     a.mult[j] = (m > 2.0 * p) ? -a.D[j] : a.D[j];  // src/RSVD.hpp:85
   }
   if (threadIdx.x == 0) a.counters[2] = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
-  double* red = sm;  // kThreads
+  double* red = sm;                // kThreads
+  double* cpart = red + kThreads;  // l
   int64_t r0, r1;
   row_range(a.N, r0, r1);
   const int T = col_threads(l);
@@ -273,6 +275,7 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   if (threadIdx.x < T) {
     const int j = threadIdx.x % l;
     const double mj = a.mult[j];
+#pragma unroll 4
     for (int64_t r = r0 + threadIdx.x / l; r < r1; r += T / l) {
       const double v = a.Q[r * l + j] * mj;
       a.Omg[r * l + j] = v;
@@ -290,53 +293,66 @@ __global__ void __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   }
   red[threadIdx.x] = cs;
   __syncthreads();
-  for (int c = threadIdx.x; c < l; c += blockDim.x) {
+  for (int j = threadIdx.x; j < l; j += blockDim.x) {
     double s = 0.0;
-    for (int t = c; t < T; t += l) s += red[t];
-    a.part[(int64_t)blockIdx.x * l + c] = s;
+    for (int t = j; t < T; t += l) s += red[t];
+    cpart[j] = s;
   }
+  cluster_sum(cpart, l, a.part);
   if (!last_cta(&a.counters[3])) return;
-  for (int j = threadIdx.x; j < l; j += blockDim.x) a.wsum[j] = sum_strided(a.part + j, gridDim.x, l);
+  const int ncl = gridDim.x / kGramCluster;
+  for (int j = threadIdx.x; j < l; j += blockDim.x) a.wsum[j] = sum_strided<16>(a.part + j, ncl, l);
   if (threadIdx.x == 0) a.counters[3] = 0;
 }
 
+// CTAs of the update kernels: whole clusters, about 64 rows or more per CTA, at most
+// kMaxClusters clusters (the last CTA reads one partial per cluster).
+constexpr int kMaxClusters = 18;
+
+int update_ctas(pcaone_ctx* c, int64_t N) {
+  const int64_t want = (N + kGramCluster * 64 - 1) / (kGramCluster * 64);
+  const int cap = std::max(1, std::min(kMaxClusters, c->sm_count / kGramCluster));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(cap, want)) * kGramCluster;
+}
+
 template <int LMAX>
-void launch_all(pcaone_ctx* c, const UpdateArgs& a) {
-  const int l4 = (a.l + 3) & ~3;
-  const size_t sstage = (size_t)std::max(kStageRows, a.l) * l4 * 8;  // staged rows or an l x l matrix
-  const size_t s1 = sstage;
-  const size_t s2 = (size_t)LMAX * LMAX * 8 + sstage;
-  const size_t s3 = (size_t)LMAX * LMAX * 8 + (size_t)kThreads * 2 * 8;
-  const size_t s4 = (size_t)kThreads * 8;
-  static bool attr = false;  // shared memory above 48 KB for the widest sketches
-  if (!attr) {
-    PG_CUDA(cudaFuncSetAttribute(k_upd2<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)((size_t)LMAX * LMAX * 8 + (size_t)std::max(kStageRows, LMAX) * LMAX * 8)));
-    attr = true;
-  }
-  k_upd1<<<a.nblk, kThreads, s1, c->stream>>>(a);
+void launch_all(pcaone_ctx* c, const UpdateArgs& a, int nblk) {
+  const int l = a.l, rows = stage_rows(l);
+  const size_t s1 = (size_t)upd_gram_smem_doubles(l, 0) * 8;
+  const size_t s2 = (size_t)upd_gram_smem_doubles(l, LMAX) * 8;
+  const size_t s3 = ((size_t)LMAX * LMAX + 2 * (size_t)rows * l + 2 * kThreads + 2 * l) * 8;
+  const size_t s4 = ((size_t)kThreads + l) * 8;
+  PG_CUDA(cudaFuncSetAttribute(k_upd1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+  PG_CUDA(cudaFuncSetAttribute(k_upd2<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+  PG_CUDA(cudaFuncSetAttribute(k_upd3<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
+  k_upd1<<<nblk, kThreads, s1, c->stream>>>(a);
   PG_CHECK_LAUNCH();
-  k_upd2<LMAX><<<a.nblk, kThreads, s2, c->stream>>>(a);
+  k_upd2<LMAX><<<nblk, kThreads, s2, c->stream>>>(a);
   PG_CHECK_LAUNCH();
-  k_upd3<LMAX><<<a.nblk, kThreads, s3, c->stream>>>(a);
+  k_upd3<LMAX><<<nblk, kThreads, s3, c->stream>>>(a);
   PG_CHECK_LAUNCH();
-  k_upd4<<<a.nblk, kThreads, s4, c->stream>>>(a);
+  k_upd4<<<nblk, kThreads, s4, c->stream>>>(a);
   PG_CHECK_LAUNCH();
 }
 
 }  // namespace
 
+size_t update_part_doubles(int l) {
+  const GramTiling g = gram_tiling(l, l, true, kThreads);
+  return (size_t)kMaxClusters * std::max(g.ntiles * 16, 2 * l);
+}
+
 void fused_update(pcaone_ctx* c, UpdateArgs a) {
   PG_REQUIRE(a.l >= 1 && a.l <= kLmax, PCAONE_EBADARG, "sketch width out of range");
-  PG_REQUIRE(((a.l + 3) / 4) * ((a.l + 3) / 4) <= kThreads, PCAONE_EBADARG, "sketch width too large for the update");
+  const int nblk = update_ctas(c, a.N);
   if (a.l <= 16)
-    launch_all<16>(c, a);
+    launch_all<16>(c, a, nblk);
   else if (a.l <= 32)
-    launch_all<32>(c, a);
+    launch_all<32>(c, a, nblk);
   else if (a.l <= 48)
-    launch_all<48>(c, a);
+    launch_all<48>(c, a, nblk);
   else
-    launch_all<64>(c, a);
+    launch_all<64>(c, a, nblk);
   c->launches += 4;
 }
 

@@ -192,8 +192,7 @@ struct Engine {
     a.bt1 = gemm.omega_bt ? gemm.omega_bt(c, l, &a.bt_half) : nullptr;
     a.kpad = Npad;
     a.wsum = wsum;
-    a.nblk = 64;
-    a.part = (double*)scratch(c, "upd_part", (size_t)a.nblk * l * l * 8);
+    a.part = (double*)scratch(c, "upd_part", update_part_doubles(l) * 8);
     a.R1 = (double*)scratch(c, "upd_R1", (size_t)l * l * 8);
     a.R2 = (double*)scratch(c, "upd_R2", (size_t)l * l * 8);
     a.D = Dsig;

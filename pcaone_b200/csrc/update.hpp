@@ -19,7 +19,7 @@ struct UpdateArgs {
   int64_t kpad = 0;
   int bt_half = 0;               // row offset of the lo half in bt1 (= NP / 2)
   double* wsum = nullptr;      // l
-  double* part = nullptr;      // nblk * l * l work
+  double* part = nullptr;      // update_part_doubles(l) work
   double* R1 = nullptr;        // l x l work
   double* R2 = nullptr;
   double* D = nullptr;         // l
@@ -27,9 +27,11 @@ struct UpdateArgs {
   unsigned* counters = nullptr;  // 4 tickets, zero between calls
   int* status = nullptr;
   int64_t N = 0;
-  int l = 0, nblk = 64;
+  int l = 0;
 };
 
+// doubles of UpdateArgs::part for sketch width l
+size_t update_part_doubles(int l);
 void fused_update(pcaone_ctx* c, UpdateArgs a);
 
 }  // namespace pg

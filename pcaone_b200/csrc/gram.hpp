@@ -189,6 +189,92 @@ __device__ __forceinline__ bool last_cta(unsigned* counter) {
   return last;
 }
 
+// In-place Cholesky of the SPD l x l matrix in s (shared memory, row-major; the upper triangle
+// is read): on return s holds the upper factor R (W = R^T R) with zeros below the diagonal.
+// Right-looking with the row scaling deferred: step j subtracts s[j][a] s[j][b] / s[j][j]
+// from the trailing upper triangle (a warp per row, lanes over columns), one barrier a step;
+// row j is divided by sqrt(s[j][j]) at the end. A pivot that is not positive and finite is
+// replaced by 1. Returns 1 + the first such column, else 0 (the same in every thread).
+__device__ __forceinline__ int chol_upper_smem(double* s, int l) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int bad = 0;
+  __syncthreads();
+  for (int j = 0; j < l; ++j) {
+    double p = s[j * l + j];
+    if (!(p > 0.0) || !isfinite(p)) {
+      if (!bad) bad = j + 1;
+      p = 1.0;
+    }
+    for (int a = j + 1 + warp; a < l; a += nw) {
+      const double f = s[j * l + a] / p;
+      for (int b = a + lane; b < l; b += 32) s[a * l + b] -= f * s[j * l + b];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) {  // off-diagonal first: diagonals still pivots
+    const int i = t / l, j = t - i * l;
+    if (j > i) {
+      const double p = s[i * l + i];
+      s[t] /= (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
+    } else if (j < i) {
+      s[t] = 0.0;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < l; i += blockDim.x) {
+    const double p = s[i * l + i];
+    s[i * l + i] = (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
+  }
+  __syncthreads();
+  return bad;
+}
+
+// Householder column signs D (l) from the modified LU of the l x l block T (shared memory,
+// overwritten): step i takes the pivot s = T[i][i], D_i = -sign(s) with sign(0) = +, and
+// eliminates below it with the shifted pivot s - D_i (Ballard et al. 2015). One barrier a
+// step; a warp per row. D is written by thread 0 and visible to the CTA on return.
+__device__ __forceinline__ void householder_signs_smem(double* T, int l, double* D) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  for (int i = 0; i < l; ++i) {
+    const double piv = T[i * l + i];
+    const double di = piv >= 0.0 ? -1.0 : 1.0;
+    const double p = piv - di;
+    if (threadIdx.x == 0) D[i] = di;
+    for (int r = i + 1 + warp; r < l; r += nw) {
+      const double f = T[r * l + i] / p;
+      for (int cc = i + 1 + lane; cc < l; cc += 32) T[r * l + cc] -= f * T[i * l + cc];
+    }
+    __syncthreads();
+  }
+}
+
+// Clusters of kGramCluster CTAs of kernel (threads, smem bytes) that fit on the device at
+// once, cached in the context by (kernel, key); 0 when the runtime cannot tell.
+inline int resident_clusters(pcaone_ctx* c, const void* kernel, uint64_t key, int threads, size_t smem) {
+  const auto k = std::make_pair(kernel, key);
+  auto it = c->cluster_occupancy.find(k);
+  if (it != c->cluster_occupancy.end()) return it->second;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kGramCluster * 64);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = kGramCluster;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    n = 0;
+  }
+  c->cluster_occupancy[k] = n;
+  return n;
+}
+
 // Row range of this CTA when n rows are split over the grid in contiguous blocks.
 __device__ __forceinline__ void row_range(int64_t n, int64_t& r0, int64_t& r1) {
   const int64_t rpb = (n + gridDim.x - 1) / gridDim.x;

@@ -130,6 +130,9 @@ struct pcaone_ctx {
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;
 
+  // resident clusters of the cluster kernels, by kernel and shape (gram.hpp)
+  std::map<std::pair<const void*, uint64_t>, int> cluster_occupancy;
+
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double gemm_ms_accum = 0.0;

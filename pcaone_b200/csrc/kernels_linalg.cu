@@ -91,34 +91,8 @@ __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restri
                            int* __restrict__ status) {
   extern __shared__ double s[];  // l x l
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) s[t] = W[t];
-  __syncthreads();
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  // right-looking: s holds the trailing matrix; row j of R is written into row j of s
-  for (int j = 0; j < l; ++j) {
-    if (threadIdx.x == 0) {
-      double d = s[j * l + j];
-      if (!(d > 0.0) || !isfinite(d)) {
-        bad = j + 1;
-        d = 1.0;
-      }
-      s[j * l + j] = sqrt(d);
-    }
-    __syncthreads();
-    double djj = s[j * l + j];
-    for (int i = j + 1 + threadIdx.x; i < l; i += blockDim.x) s[j * l + i] /= djj;
-    __syncthreads();
-    for (int t = threadIdx.x; t < (l - j - 1) * (l - j - 1); t += blockDim.x) {
-      int a = j + 1 + t / (l - j - 1), b = j + 1 + t % (l - j - 1);
-      if (b >= a) s[a * l + b] -= s[j * l + a] * s[j * l + b];
-    }
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
-    int i = t / l, j = t % l;
-    R[t] = (j >= i) ? s[t] : 0.0;
-  }
+  const int bad = chol_upper_smem(s, l);
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) R[t] = s[t];
   __syncthreads();
   if (Rprev) {
     for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
@@ -293,14 +267,16 @@ void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int6
   const int rows = std::max(8, std::min(128, (kCrossSmemBudget - fixed) / (2 * w * 8)));
   const size_t smem = (size_t)fixed + (size_t)2 * rows * w * 8;
   const int64_t want = (n + (int64_t)kGramCluster * 4 * rows - 1) / ((int64_t)kGramCluster * 4 * rows);
-  const int cap = std::max(1, std::min(kCrossMaxClusters, 2 * c->sm_count / kGramCluster));
+  int cap = std::max(1, std::min(kCrossMaxClusters, 2 * c->sm_count / kGramCluster));
+  const void* kern = sym ? (const void*)k_cross<true> : (const void*)k_cross<false>;
+  PG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int resident = resident_clusters(c, kern, ((uint64_t)la << 32) | (uint64_t)lb, kCrossThreads, smem);
+  if (resident > 0) cap = std::min(cap, resident);
   const int ncl = (int)std::max<int64_t>(1, std::min<int64_t>(cap, want));
   double* gpart = (double*)scratch(c, "cross_part", (size_t)ncl * g.ntiles * 16 * 8);
   if (sym) {
-    PG_CUDA(cudaFuncSetAttribute(k_cross<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_cross<true><<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, la, A, lb, n, rows, gpart);
   } else {
-    PG_CUDA(cudaFuncSetAttribute(k_cross<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_cross<false><<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, la, B, lb, n, rows, gpart);
   }
   PG_CHECK_LAUNCH();

@@ -4,8 +4,8 @@
 // (src/Halko.cpp:213-216) and of the Halko epochs (src/Halko.cpp:118-122, src/RSVD.hpp:81-90).
 //
 //   K1  H = H1 + H2 (winSVD), W1 = H^T H                     last CTA: R1 = chol(W1)
-//   K2  Q1 = H R1^-1, W2 = Q1^T Q1                          last CTA: R2 = chol(W2), signs D
-//   K3  Q = Q1 R2^-1, flip sums |O2 - Q D|, |O2 + Q D|      last CTA: multipliers m = +-D
+//   K2  Q1 = H R1^-1, W2 = Q1^T Q1                          last CTA: R2 = chol(W2)
+//   K3  Q = Q1 R2^-1, flip sums |O2 - Q|, |O2 + Q|          last CTA: signs D, multipliers m = +-D
 //   K4  Omega = Q m, Omega2 = Omega, operand copies, column sums  last CTA: sum of Omega
 //
 // Each kernel runs as clusters of kGramCluster CTAs that own fixed row ranges. A CTA stages
@@ -35,33 +35,6 @@ constexpr int kThreads = 256;
 // rows staged per batch: a batch of rows, the group sums and R fit in about 100 KB, so two
 // CTAs (two clusters' worth per 8 SMs) fit on an SM
 __host__ __device__ constexpr int stage_rows(int l) { return l <= 48 ? 128 : 64; }
-
-// Shared-memory Cholesky of an l x l SPD matrix (upper R, W = R^T R), in place in s.
-__device__ void chol_smem(double* s, int l, int* status) {
-  for (int j = 0; j < l; ++j) {
-    if (threadIdx.x == 0) {
-      double d = s[j * l + j];
-      if (!(d > 0.0) || !isfinite(d)) {
-        atomicMax(status, j + 1);
-        d = 1.0;
-      }
-      s[j * l + j] = sqrt(d);
-    }
-    __syncthreads();
-    const double djj = s[j * l + j];
-    for (int i = j + 1 + threadIdx.x; i < l; i += blockDim.x) s[j * l + i] /= djj;
-    __syncthreads();
-    const int w = l - j - 1;
-    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-      const int a = j + 1 + t / w, b = j + 1 + t % w;
-      if (b >= a) s[a * l + b] -= s[j * l + a] * s[j * l + b];
-    }
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x)
-    if (t % l < t / l) s[t] = 0.0;
-  __syncthreads();
-}
 
 // Column-strided pass over this CTA's rows: thread t owns column t % l of rows
 // r0 + t / l, r0 + t / l + T / l, ... with T = l * (blockDim / l) threads.
@@ -112,7 +85,8 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   cluster_sum(cpart, g.ntiles * 16, a.part);
   if (!last_cta(&a.counters[0])) return;
   gram_final(g, a.part, gridDim.x / kGramCluster, l, l, stage);
-  chol_smem(stage, l, a.status);
+  const int bad = chol_upper_smem(stage, l);
+  if (bad && threadIdx.x == 0) atomicMax(a.status, bad);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R1[t] = stage[t];
   if (threadIdx.x == 0) a.counters[0] = 0;
 }
@@ -170,42 +144,15 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   if (!last_cta(&a.counters[1])) return;
   double* Rn = stage;  // W2, then R2 (row stride l)
   gram_final(g, a.part, gridDim.x / kGramCluster, l, l, Rn);
-  chol_smem(Rn, l, a.status);
+  const int bad = chol_upper_smem(Rn, l);
+  if (bad && threadIdx.x == 0) atomicMax(a.status, bad);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R2[t] = Rn[t];
-  __syncthreads();
-  // top l x l block of Q = Q1[0:l] R2^-1 (substitution in shared memory), then the modified
-  // LU for the Householder signs
-  double* top = R;  // R1 is no longer needed
-  for (int r = threadIdx.x; r < l; r += blockDim.x) {
-    const double* q = a.Q + (int64_t)r * l;
-    for (int j = 0; j < l; ++j) {
-      double v = q[j];
-      for (int k = 0; k < j; ++k) v -= top[r * l + k] * Rn[k * l + j];
-      top[r * l + j] = v / Rn[j * l + j];
-    }
-  }
-  __syncthreads();
-  for (int i = 0; i < l; ++i) {
-    const double piv = top[i * l + i];
-    const double di = piv >= 0.0 ? -1.0 : 1.0;
-    const double p = piv - di;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      a.D[i] = di;
-      top[i * l + i] = p;
-    }
-    for (int r = i + 1 + threadIdx.x; r < l; r += blockDim.x) top[r * l + i] /= p;
-    __syncthreads();
-    const int w = l - i - 1;
-    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-      const int r = i + 1 + t / w, cc = i + 1 + t % w;
-      top[r * l + cc] -= top[r * l + i] * top[i * l + cc];
-    }
-    __syncthreads();
-  }
   if (threadIdx.x == 0) a.counters[1] = 0;
 }
 
+// K3. The flip sums are taken without the signs: A_c = sum |O2 - Q| and B_c = sum |O2 + Q|
+// per column; with D_c = +1 they are |O2 - Q D| and |O2 + Q D|, with D_c = -1 swapped (the
+// same values bit for bit). The last CTA reads the top l x l block of the final Q for D.
 template <int LMAX>
 __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd3(UpdateArgs a) {
   extern __shared__ double sm[];
@@ -221,8 +168,7 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   row_range(a.N, r0, r1);
   const int T = col_threads(l);
   const int c = threadIdx.x % l;
-  const double d = threadIdx.x < T ? a.D[c] : 0.0;
-  double dm = 0.0, dp = 0.0;
+  double sa = 0.0, sb = 0.0;
   for (int64_t b = r0; b < r1; b += rows) {
     const int nr = (int)(r1 - b < rows ? r1 - b : rows);
     __syncthreads();  // R staged; the previous batch is consumed
@@ -234,14 +180,14 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
     for (int t = threadIdx.x; t < nr * l; t += blockDim.x) a.Q[b * l + t] = sq[t];
     if (threadIdx.x < T) {
       for (int r = threadIdx.x / l; r < nr; r += T / l) {
-        const double o = so[r * l + c], q = sq[r * l + c] * d;
-        dm += fabs(o - q);
-        dp += fabs(o + q);
+        const double o = so[r * l + c], q = sq[r * l + c];
+        sa += fabs(o - q);
+        sb += fabs(o + q);
       }
     }
   }
-  red[threadIdx.x * 2] = dm;
-  red[threadIdx.x * 2 + 1] = dp;
+  red[threadIdx.x * 2] = sa;
+  red[threadIdx.x * 2 + 1] = sb;
   __syncthreads();
   for (int j = threadIdx.x; j < l; j += blockDim.x) {  // fixed-order sum over this column's threads
     double m = 0.0, p = 0.0;
@@ -254,34 +200,44 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   }
   cluster_sum(cpart, 2 * l, a.part);
   if (!last_cta(&a.counters[2])) return;
+  double* top = R;  // the top l x l block of Q, written by this kernel's CTAs
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) top[t] = a.Q[t];
+  householder_signs_smem(top, l, a.D);
   const int ncl = gridDim.x / kGramCluster;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
-    const double m = sum_strided<16>(a.part + j, ncl, 2 * l);
-    const double p = sum_strided<16>(a.part + l + j, ncl, 2 * l);
-    a.mult[j] = (m > 2.0 * p) ? -a.D[j] : a.D[j];  // src/RSVD.hpp:85
+    const double A = sum_strided<16>(a.part + j, ncl, 2 * l);
+    const double B = sum_strided<16>(a.part + l + j, ncl, 2 * l);
+    const double d = a.D[j];
+    const double m = d > 0.0 ? A : B, p = d > 0.0 ? B : A;
+    a.mult[j] = (m > 2.0 * p) ? -d : d;  // src/RSVD.hpp:85
   }
   if (threadIdx.x == 0) a.counters[2] = 0;
 }
 
+// K4. Writes in row-major order (coalesced), column sums from the staged batch.
 __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads) k_upd4(UpdateArgs a) {
   extern __shared__ double sm[];
   const int l = a.l;
+  const int rows = stage_rows(l);
   double* red = sm;                // kThreads
   double* cpart = red + kThreads;  // l
+  double* st = cpart + l;          // rows x l
   int64_t r0, r1;
   row_range(a.N, r0, r1);
   const int T = col_threads(l);
   double cs = 0.0;
-  if (threadIdx.x < T) {
-    const int j = threadIdx.x % l;
-    const double mj = a.mult[j];
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    __syncthreads();  // the previous batch is summed
 #pragma unroll 4
-    for (int64_t r = r0 + threadIdx.x / l; r < r1; r += T / l) {
-      const double v = a.Q[r * l + j] * mj;
-      a.Omg[r * l + j] = v;
-      a.Omg2[r * l + j] = v;
-      cs += v;
-      if (a.Omgf) a.Omgf[r * l + j] = (float)v;
+    for (int t = threadIdx.x; t < nr * l; t += blockDim.x) {
+      const int rr = t / l, j = t - rr * l;
+      const int64_t r = b + rr, o = b * l + t;
+      const double v = a.Q[o] * a.mult[j];
+      a.Omg[o] = v;
+      a.Omg2[o] = v;
+      st[t] = v;
+      if (a.Omgf) a.Omgf[o] = (float)v;
       if (a.bt1) {
         const int64_t kp = tc_pos(r);
         const float x = (float)v;
@@ -290,6 +246,9 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
         a.bt1[bt_elem(a.bt_half + j, kp, 2 * a.bt_half)] = __float2bfloat16_rn(x - __bfloat162float(hi));
       }
     }
+    __syncthreads();
+    if (threadIdx.x < T)
+      for (int rr = threadIdx.x / l; rr < nr; rr += T / l) cs += st[rr * l + threadIdx.x % l];
   }
   red[threadIdx.x] = cs;
   __syncthreads();
@@ -306,25 +265,35 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
 }
 
 // CTAs of the update kernels: whole clusters, about 64 rows or more per CTA, at most
-// kMaxClusters clusters (the last CTA reads one partial per cluster).
-constexpr int kMaxClusters = 18;
+// kMaxClusters clusters (two CTAs an SM; the last CTA reads one partial per cluster).
+constexpr int kMaxClusters = 36;
 
-int update_ctas(pcaone_ctx* c, int64_t N) {
+int update_ctas(pcaone_ctx* c, int64_t N, int resident) {
   const int64_t want = (N + kGramCluster * 64 - 1) / (kGramCluster * 64);
-  const int cap = std::max(1, std::min(kMaxClusters, c->sm_count / kGramCluster));
+  int cap = std::max(1, std::min(kMaxClusters, 2 * c->sm_count / kGramCluster));
+  if (resident > 0) cap = std::min(cap, resident);
   return (int)std::max<int64_t>(1, std::min<int64_t>(cap, want)) * kGramCluster;
 }
 
 template <int LMAX>
-void launch_all(pcaone_ctx* c, const UpdateArgs& a, int nblk) {
+void launch_all(pcaone_ctx* c, const UpdateArgs& a) {
   const int l = a.l, rows = stage_rows(l);
   const size_t s1 = (size_t)upd_gram_smem_doubles(l, 0) * 8;
   const size_t s2 = (size_t)upd_gram_smem_doubles(l, LMAX) * 8;
   const size_t s3 = ((size_t)LMAX * LMAX + 2 * (size_t)rows * l + 2 * kThreads + 2 * l) * 8;
-  const size_t s4 = ((size_t)kThreads + l) * 8;
+  const size_t s4 = ((size_t)kThreads + l + (size_t)rows * l) * 8;
   PG_CUDA(cudaFuncSetAttribute(k_upd1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
   PG_CUDA(cudaFuncSetAttribute(k_upd2<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
   PG_CUDA(cudaFuncSetAttribute(k_upd3<LMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
+  // every cluster of every kernel resident at once: the tightest of the four bounds
+  int resident = 0;
+  const void* ks[4] = {(const void*)k_upd1, (const void*)k_upd2<LMAX>, (const void*)k_upd3<LMAX>, (const void*)k_upd4};
+  const size_t ss[4] = {s1, s2, s3, s4};
+  for (int i = 0; i < 4; ++i) {
+    const int n = resident_clusters(c, ks[i], (uint64_t)l, kThreads, ss[i]);
+    if (n > 0) resident = resident > 0 ? std::min(resident, n) : n;
+  }
+  const int nblk = update_ctas(c, a.N, resident);
   k_upd1<<<nblk, kThreads, s1, c->stream>>>(a);
   PG_CHECK_LAUNCH();
   k_upd2<LMAX><<<nblk, kThreads, s2, c->stream>>>(a);
@@ -344,15 +313,14 @@ size_t update_part_doubles(int l) {
 
 void fused_update(pcaone_ctx* c, UpdateArgs a) {
   PG_REQUIRE(a.l >= 1 && a.l <= kLmax, PCAONE_EBADARG, "sketch width out of range");
-  const int nblk = update_ctas(c, a.N);
   if (a.l <= 16)
-    launch_all<16>(c, a, nblk);
+    launch_all<16>(c, a);
   else if (a.l <= 32)
-    launch_all<32>(c, a, nblk);
+    launch_all<32>(c, a);
   else if (a.l <= 48)
-    launch_all<48>(c, a, nblk);
+    launch_all<48>(c, a);
   else
-    launch_all<64>(c, a, nblk);
+    launch_all<64>(c, a);
   c->launches += 4;
 }
 

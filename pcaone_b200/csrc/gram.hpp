@@ -12,7 +12,8 @@ namespace pg {
 
 namespace cg = cooperative_groups;
 
-constexpr int kGramCluster = 8;  // CTAs per cluster of the Gram kernels
+constexpr int kGramCluster = 8;    // CTAs per cluster of the Gram kernels
+constexpr int kGramMaxParts = 36;  // cluster sums read at once by the final reductions
 
 // The la4 x lb4 output (widths rounded up to 4) is cut into 4 x 4 tiles; a symmetric product
 // keeps the tiles on and above the diagonal. The CTA's threads form ngrp groups of ntiles
@@ -136,6 +137,21 @@ __device__ __forceinline__ double sum_strided(const double* x, int n, int64_t st
   return s;
 }
 
+// sum_{b < n} x[b * stride] in b order with every load issued before the adds (n <= WMAX);
+// longer sums go to sum_strided.
+template <int WMAX>
+__device__ __forceinline__ double sum_all(const double* x, int n, int64_t stride) {
+  if (n > WMAX) return sum_strided<16>(x, n, stride);
+  double v[WMAX];
+#pragma unroll
+  for (int k = 0; k < WMAX; ++k) v[k] = k < n ? x[(int64_t)k * stride] : 0.0;
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < WMAX; ++k)
+    if (k < n) s += v[k];
+  return s;
+}
+
 // Cluster sum of the CTAs' part[n] (shared memory), in rank order, written to
 // gout[cluster index * n + e]. Every CTA of the cluster calls it; the rank-r CTA sums the
 // elements r * blockDim + t, ... through distributed shared memory. The second cluster barrier
@@ -163,7 +179,7 @@ __device__ __forceinline__ void gram_final(const GramTiling& g, const double* gp
                                            double* W) {
   const int n = g.ntiles * 16;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const double v = sum_strided<16>(gpart + e, nparts, n);
+    const double v = sum_all<kGramMaxParts>(gpart + e, nparts, n);
     int i0, j0;
     gram_tile_origin(g, e / 16, i0, j0);
     const int i = i0 + (e % 16) / 4, j = j0 + e % 4;
@@ -189,14 +205,48 @@ __device__ __forceinline__ bool last_cta(unsigned* counter) {
   return last;
 }
 
-// In-place Cholesky of the SPD l x l matrix in s (shared memory, row-major; the upper triangle
-// is read): on return s holds the upper factor R (W = R^T R) with zeros below the diagonal.
-// Right-looking with the row scaling deferred: step j subtracts s[j][a] s[j][b] / s[j][j]
-// from the trailing upper triangle (a warp per row, lanes over columns), one barrier a step;
-// row j is divided by sqrt(s[j][j]) at the end. A pivot that is not positive and finite is
-// replaced by 1. Returns 1 + the first such column, else 0 (the same in every thread).
-__device__ __forceinline__ int chol_upper_smem(double* s, int l) {
+// One elimination step on the l x l matrix s (shared memory, row-major): for the rows
+// a = j + 1, ..., l - 1 (a warp per row, eight rows a warp in flight) and the columns b > j
+// (b >= a when upper; lanes over columns, two a lane for l <= 64),
+//   s[a][b] -= (s[a][j] or s[j][a]) * inv * s[j][b],
+// with the multiplier from column j (lu) or row j (upper). All loads of a batch of rows are
+// issued before its stores, so the step costs about one shared-memory round trip.
+template <bool kUpper>
+__device__ __forceinline__ void elim_step(double* s, int l, int j, double inv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int b0 = lane, b1 = lane + 32;
+  const double rj0 = (b0 > j && b0 < l) ? s[j * l + b0] : 0.0;
+  const double rj1 = (b1 > j && b1 < l) ? s[j * l + b1] : 0.0;
+  for (int a0 = j + 1 + warp; a0 < l; a0 += 8 * nw) {
+    double f[8], v0[8], v1[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int a = a0 + k * nw;
+      const bool ok = a < l;
+      const int lo = kUpper ? a : j + 1;  // first column updated in row a
+      f[k] = ok ? (kUpper ? s[j * l + a] : s[a * l + j]) * inv : 0.0;
+      v0[k] = (ok && b0 >= lo && b0 < l) ? s[a * l + b0] : 0.0;
+      v1[k] = (ok && b1 >= lo && b1 < l) ? s[a * l + b1] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int a = a0 + k * nw;
+      if (a >= l) break;
+      const int lo = kUpper ? a : j + 1;
+      if (b0 >= lo && b0 < l) s[a * l + b0] = v0[k] - f[k] * rj0;
+      if (b1 >= lo && b1 < l) s[a * l + b1] = v1[k] - f[k] * rj1;
+    }
+  }
+}
+
+// In-place Cholesky of the SPD l x l matrix in s (shared memory, row-major; the upper triangle
+// is read; l <= 64): on return s holds the upper factor R (W = R^T R) with zeros below the
+// diagonal. Right-looking with the row scaling deferred: step j subtracts
+// s[j][a] s[j][b] / s[j][j] from the trailing upper triangle (elim_step; one reciprocal of the
+// pivot a step), one barrier a step; row j is divided by sqrt(s[j][j]) at the end. A pivot
+// that is not positive and finite is replaced by 1. Returns 1 + the first such column, else 0
+// (the same in every thread).
+__device__ __forceinline__ int chol_upper_smem(double* s, int l) {
   int bad = 0;
   __syncthreads();
   for (int j = 0; j < l; ++j) {
@@ -205,10 +255,7 @@ __device__ __forceinline__ int chol_upper_smem(double* s, int l) {
       if (!bad) bad = j + 1;
       p = 1.0;
     }
-    for (int a = j + 1 + warp; a < l; a += nw) {
-      const double f = s[j * l + a] / p;
-      for (int b = a + lane; b < l; b += 32) s[a * l + b] -= f * s[j * l + b];
-    }
+    elim_step<true>(s, l, j, __drcp_rn(p));
     __syncthreads();
   }
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) {  // off-diagonal first: diagonals still pivots
@@ -230,21 +277,17 @@ __device__ __forceinline__ int chol_upper_smem(double* s, int l) {
 }
 
 // Householder column signs D (l) from the modified LU of the l x l block T (shared memory,
-// overwritten): step i takes the pivot s = T[i][i], D_i = -sign(s) with sign(0) = +, and
-// eliminates below it with the shifted pivot s - D_i (Ballard et al. 2015). One barrier a
-// step; a warp per row. D is written by thread 0 and visible to the CTA on return.
+// overwritten; l <= 64): step i takes the pivot s = T[i][i], D_i = -sign(s) with
+// sign(0) = +, and eliminates below it with the shifted pivot s - D_i (Ballard et al. 2015);
+// the multipliers T[r][i] / (s - D_i) are used, not stored. One barrier a step. D is
+// written by thread 0 and visible to the CTA on return.
 __device__ __forceinline__ void householder_signs_smem(double* T, int l, double* D) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
   for (int i = 0; i < l; ++i) {
     const double piv = T[i * l + i];
     const double di = piv >= 0.0 ? -1.0 : 1.0;
-    const double p = piv - di;
     if (threadIdx.x == 0) D[i] = di;
-    for (int r = i + 1 + warp; r < l; r += nw) {
-      const double f = T[r * l + i] / p;
-      for (int cc = i + 1 + lane; cc < l; cc += 32) T[r * l + cc] -= f * T[i * l + cc];
-    }
+    elim_step<false>(T, l, i, __drcp_rn(piv - di));
     __syncthreads();
   }
 }

@@ -18,7 +18,7 @@ namespace {
 // sums through distributed shared memory into gpart[cluster] (ntiles * 16 values in tile
 // layout). SYM (A == B): only the tiles on and above the diagonal, one staged copy.
 constexpr int kCrossThreads = 256;
-constexpr int kCrossMaxClusters = 36;
+constexpr int kCrossMaxClusters = kGramMaxParts;
 constexpr int kCrossSmemBudget = 96 * 1024;  // two CTAs an SM
 
 __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {

@@ -205,8 +205,8 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   householder_signs_smem(top, l, a.D);
   const int ncl = gridDim.x / kGramCluster;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
-    const double A = sum_strided<16>(a.part + j, ncl, 2 * l);
-    const double B = sum_strided<16>(a.part + l + j, ncl, 2 * l);
+    const double A = sum_all<kGramMaxParts>(a.part + j, ncl, 2 * l);
+    const double B = sum_all<kGramMaxParts>(a.part + l + j, ncl, 2 * l);
     const double d = a.D[j];
     const double m = d > 0.0 ? A : B, p = d > 0.0 ? B : A;
     a.mult[j] = (m > 2.0 * p) ? -d : d;  // src/RSVD.hpp:85
@@ -260,13 +260,13 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   cluster_sum(cpart, l, a.part);
   if (!last_cta(&a.counters[3])) return;
   const int ncl = gridDim.x / kGramCluster;
-  for (int j = threadIdx.x; j < l; j += blockDim.x) a.wsum[j] = sum_strided<16>(a.part + j, ncl, l);
+  for (int j = threadIdx.x; j < l; j += blockDim.x) a.wsum[j] = sum_all<kGramMaxParts>(a.part + j, ncl, l);
   if (threadIdx.x == 0) a.counters[3] = 0;
 }
 
 // CTAs of the update kernels: whole clusters, about 64 rows or more per CTA, at most
 // kMaxClusters clusters (two CTAs an SM; the last CTA reads one partial per cluster).
-constexpr int kMaxClusters = 36;
+constexpr int kMaxClusters = kGramMaxParts;
 
 int update_ctas(pcaone_ctx* c, int64_t N, int resident) {
   const int64_t want = (N + kGramCluster * 64 - 1) / (kGramCluster * 64);

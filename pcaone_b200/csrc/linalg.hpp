@@ -25,10 +25,10 @@ void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);
 void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y);
 void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out);
 
-// Forward substitution for one row: x R = a with R upper l x l stored row-major with the
-// compile-time row stride LMAX (so every R address is a constant offset), x kept in registers
-// (LMAX >= l; the loops unroll over LMAX and skip j >= l). Every element of a is read before
-// out is written, so out may alias a.
+// Forward substitution for one row: x R = a with R upper l x l staged by stage_r (row stride
+// LMAX, so every R address is a constant offset; the diagonal slots hold 1 / R_jj, so the
+// dependent chain has no division), x kept in registers (LMAX >= l; the loops unroll over LMAX
+// and skip j >= l). Every element of a is read before out is written, so out may alias a.
 template <int LMAX>
 __device__ __forceinline__ void solve_row_upper(const double* a, const double* Rs, int l, double* out) {
   double x[LMAX];
@@ -38,7 +38,7 @@ __device__ __forceinline__ void solve_row_upper(const double* a, const double* R
       double v = a[j];
 #pragma unroll
       for (int k = 0; k < j; ++k) v -= x[k] * Rs[k * LMAX + j];
-      x[j] = v / Rs[j * LMAX + j];
+      x[j] = v * Rs[j * LMAX + j];
     } else {
       x[j] = 0.0;
     }
@@ -48,10 +48,14 @@ __device__ __forceinline__ void solve_row_upper(const double* a, const double* R
     if (j < l) out[j] = x[j];
 }
 
-// Copy R (l x l row-major) into shared memory with row stride LMAX.
+// Copy R (l x l row-major, upper) into shared memory with row stride LMAX for
+// solve_row_upper: the diagonal slots get 1 / R_jj.
 template <int LMAX>
 __device__ __forceinline__ void stage_r(const double* R, int l, double* Rs) {
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) Rs[(t / l) * LMAX + t % l] = R[t];
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
+    const int i = t / l, j = t - i * l;
+    Rs[i * LMAX + j] = i == j ? 1.0 / R[t] : R[t];
+  }
 }
 
 }  // namespace pg

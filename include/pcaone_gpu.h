@@ -179,6 +179,19 @@ int pcaone_gpu_gl_freq(pcaone_ctx* ctx, int maxiter, double tolmaf, double* F, i
 int pcaone_gpu_gl_update(pcaone_ctx* ctx, const double* U, const double* S, const double* V,
                          uint32_t k);
 
+/* PCAngsd genetic relationship matrix, the stage after the EM loop (src/Halko.cpp:317-331
+ * with Data::pcangsd_standardize_E, src/Data.cpp:301-343). The posterior E is rebuilt in FP64
+ * from U, S and V as pcaone_gpu_gl_update does (same arguments and index semantics), site j
+ * divided by sqrt(2 F_j (1 - F_j)) when that exceeds 1e-9, and per sample
+ * Dc_i = sum_j sum_g (g - 2F_j)^2 P(g) / (2 F_j (1 - F_j)). Then C = E E^T / M with
+ * diag(C) = Dc / M: nsamples x nsamples, column-major FP64 host (symmetric), or NULL.
+ * evecs (nsamples x nsamples column-major host, or NULL) and svals (nsamples, or NULL): the
+ * singular vectors and values of C that the reference's JacobiSVD gives, i.e. the
+ * eigenvectors of the symmetric C ordered by decreasing |eigenvalue| and those |eigenvalues|.
+ * The sign of each vector is arbitrary, as in any SVD. */
+int pcaone_gpu_gl_grm(pcaone_ctx* ctx, const double* U, const double* S, const double* V, uint32_t k,
+                      double* C, double* evecs, double* svals);
+
 /* Allocation-free Z^T B for callers that cannot let a library call cudaMalloc: code running
  * inside another framework's device memory pool, or an outer solver loop that must not
  * allocate per call (e.g. an eigensolver using this product as its operator). It has no

@@ -28,7 +28,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
-           "pcaone_gpu_gl_update", "pcaone_gpu_product_t_noalloc"]
+           "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc"]
 
 
 class PcaoneError(RuntimeError):
@@ -86,6 +86,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
+        L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
         for name in EXPORTS:
             getattr(L, name).restype = ctypes.c_int if name != "pcaone_gpu_last_error" else ctypes.c_char_p
@@ -284,6 +285,21 @@ def _gl_update(self, U=None, S=None, V=None):
     self._check(lib().pcaone_gpu_gl_update(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(S)))
 
 
+def _gl_grm(self, U, S, V, vectors=True):
+    """PCAngsd GRM from the final factors (pcaone_gpu_gl_grm): returns (C, evecs, svals) with
+    C nsamples x nsamples, evecs its singular vectors as columns (None unless vectors) and
+    svals the singular values (None unless vectors)."""
+    Uf, Vf = np.asfortranarray(U, dtype=np.float64), np.asfortranarray(V, dtype=np.float64)
+    Sf = np.ascontiguousarray(S, dtype=np.float64)
+    n = Uf.shape[0]
+    C = np.empty((n, n), dtype=np.float64, order="F")
+    ev = np.empty((n, n), dtype=np.float64, order="F") if vectors else None
+    sv = np.empty(n, dtype=np.float64) if vectors else None
+    self._check(lib().pcaone_gpu_gl_grm(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(Sf), _ptr(C),
+                                        _ptr(ev) if vectors else None, _ptr(sv) if vectors else None))
+    return C, ev, sv
+
+
 def _product_t_noalloc(self, d_B: int, ncols: int, d_out: int, standardize=True, ploidy=2):
     """Allocation-free Z^T B on caller-owned device buffers (raw device addresses of column-major
     FP64 nsamples x ncols B and nsnps x ncols out); see pcaone_gpu_product_t_noalloc."""
@@ -295,14 +311,17 @@ GpuContext.product_t_noalloc = _product_t_noalloc
 GpuContext.load_gl = _load_gl
 GpuContext.gl_freq = _gl_freq
 GpuContext.gl_update = _gl_update
+GpuContext.gl_grm = _gl_grm
 
 
 def run_pcangsd(ctx: "GpuContext", P: np.ndarray, k: int = 10, svd: int = 2, bands: int = 64,
                 maxp: int = 20, oversamples: int = 10, tol: float = 1e-4, maxiter: int = 100,
                 tolem: float = 1e-5, tolmaf: float = 1e-6, seed: int = 101, rand: int = 1,
-                shuffle: bool = True, reference_index: bool = True):
+                shuffle: bool = True, reference_index: bool = True, grm: bool = False):
     """PCAngsd on the GPU: the impute branch of run_pca_with_halko for Beagle input
-    (src/Halko.cpp:294-316). Returns (eigvals, S, U, V in input order, iterations, F).
+    (src/Halko.cpp:294-316). Returns (eigvals, S, U, V in input order, iterations, F); with
+    grm, also (C, evecs, svals) of the GRM stage (src/Halko.cpp:317-331) from the final
+    factors.
 
     The in-core shuffle is applied by feeding the RSVD the permuted posterior matrix: the
     likelihood columns are loaded in permuted order, and under the reference's index
@@ -327,7 +346,10 @@ def run_pcangsd(ctx: "GpuContext", P: np.ndarray, k: int = 10, svd: int = 2, ban
     V[perm] = r.V
     F = np.empty_like(F_perm)
     F[perm] = F_perm
-    return r.S ** 2 / M * 2, r.S, r.U, V, it + 1, F
+    out = (r.S ** 2 / M * 2, r.S, r.U, V, it + 1, F)
+    if grm:
+        out += ctx.gl_grm(r.U, r.S, r.V[perm] if reference_index else r.V)
+    return out
 GpuContext.fit_emu = _fit_emu
 GpuContext.clear_imputed = _clear_imputed
 

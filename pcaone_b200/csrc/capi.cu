@@ -81,6 +81,27 @@ int guarded(pcaone_ctx* c, F&& f) {
 
 }  // namespace
 
+namespace {
+
+// U diag(S) (N x k) and V (M x k), both row-major, on the device for the posterior kernels;
+// U and V are column-major host matrices.
+void upload_factors(pcaone_ctx* c, const double* U, const double* S, const double* V, uint32_t k, double** dUS,
+                    double** dV) {
+  PG_REQUIRE(S && V && k >= 1 && k <= (uint32_t)pg::kLmax, PCAONE_EBADARG, "bad factors");
+  std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
+  for (uint32_t i = 0; i < c->N; ++i)
+    for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+  for (uint64_t j = 0; j < c->M; ++j)
+    for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
+  *dUS = (double*)pg::scratch(c, "gl_US", us.size() * 8);
+  *dV = (double*)pg::scratch(c, "gl_V", v.size() * 8);
+  PG_CUDA(cudaMemcpyAsync(*dUS, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  PG_CUDA(cudaMemcpyAsync(*dV, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+}  // namespace
+
 extern "C" {
 
 int pcaone_gpu_create(int device, pcaone_ctx** out) {
@@ -112,6 +133,7 @@ int pcaone_gpu_destroy(pcaone_ctx* c) {
   if (!c) return PCAONE_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  pg::gl_release(c);
   free_all(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -356,21 +378,20 @@ int pcaone_gpu_gl_update(pcaone_ctx* c, const double* U, const double* S, const 
   return guarded(c, [&] {
     PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");
     double *dUS = nullptr, *dV = nullptr;
-    if (U) {
-      PG_REQUIRE(S && V && k >= 1 && k <= (uint32_t)kLmax, PCAONE_EBADARG, "bad factors");
-      std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
-      for (uint32_t i = 0; i < c->N; ++i)
-        for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
-      for (uint64_t j = 0; j < c->M; ++j)
-        for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
-      dUS = (double*)scratch(c, "gl_US", us.size() * 8);
-      dV = (double*)scratch(c, "gl_V", v.size() * 8);
-      PG_CUDA(cudaMemcpyAsync(dUS, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
-      PG_CUDA(cudaMemcpyAsync(dV, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
-      PG_CUDA(cudaStreamSynchronize(c->stream));
-    }
+    if (U) upload_factors(c, U, S, V, k, &dUS, &dV);
     gl_posterior(c, dUS, dV, U ? (int)k : 0, false, nullptr);
     PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int pcaone_gpu_gl_grm(pcaone_ctx* c, const double* U, const double* S, const double* V, uint32_t k, double* C,
+                      double* evecs, double* svals) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded && c->dense && c->d_P, PCAONE_ESTATE, "no likelihoods loaded");
+    PG_REQUIRE(U, PCAONE_EBADARG, "the GRM needs the factors U, S, V");
+    double *dUS = nullptr, *dV = nullptr;
+    upload_factors(c, U, S, V, k, &dUS, &dV);
+    gl_grm(c, dUS, dV, (int)k, C, evecs, svals);
   });
 }
 

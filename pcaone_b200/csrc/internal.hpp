@@ -127,6 +127,10 @@ struct pcaone_ctx {
   void* tile1_ptr = nullptr;
   void* tile2_ptr = nullptr;
 
+  // cuBLAS / cuSOLVER handles of the PCAngsd GRM (created on first use)
+  void* blas = nullptr;
+  void* solver = nullptr;
+
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;
 

@@ -12,8 +12,14 @@
 // Layout: GL pairs are SNP-major floats, P[j][2i + {0,1}] (the reference's 2N x M column-major
 // P); E is SNP-major floats E[j][i] with rows padded to Npad samples (zeros beyond N).
 // Posterior arithmetic is FP64 in registers.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
 
 #include "internal.hpp"
 #include "rsvd.hpp"
@@ -224,6 +230,66 @@ void dense_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t r
 void dense_none_omega(pcaone_ctx*, const double*, int, int64_t) {}
 void dense_none_b2(pcaone_ctx*, const float*, int, int64_t) {}
 
+// Standardised posterior E of Data::pcangsd_standardize_E (src/Data.cpp:301-343) for the
+// sites [j0, j0 + mc) in FP64, with the per-sample diagonal terms. Thread (i, slice): sample
+// i over the slice's sites of the chunk, in site order; e is written to E[(j - j0) * lde + i]
+// and the slice's diagonal sum is added to dpart[slice * N + i] (each entry has one owner and
+// the chunks run in stream order, so the sums are deterministic). US: N x k (U diag S) and
+// V: M x k row-major as in k_posterior_e; V null: pt = F_j.
+__global__ void __launch_bounds__(128) k_grm_e(const float* __restrict__ P, uint32_t N, uint32_t ldp,
+                                               const double* __restrict__ F, const double* __restrict__ US,
+                                               const double* __restrict__ V, int k, uint64_t j0, uint64_t mc,
+                                               double* __restrict__ E, uint32_t lde, double* __restrict__ dpart) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint64_t per = (mc + gridDim.y - 1) / gridDim.y;
+  const uint64_t a = (uint64_t)blockIdx.y * per, b = (a + per < mc ? a + per : mc);
+  double dc = 0.0;
+  for (uint64_t jl = a; jl < b; ++jl) {
+    const uint64_t j = j0 + jl;
+    const double f = F[j];
+    double pt = f;
+    if (V) {
+      double pred = 0.0;
+      for (int t = 0; t < k; ++t) pred += US[(uint64_t)i * k + t] * V[j * k + t];
+      pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
+    }
+    const float2 pp = *reinterpret_cast<const float2*>(P + j * ldp + 2 * i);
+    double p0, p1, p2;
+    posterior(pp.x, pp.y, pt, p0, p1, p2);
+    const double sum = p0 + p1 + p2;
+    double e = (p1 + 2.0 * p2) / sum - 2.0 * f;
+    const double norm = sqrt(2.0 * f * (1.0 - f));
+    if (norm > 1e-9) e /= norm;
+    const double f2 = 2.0 * f;
+    double t = (0.0 - f2) * (0.0 - f2) * (p0 / sum);
+    t += (1.0 - f2) * (1.0 - f2) * (p1 / sum);
+    t += (2.0 - f2) * (2.0 - f2) * (p2 / sum);
+    dc += t / (2.0 * f * (1.0 - f));
+    E[jl * lde + i] = e;
+  }
+  dpart[(uint64_t)blockIdx.y * N + i] += dc;
+}
+
+// C (N x N, column-major, full) = the lower triangle of L (E E^T from the SYRK) mirrored,
+// divided by M, with the diagonal replaced by Dc / M, Dc_i = sum over slices of dpart in
+// slice order (src/Halko.cpp:322-324).
+__global__ void k_grm_finish(const double* __restrict__ L, const double* __restrict__ dpart, int nsl, uint32_t N,
+                             double M, double* __restrict__ C) {
+  const uint64_t n2 = (uint64_t)N * N;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n2; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = (uint32_t)(t / N), i = (uint32_t)(t - (uint64_t)j * N);
+    double v;
+    if (i == j) {
+      v = 0.0;
+      for (int sl = 0; sl < nsl; ++sl) v += dpart[(uint64_t)sl * N + i];
+    } else {
+      v = i > j ? L[t] : L[(uint64_t)i * N + j];
+    }
+    C[t] = v / M;
+  }
+}
+
 }  // namespace
 
 GemmFnT<float> gemm_dense_float() {
@@ -277,6 +343,91 @@ void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool 
   k_sum_rows<<<(c->N + 255) / 256, 256, 0, c->stream>>>(part, nblk, c->N, Dc);
   PG_CHECK_LAUNCH();
   c->launches += 2;
+}
+
+#define PG_BLAS(call)                                                                          \
+  do {                                                                                         \
+    const int st_ = (int)(call);                                                               \
+    PG_REQUIRE(st_ == 0, PCAONE_ECUDA, std::string(#call) + " failed with status " + std::to_string(st_)); \
+  } while (0)
+
+void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, double* evecs, double* svals) {
+  const uint32_t N = c->N;
+  const uint64_t M = c->M;
+  if (!c->blas) {
+    cublasHandle_t h = nullptr;
+    PG_BLAS(cublasCreate(&h));
+    c->blas = h;
+  }
+  cublasHandle_t blas = (cublasHandle_t)c->blas;
+  PG_BLAS(cublasSetStream(blas, c->stream));
+  // E in chunks of sites: at most 2^27 doubles (1 GiB) a chunk
+  const uint32_t lde = c->Npad;
+  const uint64_t mc_max = std::max<uint64_t>(1, std::min<uint64_t>(M, (1ull << 27) / lde));
+  const int nsl = (int)std::max<uint64_t>(1, std::min<uint64_t>(64, (4ull * c->sm_count * 128 + N - 1) / N));
+  double* E = (double*)scratch(c, "grm_E", (size_t)mc_max * lde * 8);
+  double* dpart = (double*)scratch(c, "grm_dpart", (size_t)nsl * N * 8);
+  double* L = (double*)scratch(c, "grm_L", (size_t)N * N * 8);
+  double* dC = (double*)scratch(c, "grm_C", (size_t)N * N * 8);
+  PG_CUDA(cudaMemsetAsync(dpart, 0, (size_t)nsl * N * 8, c->stream));
+  for (uint64_t j0 = 0; j0 < M; j0 += mc_max) {
+    const uint64_t mc = std::min<uint64_t>(mc_max, M - j0);
+    k_grm_e<<<dim3((N + 127) / 128, nsl), 128, 0, c->stream>>>(c->d_P, N, 2 * N, c->d_F, US, V, k, j0, mc, E, lde,
+                                                              dpart);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+    const double one = 1.0, beta = j0 == 0 ? 0.0 : 1.0;
+    PG_BLAS(cublasDsyrk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)N, (int)mc, &one, E, (int)lde, &beta, L,
+                        (int)N));
+  }
+  const uint64_t n2 = (uint64_t)N * N;
+  k_grm_finish<<<(unsigned)std::min<uint64_t>(8ull * c->sm_count, (n2 + 255) / 256), 256, 0, c->stream>>>(
+      L, dpart, nsl, N, (double)M, dC);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+  if (C) PG_CUDA(cudaMemcpyAsync(C, dC, n2 * 8, cudaMemcpyDeviceToHost, c->stream));
+  if (evecs || svals) {
+    // singular vectors of the symmetric C (JacobiSVD in the reference, src/Halko.cpp:328):
+    // eigenvectors ordered by decreasing |eigenvalue|
+    if (!c->solver) {
+      cusolverDnHandle_t h = nullptr;
+      PG_BLAS(cusolverDnCreate(&h));
+      c->solver = h;
+    }
+    cusolverDnHandle_t sol = (cusolverDnHandle_t)c->solver;
+    PG_BLAS(cusolverDnSetStream(sol, c->stream));
+    double* W = (double*)scratch(c, "grm_W", (size_t)N * 8);
+    int* info = (int*)scratch(c, "grm_info", sizeof(int));
+    int lwork = 0;
+    PG_BLAS(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W,
+                                        &lwork));
+    double* work = (double*)scratch(c, "grm_work", (size_t)std::max(lwork, 1) * 8);
+    PG_BLAS(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W, work,
+                             lwork, info));
+    std::vector<double> w(N), vec(evecs ? n2 : 0);
+    int hinfo = 0;
+    PG_CUDA(cudaMemcpyAsync(w.data(), W, (size_t)N * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (evecs) PG_CUDA(cudaMemcpyAsync(vec.data(), dC, n2 * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    PG_REQUIRE(hinfo == 0, PCAONE_ENUMERIC, "eigendecomposition of the PCAngsd GRM failed (info " +
+                                                std::to_string(hinfo) + ")");
+    std::vector<uint32_t> ord(N);
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return std::fabs(w[x]) > std::fabs(w[y]); });
+    for (uint32_t r = 0; r < N; ++r) {
+      if (svals) svals[r] = std::fabs(w[ord[r]]);
+      if (evecs) std::memcpy(evecs + (size_t)r * N, vec.data() + (size_t)ord[r] * N, (size_t)N * 8);
+    }
+  }
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void gl_release(pcaone_ctx* c) {
+  if (c->blas) cublasDestroy((cublasHandle_t)c->blas);
+  if (c->solver) cusolverDnDestroy((cusolverDnHandle_t)c->solver);
+  c->blas = nullptr;
+  c->solver = nullptr;
 }
 
 }  // namespace pg

@@ -36,6 +36,11 @@ GemmFnT<float> gemm_dense_float();  // dense float E (PCAngsd), kernels_gl.cu
 // PCAngsd device steps (kernels_gl.cu)
 void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters);
 void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool standardize, double* Dc);
+// PCAngsd GRM (pcaone_gpu_gl_grm): C (host N x N, or null), its singular vectors (host N x N
+// column-major, or null) and values (host N, or null); US, V as for gl_posterior.
+void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, double* evecs, double* svals);
+// Frees the context's cuBLAS / cuSOLVER handles.
+void gl_release(pcaone_ctx* c);
 
 void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);
 void jacobi_svd(int n, const double* A, double* U, double* s, double* V);

@@ -264,6 +264,60 @@ void write_matrix(std::ostream& o, const double* a, size_t rows, size_t cols) {
   o << s.str();
 }
 
+// A coefficient as a stream of precision 6 prints it (std::num_put formats with "%.*g").
+inline int fmt_g6(char* b, double v) { return std::snprintf(b, 32, "%.6g", v); }
+
+// Eigen's default `stream << matrix` (IOFormat(): stream precision, aligned columns): every
+// coefficient right-aligned to the widest one of the whole matrix, " " between coefficients,
+// "\n" between rows, nothing after the last row. rows x cols, element (i, j) at a[i + j * ld].
+// The .cov matrix and the rows of the PCAngsd .eigvecs2 are written this way
+// (src/Halko.cpp:325, src/Utils.cpp:435).
+void write_aligned(std::ostream& o, const double* a, size_t rows, size_t cols, size_t ld) {
+  int width = 0;
+#pragma omp parallel for reduction(max : width) schedule(static)
+  for (long j = 0; j < (long)cols; ++j) {
+    char b[32];
+    for (size_t i = 0; i < rows; ++i) width = std::max(width, fmt_g6(b, a[i + (size_t)j * ld]));
+  }
+  std::vector<std::string> lines(rows);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long i = 0; i < (long)rows; ++i) {
+    std::string& s = lines[i];
+    s.reserve(cols * (width + 1));
+    char b[32];
+    for (size_t j = 0; j < cols; ++j) {
+      if (j) s.push_back(' ');
+      const int n = fmt_g6(b, a[i + j * ld]);
+      s.append((size_t)(width - n), ' ');
+      s.append(b, (size_t)n);
+    }
+  }
+  for (size_t i = 0; i < rows; ++i) {
+    o << lines[i];
+    if (i + 1 < rows) o << '\n';
+  }
+}
+
+// Sample names of a Beagle file: every third header token from the fourth on
+// (parse_beagle_samples, src/Utils.cpp:407-424).
+std::vector<std::string> beagle_samples(const std::string& path) {
+  gzFile gz = gzopen(path.c_str(), "rb");
+  if (!gz) fail("can not open " + path);
+  std::string head;
+  std::vector<char> buf(1 << 20);
+  while (gzgets(gz, buf.data(), (int)buf.size())) {
+    head += buf.data();
+    if (!head.empty() && head.back() == '\n') break;
+  }
+  gzclose(gz);
+  std::vector<std::string> names;
+  std::istringstream hs(head);
+  std::string t;
+  for (size_t idx = 0; hs >> t; ++idx)
+    if (idx >= 3 && idx % 3 == 0) names.push_back(t);
+  return names;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- LD r2 output
@@ -466,6 +520,33 @@ int run_pcangsd(const Params& p, std::chrono::steady_clock::time_point t_start) 
     if (diff < p.tolem) {
       g_log.print(date(), "come to convergence!");
       break;
+    }
+  }
+  // GRM stage (src/Halko.cpp:317-331): standardised posterior from the final factors, with the
+  // same index semantics as the EM updates; C = E E^T / M with diag Dc / M, and its singular
+  // vectors written with the sample names
+  g_log.print(date(), "estimate GRM for pcangsd");
+  g_log.print(date(), "begin to standardize the matrix for pcangsd procedure");
+  for (unsigned t = 0; t < p.k; ++t)
+    for (size_t j = 0; j < M; ++j) Vuse[t * M + j] = p.fix_index ? V[t * M + j] : V[t * M + perm[j]];
+  {
+    std::vector<double> C(N * N), Ev(N * N);
+    check(ctx, pcaone_gpu_gl_grm(ctx, U.data(), S.data(), Vuse.data(), p.k, C.data(), Ev.data(), nullptr),
+          "gl_grm");
+    std::ofstream fcov(p.fileout + ".cov");
+    write_aligned(fcov, C.data(), N, N, N);
+    fcov << '\n';
+    std::ofstream feig2(p.fileout + ".eigvecs2");
+    feig2 << "#FID\tIID";
+    for (size_t i = 0; i < N; ++i) feig2 << "\tPC" << i + 1;
+    feig2 << '\n';
+    size_t i = 0;
+    for (const auto& s : beagle_samples(p.beagle)) {
+      if (i >= N) break;
+      feig2 << s << '\t' << s << '\t';
+      write_aligned(feig2, Ev.data() + i, 1, N, N);
+      feig2 << '\n';
+      ++i;
     }
   }
   pcaone_gpu_destroy(ctx);

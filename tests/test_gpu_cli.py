@@ -1,5 +1,6 @@
 """The PCAone drop-in CLI (pcaone_b200/bin/PCAone) against the reference's own output files
 for the same flags (golden fixtures), plus its input-error behaviour."""
+import gzip
 import os
 import shutil
 import subprocess
@@ -8,7 +9,8 @@ import numpy as np
 import pytest
 
 from oracle import pcaone_oracle as O
-from tests.helpers import GOLDEN, assert_cols_close, assert_eig_close, case, ref_out, ref_table
+from tests.helpers import (GOLDEN, assert_cols_close, assert_eig_close, case, eigen_aligned, ref_out,
+                           ref_table, top_vectors_match)
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "pcaone_b200", "bin", "PCAone")
@@ -117,3 +119,25 @@ def test_cli_pcangsd_matches_reference_outputs(tmp_path, name):
     out = str(tmp_path / name)
     assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table(name, ".eigvals")[:, 0], 1e-5)
     assert_cols_close(O.read_table(out + ".eigvecs"), ref_table(name, ".eigvecs"), 5e-4)
+    # GRM stage: .cov in Eigen's aligned text, .eigvecs2 = sample names + singular vectors
+    with open(out + ".cov") as f:
+        text = f.read()
+    C = O.read_eigen_matrix(out + ".cov")
+    assert text == eigen_aligned(C) + "\n"
+    N = C.shape[0]
+    np.testing.assert_array_equal(C, C.T)
+    if name == "g3_pcangsd":  # the reference wrote its .cov for the unshuffled run
+        np.testing.assert_allclose(C, O.read_eigen_matrix(ref_out(name, ".cov")), atol=1e-5)
+    with open(out + ".eigvecs2") as f:
+        lines = f.read().split("\n")
+    assert lines[0] == "#FID\tIID" + "".join(f"\tPC{i + 1}" for i in range(N))
+    with gzip.open(os.path.join(GOLDEN, "g3.beagle.gz"), "rt") as g:
+        names = g.readline().split()[3::3]
+    ev = np.empty((N, N))
+    for i in range(N):
+        a, b, row = lines[1 + i].split("\t")
+        assert a == b == names[i]
+        ev[i] = [float(t) for t in row.split()]
+        assert row == eigen_aligned(ev[i])
+    assert lines[1 + N] == ""
+    top_vectors_match(ev, C, 3, 1e-4)

@@ -111,3 +111,13 @@ def test_oracle_pcangsd_matches_reference(name, shuffle):
         assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)
         Cr = O.read_eigen_matrix(os.path.join(GOLDEN, "ref", name + ".cov"))
         np.testing.assert_allclose(C, Cr, atol=1e-5)
+
+
+def test_eigen_aligned_format_reproduces_reference_cov():
+    """The text rule the CLI writes .cov and .eigvecs2 rows with (Eigen's default aligned
+    stream output) reproduces the reference's own .cov byte for byte."""
+    from tests.helpers import eigen_aligned
+    path = os.path.join(GOLDEN, "ref", "g3_pcangsd.cov")
+    with open(path) as f:
+        text = f.read()
+    assert eigen_aligned(O.read_eigen_matrix(path)) + "\n" == text

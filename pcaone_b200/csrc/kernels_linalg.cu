@@ -1,9 +1,10 @@
-// FP64 kernels for the (k+p)-wide sketch: Gram matrices, Cholesky, triangular solves
-// (CholeskyQR2), recovery of the Householder-QR column signs, flipOmg, and small products.
+// FP64 kernels for the (k+p)-wide sketch outside the fused Omega update: Gram matrices,
+// Cholesky and triangular solves (CholeskyQR2 of the epoch tail), column sums and small
+// products.
 //
 // Tall matrices are row-major n x l (one sample or SNP per row, l <= kLmax columns).
-// All reductions are two-pass (per-CTA partials, then a fixed-order sum) so results are
-// deterministic run to run.
+// All reductions run in a fixed order (per-CTA or per-cluster partials, then a fixed-order
+// sum), so results are deterministic run to run.
 #include "gram.hpp"
 #include "internal.hpp"
 #include "linalg.hpp"
@@ -118,89 +119,6 @@ __global__ void __launch_bounds__(128) k_trsm_right_upper(const double* A, const
   solve_row_upper<LMAX>(A + r * l, sr, l, Q + r * l);
 }
 
-// Householder column signs of an orthonormal Q from the modified LU of its top l x l block
-// (Ballard et al., "Reconstructing Householder vectors from tall-skinny QR", 2015):
-// at step i the pivot's sign s gives D_ii = -sign(s) (sign(0) = +), matching the stable
-// Householder choice R_ii = -sign(x_0)||x|| of Eigen::HouseholderQR and LAPACK dgeqrf.
-__global__ void k_householder_signs(const double* __restrict__ Q, int l, double* __restrict__ D) {
-  extern __shared__ double a[];  // l x l
-  for (int t = threadIdx.x; t < l * l; t += blockDim.x) a[t] = Q[t];
-  __syncthreads();
-  for (int i = 0; i < l; ++i) {
-    double piv = a[i * l + i];
-    double di = piv >= 0.0 ? -1.0 : 1.0;
-    double p = piv - di;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      D[i] = di;
-      a[i * l + i] = p;
-    }
-    // eliminate rows below i
-    for (int r = i + 1 + threadIdx.x; r < l; r += blockDim.x) a[r * l + i] /= p;
-    __syncthreads();
-    for (int t = threadIdx.x; t < (l - i - 1) * (l - i - 1); t += blockDim.x) {
-      int r = i + 1 + t / (l - i - 1), cidx = i + 1 + t % (l - i - 1);
-      a[r * l + cidx] -= a[r * l + i] * a[i * l + cidx];
-    }
-    __syncthreads();
-  }
-}
-
-// flipOmg partials: per column, sum |O2 - Qd| and |O2 + Qd| with Qd = Q * D.
-__global__ void k_flip_partial(const double* __restrict__ O2, const double* __restrict__ Q,
-                               const double* __restrict__ D, int l, int64_t n,
-                               double* __restrict__ part) {
-  __shared__ double sm[2][256];
-  const int col = blockIdx.y;
-  double dm = 0.0, dp = 0.0;
-  const double d = D[col];
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    double o = O2[r * l + col], q = Q[r * l + col] * d;
-    dm += fabs(o - q);
-    dp += fabs(o + q);
-  }
-  sm[0][threadIdx.x] = dm;
-  sm[1][threadIdx.x] = dp;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s; s >>= 1) {
-    if (threadIdx.x < s) {
-      sm[0][threadIdx.x] += sm[0][threadIdx.x + s];
-      sm[1][threadIdx.x] += sm[1][threadIdx.x + s];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    part[((int64_t)col * gridDim.x + blockIdx.x) * 2 + 0] = sm[0][0];
-    part[((int64_t)col * gridDim.x + blockIdx.x) * 2 + 1] = sm[1][0];
-  }
-}
-
-// Final column multipliers: D_c, negated when |O2 - Qd|_1 > 2 |O2 + Qd|_1 (src/RSVD.hpp:85).
-__global__ void k_flip_final(const double* __restrict__ part, int nblk, const double* __restrict__ D,
-                             int l, double* __restrict__ mult) {
-  int col = threadIdx.x;
-  if (col >= l) return;
-  double dm = 0.0, dp = 0.0;
-  for (int b = 0; b < nblk; ++b) {
-    dm += part[((int64_t)col * nblk + b) * 2 + 0];
-    dp += part[((int64_t)col * nblk + b) * 2 + 1];
-  }
-  mult[col] = (dm > 2.0 * dp) ? -D[col] : D[col];
-}
-
-// Omega = Q * diag(mult); Omega2 = Omega; optional FP32 copy (row-major, ld l).
-__global__ void k_apply_cols(const double* __restrict__ Q, const double* __restrict__ mult, int l,
-                             int64_t n, double* __restrict__ O, double* __restrict__ O2,
-                             float* __restrict__ Of) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n * l) return;
-  double v = Q[t] * mult[t % l];
-  O[t] = v;
-  if (O2) O2[t] = v;
-  if (Of) Of[t] = (float)v;
-}
-
 // Column sums of A (n x l) into partials (grid.y = column).
 __global__ void k_colsum_partial(const double* __restrict__ A, int l, int64_t n,
                                  double* __restrict__ part) {
@@ -248,12 +166,6 @@ __global__ void __launch_bounds__(128) k_rowmat(const double* __restrict__ X, in
       if (j < l) s = fma(xr[j], sc[j * kc + c], s);
     Y[r * kc + c] = s;
   }
-}
-
-__global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
-                      double* __restrict__ out) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t < n) out[t] = a[t] + b[t];
 }
 
 }  // namespace
@@ -318,27 +230,6 @@ void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double
   trsm_right_upper(c, Q, R2, l, n, Q);
 }
 
-void householder_signs(pcaone_ctx* c, const double* Q, int l, double* D) {
-  k_householder_signs<<<1, 128, (size_t)l * l * 8, c->stream>>>(Q, l, D);
-  PG_CHECK_LAUNCH();
-  c->launches++;
-}
-
-void flip_and_apply(pcaone_ctx* c, const double* Q, const double* D, int l, int64_t n, double* O,
-                    double* O2, float* Of) {
-  const int nblk = 64;
-  double* part = (double*)scratch(c, "flip_part", (size_t)l * nblk * 2 * 8);
-  double* mult = (double*)scratch(c, "flip_mult", (size_t)l * 8);
-  k_flip_partial<<<dim3(nblk, l), 256, 0, c->stream>>>(O2, Q, D, l, n, part);
-  PG_CHECK_LAUNCH();
-  k_flip_final<<<1, 128, 0, c->stream>>>(part, nblk, D, l, mult);
-  PG_CHECK_LAUNCH();
-  int64_t tot = n * l;
-  k_apply_cols<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(Q, mult, l, n, O, O2, Of);
-  PG_CHECK_LAUNCH();
-  c->launches += 3;
-}
-
 void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out) {
   const int nblk = 64;
   double* part = (double*)scratch(c, "colsum_part", (size_t)l * nblk * 8);
@@ -360,12 +251,6 @@ void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int
     k_rowmat<48><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
   else
     k_rowmat<64><<<grid, 128, smem, c->stream>>>(X, l, C, ldc, kc, n, Y);
-  PG_CHECK_LAUNCH();
-  c->launches++;
-}
-
-void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out) {
-  k_add<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(a, b, n, out);
   PG_CHECK_LAUNCH();
   c->launches++;
 }

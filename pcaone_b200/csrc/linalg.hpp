@@ -15,15 +15,9 @@ void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rp
 void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q);
 // CholeskyQR2: A = Q R with Q orthonormal (Q may alias A).
 void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double* R, int* d_status);
-// D (l) such that Q * diag(D) is the thin Q of a Householder QR of the same matrix.
-void householder_signs(pcaone_ctx* c, const double* Q, int l, double* D);
-// flipOmg against O2 (src/RSVD.hpp:81-90), then O = Q diag(D*flip), O2 = O, Of = float(O).
-void flip_and_apply(pcaone_ctx* c, const double* Q, const double* D, int l, int64_t n, double* O,
-                    double* O2, float* Of);
 void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);
 // Y (n x kc) = X (n x l) * C[:, :kc] with C l x ldc row-major.
 void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y);
-void add(pcaone_ctx* c, const double* a, const double* b, int64_t n, double* out);
 
 // Forward substitution for one row: x R = a with R upper l x l staged by stage_r (row stride
 // LMAX, so every R address is a constant offset; the diagonal slots hold 1 / R_jj, so the

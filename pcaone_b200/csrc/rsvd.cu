@@ -6,7 +6,7 @@
 // Differences of form (not of result) from the reference:
 //  * thin QR is CholeskyQR2 in FP64 instead of Householder; the Householder column signs,
 //    which steer the winSVD trajectory through flipOmg, are recovered exactly from the
-//    CholeskyQR2 factor (kernels_linalg.cu, k_householder_signs);
+//    final Q of each Omega update (kernels_update.cu, modified LU of its top block);
 //  * B = R^-T H^T is never formed: its SVD comes from CholeskyQR2 of B^T = H R^-1 and a
 //    one-sided Jacobi SVD of the l x l triangular factor on the host.
 #include <algorithm>

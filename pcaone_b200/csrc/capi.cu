@@ -379,7 +379,7 @@ int pcaone_gpu_gl_update(pcaone_ctx* c, const double* U, const double* S, const 
     PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");
     double *dUS = nullptr, *dV = nullptr;
     if (U) upload_factors(c, U, S, V, k, &dUS, &dV);
-    gl_posterior(c, dUS, dV, U ? (int)k : 0, false, nullptr);
+    gl_posterior(c, dUS, dV, U ? (int)k : 0);
     PG_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

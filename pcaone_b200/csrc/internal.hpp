@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <map>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -133,6 +134,9 @@ struct pcaone_ctx {
 
   // named scratch buffers (grown on demand, freed with the context)
   std::map<std::string, pg::DevBuf> bufs;
+
+  // kernels whose dynamic shared-memory limit was raised on this context's device
+  std::set<const void*> smem_attr_set;
 
   // resident clusters of the cluster kernels, by kernel and shape (gram.hpp)
   std::map<std::pair<const void*, uint64_t>, int> cluster_occupancy;

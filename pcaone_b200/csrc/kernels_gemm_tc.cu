@@ -513,12 +513,10 @@ TcPlan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K) {
 
 template <int NP>
 void launch_np(pcaone_ctx* c, const TcArgs& a) {
-  static bool attr = false;
   const size_t smem = smem_bytes(NP);
-  if (!attr) {
+  // the attribute belongs to the device's context: set once per library context (one device)
+  if (c->smem_attr_set.insert((const void*)k_decode_gemm_tc<NP>).second)
     PG_CUDA(cudaFuncSetAttribute(k_decode_gemm_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
   k_decode_gemm_tc<NP><<<a.grid, kThreads, smem, c->stream>>>(a);
   PG_CHECK_LAUNCH();
 }

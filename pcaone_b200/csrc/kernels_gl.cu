@@ -56,25 +56,19 @@ __global__ void k_em_maf(const float* __restrict__ P, uint64_t M, uint32_t N, ui
   }
 }
 
-// E (or the standardised E and per-CTA partial Dc) for SNP rows; warp per SNP.
+// E_ij = E[g | likelihoods, pt_ij] - 2 F_j for SNP rows (fit_with_pi, src/Data.cpp:249-270);
+// warp per SNP. The standardised E of the GRM stage is k_grm_e.
 // US: N x k (U diag S) row-major, V: M x k row-major (row j = the loading used for SNP j).
-template <bool STD>
 __global__ void k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
                               const double* __restrict__ F, const double* __restrict__ US,
-                              const double* __restrict__ V, int k, float* __restrict__ E,
-                              uint32_t lde, double* __restrict__ dc_part) {
+                              const double* __restrict__ V, int k, float* __restrict__ E, uint32_t lde) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  extern __shared__ double sdc[];  // [nwarps][N] only when STD
-  if (STD)
-    for (uint32_t i = threadIdx.x; i < (uint32_t)nwarps * N; i += blockDim.x) sdc[i] = 0.0;
-  if (STD) __syncthreads();
   for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
     const double f = F[j];
     double v[kLmax];
     if (V)
       for (int t = 0; t < k; ++t) v[t] = V[j * k + t];
     const float* row = P + j * ldp;
-    const double norm = sqrt(2.0 * f * (1.0 - f));
     for (uint32_t i = lane; i < N; i += 32) {
       double pt = f;
       if (V) {
@@ -85,35 +79,11 @@ __global__ void k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t 
       double p0, p1, p2;
       posterior(row[2 * i], row[2 * i + 1], pt, p0, p1, p2);
       const double s = p0 + p1 + p2;
-      double e = (p1 + 2.0 * p2) / s - 2.0 * f;
-      if (STD) {
-        if (norm > 1e-9) e /= norm;
-        const double f2 = 2.0 * f;
-        double t = (0.0 - f2) * (0.0 - f2) * (p0 / s);
-        t += (1.0 - f2) * (1.0 - f2) * (p1 / s);
-        t += (2.0 - f2) * (2.0 - f2) * (p2 / s);
-        sdc[(uint64_t)warp * N + i] += t / (2.0 * f * (1.0 - f));
-      }
-      E[j * lde + i] = (float)e;
-    }
-  }
-  if (STD) {
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-      double acc = 0.0;
-      for (int w = 0; w < nwarps; ++w) acc += sdc[(uint64_t)w * N + i];
-      dc_part[(uint64_t)blockIdx.x * N + i] = acc;
+      E[j * lde + i] = (float)((p1 + 2.0 * p2) / s - 2.0 * f);
     }
   }
 }
 
-__global__ void k_sum_rows(const double* __restrict__ part, int nblk, uint32_t n, double* __restrict__ out) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[(uint64_t)b * n + i];
-  out[i] = s;
-}
 
 // Dense SIMT GEMM: out[s][r][c] = sum_{k in split s} A(r, k) * B[k][c]. A(r, k) is
 // A[r * lda + k] when !AT (rows = SNPs, K = samples) and A[k * lda + r] when AT (rows =
@@ -317,32 +287,12 @@ void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {
   if (iters) *iters = std::min(it + 1, maxiter);
 }
 
-void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool standardize, double* Dc) {
+void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
   const int threads = 256, nwarps = threads / 32;
-  if (!standardize) {
-    int nblk = (int)std::min<uint64_t>(8 * c->sm_count, (c->M + nwarps - 1) / nwarps);
-    k_posterior_e<false><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E,
-                                                           c->Npad, nullptr);
-    PG_CHECK_LAUNCH();
-    c->launches++;
-    return;
-  }
-  // per-warp Dc rows in shared memory: keep them within 200 KB
-  const size_t smem = (size_t)nwarps * c->N * 8;
-  PG_REQUIRE(smem <= 200 * 1024, PCAONE_EBADARG, "too many samples for the PCAngsd diagonal kernel");
-  static bool attr = false;
-  if (!attr) {
-    PG_CUDA(cudaFuncSetAttribute(k_posterior_e<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
-  int nblk = (int)std::min<uint64_t>(2 * c->sm_count, (c->M + nwarps - 1) / nwarps);
-  double* part = (double*)scratch(c, "gl_dc_part", (size_t)nblk * c->N * 8);
-  k_posterior_e<true><<<nblk, threads, smem, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E,
-                                                         c->Npad, part);
+  int nblk = (int)std::min<uint64_t>(8 * c->sm_count, (c->M + nwarps - 1) / nwarps);
+  k_posterior_e<<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   PG_CHECK_LAUNCH();
-  k_sum_rows<<<(c->N + 255) / 256, 256, 0, c->stream>>>(part, nblk, c->N, Dc);
-  PG_CHECK_LAUNCH();
-  c->launches += 2;
+  c->launches++;
 }
 
 #define PG_BLAS(call)                                                                          \

@@ -35,7 +35,7 @@ GemmFnT<float> gemm_dense_float();  // dense float E (PCAngsd), kernels_gl.cu
 
 // PCAngsd device steps (kernels_gl.cu)
 void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters);
-void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k, bool standardize, double* Dc);
+void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k);
 // PCAngsd GRM (pcaone_gpu_gl_grm): C (host N x N, or null), its singular vectors (host N x N
 // column-major, or null) and values (host N, or null); US, V as for gl_posterior.
 void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, double* evecs, double* svals);

@@ -623,9 +623,41 @@ def run_pcangsd(beagle: str, k: int = 10, svd: int = 2, maxp: int = 20, oversamp
     (eigvals, S, U, V in input order, F, iterations, C (GRM), Dc)."""
     P, N, M = parse_beagle(beagle)
     F = em_maf(P, maxiter, tolmaf)
+    return _pcangsd_loop(P, F, pcangsd_e(P, F, None), k, svd, maxp, oversamples, bands, tol,
+                         maxiter, tolem, seed, rand, shuffle, reference_index)
+
+
+def bed_pseudo_gl(bed: Bed):
+    """FileBed::read_all with --pcangsd (src/FilePlink.cpp:36-115): F from the genotypes,
+    pseudo-likelihood pairs RR -> (1, 0), AA -> (0, 0), RA -> (0, 1), missing ->
+    (0.333333, 0.333333) (P is 2N x M), and the centred matrix E = BED2GENO - F with
+    missing -> 0 (N x M, not standardised)."""
+    codes = decode_codes(bed)
+    F = allele_freq(codes)
+    P = np.empty((2 * bed.N, bed.M))
+    c = codes.T  # N x M
+    P[0::2] = np.where(c == 3, 1.0, np.where(c == 1, 0.333333, 0.0))
+    P[1::2] = np.where(c == 2, 1.0, np.where(c == 1, 0.333333, 0.0))
+    return P, F, centered_matrix(codes, F)
+
+
+def run_pcangsd_bed(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: int = 10,
+                    bands: int = 64, tol: float = 1e-4, maxiter: int = 100, tolem: float = 1e-5,
+                    seed: int = 101, rand: int = 1, shuffle: bool = True,
+                    reference_index: bool = True):
+    """PCAngsd on PLINK input (-b with --pcangsd, src/Cmd.cpp:205-207): the EM loop of
+    run_pca_with_halko (src/Halko.cpp:294-316) on the pseudo-likelihoods of bed_pseudo_gl,
+    starting from the centred genotypes. Same return value as run_pcangsd."""
+    P, F, E0 = bed_pseudo_gl(bed)
+    return _pcangsd_loop(P, F, E0, k, svd, maxp, oversamples, bands, tol, maxiter, tolem, seed,
+                         rand, shuffle, reference_index)
+
+
+def _pcangsd_loop(P, F, E, k, svd, maxp, oversamples, bands, tol, maxiter, tolem, seed, rand,
+                  shuffle, reference_index):
+    N, M = P.shape[0] // 2, P.shape[1]
     os_ = max(oversamples, k)
     perm = shuffle_perm(M) if (svd == 2 and shuffle) else np.arange(M, dtype=np.int32)
-    E = pcangsd_e(P, F, None)
     state = {}
 
     def rsvd(Z):

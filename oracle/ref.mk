@@ -1,14 +1,15 @@
 # Builds the unmodified reference PCAone (v0.6.0) CLI from the read-only source tree
 # into oracle/_ref/ for use as the parity oracle and the timed CPU baseline.
 #
-#   make -f oracle/ref.mk REF=/root/reference -j8
+#   make -f oracle/ref.mk REF=<reference source tree> -j8
+# (REF defaults to $PCAONE_REF, else /root/reference)
 #
 # This is our own short recipe (the reference's own build system is not run).
 # Sources are compiled where they lie; objects and the binary go to oracle/_ref/ only.
 # -march=x86-64-v3 (AVX2+FMA) instead of -march=native so the binary also runs on the
 # host CPU of another machine; OpenMP is enabled as in the reference build.
 
-REF      ?= /root/reference
+REF      ?= $(if $(PCAONE_REF),$(PCAONE_REF),/root/reference)
 OUT      := $(dir $(lastword $(MAKEFILE_LIST)))_ref
 OBJ      := $(OUT)/obj
 CXX      := /usr/bin/g++

@@ -5,14 +5,21 @@ Inputs are small seeded synthetic datasets written by the package's simulator
 v0.6.0 binary built from its own sources by ``oracle/ref.mk`` into ``oracle/_ref/PCAone``.
 Run from the repository root in the container that has the reference sources:
 
-    make -f oracle/ref.mk REF=/root/reference -j8
+    make -f oracle/ref.mk -j8            # REF defaults to $PCAONE_REF, else /root/reference
     python tests/golden/make_golden.py
 
 Each case in ``CASES`` is (name, dataset, reference arguments, output suffixes kept).
 ``cases.json`` records the exact commands so the tests can reproduce them.
+
+``LARGE`` datasets are full benchmark shapes (config 1: 2000 samples x 50000 SNPs). They are
+too large to commit: the tests regenerate them with the same simulator flags and check the
+.bed against the sha256 recorded here; only the reference's outputs are kept (.loadings: the
+first LARGE_LOADING_ROWS SNPs, gzip-compressed).
 """
 from __future__ import annotations
 
+import gzip
+import hashlib
 import json
 import os
 import shutil
@@ -41,6 +48,14 @@ DATASETS = {
            "--seed", "14"],
 }
 
+# full-shape datasets, regenerated by the tests (not committed); same flags as bench.py "c1"
+LARGE = {
+    "c1": ["--n", "2000", "--m", "50000", "--pops", "3", "--fst-lo", "0.05", "--fst-hi", "0.05",
+           "--pmin", "0.05", "--pmax", "0.5", "--miss", "0.01", "--seed", "1"],
+}
+
+LARGE_LOADING_ROWS = 5000
+
 EIG = [".eigvals", ".sigvals", ".eigvecs"]
 CASES = [
     ("g1_halko", "g1", ["-b", "{d}", "-d", "1", "-k", "4", "--oversamples", "10", "-p", "7",
@@ -60,7 +75,7 @@ CASES = [
     ("g3_pcangsd", "g3", ["-G", "{d}.beagle.gz", "-k", "3", "-S", "-w", "8", "--maxiter", "30",
                           "-V"], EIG + [".loadings", ".cov"]),
     ("g3_pcangsd_shuf", "g3", ["-G", "{d}.beagle.gz", "-k", "3", "-w", "8", "--maxiter", "30"],
-     EIG),
+     EIG + [".cov"]),
     ("g4_pcs", "g4", ["-b", "{d}", "-d", "1", "-k", "3", "-p", "7", "--tol-rsvd", "0", "-V"],
      EIG + [".mbim"]),
     ("g4_ldA", "g4", ["-b", "{d}", "--read-U", "{g}/ref/g4_pcs.eigvecs", "-f",
@@ -69,7 +84,23 @@ CASES = [
      [".residuals", ".mbim"] + EIG),
     ("g4_ldB", "g4", ["-B", "{g}/ref/g4_adj.residuals", "-f", "{g}/ref/g4_adj.mbim",
                       "--ld-bp", "5000", "-R"], [".ld.gz"]),
+    # PCAngsd on PLINK input: pseudo-likelihoods from the genotypes (shuffled and -S)
+    ("g1_pcangsd_bed", "g1", ["-b", "{d}", "--pcangsd", "-k", "3", "-w", "8", "--maxiter", "30",
+                              "-V"], EIG + [".loadings"]),
+    ("g1_pcangsd_bedS", "g1", ["-b", "{d}", "--pcangsd", "-k", "3", "-w", "8", "-S",
+                               "--maxiter", "30", "-V"], EIG + [".loadings"]),
+    # config 1 at its full shape: Halko k=10, oversampling 10, 8 epochs
+    ("c1_halko", "c1", ["-b", "{d}", "-d", "1", "-k", "10", "--oversamples", "10", "-p", "7",
+                        "--tol-rsvd", "0", "-V"], EIG + [".loadings"]),
 ]
+
+
+def sha256(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        for blk in iter(lambda: f.read(1 << 20), b""):
+            h.update(blk)
+    return h.hexdigest()
 
 
 def main() -> int:
@@ -83,17 +114,32 @@ def main() -> int:
     os.makedirs(refdir, exist_ok=True)
     for name, args in DATASETS.items():
         subprocess.check_call([SIM, "--out", os.path.join(HERE, name)] + args)
-    record = {"datasets": DATASETS, "cases": []}
+    large_dir = tempfile.mkdtemp()
+    large_sha = {}
+    for name, args in LARGE.items():
+        subprocess.check_call([SIM, "--out", os.path.join(large_dir, name)] + args)
+        large_sha[name] = sha256(os.path.join(large_dir, name + ".bed"))
+    record = {"datasets": DATASETS, "large_datasets": LARGE, "large_bed_sha256": large_sha,
+              "cases": []}
     env = dict(os.environ, OMP_NUM_THREADS="4")
     for name, ds, args, keep in CASES:
         with tempfile.TemporaryDirectory() as tmp:
-            argv = [a.format(d=os.path.join(HERE, ds), g=HERE) for a in args]
+            dpath = os.path.join(large_dir if ds in LARGE else HERE, ds)
+            argv = [a.format(d=dpath, g=HERE) for a in args]
             out = os.path.join(tmp, name)
             subprocess.run([REF] + argv + ["-o", out, "-v", "0"], check=True, env=env,
                            stdout=subprocess.DEVNULL)
             for suf in keep:
-                shutil.copy(out + suf, os.path.join(refdir, name + suf))
+                if ds in LARGE and suf == ".loadings":
+                    with open(out + suf) as fi, gzip.open(os.path.join(refdir, name + suf + ".gz"), "wt") as fo:
+                        for i, line in enumerate(fi):
+                            if i >= LARGE_LOADING_ROWS:
+                                break
+                            fo.write(line)
+                else:
+                    shutil.copy(out + suf, os.path.join(refdir, name + suf))
         record["cases"].append({"name": name, "dataset": ds, "args": args, "outputs": keep})
+    shutil.rmtree(large_dir)
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(record, f, indent=1)
     return 0

@@ -121,3 +121,40 @@ def test_eigen_aligned_format_reproduces_reference_cov():
     with open(path) as f:
         text = f.read()
     assert eigen_aligned(O.read_eigen_matrix(path)) + "\n" == text
+
+
+def test_oracle_matches_reference_at_config1_shape(tmp_path):
+    """Config 1 at its full shape (2000 x 50000, Halko k=10, oversampling 10, -p 7 --tol-rsvd 0):
+    the oracle against the reference binary's outputs, on the input the seeded simulator
+    regenerates (sha256 recorded with the outputs)."""
+    import gzip
+    import hashlib
+    import json
+
+    root = os.path.dirname(O._HERE)
+    sim = os.path.join(root, "pcaone_b200", "bin", "pcaone-sim")
+    if not os.path.exists(sim):
+        pytest.skip("simulator not built")
+    with open(os.path.join(GOLDEN, "cases.json")) as f:
+        rec = json.load(f)
+    prefix = str(tmp_path / "c1")
+    subprocess.check_call([sim, "--out", prefix] + rec["large_datasets"]["c1"], stdout=subprocess.DEVNULL)
+    with open(prefix + ".bed", "rb") as f:
+        assert hashlib.sha256(f.read()).hexdigest() == rec["large_bed_sha256"]["c1"]
+    bed = O.read_bed(prefix)
+    eig, S, U, V, F, ep = O.run_pca(bed, svd=1, k=10, oversamples=10, maxp=7, tol=0.0)
+    assert ep == 8
+    assert_eig_close(eig, ref_eigvals("c1_halko"), 1e-5)
+    assert_cols_close(U, ref_table("c1_halko", ".eigvecs"), 2e-6)
+    with gzip.open(os.path.join(GOLDEN, "ref", "c1_halko.loadings.gz"), "rt") as f:
+        Vref = np.array([[float(t) for t in line.split()] for line in f])
+    assert_cols_close(V[:Vref.shape[0]], Vref, 2e-6)
+
+
+@pytest.mark.parametrize("name,shuffle", [("g1_pcangsd_bed", True), ("g1_pcangsd_bedS", False)])
+def test_oracle_pcangsd_on_plink_matches_reference(name, shuffle):
+    """-b with --pcangsd: pseudo-likelihoods from the genotypes (src/FilePlink.cpp:89-105)."""
+    eig, S, U, V, F, it, C, Dc = O.run_pcangsd_bed(g("g1"), k=3, bands=8, maxiter=30, shuffle=shuffle)
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(U, ref_table(name, ".eigvecs"), 2e-6)
+    assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)

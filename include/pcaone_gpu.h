@@ -44,8 +44,11 @@ typedef enum {
 
 typedef enum {
   PCAONE_PREC_FP32 = 0,  /* FP32 SIMT decode-GEMMs (the plain FP32 GPU path) */
-  PCAONE_PREC_MIXED = 1, /* tcgen05 BF16 decode-GEMMs, split BF16 hi+lo sketch, FP32 accum */
-  PCAONE_PREC_FP64 = 2   /* FP64 SIMT decode-GEMMs (algorithm-matched FP64 run) */
+  PCAONE_PREC_MIXED = 1, /* tcgen05 int8 decode-GEMMs: genotypes as exact unsigned 8-bit
+                            integers, the sketch as three signed 8-bit fixed-point pieces per
+                            column (21 bits below the column maximum), exact int32 accumulation */
+  PCAONE_PREC_FP64 = 2,  /* FP64 SIMT decode-GEMMs (algorithm-matched FP64 run) */
+  PCAONE_PREC_BF16 = 3   /* tcgen05 BF16 decode-GEMMs, split BF16 hi+lo sketch, FP32 accum */
 } pcaone_precision;
 
 /* Create / destroy a context on CUDA device `device`. Replaces nothing in the reference

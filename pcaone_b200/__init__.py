@@ -16,8 +16,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libpcaone_gpu.so")
 BIN_DIR = os.path.join(_HERE, "bin")
 
-PREC_FP32, PREC_MIXED, PREC_FP64 = 0, 1, 2
-PRECISIONS = {"fp32": PREC_FP32, "mixed": PREC_MIXED, "bf16": PREC_MIXED, "fp64": PREC_FP64}
+PREC_FP32, PREC_MIXED, PREC_FP64, PREC_BF16 = 0, 1, 2, 3
+PRECISIONS = {"fp32": PREC_FP32, "mixed": PREC_MIXED, "int8": PREC_MIXED, "bf16": PREC_BF16,
+              "fp64": PREC_FP64}
 
 STATUS = {0: "OK", 1: "EBADARG", 2: "EOOM", 3: "ECUDA", 4: "ETIMEOUT", 5: "ENUMERIC",
           6: "ESTATE", 7: "ENODEV"}

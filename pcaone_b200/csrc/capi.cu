@@ -53,6 +53,7 @@ void free_all(pcaone_ctx* c) {
   c->bt2_shape = -1;
   c->bt2_ptr = nullptr;
   c->tiles_valid = false;
+  c->tiles8_valid = false;
   c->tile1_ptr = c->tile2_ptr = nullptr;
 }
 

@@ -15,10 +15,13 @@ struct EpiP1 {          // after the Z^T Omega product of one window
   const double* scale = nullptr;     // M, per-SNP scale s_j
   const double* wsum = nullptr;      // l: column sums of Omega
   const double* omega = nullptr;     // Npad x l
+  const float* omega_f = nullptr;    // FP32 copy of omega: when set, the sparse gather reads it
   const int64_t* miss_ptr = nullptr; // by-SNP CSR
   const int32_t* miss_idx = nullptr;
   const double* miss_val = nullptr;  // e_ij per entry (EM-imputed), or null for 0
   double* G = nullptr;               // M x l (rows start..start+m written)
+  float* Gf = nullptr;               // when set: FP32 copy of the window's G rows (window-local)
+  unsigned long long* qmax = nullptr;  // when set: atomicMax of |B2| per column (double bits)
   __nv_bfloat16* bt2 = nullptr;      // when set: B2 written as split BF16 (tc_layout.hpp)
   int64_t kpad2 = 0;                 // K extent of bt2 (multiple of 64)
   int bt_half = 0;                   // row offset of the lo half in bt2 (= NP / 2)
@@ -31,6 +34,8 @@ struct EpiP2 {          // after the Z * G product of one window
   const double* F = nullptr;
   const double* scale = nullptr;
   const double* G = nullptr;         // M x l
+  const float* Gf = nullptr;         // when set: window-local FP32 copy of G read by the gather
+  int64_t g_start = 0;               // first SNP of the window (row 0 of Gf)
   const double* h0 = nullptr;        // l
   const int64_t* miss_ptr = nullptr; // by (window, sample) CSR
   const int32_t* miss_idx = nullptr;

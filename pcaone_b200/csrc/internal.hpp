@@ -127,6 +127,12 @@ struct pcaone_ctx {
   uint64_t tiles_key = 0;
   void* tile1_ptr = nullptr;
   void* tile2_ptr = nullptr;
+  // the same for the tiled copies of the int8 tensor-core back end (kernels_gemm_i8.cu)
+  bool tiles8_valid = false;
+  uint64_t tiles8_key = 0;
+  void* tile81_ptr = nullptr;
+  void* tile82_ptr = nullptr;
+  bool i8_b2_max_ready = false;  // the first epilogue filled the window operand's column maxima
 
   // cuBLAS / cuSOLVER handles of the PCAngsd GRM (created on first use)
   void* blas = nullptr;

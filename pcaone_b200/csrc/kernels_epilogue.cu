@@ -27,9 +27,9 @@ namespace {
 // 64-byte segment of a row per group and each entry costs a few warp instructions. The
 // groups' sums are combined with two shuffle levels in a fixed order (deterministic) and
 // written to out (shared memory of this warp). CPL = ceil(l / 8).
-template <int CPL, typename Wt>
+template <int CPL, typename R, typename Wt>
 __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
-                                            const double* __restrict__ rows, int l, Wt weight,
+                                            const R* __restrict__ rows, int64_t row0, int l, Wt weight,
                                             double* out) {
   constexpr int kSteps = 2;
   const int lane = threadIdx.x & 31, grp = lane >> 3, q = lane & 7;
@@ -57,10 +57,10 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
       }
 #pragma unroll
       for (int h = 0; h < kSteps; ++h) {
-        const double* r = rows + (int64_t)it[h] * l + q;
+        const R* r = rows + ((int64_t)it[h] - row0) * l + q;
         const bool ok = t + 4 * h + grp < cnt;
 #pragma unroll
-        for (int k = 0; k < CPL; ++k) v[h][k] = (ok && q + 8 * k < l) ? r[8 * k] : 0.0;
+        for (int k = 0; k < CPL; ++k) v[h][k] = (ok && q + 8 * k < l) ? (double)r[8 * k] : 0.0;
       }
 #pragma unroll
       for (int h = 0; h < kSteps; ++h)
@@ -82,29 +82,41 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
 }
 
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
-// per-CTA partials of h0.
+// per-CTA partials of h0; with p.Gf also the FP32 copy of G the second gather reads, with
+// p.qmax the column maxima of |B2| the int8 quantiser needs. The sparse gather reads the
+// FP32 copy of Omega when p.omega_f is set (half the L2 bytes of the FP64 rows).
 template <typename T, int CPL>
 __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
   extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = sh0 + nwarps * p.l + warp * p.l;
+  unsigned long long* smax = (unsigned long long*)(sh0 + 2 * nwarps * p.l);  // l column maxima
   for (int c = lane; c < p.l; c += 32) sh0[warp * p.l + c] = 0.0;
+  if (p.qmax) {
+    for (int c = threadIdx.x; c < p.l; c += blockDim.x) smax[c] = 0ull;
+    __syncthreads();
+  }
   for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < p.m; jl += (int64_t)gridDim.x * nwarps) {
     const int64_t j = p.start + jl;
     const double F = p.F[j];
     const double s = p.scale[j];
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
     const double* mv = p.miss_val;
-    gather_rows<CPL>(e0, e1, p.miss_idx, p.omega, p.l, [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; },
-                     ssp);
+    auto w = [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; };
+    if (p.omega_f)
+      gather_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, w, ssp);
+    else
+      gather_rows<CPL>(e0, e1, p.miss_idx, p.omega, 0, p.l, w, ssp);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * p.m + jl) * p.l + c];
       const double sparse = ssp[c];
       double g = s * (0.5 * d - F * p.wsum[c] + sparse);
       p.G[j * p.l + c] = g;
+      if (p.Gf) p.Gf[jl * p.l + c] = (float)g;
       const T b2 = (T)(0.5 * s * g);
+      if (p.qmax) atomicMax(&smax[c], (unsigned long long)__double_as_longlong(fabs((double)b2)));
       if (p.bt2) {
         const float x = (float)b2;
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
@@ -132,6 +144,7 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
     double acc = 0.0;
     for (int w = 0; w < nwarps; ++w) acc += sh0[w * p.l + c];
     h0_part[(int64_t)blockIdx.x * p.l + c] = acc;
+    if (p.qmax && smax[c]) atomicMax(&p.qmax[c], smax[c]);
   }
 }
 
@@ -199,8 +212,11 @@ __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
     const int64_t e0 = p.miss_ptr[row], e1 = p.miss_ptr[row + 1];
     const double* mv = p.miss_val;
     const double *sc = p.scale, *F = p.F;
-    gather_rows<CPL>(e0, e1, p.miss_idx, p.G, p.l,
-                     [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); }, ssp);
+    auto w = [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); };
+    if (p.Gf)
+      gather_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, w, ssp);
+    else
+      gather_rows<CPL>(e0, e1, p.miss_idx, p.G, 0, p.l, w, ssp);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
       for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D2[((int64_t)sp * p.n + i) * p.l + c];
@@ -218,7 +234,7 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
   const int threads = 256, nwarps = threads / 32;
   int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
   double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
-  const size_t smem = (size_t)2 * nwarps * p.l * 8;
+  const size_t smem = (size_t)2 * nwarps * p.l * 8 + (size_t)p.l * 8;
   switch ((p.l + 7) / 8) {
     case 1: k_prep<T, 1><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
     case 2: k_prep<T, 2><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;

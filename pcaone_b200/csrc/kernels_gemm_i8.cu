@@ -1,0 +1,636 @@
+// tcgen05 (sm_100a) int8 decode-GEMM: the mixed-precision back end of the two sketch
+// products G = Z^T Omega and H = Z G.
+//
+//   out[s][r][c] = sum_{k in split s} val(code[r][k]) * B[k][c]
+//
+// val(00, 01, 10, 11) = (2, 0, 1, 0) is exact as an unsigned 8-bit integer. The FP64 sketch
+// operand B (Omega, or s/2 * G of the current window) enters as three signed 8-bit fixed-point
+// pieces per column,
+//
+//   B[k][c] ~= sig0_c * q0[k][c] + sig1_c * q1[k][c] + sig2_c * q2[k][c],
+//   sig0_c = max_k |B[k][c]| / 127,  sig1_c = sig0_c / 254,  sig2_c = sig1_c / 254,
+//
+// each piece the rounded residual of the previous ones (|q| <= 127). The absolute error of an
+// entry is at most sig2_c / 2 = max_k |B[k][c]| / (2 * 127 * 254^2): 21 bits below the column
+// maximum, finer than a split BF16 hi+lo pair for the entries that carry the product. The
+// tensor core accumulates each piece exactly in int32 (|acc| <= 254 K); the readout combines
+// the pieces in FP64 and stores FP32 partial sums. The epilogue kernels (kernels_epilogue.cu)
+// add the rank-1 centring term and the sparse missing-entry term in FP64.
+//
+// Work split: rows are cut into 128-row tiles and tiles into pairs; a unit is one tile pair x
+// UC consecutive 128-code K chunks. Both tiles of a pair multiply the same B chunk, so each B
+// chunk crosses L2 once for 256 rows. Units are in pair-major order and CTA j of G (one CTA per
+// SM, the whole tensor memory) owns units [j U / G, (j+1) U / G) (stream-K). Segment q of a
+// pair writes its partial sums to output slot q and the CTA holding a pair's last unit
+// zero-fills the slots the pair does not use, so every row has exactly `ks` slots that the
+// epilogue sums in a fixed order (deterministic, no atomics).
+//
+// Roles (15 warps):
+//   * warps 0-7 (decoders): warp w owns the 32 rows 32 (w % 4) .. of tile w / 4 = its TMEM
+//     lanes; a thread decodes its row's 128 codes of a chunk with four PRMT byte lookups per
+//     16 codes and writes the 128 int8 values with one tcgen05.st into an A slot of its tile;
+//   * warp 8 (producer): lane 0 copies a unit's tiled codes (UC x 8 KB, contiguous) and lane
+//     1 its B chunks (UC x NP x 128 bytes, already in the 128-byte-swizzled shared-memory
+//     image) with 1-D bulk copies into a ring of S shared-memory stages;
+//   * warps 9 and 10 (MMA): lane 0 of warp 9 + t issues the 128 x NP x 32 kind::i8 MMAs of
+//     tile t (A from TMEM, B from shared memory) into the tile's TMEM accumulator and one
+//     tcgen05.commit per unit, which frees the stage once both tiles' MMAs have read it;
+//   * warps 11-14 (readout): at the end of a segment, move both accumulators to registers
+//     with tcgen05.ld, combine the three pieces, store the FP32 partial sums.
+// Tensor memory (512 columns): accumulator of tile t in [t NP, (t+1) NP); A slots (one
+// 128-code chunk of one tile = 32 columns) from 2 NP on, RA per tile.
+//
+// Every mbarrier wait is bounded (about one second of %globaltimer); on timeout the CTA sets
+// an error flag, stops issuing work, waits (bounded) for its copies and MMAs in flight, frees
+// its tensor memory and returns, and the host reports PCAONE_ETIMEOUT.
+#include <algorithm>
+
+#include "internal.hpp"
+#include "rsvd.hpp"
+#include "tc_ptx.hpp"
+
+namespace pg {
+
+namespace {
+
+using tc::bulk_load;
+using tc::mbar_arrive;
+using tc::mbar_arrive_tx;
+using tc::mbar_drain;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::smem_desc_sw128;
+using tc::smem_u32;
+
+constexpr int kRows = 128;                       // rows per tile
+constexpr int kChunk = 128;                      // codes per K chunk (32 packed bytes per row)
+constexpr int kPairChunkBytes = 2 * kRows * 32;  // one chunk of a tile pair: 8192 bytes
+constexpr int kHalfBytes = kRows * 16;           // 64 codes of one tile: 2048 bytes
+constexpr int kThreads = 480;                    // 8 decoders + producer + 2 MMA + 4 readout warps
+constexpr int kTmemCols = 512;
+constexpr int kMinUnitsPerCta = 2;
+
+// Column layout of the quantised operand: piece p of column c is row p * LP + c of B (and
+// column p * LP + c of the accumulator), LP = l rounded up to 8.
+__host__ __device__ constexpr int lp_of(int l) { return (l + 7) / 8 * 8; }
+__host__ __device__ constexpr int np_of(int l) { return (3 * lp_of(l) + 15) / 16 * 16; }
+
+template <int NP>
+struct Cfg {
+  static constexpr int UC = NP <= 128 ? 2 : 1;  // K chunks per unit
+  static constexpr int RA = NP <= 128 ? 4 : 2;  // A slots per tile (one chunk each)
+  static constexpr int NU = RA / UC;            // units in flight in tensor memory per tile
+  static constexpr int SB = NP * 128;           // B bytes per chunk
+  static constexpr int STAGE = UC * (kPairChunkBytes + SB);
+  static constexpr int S = (192 * 1024) / STAGE < 8 ? (192 * 1024) / STAGE : 8;
+  static constexpr int ACOL = 2 * NP;
+  static_assert(2 * NP + 2 * RA * 32 <= kTmemCols, "tensor memory over-subscribed");
+  static_assert(S >= 2, "shared-memory ring too shallow");
+};
+
+// Decode one 32-bit word (16 codes c0..c15, 2 bits each, LSB first) into 16 unsigned bytes:
+// o[0] = (c0, c2, c4, c6), o[1] = (c8, .., c14), o[2] = (c1, .., c7), o[3] = (c9, .., c15),
+// i.e. code c lands at byte position 8 (c & 1) + (c >> 1). Byte value: 00 -> 2, 01 -> 0
+// (missing), 10 -> 1, 11 -> 0; each PRMT selector nibble holds one code.
+__device__ __forceinline__ void decode_word_i8(uint32_t w, uint32_t* o) {
+  constexpr uint32_t kLut = 0x00010002u;
+  const uint32_t x = w & 0x33333333u, y = (w >> 2) & 0x33333333u;
+  o[0] = __byte_perm(kLut, 0u, x);
+  o[1] = __byte_perm(kLut, 0u, x >> 16);
+  o[2] = __byte_perm(kLut, 0u, y);
+  o[3] = __byte_perm(kLut, 0u, y >> 16);
+}
+
+struct I8Args {
+  const uint8_t* a_tiles;  // tiled codes: block (pair, chunk) of 8192 bytes, chunk-fastest
+  const int8_t* bq;        // quantised B, per chunk NP rows x 128 bytes (swizzled)
+  const float* sig;        // 3 x LP piece scales
+  int64_t a_stride;        // chunks per pair in a_tiles (>= chunks)
+  int64_t rows;            // valid rows (outputs written for r < rows)
+  int64_t chunks;          // K chunks (C)
+  int64_t upp;             // units per pair (P = ceil(C / UC))
+  int64_t units;           // pairs x P
+  int grid, ks, l, lp;
+  float* out;  // [ks][rows][l]
+  int* err;
+};
+
+__device__ __forceinline__ int64_t unit_begin(int64_t j, const I8Args& a) { return j * a.units / a.grid; }
+__device__ __forceinline__ int64_t cta_of_unit(int64_t x, const I8Args& a) {
+  return ((x + 1) * a.grid + a.units - 1) / a.units - 1;
+}
+
+template <int NP>
+__global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_constant__ I8Args args) {
+  using C = Cfg<NP>;
+  constexpr int S = C::S, UC = C::UC, RA = C::RA, NU = C::NU;
+  constexpr uint32_t kStageA = UC * kPairChunkBytes, kStageB = UC * C::SB;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* sB = smem;                      // S x kStageB (1024-byte aligned swizzle atoms)
+  uint8_t* sA = smem + S * kStageB;        // S x kStageA
+  uint64_t* bars = (uint64_t*)(sA + S * kStageA);
+  uint64_t* full = bars;                   // [S]  bulk copies landed
+  uint64_t* empty = bars + S;              // [S]  both tiles' MMAs done with the stage
+  uint64_t* dec_full = bars + 2 * S;       // [2][NU] a unit of tile t decoded into TMEM
+  uint64_t* acc_full = dec_full + 2 * NU;  // [2]  accumulator of tile t complete
+  uint64_t* acc_empty = acc_full + 2;      // [2]  accumulator of tile t read out
+  uint64_t* done = acc_full + 4;           // [2]  every MMA of issuer t complete
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(acc_full + 6);
+  volatile int* abort_flag = (volatile int*)(acc_full + 7);
+  float* sig_s = (float*)(acc_full + 8);  // [3 * lp]
+  float* stg_all = sig_s + 3 * 64;        // [4 readout warps][32 rows][9]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t u0 = unit_begin(blockIdx.x, args), u1 = unit_begin(blockIdx.x + 1, args);
+  const int n = (int)(u1 - u0);
+  const int64_t P = args.upp, Cn = args.chunks;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 2);
+    }
+    for (int b = 0; b < 2 * NU; ++b) mbar_init(smem_u32(&dec_full[b]), 4);
+    for (int t = 0; t < 2; ++t) {
+      mbar_init(smem_u32(&acc_full[t]), 1);
+      mbar_init(smem_u32(&acc_empty[t]), 4);
+      mbar_init(smem_u32(&done[t]), 1);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = threadIdx.x; i < 3 * args.lp; i += blockDim.x) sig_s[i] = args.sig[i];
+  if (warp == 9) tc::tmem_alloc(smem_u32((const void*)tmem_slot), kTmemCols);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < 8) {
+    // ---------------- decoders: tile t, row r = 32 q + lane, TMEM lanes 32 q ..
+    const int t = warp >> 2, q = warp & 3, r = q * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    int64_t p = u0 % P;
+    for (int i = 0; i < n; ++i) {
+      const int s = i % S, ua = i % NU;
+      const int nch = (int)(Cn - p * UC < UC ? Cn - p * UC : UC);
+      if (!mbar_wait(smem_u32(&full[s]), (i / S) & 1, abort_flag, args.err, 8)) break;
+      if (i >= NU) {  // the MMAs of unit i - NU have released this tile's A slots
+        const int j = i - NU;
+        if (!mbar_wait(smem_u32(&empty[j % S]), (j / S) & 1, abort_flag, args.err, 8)) break;
+      }
+      tc::fence_after();
+      for (int ch = 0; ch < nch; ++ch) {
+        const uint8_t* base = sA + s * kStageA + ch * kPairChunkBytes + t * (2 * kHalfBytes) + r * 16;
+        const uint4 h0 = *reinterpret_cast<const uint4*>(base);
+        const uint4 h1 = *reinterpret_cast<const uint4*>(base + kHalfBytes);
+        uint32_t v[32];
+        decode_word_i8(h0.x, v + 0);
+        decode_word_i8(h0.y, v + 4);
+        decode_word_i8(h0.z, v + 8);
+        decode_word_i8(h0.w, v + 12);
+        decode_word_i8(h1.x, v + 16);
+        decode_word_i8(h1.y, v + 20);
+        decode_word_i8(h1.z, v + 24);
+        decode_word_i8(h1.w, v + 28);
+        tc::tmem_st32(tmem + lane_base + C::ACOL + t * (RA * 32) + (ua * UC + ch) * 32, v);
+      }
+      tc::tmem_wait_st();
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&dec_full[t * NU + ua]));
+      if (++p == P) p = 0;
+    }
+  } else if (warp == 8) {
+    // ---------------- producer: lane 0 the codes, lane 1 the B chunks of each unit
+    if (lane < 2) {  // the two lanes move in lockstep, so every issued unit has its arrive
+      int issued = 0;
+      int64_t pair = u0 / P, p = u0 - pair * P;
+      for (int i = 0; i < n; ++i) {
+        const int s = i % S;
+        int ok = 1;
+        if (lane == 0) ok = mbar_wait(smem_u32(&empty[s]), ((i / S) & 1) ^ 1, abort_flag, args.err, 1);
+        ok = __shfl_sync(0x3u, ok, 0);
+        if (!ok) break;
+        const int64_t kc = p * UC;
+        const uint32_t nch = (uint32_t)(Cn - kc < UC ? Cn - kc : UC);
+        const uint32_t bar = smem_u32(&full[s]);
+        if (lane == 0) {
+          mbar_arrive_tx(bar, nch * (kPairChunkBytes + C::SB));
+          bulk_load(smem_u32(sA + s * kStageA), args.a_tiles + (pair * args.a_stride + kc) * kPairChunkBytes,
+                    nch * kPairChunkBytes, bar);
+        } else {
+          bulk_load(smem_u32(sB + s * kStageB), args.bq + kc * C::SB, nch * C::SB, bar);
+        }
+        issued = i + 1;
+        if (++p == P) {
+          p = 0;
+          ++pair;
+        }
+      }
+      if (*abort_flag && lane == 0) {  // drain copies in flight before the CTA exits
+        for (int i = max(0, issued - S); i < issued; ++i) mbar_drain(smem_u32(&full[i % S]), (i / S) & 1);
+      }
+    }
+  } else if (warp == 9 || warp == 10) {
+    // ---------------- MMA issuer of tile t
+    const int t = warp - 9;
+    if (lane == 0) {
+      constexpr uint32_t idesc = (2u << 4)                 // D: S32
+                                 | (0u << 7) | (1u << 10)  // A: unsigned 8-bit, B: signed 8-bit
+                                 | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
+      int seg = 0;
+      int64_t p = u0 % P;
+      const uint32_t d_col = tmem + t * NP;
+      for (int i = 0; i < n; ++i) {
+        const int s = i % S, ua = i % NU;
+        const bool first = (i == 0 || p == 0), last = (i == n - 1 || p == P - 1);
+        const int nch = (int)(Cn - p * UC < UC ? Cn - p * UC : UC);
+        if (first) {
+          if (!mbar_wait(smem_u32(&acc_empty[t]), (seg & 1) ^ 1, abort_flag, args.err, 2)) break;
+        }
+        if (!mbar_wait(smem_u32(&full[s]), (i / S) & 1, abort_flag, args.err, 2)) break;
+        if (!mbar_wait(smem_u32(&dec_full[t * NU + ua]), (i / NU) & 1, abort_flag, args.err, 4)) break;
+        tc::fence_after();
+        const uint32_t b_addr = smem_u32(sB + s * kStageB);
+        const uint32_t a_col = tmem + C::ACOL + t * (RA * 32) + ua * UC * 32;
+        for (int ch = 0; ch < nch; ++ch) {
+#pragma unroll
+          for (int kk = 0; kk < kChunk / 32; ++kk)
+            tc::mma_i8(d_col, a_col + ch * 32 + kk * 8, smem_desc_sw128(b_addr + ch * C::SB + kk * 32), idesc,
+                       (first && ch == 0 && kk == 0) ? 0u : 1u);
+        }
+        tc::commit(smem_u32(&empty[s]));
+        if (last) {
+          tc::commit(smem_u32(&acc_full[t]));
+          ++seg;
+        }
+        if (++p == P) p = 0;
+      }
+      tc::commit(smem_u32(&done[t]));  // tracks every MMA issued above
+      mbar_drain(smem_u32(&done[t]), 0);
+    }
+  } else {
+    // ---------------- readout warps 11-14: TMEM lanes 32 (warp % 4) .. + 31 of both tiles
+    const int q4 = warp & 3;
+    const uint32_t lane_base = (uint32_t)(q4 * 32) << 16;
+    const int l = args.l, lp = args.lp;
+    float* stg = stg_all + q4 * 32 * 9;
+    int64_t u = u0;
+    bool ok = true;
+    for (int seg = 0; u < u1 && ok; ++seg) {
+      const int64_t pair = u / P;
+      const int64_t seg_end = min(u1, (pair + 1) * P);
+      const bool pair_end = seg_end == (pair + 1) * P;
+      const int slot = (int)(blockIdx.x - cta_of_unit(pair * P, args));
+      for (int t = 0; t < 2; ++t) {
+        if (!mbar_wait(smem_u32(&acc_full[t]), seg & 1, abort_flag, args.err, 16)) {
+          ok = false;
+          break;
+        }
+        tc::fence_after();
+        const int64_t row0 = (pair * 2 + t) * kRows + q4 * 32;
+        const int nvalid = (int)(args.rows - row0 < 32 ? (args.rows - row0 > 0 ? args.rows - row0 : 0) : 32);
+        float* o = args.out + ((int64_t)slot * args.rows + row0) * l;
+        const uint32_t acc = tmem + lane_base + t * NP;
+        for (int c0 = 0; c0 < lp; c0 += 8) {
+          uint32_t v0[8], v1[8], v2[8];
+          tc::tmem_ld8(acc + c0, v0);
+          tc::tmem_ld8(acc + lp + c0, v1);
+          tc::tmem_ld8(acc + 2 * lp + c0, v2);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int c = c0 + j;
+            const double x = (double)(int)v0[j] * (double)sig_s[c] + (double)(int)v1[j] * (double)sig_s[lp + c] +
+                             (double)(int)v2[j] * (double)sig_s[2 * lp + c];
+            stg[lane * 9 + j] = (float)x;
+          }
+          __syncwarp();
+          // each store instruction writes 4 rows x 8 columns
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int rr = 4 * k + (lane >> 3), e = lane & 7;
+            if (rr < nvalid && c0 + e < l) o[(int64_t)rr * l + c0 + e] = stg[rr * 9 + e];
+          }
+          __syncwarp();
+        }
+        tc::fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&acc_empty[t]));
+        if (pair_end) {  // zero the slots this pair does not use: nvalid contiguous rows each
+          for (int sl = slot + 1; sl < args.ks; ++sl) {
+            float* z = args.out + ((int64_t)sl * args.rows + row0) * l;
+            for (int e = lane; e < nvalid * l; e += 32) z[e] = 0.0f;
+          }
+        }
+      }
+      u = seg_end;
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    tc::fence_after();
+    tc::tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+// Tiled copy of one window's codes for this kernel: block (pair, chunk) = [tile 2p: codes
+// 0-63 of the chunk (128 rows x 16 bytes), codes 64-127][tile 2p+1: same]. src holds `rows`
+// valid rows of `pitch` bytes; rows past `rows` and bytes past the pitch are code 11 (value
+// 0). One thread per (row, 16-byte half chunk).
+__global__ void k_tile_codes_i8(const uint8_t* __restrict__ src, uint32_t pitch, int64_t rows, int64_t pairs,
+                                int64_t chunks, uint8_t* __restrict__ dst) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t halves = 2 * chunks;
+  if (t >= pairs * 2 * kRows * halves) return;
+  const int64_t hc = t % halves, row = t / halves;
+  uint4 v = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+  if (row < rows && (hc + 1) * 16 <= (int64_t)pitch)
+    v = *reinterpret_cast<const uint4*>(src + row * (int64_t)pitch + hc * 16);
+  const int64_t pair = row / (2 * kRows), rin2 = row - pair * 2 * kRows;
+  const int64_t tile = rin2 / kRows, rin = rin2 - tile * kRows;
+  const int64_t kc = hc >> 1, h = hc & 1;
+  *reinterpret_cast<uint4*>(dst + (pair * chunks + kc) * kPairChunkBytes + tile * 2 * kHalfBytes + h * kHalfBytes +
+                            rin * 16) = v;
+}
+
+// Largest |X[k][c]| over the K rows of a row-major K x l matrix, as the bits of a double
+// (monotone in |x|, so atomicMax is order-independent and the result deterministic).
+template <typename T>
+__global__ void k_colmax(const T* __restrict__ X, int64_t K, int l, unsigned long long* __restrict__ qmax) {
+  __shared__ unsigned long long sm[64];
+  for (int c = threadIdx.x; c < l; c += blockDim.x) sm[c] = 0ull;
+  __syncthreads();
+  const int64_t tot = K * l;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const double x = fabs((double)X[e]);
+    atomicMax(&sm[e % l], (unsigned long long)__double_as_longlong(x));
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < l; c += blockDim.x)
+    if (sm[c]) atomicMax(&qmax[c], sm[c]);
+}
+
+// Piece scales of column c from its maximum: sig0 = max / 127, sig1 = sig0 / 254,
+// sig2 = sig1 / 254, in FP32 (the same values in the quantiser and in the GEMM readout).
+__device__ __forceinline__ void piece_scales(unsigned long long bits, float* s) {
+  const double mx = __longlong_as_double((long long)bits);
+  s[0] = mx > 0.0 ? (float)(mx / 127.0) : 1.0f;
+  s[1] = s[0] / 254.0f;
+  s[2] = s[1] / 254.0f;
+}
+
+__device__ __forceinline__ int8_t quant_piece(double x, const float* s, int p) {
+  double r = x, q = 0.0;
+  for (int i = 0; i <= p; ++i) {
+    q = fmin(127.0, fmax(-127.0, rint(r / (double)s[i])));
+    r -= q * (double)s[i];
+  }
+  return (int8_t)(int)q;
+}
+
+// Quantised B of one chunk per CTA: every byte of the chunk's NP x 128 image is written
+// (piece rows, zero rows past 3 LP and past l, zero K positions past K). Thread task (n, u)
+// = the 16-byte unit u (K positions 16u..16u+15 in decode order) of row n; position pp of
+// the unit holds code 16u + 2 (pp & 7) + (pp >> 3) (inverse of decode_word_i8). CTA 0
+// also writes the 3 x LP scales.
+template <typename T>
+__global__ void k_quant(const T* __restrict__ X, int64_t K, int l, int lp, int np,
+                        const unsigned long long* __restrict__ qmax, int8_t* __restrict__ bq, float* __restrict__ sig) {
+  const int64_t kc = blockIdx.x;
+  if (kc == 0)
+    for (int n = threadIdx.x; n < 3 * lp; n += blockDim.x) {
+      const int p = n / lp, c = n - p * lp;
+      float s[3] = {1.0f, 1.0f, 1.0f};
+      if (c < l) piece_scales(qmax[c], s);
+      sig[n] = s[p];
+    }
+  for (int task = threadIdx.x; task < np * 8; task += blockDim.x) {
+    const int nrow = task >> 3, u = task & 7;
+    const int p = nrow / lp, c = nrow - p * lp;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (p < 3 && c < l) {
+      float s[3];
+      piece_scales(qmax[c], s);
+#pragma unroll
+      for (int pp = 0; pp < 16; ++pp) {
+        const int64_t k = kc * kChunk + 16 * u + 2 * (pp & 7) + (pp >> 3);
+        const double x = k < K ? (double)X[k * l + c] : 0.0;
+        const uint32_t b = (uint32_t)(uint8_t)quant_piece(x, s, p);
+        w[pp >> 2] |= b << (8 * (pp & 3));
+      }
+    }
+    *reinterpret_cast<uint4*>(bq + kc * (int64_t)np * 128 + (int64_t)nrow * 128 + ((u ^ (nrow & 7)) << 4)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+template <int NP>
+constexpr size_t smem_of() {
+  using C = Cfg<NP>;
+  return (size_t)1024 + (size_t)C::S * C::STAGE + (size_t)(2 * C::S + 2 * C::NU + 8) * 8 + (3 * 64 + 4 * 32 * 9) * 4;
+}
+
+int uc_of(int np) { return np <= 128 ? 2 : 1; }
+
+struct I8Plan {
+  int64_t tiles = 0, pairs = 0, chunks = 0, upp = 0, units = 0;
+  int grid = 0, ks = 1;
+};
+
+int64_t plan_cta_of_unit(int64_t x, int64_t units, int grid) { return ((x + 1) * grid + units - 1) / units - 1; }
+
+I8Plan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K, int np) {
+  I8Plan p;
+  p.tiles = (rows + kRows - 1) / kRows;
+  p.pairs = (p.tiles + 1) / 2;
+  p.chunks = (K + kChunk - 1) / kChunk;
+  p.upp = (p.chunks + uc_of(np) - 1) / uc_of(np);
+  p.units = p.pairs * p.upp;
+  if (p.units == 0) return p;
+  p.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->sm_count, p.units / kMinUnitsPerCta));
+  int ks = 1;
+  for (int64_t t = 0; t < p.pairs; ++t) {
+    const int64_t a = plan_cta_of_unit(t * p.upp, p.units, p.grid);
+    const int64_t b = plan_cta_of_unit(t * p.upp + p.upp - 1, p.units, p.grid);
+    ks = std::max<int>(ks, (int)(b - a + 1));
+  }
+  p.ks = ks;
+  return p;
+}
+
+template <int NP>
+void launch_np(pcaone_ctx* c, const I8Args& a) {
+  constexpr size_t smem = smem_of<NP>();
+  static_assert(smem <= 227 * 1024, "shared memory above the per-CTA limit");
+  if (c->smem_attr_set.insert((const void*)k_decode_gemm_i8<NP>).second)
+    PG_CUDA(cudaFuncSetAttribute(k_decode_gemm_i8<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_decode_gemm_i8<NP><<<a.grid, kThreads, smem, c->stream>>>(a);
+  PG_CHECK_LAUNCH();
+}
+
+// One product over the tiled codes of one window (a_stride chunks per pair row, rows valid,
+// K codes) and the quantised B (kpad K positions); out holds ks = make_plan(rows, K).ks
+// slots of rows x l partial sums.
+void run_i8(pcaone_ctx* c, const uint8_t* a_tiles, int64_t a_stride, int64_t rows, int64_t K, const int8_t* bq,
+            const float* sig, int64_t kpad, int l, int ks, float* out) {
+  const int np = np_of(l);
+  PG_REQUIRE(np <= 192, PCAONE_EBADARG, "sketch width too large for the int8 tensor-core path");
+  const I8Plan p = make_plan(c, rows, K, np);
+  PG_REQUIRE(ks == p.ks, PCAONE_EBADARG, "output slot count does not match the product plan");
+  if (p.units == 0) {
+    PG_CUDA(cudaMemsetAsync(out, 0, (size_t)ks * rows * l * sizeof(float), c->stream));
+    return;
+  }
+  PG_REQUIRE(p.chunks <= a_stride && p.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
+  PG_REQUIRE(((uintptr_t)a_tiles & 15) == 0 && ((uintptr_t)bq & 15) == 0, PCAONE_EBADARG,
+             "operands not 16-byte aligned");
+  I8Args a;
+  a.a_tiles = a_tiles;
+  a.bq = bq;
+  a.sig = sig;
+  a.a_stride = a_stride;
+  a.rows = rows;
+  a.chunks = p.chunks;
+  a.upp = p.upp;
+  a.units = p.units;
+  a.grid = p.grid;
+  a.ks = p.ks;
+  a.l = l;
+  a.lp = lp_of(l);
+  a.out = out;
+  a.err = (int*)scratch(c, "tc_err", sizeof(int));
+  switch (np) {
+    case 32: launch_np<32>(c, a); break;
+    case 48: launch_np<48>(c, a); break;
+    case 64: launch_np<64>(c, a); break;
+    case 80: launch_np<80>(c, a); break;
+    case 96: launch_np<96>(c, a); break;
+    case 112: launch_np<112>(c, a); break;
+    case 128: launch_np<128>(c, a); break;
+    case 144: launch_np<144>(c, a); break;
+    case 160: launch_np<160>(c, a); break;
+    case 176: launch_np<176>(c, a); break;
+    default: launch_np<192>(c, a); break;
+  }
+  c->launches++;
+  c->gemm_launches++;
+}
+
+// Tiled copies of the codes for the current window layout: "i8_tile1" (per window: SNP
+// pairs x sample chunks, for Z^T Omega) from the SNP-major matrix and "i8_tile2" (per window:
+// sample pairs x SNP chunks, for Z G) from the per-window transposed copy. Rebuilt when the
+// matrix (load, permutation) or the window layout changes.
+struct TileGeom {
+  int64_t p1, c1, p2, c2;  // pairs per window and chunk stride of tile1 / tile2
+};
+TileGeom tile_geom(const pcaone_ctx* c) {
+  const int64_t bs = (int64_t)c->win.blocksize, N = (int64_t)c->N;
+  return TileGeom{((bs + kRows - 1) / kRows + 1) / 2, (N + kChunk - 1) / kChunk, ((N + kRows - 1) / kRows + 1) / 2,
+                  (bs + kChunk - 1) / kChunk};
+}
+void ensure_tiles(pcaone_ctx* c) {
+  PG_REQUIRE(c->bedT_valid, PCAONE_ESTATE, "transposed copy not built");
+  const uint64_t key = (c->generation << 24) ^ ((uint64_t)c->win.bands << 44) ^ (uint64_t)c->win.blocksize;
+  const TileGeom g = tile_geom(c);
+  const int bands = c->win.bands;
+  const size_t w1 = (size_t)g.p1 * g.c1 * kPairChunkBytes, w2 = (size_t)g.p2 * g.c2 * kPairChunkBytes;
+  uint8_t* d1 = (uint8_t*)scratch(c, "i8_tile1", (size_t)bands * w1);
+  uint8_t* d2 = (uint8_t*)scratch(c, "i8_tile2", (size_t)bands * w2);
+  if (c->tiles8_valid && c->tiles8_key == key && c->tile81_ptr == d1 && c->tile82_ptr == d2) return;
+  for (int b = 0; b < bands; ++b) {
+    const int64_t s = (int64_t)c->win.start[b], m = (int64_t)c->win.stop[b] - s;
+    const int64_t n1 = g.p1 * 2 * kRows * 2 * g.c1, n2 = g.p2 * 2 * kRows * 2 * g.c2;
+    k_tile_codes_i8<<<(unsigned)((n1 + 255) / 256), 256, 0, c->stream>>>(c->d_bed + s * c->pitch, c->pitch, m, g.p1,
+                                                                       g.c1, d1 + (size_t)b * w1);
+    PG_CHECK_LAUNCH();
+    k_tile_codes_i8<<<(unsigned)((n2 + 255) / 256), 256, 0, c->stream>>>(
+        c->d_bedT + (int64_t)b * c->Npad * c->win.pitch, c->win.pitch, (int64_t)c->N, g.p2, g.c2, d2 + (size_t)b * w2);
+    PG_CHECK_LAUNCH();
+    c->launches += 2;
+  }
+  c->tiles8_key = key;
+  c->tiles8_valid = true;
+  c->tile81_ptr = d1;
+  c->tile82_ptr = d2;
+}
+
+// Quantise a row-major K x l operand into the chunked piece layout (kpad / 128 chunks).
+// have_max: the column maxima in "i8_qmax<tag>" were already accumulated (by the first
+// epilogue); otherwise they are computed here.
+template <typename T>
+void quantize(pcaone_ctx* c, const T* X, int64_t K, int l, int64_t kpad, const char* tag, bool have_max) {
+  const int np = np_of(l), lp = lp_of(l);
+  const std::string t(tag);
+  auto* qmax = (unsigned long long*)scratch(c, "i8_qmax" + t, 64 * sizeof(unsigned long long));
+  auto* bq = (int8_t*)scratch(c, "i8_bq" + t, (size_t)kpad * np);
+  auto* sig = (float*)scratch(c, "i8_sig" + t, 3 * 64 * sizeof(float));
+  if (!have_max) {
+    PG_CUDA(cudaMemsetAsync(qmax, 0, (size_t)l * sizeof(unsigned long long), c->stream));
+    const int64_t tot = K * l;
+    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(2 * c->sm_count, (tot + 1023) / 1024));
+    k_colmax<T><<<nblk, 256, 0, c->stream>>>(X, K, l, qmax);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+  }
+  k_quant<T><<<(unsigned)(kpad / kChunk), 256, 0, c->stream>>>(X, K, l, lp, np, qmax, bq, sig);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+int i8_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int l) { return make_plan(c, rows, K, np_of(l)).ks; }
+
+void i8_omega(pcaone_ctx* c, const double* omega, int l, int64_t npad) {
+  quantize<double>(c, omega, (int64_t)c->N, l, npad, "1", false);
+}
+
+void i8_b2(pcaone_ctx* c, const float* B2, int l, int64_t m) {
+  quantize<float>(c, B2, m, l, (int64_t)round_up(c->win.blocksize, 256), "2", c->i8_b2_max_ready);
+  c->i8_b2_max_ready = false;
+}
+
+unsigned long long* i8_b2_qmax(pcaone_ctx* c, int) {
+  auto* qmax = (unsigned long long*)scratch(c, "i8_qmax2", 64 * sizeof(unsigned long long));
+  PG_CUDA(cudaMemsetAsync(qmax, 0, 64 * sizeof(unsigned long long), c->stream));
+  c->i8_b2_max_ready = true;
+  return qmax;
+}
+
+void i8_p1(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t row_off, int64_t rows, int64_t K, const float*, int l,
+           int ks, float* out) {
+  ensure_tiles(c);
+  const TileGeom g = tile_geom(c);
+  const int64_t b = row_off / (int64_t)c->win.blocksize;
+  PG_REQUIRE(b < c->win.bands && (uint64_t)row_off == c->win.start[b] && K == (int64_t)c->N, PCAONE_EBADARG,
+             "first product must cover one window");
+  const int np = np_of(l);
+  auto* bq = (const int8_t*)scratch(c, "i8_bq1", (size_t)c->Npad * np);
+  auto* sig = (const float*)scratch(c, "i8_sig1", 3 * 64 * sizeof(float));
+  run_i8(c, (const uint8_t*)c->tile81_ptr + (size_t)b * g.p1 * g.c1 * kPairChunkBytes, g.c1, rows, K, bq, sig,
+         c->Npad, l, ks, out);
+}
+
+void i8_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t rows, int64_t K, const float*, int l,
+           int ks, float* out) {
+  ensure_tiles(c);
+  const TileGeom g = tile_geom(c);
+  PG_REQUIRE(window < c->win.bands && rows == (int64_t)c->N, PCAONE_EBADARG, "second product must cover one window");
+  const int64_t kpad = round_up(c->win.blocksize, 256);
+  const int np = np_of(l);
+  auto* bq = (const int8_t*)scratch(c, "i8_bq2", (size_t)kpad * np);
+  auto* sig = (const float*)scratch(c, "i8_sig2", 3 * 64 * sizeof(float));
+  run_i8(c, (const uint8_t*)c->tile82_ptr + (size_t)window * g.p2 * g.c2 * kPairChunkBytes, g.c2, rows, K, bq, sig,
+         kpad, l, ks, out);
+}
+
+}  // namespace
+
+GemmFnT<float> gemm_i8() {
+  return GemmFnT<float>{i8_ksplit, i8_p1, i8_p2, i8_omega, i8_b2, nullptr, nullptr, i8_b2_qmax};
+}
+
+}  // namespace pg

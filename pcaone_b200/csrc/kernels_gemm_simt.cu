@@ -149,7 +149,7 @@ void simt_gemm(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t, int
                const T* B, int l, int ks, T* out) {
   launch_decode_gemm_simt<T>(c, codes, pitch, rows, K, B, l, l, ks, out);
 }
-int simt_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) {
+int simt_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int) {
   int64_t tiles = (rows + kTR - 1) / kTR;
   int64_t chunks = (K + kKC - 1) / kKC;
   int64_t want = (2 * (int64_t)c->sm_count + tiles - 1) / tiles;

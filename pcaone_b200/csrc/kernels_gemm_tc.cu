@@ -46,6 +46,7 @@
 #include "internal.hpp"
 #include "rsvd.hpp"
 #include "tc_layout.hpp"
+#include "tc_ptx.hpp"
 
 namespace pg {
 
@@ -59,7 +60,6 @@ constexpr int kThreads = 320;     // 4 decoder warps + producer + MMA + 4 readou
 constexpr int kTmemCols = 256;    // accumulators in [0, 128), A stages in [128, 256)
 constexpr int kAColBase = 128;
 constexpr int kMinUnitsPerCta = 4;
-constexpr uint64_t kWaitNs = 1000000000ull;  // bounded waits: 1 s
 
 // Shared-memory ring depth for NP accumulator columns: about 104 KB of stages, so two CTAs
 // (and their 2 x 256 TMEM columns) fit on one SM and a third cannot become resident.
@@ -70,112 +70,23 @@ __host__ __device__ constexpr int ring_stages(int np) {
 __host__ __device__ constexpr int acc_bufs(int np) { return np <= 64 ? 2 : 1; }
 static_assert(kAColBase + kAStages * kUnitChunks * 32 <= kTmemCols, "TMEM A stages exceed the allocation");
 
-// ------------------------------------------------------------------ PTX wrappers
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ uint64_t globaltimer() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait. Returns false (and raises the CTA abort flag / global error) on timeout or
-// when another role already aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
-                                          int* err, int code) {
-  if (mbar_try(bar, parity)) return true;
-  const uint64_t t0 = globaltimer();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try(bar, parity)) return true;
-    if ((it & 255) == 0) {
-      if (*abort_flag) return false;
-      if (globaltimer() - t0 > kWaitNs) {
-        *abort_flag = 1;
-        atomicOr(err, code);
-        return false;
-      }
-    }
-  }
-}
-// Bounded wait that ignores the abort flag: used to drain copies and MMAs in flight.
-__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
-  const uint64_t t0 = globaltimer();
-  while (!mbar_try(bar, parity))
-    if (globaltimer() - t0 > kWaitNs) return;
-}
-// 1-D bulk copy global -> this CTA's shared memory, completing on an mbarrier (no multicast).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
-      : "memory");
-}
-
-// Eight 32-bit TMEM columns per call would need eight calls per chunk; one .x32 store
-// writes this thread's 32 columns (lane = row) in one instruction.
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-      "%30, %31, %32};" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
-      "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),
-      "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),
-      "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
-      : "memory");
-}
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(taddr)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row atoms of 1024 bytes.
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+using tc::bulk_load;
+using tc::mbar_arrive;
+using tc::mbar_arrive_tx;
+using tc::mbar_drain;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::smem_desc_sw128;
+using tc::smem_u32;
+using tc::tmem_ld8;
+using tc::tmem_st32;
+using tc::tmem_wait_ld;
+using tc::tmem_wait_st;
+__device__ __forceinline__ void tc_fence_before() { tc::fence_before(); }
+__device__ __forceinline__ void tc_fence_after() { tc::fence_after(); }
+__device__ __forceinline__ void tc_commit(uint32_t bar) { tc::commit(bar); }
+__device__ __forceinline__ void tc_mma(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  tc::mma_f16(d, a, b, idesc, acc);
 }
 
 // Decode one 32-bit word (16 codes c0..c15) into 8 BF16 pairs. Output word order:
@@ -613,7 +524,7 @@ void split_bf16(pcaone_ctx* c, const T* B, int64_t K, int l, int64_t kpad, __nv_
 }
 
 // ---- back-end state kept in named scratch buffers
-int tc_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) { return make_plan(c, rows, K).ks; }
+int tc_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int) { return make_plan(c, rows, K).ks; }
 
 void tc_omega(pcaone_ctx* c, const double* omega, int l, int64_t npad) {
   auto* Bt = (__nv_bfloat16*)scratch(c, "tc_bt1", (size_t)npad * np_of(l) * 2);

@@ -184,7 +184,7 @@ void launch_dense(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int
 
 // Back end for the RSVD engine: "codes" are the float rows of E (the engine passes the row
 // offset through the pointer), "pitch" is unused.
-int dense_ksplit(pcaone_ctx* c, int64_t rows, int64_t K) {
+int dense_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int) {
   int64_t tiles = (rows + 127) / 128, chunks = (K + 31) / 32;
   int64_t want = (2 * (int64_t)c->sm_count + tiles - 1) / tiles;
   return (int)std::max<int64_t>(1, std::min<int64_t>({want, chunks / 4, 64}));

@@ -209,7 +209,7 @@ struct Engine {
   void process_window(int b, double* Ht) {
     const int64_t s = (int64_t)c->win.start[b], e = (int64_t)c->win.stop[b], m = e - s;
     // product 1: D1 = R_b^T Omega
-    int ks1 = gemm.ksplit(c, m, N);
+    int ks1 = gemm.ksplit(c, m, N, l);
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * m * l * sizeof(T));
     const uint8_t* codes = c->dense ? nullptr : c->d_bed + s * (int64_t)c->pitch;
     timed([&] { gemm.p1(c, codes, c->pitch, s, m, N, OmgT, l, ks1, D1); });
@@ -222,6 +222,7 @@ struct Engine {
     p1.scale = c->d_scale;
     p1.wsum = wsum;
     p1.omega = Omg;
+    p1.omega_f = omg_float();
     p1.miss_ptr = c->d_miss_snp_ptr;
     p1.miss_idx = c->d_miss_snp_idx;
     p1.miss_val = c->imputed ? c->d_miss_snp_val : nullptr;
@@ -229,12 +230,18 @@ struct Engine {
     T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
     double* h0 = (double*)scratch(c, "r_h0", l * 8);
     if (gemm.b2_bt) p1.bt2 = gemm.b2_bt(c, l, &p1.kpad2, &p1.bt_half);
+    if (gemm.b2_qmax) p1.qmax = gemm.b2_qmax(c, l);
+    // FP32 copy of the window's G rows for the second gather (FP32 engines)
+    float* Gf = std::is_same<T, float>::value
+                    ? (float*)scratch(c, "r_Gf", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(float))
+                    : nullptr;
+    p1.Gf = Gf;
     timed([&] {
       launch_prep<T>(c, p1, D1, B2, h0);
       if (!p1.bt2) gemm.b2_ready(c, B2, l, m);
     }, 1);
     // product 2: D2 = R_b B2
-    int ks2 = gemm.ksplit(c, N, m);
+    int ks2 = gemm.ksplit(c, N, m, l);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
     const uint8_t* codesT = c->dense ? nullptr : c->d_bedT + (int64_t)b * Npad * c->win.pitch;
     timed([&] { gemm.p2(c, codesT, c->win.pitch, b, N, m, B2, l, ks2, D2); });
@@ -247,6 +254,8 @@ struct Engine {
     p2.F = Fcent;
     p2.scale = c->d_scale;
     p2.G = G;
+    p2.Gf = Gf;
+    p2.g_start = s;
     p2.h0 = h0;
     p2.miss_ptr = c->d_miss_ws_ptr;
     p2.miss_idx = c->d_miss_ws_idx;
@@ -338,7 +347,7 @@ struct Engine {
   }
 
   void check_status() {
-    if (o.precision == PCAONE_PREC_MIXED) tc_check_error(c);
+    if (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) tc_check_error(c);
     int st = 0;
     PG_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
@@ -467,7 +476,7 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     }
     colsum(c, Bd, l, N, wsum);
     gemm.omega_changed(c, Bd, l, Npad);
-    const int ks = gemm.ksplit(c, M, N);
+    const int ks = gemm.ksplit(c, M, N, l);
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks * M * l * sizeof(T));
     gemm.p1(c, c->d_bed, c->pitch, 0, M, N, BT, l, ks, D1);
     EpiP1 p1;
@@ -490,7 +499,7 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     p1.F = c->d_F; p1.scale = c->d_scale; p1.G = G;
     launch_scale_g<T>(c, p1, B2, h0);
     gemm.b2_ready(c, B2, l, M);
-    const int ks = gemm.ksplit(c, N, M);
+    const int ks = gemm.ksplit(c, N, M, l);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks * N * l * sizeof(T));
     gemm.p2(c, c->d_bedT, c->win.pitch, 0, N, M, B2, l, ks, D2);
     zero(c, H, Npad * l);
@@ -523,10 +532,11 @@ void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, i
     product_t<double>(c, gemm_simt_double(), transpose, standardize, ploidy, B, l, out);
   } else if (precision == PCAONE_PREC_FP32) {
     product_t<float>(c, gemm_simt_float(), transpose, standardize, ploidy, B, l, out);
-  } else if (precision == PCAONE_PREC_MIXED) {
+  } else if (precision == PCAONE_PREC_MIXED || precision == PCAONE_PREC_BF16) {
     PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
     tc_clear_error(c);
-    product_t<float>(c, gemm_tc(), transpose, standardize, ploidy, B, l, out);
+    product_t<float>(c, precision == PCAONE_PREC_MIXED ? gemm_i8() : gemm_tc(), transpose, standardize, ploidy, B, l,
+                     out);
     tc_check_error(c);
   } else {
     throw Error(PCAONE_EBADARG, "unknown precision");
@@ -574,10 +584,10 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
   } else if (o.precision == PCAONE_PREC_FP32) {
     Engine<float> e(c, o, gemm_simt_float());
     e.run(U, S, V, rep);
-  } else if (o.precision == PCAONE_PREC_MIXED) {
+  } else if (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) {
     PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
     tc_clear_error(c);
-    Engine<float> e(c, o, gemm_tc());
+    Engine<float> e(c, o, o.precision == PCAONE_PREC_MIXED ? gemm_i8() : gemm_tc());
     e.run(U, S, V, rep);
   } else {
     throw Error(PCAONE_EBADARG, "unknown precision");

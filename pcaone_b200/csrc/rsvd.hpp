@@ -12,7 +12,7 @@ namespace pg {
 // omega_changed / b2_ready let a back end re-pack the B operands into its own layout.
 template <typename T>
 struct GemmFnT {
-  int (*ksplit)(pcaone_ctx* c, int64_t rows, int64_t K);
+  int (*ksplit)(pcaone_ctx* c, int64_t rows, int64_t K, int l);
   // p1: rows = SNPs row0..row0+rows of the SNP-major matrix; p2: rows = samples of window
   // `window` of the sample-major copy. `codes` points at the first row of the packed data.
   void (*p1)(pcaone_ctx* c, const uint8_t* codes, uint32_t pitch, int64_t row0, int64_t rows,
@@ -26,11 +26,14 @@ struct GemmFnT {
   // *half receives the row offset of the lo halves.
   __nv_bfloat16* (*omega_bt)(pcaone_ctx* c, int l, int* half) = nullptr;
   __nv_bfloat16* (*b2_bt)(pcaone_ctx* c, int l, int64_t* kpad, int* half) = nullptr;
+  // Zeroed per-column maxima of |B2| for the first epilogue to fill (int8 back end), or null.
+  unsigned long long* (*b2_qmax)(pcaone_ctx* c, int l) = nullptr;
 };
 
 GemmFnT<float> gemm_simt_float();
 GemmFnT<double> gemm_simt_double();
 GemmFnT<float> gemm_tc();
+GemmFnT<float> gemm_i8();  // int8 three-piece tensor-core back end, kernels_gemm_i8.cu
 GemmFnT<float> gemm_dense_float();  // dense float E (PCAngsd), kernels_gl.cu
 
 // PCAngsd device steps (kernels_gl.cu)

@@ -108,7 +108,8 @@ void usage() {
                "  -V, --printv     write .loadings and .mbim\n"
                "  -o, --out        output prefix [pcaone]\n"
                "  -v, --verbose    0 silent, 1 screen\n"
-               "      --precision  mixed (BF16 tensor cores, default), fp32 or fp64\n"
+               "      --precision  mixed (int8 tensor cores, three-piece sketch; default), bf16 (split\n"
+               "                   BF16 tensor cores), fp32 or fp64\n"
                "      --device     CUDA device index [0]\n";
 }
 
@@ -180,10 +181,11 @@ Params parse(int argc, char** argv) {
     else if (a == "--device") p.device = (int)num(next());
     else if (a == "--precision") {
       std::string v = next();
-      if (v == "mixed" || v == "bf16") p.precision = PCAONE_PREC_MIXED;
+      if (v == "mixed" || v == "int8") p.precision = PCAONE_PREC_MIXED;
+      else if (v == "bf16") p.precision = PCAONE_PREC_BF16;
       else if (v == "fp32") p.precision = PCAONE_PREC_FP32;
       else if (v == "fp64") p.precision = PCAONE_PREC_FP64;
-      else fail("--precision must be mixed, fp32 or fp64");
+      else fail("--precision must be mixed, bf16, fp32 or fp64");
     } else if (kUnsupported.count(a)) {
       fail("option " + a + " belongs to a mode this build does not provide");
     } else {

@@ -208,7 +208,11 @@ int pcaone_gpu_gl_grm(pcaone_ctx* ctx, const double* U, const double* S, const d
  * builds the missing-genotype list; PCAONE_ESTATE otherwise). The first call on a device
  * resolves the array's device address (cudaGetSymbolAddress), so make that first call before
  * any stream capture. All calls share the array and overwrite what they use; calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * overlap on the GPU race and must be serialised by the caller.
+ * Stream semantics: the call runs on the context's own stream, which is created non-blocking
+ * and is not ordered after any of the caller's streams. Every kernel that writes d_B must
+ * therefore be complete before the call (e.g. synchronise the producing stream first); the
+ * call synchronises its stream before returning, so d_out is complete when it returns. */
 int pcaone_gpu_product_t_noalloc(pcaone_ctx* ctx, int standardize, int ploidy, const double* B,
                                  uint32_t ncols, double* out);
 

@@ -9,15 +9,17 @@ from tests.test_gpu_rsvd import random_bed
 
 pytestmark = pytest.mark.gpu
 
-# max |err| / max |ref| per output column; the mixed path uses split-BF16 (hi+lo, 16 bits)
-TOL = {"fp64": 1e-12, "fp32": 2e-6, "mixed": 5e-5}
+# max |err| / max |ref| per output column. mixed: int8 tensor cores with the sketch as three
+# 8-bit fixed-point pieces per column (21 bits below the column maximum); bf16: split BF16
+# hi+lo pairs (16 significant bits), FP32 accumulation.
+TOL = {"fp64": 1e-12, "fp32": 2e-6, "mixed": 5e-6, "bf16": 5e-5}
 
 
 def rel_col_err(got, ref):
     return float((np.abs(got - ref).max(axis=0) / np.abs(ref).max(axis=0)).max())
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed", "bf16"])
 @pytest.mark.parametrize("N,M,l", [(1003, 2500, 40), (517, 777, 20), (2048, 1300, 7), (300, 4100, 64)])
 def test_products_match_dense(gpu, prec, N, M, l):
     bed = random_bed(N, M, seed=N * 7 + l, miss=0.02)
@@ -32,7 +34,7 @@ def test_products_match_dense(gpu, prec, N, M, l):
     assert rel_col_err(got2, Z @ B2) <= TOL[prec]
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "bf16"])
 def test_products_unstandardised_haploid(gpu, prec):
     bed = random_bed(640, 900, seed=3, miss=0.05)
     codes = O.decode_codes(bed)

@@ -85,7 +85,7 @@ def run_gpu(gpu, bed, shuffle, **kw):
     return r, V
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed", "bf16"])
 @pytest.mark.parametrize("name,kw,shuffle", GOLDEN_CASES)
 def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
     bed = O.read_bed(os.path.join(GOLDEN, "g1"))
@@ -97,7 +97,7 @@ def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
     lpath = os.path.join(GOLDEN, "ref", name + ".loadings")
     if os.path.exists(lpath):
         assert_cols_close(V, O.read_table(lpath), 2e-6 if prec == "fp64" else 5e-4)
-    if prec == "mixed":
+    if prec in ("mixed", "bf16"):
         assert r.gemm_launches > 0
 
 
@@ -106,7 +106,8 @@ def test_rsvd_matches_oracle_larger(gpu, svd, bands):
     bed = random_bed(1502, 9001, seed=5, miss=0.01)
     kw = dict(k=6, maxp=6, tol=0.0) if svd == 1 else dict(k=6, maxp=8, bands=bands)
     eig_o, S_o, U_o, V_o, F_o, ep_o = O.run_pca(bed, svd=svd, **kw)
-    for prec, rtol, ang in [("fp64", 1e-9, 1e-7), ("fp32", 1e-5, 1e-3), ("mixed", 1e-5, 1e-3)]:
+    for prec, rtol, ang in [("fp64", 1e-9, 1e-7), ("fp32", 1e-5, 1e-3), ("mixed", 1e-5, 1e-3),
+                            ("bf16", 1e-5, 1e-3)]:
         r, V = run_gpu(gpu, bed, svd == 2, precision=prec, svd=svd, **kw)
         assert r.epochs == ep_o
         assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, rtol)
@@ -114,7 +115,7 @@ def test_rsvd_matches_oracle_larger(gpu, svd, bands):
         assert max_angle(V, V_o) <= ang
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "bf16"])
 def test_emu_matches_reference_golden(gpu, prec):
     """EMU (--emu -k 3 -w 8 --maxiter 20 --tol-em 1e-6) against the reference's outputs."""
     packed, N, M = pb.read_bed(os.path.join(GOLDEN, "g2"))
@@ -149,3 +150,24 @@ def test_pcangsd_matches_reference_golden(gpu, name, shuffle):
     assert_cols_close(U, ref_table(name, ".eigvecs"), 5e-4)
     if not shuffle:
         assert_cols_close(V, ref_table(name, ".loadings"), 5e-4)
+
+
+@pytest.fixture(scope="module")
+def bench_shape_oracle():
+    """The benchmark's schedule (k = 20, l = 40, 64 windows, shuffled, the reference's default
+    maxp/tol) on a 4000 x 32000 matrix with 0.5% missing, run once by the FP64 oracle."""
+    bed = random_bed(4000, 32000, seed=11, miss=0.005)
+    return bed, O.run_pca(bed, svd=2, k=20, maxp=20, bands=64)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "bf16"])
+def test_winsvd_bench_shape_matches_oracle(gpu, bench_shape_oracle, prec):
+    """Eigenvalues to 1e-5 relative and a largest principal angle of 1e-3 rad (the mixed-precision
+    bar) against the FP64 oracle; the population PCs 1-4 to 1e-6 rad."""
+    bed, (eig_o, S_o, U_o, V_o, F_o, ep_o) = bench_shape_oracle
+    r, V = run_gpu(gpu, bed, True, precision=prec, svd=2, k=20, maxp=20, bands=64)
+    assert r.epochs == ep_o
+    assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, 1e-5)
+    assert max_angle(r.U, U_o) <= 1e-3
+    assert max_angle(V, V_o) <= 1e-3
+    assert max_angle(r.U[:, :4], U_o[:, :4]) <= 1e-6

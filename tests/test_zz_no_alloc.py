@@ -3,10 +3,11 @@
 Callers that cannot let a library call cudaMalloc (code inside another framework's device
 memory pool, or a solver loop that must not allocate per call) pass their own device
 buffers; the entry point keeps its scratch in one fixed device array inside the library.
-Here torch plays the caller's allocator. The result must match the allocating
-pcaone_gpu_product (FP32, Z^T B) on two calls in a row, and oversize problems must be
-rejected with a clear error. The test uses its own context and data, so it passes alone in a
-fresh process and after the other tests.
+Here torch plays the caller's allocator. On two calls in a row the result must match the
+allocating pcaone_gpu_product (FP32, Z^T B) and the oracle's standardised Z^T B, free
+device memory must not change across a call, and oversize problems must be rejected with a
+clear error. The test uses its own context and data, so it passes alone in a fresh process
+and after the other tests.
 """
 import numpy as np
 import pytest
@@ -33,23 +34,32 @@ def _random_bed(N, M, seed, miss):
     return O.Bed(N, M, packed.astype(np.uint8))
 
 
-def test_product_noalloc_matches_allocating_product():
+def _rel(got, ref):
+    return float((np.abs(got - ref).max(axis=0) / np.abs(ref).max(axis=0)).max())
+
+
+def test_product_noalloc_matches_allocating_product_and_oracle():
     torch = pytest.importorskip("torch")
     bed = _random_bed(1003, 2500, seed=42, miss=0.02)
+    Z, _ = O.standardized_from_bed(bed)
     l = 40
     rng = np.random.default_rng(7)
     with pb.GpuContext(0) as ctx:
         ctx.load_bed(bed.packed, bed.N)
-        for _ in range(2):  # two calls in a row share (and overwrite) the scratch array
+        for call in range(2):  # two calls in a row share (and overwrite) the scratch array
             B = rng.standard_normal((bed.N, l))
             ref = ctx.product_t(B, precision="fp32")  # existing entry point
             d_B = torch.tensor(B.T.copy(), dtype=torch.float64, device="cuda")  # column-major N x l
             d_out = torch.full((l, bed.M), float("nan"), dtype=torch.float64, device="cuda")
-            torch.cuda.synchronize()
+            torch.cuda.synchronize()  # d_B is written on torch's stream: complete it first
+            free0 = torch.cuda.mem_get_info()[0]
             ctx.product_t_noalloc(d_B.data_ptr(), l, d_out.data_ptr())
+            free1 = torch.cuda.mem_get_info()[0]
             got = d_out.cpu().numpy().T
-            rel = float((np.abs(got - ref).max(axis=0) / np.abs(ref).max(axis=0)).max())
-            assert rel <= TOL, rel
+            assert _rel(got, ref) <= TOL
+            assert _rel(got, Z.T @ B) <= TOL
+            if call == 1:  # after the first call has resolved the array's address
+                assert free1 == free0, (free0, free1)
 
 
 def test_product_noalloc_rejects_oversize_and_unprepared():

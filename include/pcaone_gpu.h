@@ -169,6 +169,15 @@ int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t
  * posterior matrix E built by pcaone_gpu_gl_update. */
 int pcaone_gpu_load_gl(pcaone_ctx* ctx, const double* P, uint64_t nsnps, uint32_t nsamples);
 
+/* PCAngsd on PLINK input (-b with --pcangsd): switch the loaded packed genotypes, in the
+ * current SNP order (after any pcaone_gpu_permute), to the likelihood mode as
+ * FileBed::read_all does with --pcangsd (src/FilePlink.cpp:89-115): pseudo-likelihood pairs
+ * per genotype (RR -> (1, 0), AA -> (0, 0), RA -> (0, 1), missing -> (0.333333, 0.333333)),
+ * F = the genotype allele frequencies (src/FilePlink.cpp:36-64, no likelihood EM), and the
+ * initial matrix E = BED2GENO - F with missing -> 0 (not standardised). pcaone_gpu_rsvd and
+ * pcaone_gpu_gl_update then run the PCAngsd EM loop on it. */
+int pcaone_gpu_bed_to_gl(pcaone_ctx* ctx);
+
 /* Allele frequencies by EM from the likelihoods, emMAF_with_GL (src/Utils.cpp:501-531):
  * F0 = 0.25, at most maxiter sweeps, stops when sqrt(mean((F - F_prev)^2)) < tolmaf.
  * F (host, nsnps) and iters (number of sweeps run) may be NULL. */

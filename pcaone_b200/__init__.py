@@ -29,7 +29,8 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_permute", "pcaone_shuffle_perm", "pcaone_omega", "pcaone_gpu_rsvd",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
-           "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc"]
+           "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
+           "pcaone_gpu_bed_to_gl"]
 
 
 class PcaoneError(RuntimeError):
@@ -86,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_ld_r2.argtypes = [vp, vp, u32, vp, vp, u64, vp]
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
+        L.pcaone_gpu_bed_to_gl.argtypes = [vp]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
@@ -308,7 +310,14 @@ def _product_t_noalloc(self, d_B: int, ncols: int, d_out: int, standardize=True,
                                                    ctypes.c_void_p(d_B), ncols, ctypes.c_void_p(d_out)))
 
 
+def _bed_to_gl(self):
+    """Switch the loaded (optionally permuted) genotypes to the PCAngsd likelihood mode with
+    pseudo-likelihoods (pcaone_gpu_bed_to_gl)."""
+    self._check(lib().pcaone_gpu_bed_to_gl(self._h))
+
+
 GpuContext.product_t_noalloc = _product_t_noalloc
+GpuContext.bed_to_gl = _bed_to_gl
 GpuContext.load_gl = _load_gl
 GpuContext.gl_freq = _gl_freq
 GpuContext.gl_update = _gl_update
@@ -332,6 +341,33 @@ def run_pcangsd(ctx: "GpuContext", P: np.ndarray, k: int = 10, svd: int = 2, ban
     ctx.load_gl(P[:, perm])
     F_perm, _ = ctx.gl_freq(maxiter, tolmaf)
     ctx.gl_update()
+    return _pcangsd_em(ctx, perm, F_perm, k, svd, bands, maxp, oversamples, tol, maxiter, tolem,
+                       seed, rand, reference_index, grm)
+
+
+def run_pcangsd_bed(ctx: "GpuContext", packed: np.ndarray, N: int, k: int = 10, svd: int = 2,
+                    bands: int = 64, maxp: int = 20, oversamples: int = 10, tol: float = 1e-4,
+                    maxiter: int = 100, tolem: float = 1e-5, seed: int = 101, rand: int = 1,
+                    shuffle: bool = True, reference_index: bool = True):
+    """PCAngsd on PLINK input (-b with --pcangsd): pseudo-likelihoods from the genotypes and F
+    from the genotype counts (src/FilePlink.cpp:36-115), then the same EM loop as for Beagle
+    input (src/Halko.cpp:294-316); the first RSVD runs on the centred, unstandardised
+    genotypes. Returns (eigvals, S, U, V in input order, iterations, F)."""
+    M = packed.shape[0]
+    perm = shuffle_perm(M) if (svd == 2 and shuffle) else np.arange(M, dtype=np.int32)
+    ctx.load_bed(packed, N)
+    ctx.permute(perm)
+    F_perm = ctx.allele_freq()
+    ctx.bed_to_gl()
+    return _pcangsd_em(ctx, perm, F_perm, k, svd, bands, maxp, oversamples, tol, maxiter, tolem,
+                       seed, rand, reference_index, False)
+
+
+def _pcangsd_em(ctx, perm, F_perm, k, svd, bands, maxp, oversamples, tol, maxiter, tolem, seed,
+                rand, reference_index, grm):
+    """The PCAngsd EM loop (src/Halko.cpp:294-316) on the likelihood matrix of ctx, whose SNP
+    order is perm; returns the outputs of run_pcangsd."""
+    M = len(perm)
     kw = dict(k=k, oversamples=oversamples, maxp=maxp, svd=svd, bands=bands, tol=tol,
               seed=seed, rand=rand, precision=PREC_FP32, standardize=False)
     r = ctx.rsvd(carry=False, **kw)
@@ -351,6 +387,8 @@ def run_pcangsd(ctx: "GpuContext", P: np.ndarray, k: int = 10, svd: int = 2, ban
     if grm:
         out += ctx.gl_grm(r.U, r.S, r.V[perm] if reference_index else r.V)
     return out
+
+
 GpuContext.fit_emu = _fit_emu
 GpuContext.clear_imputed = _clear_imputed
 

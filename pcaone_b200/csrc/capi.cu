@@ -365,6 +365,10 @@ int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t 
   });
 }
 
+int pcaone_gpu_bed_to_gl(pcaone_ctx* c) {
+  return guarded(c, [&] { gl_from_bed(c); });
+}
+
 int pcaone_gpu_gl_freq(pcaone_ctx* c, int maxiter, double tolmaf, double* F, int* iters) {
   return guarded(c, [&] {
     PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");

@@ -84,6 +84,37 @@ __global__ void k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t 
   }
 }
 
+// PLINK input with --pcangsd (FileBed::read_all, src/FilePlink.cpp:89-115): pseudo-likelihood
+// pairs from the genotype codes, 11 (RR) -> (1, 0), 00 (AA) -> (0, 0), 10 (RA) -> (0, 1),
+// 01 (missing) -> (0.333333, 0.333333), and the initial matrix E = BED2GENO - F_j with
+// BED2GENO = {1, -, 0.5, 0} and missing -> 0. Warp per SNP row of the packed codes.
+__global__ void k_bed_pseudo_gl(const uint8_t* __restrict__ bed, uint32_t pitch, uint64_t M, uint32_t N,
+                                const double* __restrict__ F, float* __restrict__ P, uint32_t ldp,
+                                float* __restrict__ E, uint32_t lde) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
+    const double f = F[j];
+    const uint8_t* rec = bed + j * pitch;
+    for (uint32_t i = lane; i < N; i += 32) {
+      const int code = (rec[i >> 2] >> (2 * (i & 3))) & 3;
+      float p0 = 0.0f, p1 = 0.0f, e = 0.0f;
+      if (code == 3) {
+        p0 = 1.0f;
+        e = (float)(0.0 - f);
+      } else if (code == 0) {
+        e = (float)(1.0 - f);
+      } else if (code == 2) {
+        p1 = 1.0f;
+        e = (float)(0.5 - f);
+      } else {
+        p0 = p1 = (float)0.333333;
+      }
+      P[j * ldp + 2 * i] = p0;
+      P[j * ldp + 2 * i + 1] = p1;
+      E[j * lde + i] = e;
+    }
+  }
+}
 
 // Dense SIMT GEMM: out[s][r][c] = sum_{k in split s} A(r, k) * B[k][c]. A(r, k) is
 // A[r * lda + k] when !AT (rows = SNPs, K = samples) and A[k * lda + r] when AT (rows =
@@ -264,6 +295,28 @@ __global__ void k_grm_finish(const double* __restrict__ L, const double* __restr
 
 GemmFnT<float> gemm_dense_float() {
   return GemmFnT<float>{dense_ksplit, dense_p1, dense_p2, dense_none_omega, dense_none_b2};
+}
+
+void gl_from_bed(pcaone_ctx* c) {
+  PG_REQUIRE(c->loaded && !c->dense && c->d_bed, PCAONE_ESTATE, "no packed genotypes loaded");
+  const size_t np = (size_t)c->M * 2 * c->N;
+  float* P = (float*)scratch(c, "d_P", np * 4);
+  float* E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
+  PG_CUDA(cudaMemsetAsync(E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
+  const int threads = 256, nwarps = threads / 32;
+  const int nblk = (int)std::min<uint64_t>(8 * (uint64_t)c->sm_count, (c->M + nwarps - 1) / nwarps);
+  k_bed_pseudo_gl<<<nblk, threads, 0, c->stream>>>(c->d_bed, c->pitch, c->M, c->N, c->d_F, P, 2 * c->N, E, c->Npad);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+  c->d_zero = (double*)scratch(c, "d_zero", c->M * 8);
+  PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+  c->d_P = P;
+  c->d_E = E;
+  c->dense = true;
+  c->generation++;
+  c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
+  c->imputed = false;
 }
 
 void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {

@@ -71,7 +71,7 @@ struct Params {
   int svd = 2;
   unsigned k = 10, maxp = 20, bands = 64, oversamples = 10, rand = 1, verbose = 1, threads = 12;
   int seed = 101, scale = -1;
-  bool noshuffle = false, printv = false, haploid = false, emu = false;
+  bool noshuffle = false, printv = false, haploid = false, emu = false, pcangsd = false;
   double tol = 1e-4, maf = 0.0, memory = 0.0, tolem = 1e-5;
   unsigned maxiter = 100;
   bool fix_index = false;
@@ -150,7 +150,7 @@ Params parse(int argc, char** argv) {
       std::exit(EXIT_SUCCESS);
     } else if (a == "-b" || a == "--bfile") p.bfile = next();
     else if (a == "-G" || a == "--beagle") p.beagle = next();
-    else if (a == "--pcangsd") {}  // implied by Beagle input (src/Cmd.cpp:205)
+    else if (a == "--pcangsd") p.pcangsd = true;  // implied by Beagle input (src/Cmd.cpp:205)
     else if (a == "--tol-maf") p.tolmaf = num(next());
     else if (a == "-o" || a == "--out") p.fileout = next();
     else if (a == "-k" || a == "--pc") p.k = (unsigned)num(next());
@@ -461,6 +461,43 @@ std::vector<double> read_beagle(const std::string& path, size_t& N, size_t& M) {
   return P;
 }
 
+// The EM loop of run_pca_with_halko for PCAngsd (src/Halko.cpp:294-316) on the likelihood
+// matrix of ctx: a first RSVD, then alternate the posterior update and the RSVD until
+// 1 - mev(V, Vpre) < tolem. perm is the in-core SNP order (identity without the shuffle).
+void pcangsd_em(const Params& p, pcaone_ctx* ctx, pcaone_rsvd_opts& o, size_t M, const std::vector<int32_t>& perm,
+                std::vector<double>& U, std::vector<double>& S, std::vector<double>& V) {
+  std::vector<double> Vpre, Vuse(M * p.k);
+  pcaone_rsvd_report rep{};
+  check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+  g_log.print(date(), "run EM-PCA. maxiter =", p.maxiter);
+  o.carry_window_state = 1;
+  for (unsigned it = 0; it < p.maxiter; ++it) {
+    Vpre = V;
+    // reference index semantics after the shuffle: position j is predicted from loading row
+    // perm[j] (src/Data.cpp:249-270 indexes P, F and V^T by the permuted column)
+    for (unsigned t = 0; t < p.k; ++t)
+      for (size_t j = 0; j < M; ++j) Vuse[t * M + j] = p.fix_index ? V[t * M + j] : V[t * M + perm[j]];
+    check(ctx, pcaone_gpu_gl_update(ctx, U.data(), S.data(), Vuse.data(), p.k), "gl_update");
+    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
+    double acc = 0;
+    for (unsigned b2 = 0; b2 < p.k; ++b2) {
+      double nrm = 0;
+      for (unsigned a = 0; a < p.k; ++a) {
+        double d = 0;
+        for (size_t j = 0; j < M; ++j) d += V[a * M + j] * Vpre[b2 * M + j];
+        nrm += d * d;
+      }
+      acc += std::sqrt(nrm);
+    }
+    const double diff = 1.0 - acc / p.k;
+    g_log.print(date(), "individual allele frequencies estimated iter =", it + 1, ", diff =", diff);
+    if (diff < p.tolem) {
+      g_log.print(date(), "come to convergence!");
+      break;
+    }
+  }
+}
+
 int run_pcangsd(const Params& p, std::chrono::steady_clock::time_point t_start) {
   g_log.print(date(), "start parsing BEAGLE format");
   size_t N = 0, M = 0;
@@ -494,36 +531,8 @@ int run_pcangsd(const Params& p, std::chrono::steady_clock::time_point t_start) 
   o.rand = (int)p.rand;
   o.tol = p.tol;
   o.verbose = p.verbose > 0;
-  std::vector<double> U(N * p.k), S(p.k), V(M * p.k), Vpre, Vuse(M * p.k);
-  pcaone_rsvd_report rep{};
-  check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
-  g_log.print(date(), "run EM-PCA. maxiter =", p.maxiter);
-  o.carry_window_state = 1;
-  for (unsigned it = 0; it < p.maxiter; ++it) {
-    Vpre = V;
-    // reference index semantics after the shuffle: position j is predicted from loading row
-    // perm[j] (src/Data.cpp:249-270 indexes P, F and V^T by the permuted column)
-    for (unsigned t = 0; t < p.k; ++t)
-      for (size_t j = 0; j < M; ++j) Vuse[t * M + j] = p.fix_index ? V[t * M + j] : V[t * M + perm[j]];
-    check(ctx, pcaone_gpu_gl_update(ctx, U.data(), S.data(), Vuse.data(), p.k), "gl_update");
-    check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
-    double acc = 0;
-    for (unsigned b2 = 0; b2 < p.k; ++b2) {
-      double nrm = 0;
-      for (unsigned a = 0; a < p.k; ++a) {
-        double d = 0;
-        for (size_t j = 0; j < M; ++j) d += V[a * M + j] * Vpre[b2 * M + j];
-        nrm += d * d;
-      }
-      acc += std::sqrt(nrm);
-    }
-    const double diff = 1.0 - acc / p.k;
-    g_log.print(date(), "individual allele frequencies estimated iter =", it + 1, ", diff =", diff);
-    if (diff < p.tolem) {
-      g_log.print(date(), "come to convergence!");
-      break;
-    }
-  }
+  std::vector<double> U(N * p.k), S(p.k), V(M * p.k), Vuse(M * p.k);
+  pcangsd_em(p, ctx, o, M, perm, U, S, V);
   // GRM stage (src/Halko.cpp:317-331): standardised posterior from the final factors, with the
   // same index semantics as the EM updates; C = E E^T / M with diag Dc / M, and its singular
   // vectors written with the sample names
@@ -606,6 +615,10 @@ int main(int argc, char** argv) {
     if ((size_t)f.gcount() != packed.size()) fail("the .bed file is shorter than the .bim/.fam imply");
   }
   if (p.k + p.oversamples > N) fail("k + oversamples must not exceed the number of samples");
+  if (p.pcangsd && p.emu) fail("--emu and --pcangsd are exclusive");
+  // with --maf the reference indexes the filtered pseudo-likelihoods by unfiltered SNP index
+  // (src/Data.cpp:255 with src/FilePlink.cpp:67-105), reading past them: not reproduced
+  if (p.pcangsd && p.maf > 0) fail("--pcangsd with PLINK input does not support --maf");
 
   pcaone_ctx* ctx = nullptr;
   if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
@@ -676,7 +689,19 @@ int main(int argc, char** argv) {
   std::vector<double> U(N * p.k), S(p.k), V(M * p.k);
   pcaone_rsvd_report rep{};
   double gpu_s = 0;
-  if (!p.emu) {
+  if (p.pcangsd) {
+    // PCAngsd on PLINK input (src/FilePlink.cpp:89-115, src/Halko.cpp:294-316): pseudo-
+    // likelihoods from the genotypes, F from the genotype counts, the first RSVD on the
+    // centred unstandardised genotypes; no GRM stage (Beagle input only)
+    std::vector<int32_t> order(perm);
+    if (order.empty())
+      for (size_t j = 0; j < M; ++j) order.push_back((int32_t)j);
+    check(ctx, pcaone_gpu_bed_to_gl(ctx), "bed_to_gl");
+    o.precision = PCAONE_PREC_FP32;  // the posterior matrix is dense FP32
+    o.standardize = 0;
+    o.carry_window_state = 0;
+    pcangsd_em(p, ctx, o, M, order, U, S, V);
+  } else if (!p.emu) {
     check(ctx, pcaone_gpu_rsvd(ctx, &o, U.data(), S.data(), V.data(), &rep), "rsvd");
     gpu_s += rep.gpu_ms / 1e3;
     g_log.print(date(), "stops at epoch =", rep.epochs);

@@ -51,6 +51,17 @@ def test_cli_matches_reference_outputs(tmp_path, prec, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["g1_pcangsd_bed", "g1_pcangsd_bedS"])
+def test_cli_pcangsd_on_plink_matches_reference_outputs(tmp_path, name):
+    """-b with --pcangsd: pseudo-likelihoods from the genotypes (src/FilePlink.cpp:89-105)."""
+    run_cli(golden_args(name, tmp_path), tmp_path)
+    out = str(tmp_path / name)
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table(name, ".eigvals")[:, 0], 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table(name, ".eigvecs"), 5e-4)
+    assert_cols_close(O.read_table(out + ".loadings"), ref_table(name, ".loadings"), 5e-4)
+
+
+@pytest.mark.gpu
 def test_cli_emu_matches_reference_outputs(tmp_path):
     run_cli(golden_args("g2_emu", tmp_path), tmp_path)
     out = str(tmp_path / "g2_emu")

@@ -140,6 +140,18 @@ def test_emu_matches_oracle_other_modes(gpu):
         assert max_angle(U, U_o) < 1e-7
 
 
+@pytest.mark.parametrize("name,shuffle", [("g1_pcangsd_bed", True), ("g1_pcangsd_bedS", False)])
+def test_pcangsd_on_plink_matches_reference_golden(gpu, name, shuffle):
+    """PCAngsd on PLINK input (-b g1 --pcangsd -k 3 -w 8 --maxiter 30, with and without -S):
+    pseudo-likelihoods and the first RSVD on the centred genotypes, built on the device."""
+    packed, N, M = pb.read_bed(os.path.join(GOLDEN, "g1"))
+    eig, S, U, V, iters, F = pb.run_pcangsd_bed(gpu, packed, N, k=3, bands=8, maxiter=30, shuffle=shuffle)
+    np.testing.assert_array_equal(F, O.allele_freq(O.decode_codes(O.read_bed(os.path.join(GOLDEN, "g1")))))
+    assert_eig_close(eig, ref_eigvals(name), 1e-5)
+    assert_cols_close(U, ref_table(name, ".eigvecs"), 5e-4)
+    assert_cols_close(V, ref_table(name, ".loadings"), 5e-4)
+
+
 @pytest.mark.parametrize("name,shuffle", [("g3_pcangsd", False), ("g3_pcangsd_shuf", True)])
 def test_pcangsd_matches_reference_golden(gpu, name, shuffle):
     """PCAngsd (-G g3.beagle.gz -k 3 -w 8 --maxiter 30, with and without -S)."""

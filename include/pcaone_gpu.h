@@ -168,6 +168,9 @@ int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t
  * 1 - P0 - P1). The context then holds no packed codes; pcaone_gpu_rsvd runs on the dense
  * posterior matrix E built by pcaone_gpu_gl_update. */
 int pcaone_gpu_load_gl(pcaone_ctx* ctx, const double* P, uint64_t nsnps, uint32_t nsamples);
+/* The same from FP32 likelihood pairs (the device keeps them in FP32 either way); half the
+ * host memory of the FP64 form for large inputs. */
+int pcaone_gpu_load_gl_f32(pcaone_ctx* ctx, const float* P, uint64_t nsnps, uint32_t nsamples);
 
 /* PCAngsd on PLINK input (-b with --pcangsd): switch the loaded packed genotypes, in the
  * current SNP order (after any pcaone_gpu_permute), to the likelihood mode as

@@ -30,7 +30,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
-           "pcaone_gpu_bed_to_gl"]
+           "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32"]
 
 
 class PcaoneError(RuntimeError):
@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
+        L.pcaone_gpu_load_gl_f32.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
@@ -265,10 +266,15 @@ GpuContext.ld_r2 = _ld_r2
 
 
 def _load_gl(self, P: np.ndarray):
-    """P: 2N x M likelihood pairs (first two of the three per sample and site)."""
-    Pf = np.asfortranarray(P, dtype=np.float64)
+    """P: 2N x M likelihood pairs (first two of the three per sample and site). FP32 input is
+    passed as is (pcaone_gpu_load_gl_f32), anything else as FP64."""
     N, M = P.shape[0] // 2, P.shape[1]
-    self._check(lib().pcaone_gpu_load_gl(self._h, _ptr(Pf), M, N))
+    if P.dtype == np.float32:
+        Pf = np.asfortranarray(P)
+        self._check(lib().pcaone_gpu_load_gl_f32(self._h, _ptr(Pf), M, N))
+    else:
+        Pf = np.asfortranarray(P, dtype=np.float64)
+        self._check(lib().pcaone_gpu_load_gl(self._h, _ptr(Pf), M, N))
     self.N, self.M = N, M
 
 
@@ -410,24 +416,39 @@ def run_emu(ctx: "GpuContext", packed: np.ndarray, N: int, k: int = 10, svd: int
     perm = shuffle_perm(M) if (svd == 2 and shuffle) else None
     if perm is not None:
         ctx.permute(perm)
+    eig, S, U, V, iters, _ = emu_loop(ctx, k, svd, bands, maxp, oversamples, tol, maxiter, tolem, seed,
+                                      rand, precision, reference_index)
+    if perm is not None:
+        Vo = np.empty_like(V)
+        Vo[perm] = V
+        V = Vo
+    return eig, S, U, V, iters
+
+
+def emu_loop(ctx: "GpuContext", k: int = 10, svd: int = 2, bands: int = 64, maxp: int = 20,
+             oversamples: int = 10, tol: float = 1e-4, maxiter: int = 100, tolem: float = 1e-5,
+             seed: int = 101, rand: int = 1, precision=PREC_MIXED, reference_index: bool = True):
+    """The EM iterations of EMU on the genotypes already loaded (and permuted) on ctx
+    (src/Halko.cpp:294-336). Returns (eigvals, S, U, V in the context's SNP order, iterations,
+    total epochs over all RSVD runs)."""
     kw = dict(k=k, oversamples=oversamples, maxp=maxp, svd=svd, bands=bands, tol=tol,
               seed=seed, rand=rand, precision=precision)
+    ctx.clear_imputed()
     r = ctx.rsvd(standardize=False, carry=False, **kw)
+    epochs = r.epochs
     it = 0
     for it in range(maxiter):
         Vpre = r.V
         ctx.fit_emu(r.U, r.S, r.V, reference_index)
         r = ctx.rsvd(standardize=False, carry=True, **kw)
+        epochs += r.epochs
         if 1.0 - mev(r.V, Vpre) < tolem:
             break
     ctx.fit_emu(r.U, r.S, r.V, reference_index)
     r = ctx.rsvd(standardize=True, carry=True, **kw)
+    epochs += r.epochs
     ctx.clear_imputed()
-    V = r.V
-    if perm is not None:
-        V = np.empty_like(r.V)
-        V[perm] = r.V
-    return r.S ** 2 / M * 2, r.S, r.U, V, it + 1
+    return r.S ** 2 / ctx.M * 2, r.S, r.U, r.V, it + 1, epochs
 
 
 def read_bed(prefix: str):

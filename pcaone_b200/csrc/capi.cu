@@ -334,35 +334,54 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
   });
 }
 
-int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t nsamples) {
-  return guarded(c, [&] {
-    PG_REQUIRE(P && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty likelihood matrix");
-    PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 29), PCAONE_EBADARG, "likelihood matrix too large");
-    free_data(c);
-    c->generation++;
-    c->dense = true;
-    c->N = nsamples;
-    c->M = nsnps;
-    c->Npad = (uint32_t)round_up(nsamples, kRowPad);
-    c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
-    c->pitch = 1;
-    const size_t np = (size_t)nsnps * 2 * nsamples;
+}  // extern "C"
+
+namespace {
+// Likelihood pairs (FP64 or FP32 host, 2N x M column-major) -> the context's FP32 device copy.
+template <typename T>
+void load_gl_impl(pcaone_ctx* c, const T* P, uint64_t nsnps, uint32_t nsamples) {
+  PG_REQUIRE(P && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty likelihood matrix");
+  PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 29), PCAONE_EBADARG, "likelihood matrix too large");
+  free_data(c);
+  c->generation++;
+  c->dense = true;
+  c->N = nsamples;
+  c->M = nsnps;
+  c->Npad = (uint32_t)round_up(nsamples, kRowPad);
+  c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
+  c->pitch = 1;
+  const size_t np = (size_t)nsnps * 2 * nsamples;
+  c->d_P = (float*)scratch(c, "d_P", np * 4);
+  if (std::is_same<T, float>::value) {
+    PG_CUDA(cudaMemcpyAsync(c->d_P, P, np * 4, cudaMemcpyHostToDevice, c->stream));
+  } else {
     std::vector<float> pf(np);
     for (size_t t = 0; t < np; ++t) pf[t] = (float)P[t];
-    c->d_P = (float*)scratch(c, "d_P", np * 4);
     PG_CUDA(cudaMemcpyAsync(c->d_P, pf.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
-    c->d_E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
-    PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
-    c->d_F = (double*)scratch(c, "d_F", c->M * 8);
-    c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
-    c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
-    c->d_zero = (double*)scratch(c, "d_zero", c->M * 8);
-    PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
-    std::vector<double> q(c->M, 0.25);
-    PG_CUDA(cudaMemcpyAsync(c->d_F, q.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
-    PG_CUDA(cudaStreamSynchronize(c->stream));
-    c->loaded = true;
-  });
+    PG_CUDA(cudaStreamSynchronize(c->stream));  // pf goes out of scope
+  }
+  c->d_E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
+  PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
+  c->d_F = (double*)scratch(c, "d_F", c->M * 8);
+  c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
+  c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
+  c->d_zero = (double*)scratch(c, "d_zero", c->M * 8);
+  PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
+  std::vector<double> q(c->M, 0.25);
+  PG_CUDA(cudaMemcpyAsync(c->d_F, q.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+  c->loaded = true;
+}
+}  // namespace
+
+extern "C" {
+
+int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t nsamples) {
+  return guarded(c, [&] { load_gl_impl<double>(c, P, nsnps, nsamples); });
+}
+
+int pcaone_gpu_load_gl_f32(pcaone_ctx* c, const float* P, uint64_t nsnps, uint32_t nsamples) {
+  return guarded(c, [&] { load_gl_impl<float>(c, P, nsnps, nsamples); });
 }
 
 int pcaone_gpu_bed_to_gl(pcaone_ctx* c) {

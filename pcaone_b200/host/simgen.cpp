@@ -10,6 +10,10 @@
 //   * Missingness: MCAR with a global rate, or a per-sample rate ~ Beta(a, b).
 //   * Beagle: true genotypes as above, read depth ~ Poisson(depth), reads ~ Binomial with
 //     sequencing error; GL triple P(reads | g) normalised to sum 1 per sample-site.
+//   * Block LD (--ld-switch s): each population has H founder haplotypes whose alleles at SNP
+//     j are Bernoulli(p_k); every sample haplotype copies one founder of its population and
+//     switches to a uniformly drawn founder before each SNP with probability s (a Markov
+//     copying model), so nearby SNPs are correlated. Genotype = sum of two haplotypes.
 //
 // The .bed coding follows the PLINK 1 SNP-major format: magic 6c 1b 01, then per SNP
 // ceil(N/4) bytes, sample j at bits 2*(j%4) of byte j/4 (LSB first), codes
@@ -18,6 +22,10 @@
 // Usage: pcaone-sim --out PREFIX --n N --m M [--pops K] [--fst F | --fst-lo a --fst-hi b]
 //                   [--pmin a --pmax b] [--miss r | --miss-beta a,b] [--admix alpha]
 //                   [--seed s] [--beagle depth,err] [--chroms C] [--bp-spacing S]
+//                   [--ld-switch s [--founders H]] [--gl-bin]
+// --gl-bin (with --beagle): instead of the gz text, write PREFIX.gl.f32 = the first two
+// normalised likelihoods per sample and site as float32, site-major (M x 2N), the layout of
+// the reference's 2N x M column-major P, plus PREFIX.gl.bim.
 #include <omp.h>
 #include <zlib.h>
 
@@ -96,6 +104,9 @@ struct Opts {
   double depth = 0.0, err = 0.01;
   int chroms = 1;
   double bp_spacing = 100.0;  // mean spacing between SNPs (bp)
+  double ld_switch = 0.0;     // > 0: Markov haplotype-copying model
+  int founders = 40;          // founder haplotypes per population
+  bool gl_bin = false;        // binary float32 likelihood pairs instead of Beagle text
 };
 
 void die(const char* msg) {
@@ -129,6 +140,9 @@ int main(int argc, char** argv) {
     else if (a == "--beagle") { if (sscanf(val(), "%lf,%lf", &o.depth, &o.err) != 2) die("bad --beagle"); }
     else if (a == "--chroms") o.chroms = atoi(val());
     else if (a == "--bp-spacing") o.bp_spacing = atof(val());
+    else if (a == "--ld-switch") o.ld_switch = atof(val());
+    else if (a == "--founders") o.founders = atoi(val());
+    else if (a == "--gl-bin") o.gl_bin = true;
     else die(("unknown option " + a).c_str());
   }
   if (o.n < 1 || o.m < 1 || o.pops < 1) die("bad sizes");
@@ -155,12 +169,51 @@ int main(int argc, char** argv) {
 
   const long bpr = (N + 3) / 4;
   const bool beagle = o.depth > 0;
+  if (o.ld_switch > 0 && (beagle || o.admix > 0 || o.founders < 1))
+    die("--ld-switch needs PLINK output, no --admix and --founders >= 1");
   std::vector<uint8_t> bed;
   if (!beagle) bed.assign((size_t)bpr * M, 0);
-  std::vector<std::string> gl_lines(beagle ? M : 0);
+  const bool glbin = beagle && o.gl_bin;
+  std::vector<std::string> gl_lines(beagle && !glbin ? M : 0);
+  std::vector<float> glf(glbin ? (size_t)M * 2 * N : 0);
+
+  if (o.ld_switch > 0) {
+    // founder alleles: founder f of population k at SNP j, per-SNP streams
+    const long H = o.founders;
+    std::vector<uint8_t> fa((size_t)M * K * H);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long j = 0; j < M; ++j) {
+      Rng r(o.seed, (uint64_t)j + 1);
+      const double panc = o.pmin + (o.pmax - o.pmin) * r.uni();
+      for (long k = 0; k < K; ++k) {
+        const double F = fst[k];
+        double pkk = r.beta(panc * (1 - F) / F, (1 - panc) * (1 - F) / F);
+        pkk = std::min(std::max(pkk, 1e-6), 1 - 1e-6);
+        for (long f = 0; f < H; ++f) fa[((size_t)j * K + k) * H + f] = r.uni() < pkk;
+      }
+    }
+    // haplotype paths: one thread per 4 samples (one byte column of the .bed)
+    bed.assign((size_t)bpr * M, 0);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long b = 0; b < bpr; ++b) {
+      for (long i = 4 * b; i < std::min(N, 4 * b + 4); ++i) {
+        Rng r(o.seed, (uint64_t)(M + 1000 + i));
+        const long k = (i * K) / N;
+        long h0 = (long)(r.uni() * H) % H, h1 = (long)(r.uni() * H) % H;
+        for (long j = 0; j < M; ++j) {
+          if (r.uni() < o.ld_switch) h0 = (long)(r.uni() * H) % H;
+          if (r.uni() < o.ld_switch) h1 = (long)(r.uni() * H) % H;
+          const int d = fa[((size_t)j * K + k) * H + h0] + fa[((size_t)j * K + k) * H + h1];
+          const bool missing = r.uni() < srate[i];
+          const uint8_t code = missing ? 1 : (d == 2 ? 0 : (d == 1 ? 2 : 3));
+          bed[(size_t)j * bpr + b] |= (uint8_t)(code << (2 * (i & 3)));
+        }
+      }
+    }
+  }
 
 #pragma omp parallel for schedule(dynamic, 64)
-  for (long j = 0; j < M; ++j) {
+  for (long j = 0; j < (o.ld_switch > 0 ? 0 : M); ++j) {
     Rng r(o.seed, (uint64_t)j + 1);
     double panc = o.pmin + (o.pmax - o.pmin) * r.uni();
     double pk[64];
@@ -171,7 +224,7 @@ int main(int argc, char** argv) {
     }
     uint8_t* row = beagle ? nullptr : &bed[(size_t)j * bpr];
     std::string line;
-    if (beagle) {
+    if (beagle && !glbin) {
       char head[64];
       snprintf(head, sizeof head, "%d_%ld\t0\t1", 1 + (int)(j * o.chroms / M), j + 1);
       line = head;
@@ -201,12 +254,17 @@ int main(int argc, char** argv) {
         double l1 = std::pow(0.5, depth);
         double l2 = std::pow(e, na1) * std::pow(1 - e, na2);
         double s = l0 + l1 + l2;
-        char buf[96];
-        snprintf(buf, sizeof buf, "\t%.6f\t%.6f\t%.6f", l0 / s, l1 / s, l2 / s);
-        line += buf;
+        if (glbin) {
+          glf[((size_t)j * N + i) * 2] = (float)(l0 / s);
+          glf[((size_t)j * N + i) * 2 + 1] = (float)(l1 / s);
+        } else {
+          char buf[96];
+          snprintf(buf, sizeof buf, "\t%.6f\t%.6f\t%.6f", l0 / s, l1 / s, l2 / s);
+          line += buf;
+        }
       }
     }
-    if (beagle) gl_lines[j] = std::move(line);
+    if (beagle && !glbin) gl_lines[j] = std::move(line);
   }
 
   // Positions: strictly increasing within a chromosome, gaps ~ Exp(mean spacing) with a
@@ -241,6 +299,14 @@ int main(int argc, char** argv) {
     FILE* fa = fopen((o.out + ".fam").c_str(), "w");
     for (long i = 0; i < N; ++i) fprintf(fa, "fam%ld\tind%ld\t0\t0\t0\t-9\n", i + 1, i + 1);
     fclose(fa);
+  } else if (glbin) {
+    FILE* f = fopen((o.out + ".gl.f32").c_str(), "wb");
+    if (!f) die("cannot write .gl.f32");
+    fwrite(glf.data(), sizeof(float), glf.size(), f);
+    fclose(f);
+    FILE* b = fopen((o.out + ".gl.bim").c_str(), "w");
+    for (long j = 0; j < M; ++j) fprintf(b, "%d\t%d_%ld\t0\t%ld\tA\tG\n", chr[j], chr[j], j + 1, pos[j]);
+    fclose(b);
   } else {
     gzFile gz = gzopen((o.out + ".beagle.gz").c_str(), "wb1");
     if (!gz) die("cannot write .beagle.gz");

@@ -1,26 +1,34 @@
-"""Benchmark of the PCAone B200 hot path: window-based RSVD (--svd 2) of a PLINK .bed.
+"""Benchmark of the PCAone B200 hot path.
 
-Workload (default): 20,000 samples x 500,000 SNPs, 5 Balding-Nichols populations
-(Fst ~ U(0.01, 0.1) per population, ancestral allele frequency ~ U(0.01, 0.5)), HWE
-genotypes, 0.5% of entries missing completely at random; k = 20 (l = 40), 64 windows, the
-reference's default flags otherwise (maxp 20, tol 1e-4, seed 101, in-core SNP shuffle).
-Data are synthetic, generated by the package's seeded simulator.
+Default workload (config c2, the headline): window-based RSVD (--svd 2) of a PLINK .bed of
+20,000 samples x 500,000 SNPs, 5 Balding-Nichols populations (Fst ~ U(0.01, 0.1) per
+population, ancestral allele frequency ~ U(0.01, 0.5)), HWE genotypes, 0.5% of entries
+missing completely at random; k = 20 (l = 40), 64 windows, the reference's default flags
+otherwise (maxp 20, tol 1e-4, seed 101, in-core SNP shuffle). Data are synthetic, generated by
+the package's seeded simulator (pcaone_b200/bin/pcaone-sim).
 
-One step = one full top-k PCA (all power-iteration epochs) over the packed genotypes.
-  value : bed GB/s = packed .bed bytes x epochs / step time, genotypes resident in HBM,
-          device time from CUDA events on the library's stream (summed over ranks for N > 1).
-  e2e   : the same metric through the C ABI from host buffers: every step uploads the
-          packed matrix from pinned memory, permutes/transposes it on the device, runs the
-          RSVD and reads U, S, V back.
-The packed matrix (2.5 GB) is larger than L2 (126 MB), so no L2 flush is needed between steps.
+Other configurations (--config): c1 (Halko k=10 p=7, 2000 x 50000), c3 (EMU k=10 up to 50 EM
+iterations, 10000 x 200000 admixed, Beta(2,18) per-sample missingness), c4 (PCAngsd k=6 on
+genotype likelihoods, 5000 x 200000 sites, depth ~ Poisson(4), error 0.01).
 
---impl reference times the reference PCAone (built from its own sources into oracle/_ref)
-on the host cores, on a bounded sample of the same workload (all samples, a slice of SNPs).
+One step = one full run of the configuration through the C ABI with the inputs resident in
+device memory: all power-iteration epochs of one top-k PCA (c1, c2), or the whole EM loop
+(c3, c4).
+  value : c1-c3: bed GB/s = packed .bed bytes x epochs / step time; c4: GL GB/s = FP32
+          likelihood-pair bytes x likelihood passes / step time. c1, c2: device time from CUDA
+          events on the library's stream; c3, c4: host time around the EM loop, whose every
+          library call synchronises (the loop's convergence test runs on the host).
+  e2e   : the same metric from host buffers: every step uploads the inputs from pinned memory
+          (and permutes them on the device), runs the step and reads U, S, V back.
+The inputs are larger than L2 (126 MB), so no L2 flush is needed between steps.
+
+--impl reference times the reference PCAone (built from its own sources into oracle/_ref) on
+the host cores on bounded samples of the same workload (all samples, slices of SNPs); with
+several slice sizes it fits the wall time per pass and reports the rate at the full size.
 """
 from __future__ import annotations
 
 import argparse
-import re
 import json
 import os
 import shutil
@@ -28,7 +36,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -36,22 +43,42 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# CPU slices hold at least 64 x 64 SNPs: with fewer SNPs per window than windows the reference
+# winSVD fails (std::bad_alloc), so no 64-window slice is smaller than 4096 SNPs.
+BN5 = ["--pops", "5", "--fst-lo", "0.01", "--fst-hi", "0.1", "--pmin", "0.01", "--pmax", "0.5"]
 CONFIGS = {
-    "c2": dict(workload="winSVD k=20, 64 windows, 20000 samples x 500000 SNPs, 5 BN pops",
-               n=20000, m=500000, pops=5, fst=(0.01, 0.1), pmin=0.01, pmax=0.5, miss=0.005,
-               seed=2, k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_sample_snps=8000),
+    "c2": dict(kind="rsvd", workload="winSVD k=20, 64 windows, 20000 samples x 500000 SNPs, 5 BN pops",
+               n=20000, m=500000, sim=BN5 + ["--miss", "0.005", "--seed", "2"],
+               k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_fit_snps=(4096, 8192, 16384)),
     # profiling-size case of c2 (packed matrix 250 MB > L2), same shapes per window row/column
-    "c2s": dict(workload="winSVD k=20, 64 windows, 20000 samples x 50000 SNPs, 5 BN pops",
-                n=20000, m=50000, pops=5, fst=(0.01, 0.1), pmin=0.01, pmax=0.5, miss=0.005,
-                seed=2, k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_sample_snps=8000),
-    "c1": dict(workload="Halko k=10 p=7, 2000 samples x 50000 SNPs, 3 BN pops",
-               n=2000, m=50000, pops=3, fst=(0.05, 0.05), pmin=0.05, pmax=0.5, miss=0.01,
-               seed=1, k=10, svd=1, bands=64, maxp=7, tol=0.0, cpu_sample_snps=50000),
+    "c2s": dict(kind="rsvd", workload="winSVD k=20, 64 windows, 20000 samples x 50000 SNPs, 5 BN pops",
+                n=20000, m=50000, sim=BN5 + ["--miss", "0.005", "--seed", "2"],
+                k=20, svd=2, bands=64, maxp=20, tol=1e-4, cpu_fit_snps=(4096, 8192, 16384)),
+    "c1": dict(kind="rsvd", workload="Halko k=10 p=7, 2000 samples x 50000 SNPs, 3 BN pops",
+               n=2000, m=50000, sim=["--pops", "3", "--fst-lo", "0.05", "--fst-hi", "0.05", "--pmin", "0.05",
+                                     "--pmax", "0.5", "--miss", "0.01", "--seed", "1"],
+               k=10, svd=1, bands=64, maxp=7, tol=0.0, cpu_fit_snps=(50000,)),
+    "c3": dict(kind="emu", workload="EMU k=10, up to 50 EM iterations (tol-em 5e-7), 10000 samples x 200000 "
+                                    "SNPs, 4 admixed pops (Dirichlet 0.5), per-sample missing rate ~ Beta(2,18)",
+               n=10000, m=200000, sim=["--pops", "4", "--fst-lo", "0.02", "--fst-hi", "0.1", "--pmin", "0.01",
+                                       "--pmax", "0.5", "--admix", "0.5", "--miss-beta", "2,18", "--seed", "3"],
+               k=10, svd=2, bands=64, maxp=20, tol=1e-4, maxiter=50, tolem=5e-7, cpu_fit_snps=(4096, 8192)),
+    "c4": dict(kind="pcangsd", workload="PCAngsd k=6 on genotype likelihoods, 5000 samples x 200000 sites, "
+                                        "3 pops, depth ~ Poisson(4), error 0.01, unshuffled (-S)",
+               n=5000, m=200000, sim=["--pops", "3", "--fst-lo", "0.05", "--fst-hi", "0.1", "--pmin", "0.05",
+                                      "--pmax", "0.5", "--beagle", "4,0.01", "--seed", "4"],
+               k=6, svd=2, bands=64, maxp=20, tol=1e-4, maxiter=100, tolem=1e-5, cpu_fit_snps=(4096, 8192)),
 }
 
+METRIC = ("top-k PCA bed GB/s (packed .bed bytes x epochs / s), int8/BF16 tensor-core vs FP32 GPU "
+          "path at matched eigval error")
+METRIC_GL = "PCAngsd GL GB/s (FP32 likelihood-pair bytes x likelihood passes / s)"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
-
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "PCAone")
+SIM = os.path.join(ROOT, "pcaone_b200", "bin", "pcaone-sim")
+DTYPE = {"mixed": "int8 (3-piece fixed-point sketch, int32 accumulation)",
+         "bf16": "bf16 (split hi+lo sketch, fp32 accumulation)"}
 
 _T0 = time.time()
 
@@ -65,20 +92,32 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
-def make_data(cfg, out_prefix):
-    """Generate the synthetic .bed/.bim/.fam with the package simulator (cached per box)."""
-    sim = os.path.join(ROOT, "pcaone_b200", "bin", "pcaone-sim")
-    bpr = (cfg["n"] + 3) // 4
-    want = 3 + cfg["m"] * bpr
-    if os.path.exists(out_prefix + ".bed") and os.path.getsize(out_prefix + ".bed") == want:
+def workdir():
+    d = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def make_data(cfg, prefix, m=None, text_gl=False):
+    """Generate the synthetic inputs with the package simulator (cached per box). PLINK
+    configs write prefix.bed/.bim/.fam; c4 writes prefix.gl.f32 (binary likelihood pairs), or
+    prefix.beagle.gz when text_gl (the reference's input, for its CPU samples)."""
+    m = m or cfg["m"]
+    n = cfg["n"]
+    args = [SIM, "--out", prefix, "--n", str(n), "--m", str(m)] + cfg["sim"]
+    if cfg["kind"] == "pcangsd":
+        if text_gl:
+            path, want = prefix + ".beagle.gz", None
+        else:
+            path, want = prefix + ".gl.f32", m * 2 * n * 4
+            args.append("--gl-bin")
+    else:
+        path, want = prefix + ".bed", 3 + m * ((n + 3) // 4)
+    if os.path.exists(path) and (want is None or os.path.getsize(path) == want):
         return
     t = time.time()
-    subprocess.check_call([sim, "--out", out_prefix, "--n", str(cfg["n"]), "--m", str(cfg["m"]),
-                           "--pops", str(cfg["pops"]), "--fst-lo", str(cfg["fst"][0]),
-                           "--fst-hi", str(cfg["fst"][1]), "--pmin", str(cfg["pmin"]),
-                           "--pmax", str(cfg["pmax"]), "--miss", str(cfg["miss"]),
-                           "--seed", str(cfg["seed"])])
-    log(f"generated {out_prefix}.bed in {time.time() - t:.1f}s")
+    subprocess.check_call(args)
+    log(f"generated {path} in {time.time() - t:.1f}s")
 
 
 def write_sample(prefix, sample_prefix, nsnps):
@@ -99,38 +138,84 @@ def write_sample(prefix, sample_prefix, nsnps):
     return N, nsnps
 
 
-def run_reference_sample(cfg, prefix, workdir):
-    """Time the reference PCAone binary on a bounded sample; returns a cpu_baseline dict."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "PCAone")
-    if not os.path.exists(ref):
-        return None, "reference binary oracle/_ref/PCAone not built"
-    sp = os.path.join(workdir, "cpu_sample")
-    N, ms = write_sample(prefix, sp, cfg["cpu_sample_snps"])
+def reference_run(cfg, prefix, wd, nsnps):
+    """One run of the reference binary on the first nsnps SNPs (sites) of the workload, all
+    cores. Returns dict(seconds, epochs, sweeps, snps, samples, cores); raises RuntimeError."""
+    if not os.path.exists(REF_BIN):
+        raise RuntimeError("reference binary oracle/_ref/PCAone not built")
     cores = os.cpu_count() or 1
-    args = [ref, "-b", sp, "-d", str(cfg["svd"]), "-k", str(cfg["k"]), "-n", str(cores),
-            "-o", os.path.join(workdir, "cpu_out"), "-v", "1"]
-    if cfg["svd"] == 2:
-        args += ["-w", str(cfg["bands"])]
+    sp = os.path.join(wd, f"ref_sample_{cfg['kind']}_{cfg['n']}_{nsnps}")
+    kind = cfg["kind"]
+    if kind == "pcangsd":
+        make_data(cfg, sp, m=nsnps, text_gl=True)
+        N = cfg["n"]
+        args = [REF_BIN, "-G", sp + ".beagle.gz", "-k", str(cfg["k"]), "-S", "-w", str(cfg["bands"]),
+                "--maxiter", str(cfg["maxiter"]), "--tol-em", str(cfg["tolem"])]
     else:
-        args += ["-p", str(cfg["maxp"]), "--tol-rsvd", str(cfg["tol"])]
+        N, nsnps = write_sample(prefix, sp, nsnps)
+        args = [REF_BIN, "-b", sp, "-k", str(cfg["k"])]
+        if kind == "emu":
+            args += ["--emu", "-w", str(cfg["bands"]), "--maxiter", str(cfg["maxiter"]), "--tol-em", str(cfg["tolem"])]
+        elif cfg["svd"] == 2:
+            args += ["-d", "2", "-w", str(cfg["bands"])]
+        else:
+            args += ["-d", "1", "-p", str(cfg["maxp"]), "--tol-rsvd", str(cfg["tol"])]
+    args += ["-n", str(cores), "-o", os.path.join(wd, "cpu_out"), "-v", "1"]
     env = dict(os.environ, OMP_NUM_THREADS=str(cores))
     t = time.perf_counter()
-    out = subprocess.run(args, capture_output=True, text=True, env=env)
-    wall = time.perf_counter() - t
-    if out.returncode != 0:
-        return None, "reference run failed: " + out.stderr[-300:]
-    epochs = None
-    for line in out.stdout.splitlines():
+    # PCAngsd: timed from the start (text parse, allele-frequency EM, EM-PCA) to the "estimate
+    # GRM" line; the N x N Jacobi SVD after it is not part of the timed work, so the process is
+    # stopped there
+    proc = subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, env=env)
+    epochs, sweeps, lines = 0, 0, []
+    for line in proc.stdout:
+        lines.append(line)
         if "stops at epoch" in line:
-            epochs = int(line.split("=")[-1])
-    if epochs is None:
+            epochs += int(line.split("=")[-1])
+        if "individual allele frequencies estimated" in line:
+            sweeps += 1
+        if kind == "pcangsd" and "estimate GRM" in line:
+            break
+    wall = time.perf_counter() - t
+    if kind == "pcangsd":
+        proc.kill()
+    rc = proc.wait()
+    if kind != "pcangsd" and rc != 0:
+        raise RuntimeError("reference run failed: " + "".join(lines[-5:])[-300:])
+    if kind == "rsvd" and epochs == 0:
         epochs = cfg["maxp"] + 1
-    bpr = (N + 3) // 4
-    gbs = ms * bpr * epochs / wall / 1e9
-    return {"value": round(gbs, 6), "unit": "bed GB/s", "cores": cores, "kind": "reference",
-            "sample": f"{N} samples x {ms} SNPs (first SNPs of the workload), same flags, "
-                      f"{epochs} epochs, {wall:.2f} s wall",
-            "seconds": round(wall, 3), "epochs": epochs}, None
+    # likelihood passes of PCAngsd: the initial posterior and one per EM iteration
+    return {"seconds": wall, "epochs": epochs, "sweeps": sweeps + 1, "snps": nsnps, "samples": N, "cores": cores}
+
+
+def unit_bytes(cfg, nsnps):
+    """Bytes of one pass over the input: packed .bed records, or FP32 likelihood pairs."""
+    if cfg["kind"] == "pcangsd":
+        return nsnps * 2 * cfg["n"] * 4
+    return nsnps * ((cfg["n"] + 3) // 4)
+
+
+def passes_of(cfg, r):
+    return r["sweeps"] if cfg["kind"] == "pcangsd" else r["epochs"]
+
+
+def fitted_rate(cfg, runs):
+    """Rate of the metric from reference runs: with several slice sizes, wall time per pass is
+    fitted as a + b * SNPs (least squares) and evaluated at the full size; one size is used
+    as measured."""
+    passes = [passes_of(cfg, r) for r in runs]
+    x = np.array([r["snps"] for r in runs], dtype=float)
+    yp = np.array([r["seconds"] for r in runs]) / np.array(passes)
+    desc = "; ".join(f"{r['samples']} x {r['snps']}: {r['seconds']:.2f} s, {p} passes" for r, p in zip(runs, passes))
+    if len(set(x)) > 1:
+        b, a = np.polyfit(x, yp, 1)
+        value = unit_bytes(cfg, cfg["m"]) / (a + b * cfg["m"]) / 1e9
+        sample = (f"wall time per pass fitted as a + b * SNPs over [{desc}] (a = {a:.4g} s, b = {b:.4g} s/SNP) "
+                  f"and evaluated at {cfg['m']} SNPs")
+    else:
+        value = float(np.mean([unit_bytes(cfg, r["snps"]) * p / r["seconds"] for r, p in zip(runs, passes)])) / 1e9
+        sample = desc + ("" if int(x[0]) == cfg["m"] else f" (a slice of the {cfg['m']}-SNP workload)")
+    return value, sample
 
 
 class ClockSampler:
@@ -194,131 +279,164 @@ def peaks():
         return FALLBACK_PEAKS, "fallback"
 
 
-def pinned_copy(packed):
-    """The packed matrix in page-locked host memory (torch as the allocator)."""
+def pinned_copy(arr):
+    """A copy of arr in page-locked host memory (torch as the allocator)."""
     try:
         import torch
 
-        t = torch.empty(packed.size, dtype=torch.uint8, pin_memory=True)
-        a = t.numpy().reshape(packed.shape)
-        a[:] = packed
+        t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
+        a = t.numpy().view(arr.dtype).reshape(arr.shape)
+        a[:] = arr
         return a, t
     except Exception as e:  # no CUDA torch: fall back to pageable memory, say so
         log(f"pinned allocation unavailable ({e}); e2e uses pageable memory")
-        return np.ascontiguousarray(packed), None
+        return np.ascontiguousarray(arr), None
 
 
-def run_ours(args, cfg):
+def tensor_roofline(prec, l, alg_flops, prof):
+    """Roofline of the dominant decode-GEMM from one profiled run (CUDA events around every
+    decode-GEMM launch on the library's stream)."""
+    achieved = alg_flops / (prof.gemm_ms / 1e3) / 1e12
+    pk, pk_kind = peaks()
+    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    # issued tensor work per algorithmic flop: int8 issues three pieces on NP = 3 * round_up(l, 8)
+    # rounded to 16 accumulator columns at twice the BF16 rate; split BF16 issues NP = 2l -> 16
+    np8 = (3 * ((l + 7) // 8 * 8) + 15) // 16 * 16
+    npbf = (2 * l + 15) // 16 * 16
+    issued = {"mixed": np8 / l, "bf16": npbf / l}.get(prec, 1.0)
+    rate = {"mixed": 2.0, "bf16": 1.0}.get(prec, 1.0)
+    return {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak, "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "peak_source": f"{pk_kind} bf16_tflops_sustained",
+            "kernel": {"mixed": "k_decode_gemm_i8", "bf16": "k_decode_gemm_tc"}.get(prec, "k_decode_gemm (SIMT)"),
+            "launches": prof.gemm_launches, "avg_launch_ms": round(prof.gemm_ms / max(prof.gemm_launches, 1), 5),
+            "algorithmic_flops_per_launch": alg_flops / max(prof.gemm_launches, 1),
+            "issued_ops_factor": round(issued, 4), "ceiling_frac_of_bf16_peak": round(rate / issued, 4),
+            "gemm_share_of_step": round(prof.gemm_ms / prof.gpu_ms, 4),
+            "step_breakdown_ms": {"gemm": round(prof.gemm_ms, 2), "epilogues": round(prof.epilogue_ms, 2),
+                                  "omega_updates": round(prof.update_ms, 2), "epoch_tail": round(prof.tail_ms, 2),
+                                  "total": round(prof.gpu_ms, 2)}}
+
+
+def subspace_err(Ua, Sa, Ub, Sb, k=None):
+    """Largest eigenvalue relative error and largest principal angle of the first k PCs."""
+    k = k or len(Sa)
+    e = np.abs(Sa[:k] ** 2 / Sb[:k] ** 2 - 1)
+    q1, _ = np.linalg.qr(Ua[:, :k])
+    q2, _ = np.linalg.qr(Ub[:, :k])
+    ang = float(np.arccos(np.clip(np.linalg.svd(q1.T @ q2, compute_uv=False), -1, 1)).max())
+    return float(e.max()), ang
+
+
+class Run:
+    """Process-group plumbing shared by the configurations (replicas, max over ranks)."""
+
+    def __init__(self):
+        self.rank, self.world, self.local = dist_env()
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([x], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+def prepare(cfg, config, run):
+    wd = workdir()
+    prefix = os.path.join(wd, config)
+    if run.rank == 0:
+        make_data(cfg, prefix)
+    run.barrier()
+    log("data ready")
+    return wd, prefix
+
+
+def run_rsvd_cfg(args, cfg, run):
     import pcaone_b200 as pb
 
-    rank, world, local = dist_env()
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
-    os.makedirs(workdir, exist_ok=True)
-    prefix = os.path.join(workdir, args.config)
-    if rank == 0:
-        make_data(cfg, prefix)
-    barrier()
-    log("data ready")
+    wd, prefix = prepare(cfg, args.config, run)
     packed, N, M = pb.read_bed(prefix)
-    bpr = (N + 3) // 4
-    bed_bytes = M * bpr
+    bed_bytes = M * ((N + 3) // 4)
     perm = pb.shuffle_perm(M) if cfg["svd"] == 2 else None
-    log("bed read into host memory")
     rs_kw = dict(k=cfg["k"], oversamples=10, maxp=cfg["maxp"], svd=cfg["svd"], bands=cfg["bands"],
                  tol=cfg["tol"], seed=101)
-
-    ctx = pb.GpuContext(local)
+    ctx = pb.GpuContext(run.local)
     ctx.load_bed(packed, N)
     if perm is not None:
         ctx.permute(perm)
     prec = args.precision
     log("loaded and permuted on the device")
-    # warm-up (also builds the transposed copy and missing-entry lists once)
-    for _ in range(args.warmup):
+    for _ in range(args.warmup):  # also builds the transposed copy and missing-entry lists once
         r = ctx.rsvd(precision=prec, **rs_kw)
         log(f"warm-up step: {r.gpu_ms:.1f} ms, {r.epochs} epochs, {r.kernel_launches} launches")
-    barrier()
-    with ClockSampler(local) as clk:
-        barrier()
-        res = []
-        for _ in range(args.steps):
-            res.append(ctx.rsvd(precision=prec, **rs_kw))
-        barrier()
+    run.barrier()
+    with ClockSampler(run.local) as clk:
+        run.barrier()
+        res = [ctx.rsvd(precision=prec, **rs_kw) for _ in range(args.steps)]
+        run.barrier()
     clocks = clk.summary()
     log(f"timed steps: {[round(r.gpu_ms, 2) for r in res]} ms")
-    step_ms = [r.gpu_ms for r in res]
     epochs = res[-1].epochs
-    ms_per_step = sum(step_ms) / len(step_ms)
-    # max over ranks of the per-step time
-    if dist:
-        import torch
+    ms_per_step = run.max_over_ranks(sum(r.gpu_ms for r in res) / len(res))
+    value = bed_bytes * epochs / (ms_per_step / 1e3) / 1e9 * run.world
 
-        t = torch.tensor([ms_per_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step = float(t.item())
-    gbs_rank = bed_bytes * epochs / (ms_per_step / 1e3) / 1e9
-    value = gbs_rank * world
-
-    # one profiled run: per-launch times of the decode-GEMM kernels (roofline)
     prof = ctx.rsvd(precision=prec, profile=True, **rs_kw)
     log(f"profiled step: gemm {prof.gemm_ms:.1f} of {prof.gpu_ms:.1f} ms over {prof.gemm_launches} launches; "
         f"epilogue {prof.epilogue_ms:.1f}, updates {prof.update_ms:.1f}, epoch tail {prof.tail_ms:.1f}")
     l = cfg["k"] + max(10, cfg["k"])
-    alg_flops = 4.0 * M * N * l * prof.epochs  # two products per epoch, 2*M*N*l each
-    gemm_avg_ms = prof.gemm_ms / max(prof.gemm_launches, 1)
-    achieved_tflops = alg_flops / (prof.gemm_ms / 1e3) / 1e12
-    pk, pk_kind = peaks()
-    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
-    traffic = None  # DRAM bytes per launch from the committed ncu summary of this kernel
-    tpath = os.path.join(ROOT, "profiles", "k_decode_gemm_tc_c2.md")
-    if prec == "mixed" and args.config == "c2" and os.path.exists(tpath):
-        with open(tpath) as f:
-            mt = re.search(r"^traffic_bytes_per_launch:\s*([0-9]+)", f.read(), re.M)
-        traffic = int(mt.group(1)) if mt else None
-    roofline = {"bound": "tensor", "achieved": round(achieved_tflops, 2), "peak": peak,
-                "unit": "TFLOP/s", "frac": round(achieved_tflops / peak, 4), "traffic": traffic,
-                "peak_source": f"{pk_kind} bf16_tflops_sustained",
-                "kernel": "k_decode_gemm_tc" if prec == "mixed" else "k_decode_gemm (SIMT)",
-                "launches": prof.gemm_launches, "avg_launch_ms": round(gemm_avg_ms, 5),
-                "algorithmic_flops_per_launch": alg_flops / max(prof.gemm_launches, 1),
-                "issued_flops_factor": 2.0 if prec == "mixed" else 1.0,
-                "gemm_share_of_step": round(prof.gemm_ms / prof.gpu_ms, 4),
-                "step_breakdown_ms": {"gemm": round(prof.gemm_ms, 2), "epilogues": round(prof.epilogue_ms, 2),
-                                      "omega_updates": round(prof.update_ms, 2),
-                                      "epoch_tail": round(prof.tail_ms, 2), "total": round(prof.gpu_ms, 2)}}
+    roofline = tensor_roofline(prec, l, 4.0 * M * N * l * prof.epochs, prof)
 
-    # comparison runs: the plain FP32 GPU path and the FP64 algorithm-matched path
-    acc = {}
-    fp32_ms = None
+    acc, extra = {}, {}
     if not args.skip_compare:
-        r32 = ctx.rsvd(precision="fp32", **rs_kw)
-        fp32_ms = r32.gpu_ms
-        log(f"fp32 path: {r32.gpu_ms:.1f} ms")
-        r64 = ctx.rsvd(precision="fp64", **rs_kw)
-        log(f"fp64 path: {r64.gpu_ms:.1f} ms")
-        e64 = r64.S ** 2
-        for name, r in (("mixed" if prec == "mixed" else prec, res[-1]), ("fp32", r32)):
-            e = r.S ** 2
-            q1, _ = np.linalg.qr(r.U)
-            q2, _ = np.linalg.qr(r64.U)
-            ang = float(np.arccos(np.clip(np.linalg.svd(q1.T @ q2, compute_uv=False), -1, 1)).max())
-            acc[name] = {"eig_rel_err_vs_fp64": float(np.max(np.abs(e / e64 - 1))),
-                         "max_principal_angle_vs_fp64": ang, "epochs": r.epochs}
-        acc["fp64_epochs"] = r64.epochs
+        comp = {}
+        for p2 in ("fp32", "bf16", "fp64"):
+            if p2 != prec:
+                comp[p2] = ctx.rsvd(precision=p2, **rs_kw)
+                log(f"{p2} path: {comp[p2].gpu_ms:.1f} ms")
+        r64 = comp.get("fp64", res[-1])
+        runs = [(prec, res[-1])] + [(k2, v) for k2, v in comp.items() if k2 != "fp64"]
+        for name, r in runs:
+            e, a = subspace_err(r.U, r.S, r64.U, r64.S)
+            acc[name] = {"eig_rel_err_vs_fp64": e, "max_principal_angle_vs_fp64": a, "epochs": r.epochs}
+        # dense FP64 oracle for the population PCs (well separated from the noise): an FP64
+        # Halko sketch of width 40 iterated for 40 epochs on the whole matrix
+        pops = int(cfg["sim"][cfg["sim"].index("--pops") + 1])
+        g = max(1, pops - 1)
+        dense = ctx.rsvd(precision="fp64", k=max(cfg["k"], g), oversamples=40 - max(cfg["k"], g), maxp=39,
+                         svd=1, tol=0.0, seed=7, want_v=False)
+        log(f"dense FP64 reference for PCs 1-{g}: {dense.gpu_ms:.1f} ms")
+        for name, r in runs + [("fp64", r64)]:
+            e, a = subspace_err(r.U, r.S, dense.U, dense.S, g)
+            acc.setdefault(name, {}).update({f"eig_rel_err_pcs1_{g}_vs_dense_fp64": e,
+                                             f"max_angle_pcs1_{g}_vs_dense_fp64": a})
+        for p2 in ("fp32", "bf16"):
+            if p2 in comp:
+                extra[f"{p2}_path_ms"] = round(comp[p2].gpu_ms, 3)
+        if "fp32" in comp:
+            extra["speedup_vs_fp32_path"] = round(comp["fp32"].gpu_ms / ms_per_step, 3)
 
-    # e2e: host buffers -> device -> PCA -> host, through the C ABI
+    # e2e: pinned host buffers -> device -> PCA -> host, through the C ABI
     pinned, keep = pinned_copy(packed)
     e2e_t = []
     for i in range(max(1, min(args.steps, 3)) + 1):
@@ -328,94 +446,247 @@ def run_ours(args, cfg):
             ctx.permute(perm)
         r = ctx.rsvd(precision=prec, **rs_kw)
         t1 = time.perf_counter()
-        if i > 0:  # first is warm-up (allocations)
+        if i > 0:  # the first is a warm-up (allocations)
             e2e_t.append(t1 - t0)
-    e2e_s = sum(e2e_t) / len(e2e_t)
     log(f"e2e steps: {[round(x, 3) for x in e2e_t]} s")
-    if dist:
-        import torch
-
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": round(bed_bytes * r.epochs / e2e_s / 1e9 * world, 4), "unit": "bed GB/s",
+    e2e_s = run.max_over_ranks(sum(e2e_t) / len(e2e_t))
+    e2e = {"value": round(bed_bytes * r.epochs / e2e_s / 1e9 * run.world, 4), "unit": "bed GB/s",
            "h2d_bytes_per_step": int(bed_bytes + (perm.nbytes if perm is not None else 0)),
-           "d2h_bytes_per_step": int((N + M + 1) * cfg["k"] * 8),
-           "seconds_per_pca": round(e2e_s, 4)}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu, why = run_reference_sample(cfg, prefix, workdir)
-        log(f"cpu baseline: {cpu}")
-        if cpu is None:
-            cpu = {"value": None, "unavailable": why}
+           "d2h_bytes_per_step": int((N + M + 1) * cfg["k"] * 8), "seconds_per_pca": round(e2e_s, 4)}
+    launches = int(res[-1].kernel_launches)
     ctx.close()
-    if dist:
-        dist.destroy_process_group()
-    if rank != 0:
+    cpu = cpu_baseline(args, cfg, prefix, wd, run)
+    run.close()
+    if run.rank != 0:
         return
+    emit(args, cfg, run, value, "bed GB/s", ms_per_step, prec, clocks, roofline, e2e, cpu, launches,
+         {"samples": N, "snps": M, "k": cfg["k"], "oversamples": max(10, cfg["k"]),
+          "windows": cfg["bands"] if cfg["svd"] == 2 else 1, "svd": cfg["svd"], "epochs": epochs},
+         dict(extra, pca_seconds=round(ms_per_step / 1e3, 5), accuracy=acc))
+
+
+def run_emu_cfg(args, cfg, run):
+    import pcaone_b200 as pb
+
+    wd, prefix = prepare(cfg, args.config, run)
+    packed, N, M = pb.read_bed(prefix)
+    bed_bytes = M * ((N + 3) // 4)
+    perm = pb.shuffle_perm(M)
+    kw = dict(k=cfg["k"], svd=2, bands=cfg["bands"], maxp=cfg["maxp"], tol=cfg["tol"], maxiter=cfg["maxiter"],
+              tolem=cfg["tolem"])
+    prec = args.precision
+    ctx = pb.GpuContext(run.local)
+    ctx.load_bed(packed, N)
+    ctx.permute(perm)
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        out = pb.emu_loop(ctx, precision=prec, **kw)
+        log(f"warm-up EMU: {time.perf_counter() - t0:.2f} s, {out[4]} iterations, {out[5]} epochs")
+    run.barrier()
+    times, outs = [], []
+    with ClockSampler(run.local) as clk:
+        run.barrier()
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            outs.append(pb.emu_loop(ctx, precision=prec, **kw))
+            times.append(time.perf_counter() - t0)
+        run.barrier()
+    clocks = clk.summary()
+    log(f"timed EMU runs: {[round(t, 3) for t in times]} s")
+    sec = run.max_over_ranks(sum(times) / len(times))
+    eig, S, U, V, it, epochs = outs[-1]
+    value = bed_bytes * epochs / sec / 1e9 * run.world
+    # roofline of the decode-GEMM inside the EM loop: one profiled RSVD with the imputed values
+    # of the final factors active
+    ctx.fit_emu(U, S, V, True)
+    l = cfg["k"] + max(10, cfg["k"])
+    prof = ctx.rsvd(k=cfg["k"], maxp=cfg["maxp"], svd=2, bands=cfg["bands"], tol=cfg["tol"], precision=prec,
+                    standardize=False, carry=True, profile=True)
+    ctx.clear_imputed()
+    roofline = tensor_roofline(prec, l, 4.0 * M * N * l * prof.epochs, prof)
+    acc = {}
+    if not args.skip_compare:
+        o64 = pb.emu_loop(ctx, precision="fp64", **kw)
+        e, a = subspace_err(U, S, o64[2], o64[1])
+        acc = {prec: {"eig_rel_err_vs_fp64": e, "max_principal_angle_vs_fp64": a, "iterations": it},
+               "fp64_iterations": o64[4]}
+    pinned, keep = pinned_copy(packed)
+    e2e_t = []
+    for i in range(2):
+        t0 = time.perf_counter()
+        ctx.load_bed(pinned, N)
+        ctx.permute(perm)
+        o = pb.emu_loop(ctx, precision=prec, **kw)
+        if i > 0:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = run.max_over_ranks(e2e_t[0])
+    e2e = {"value": round(bed_bytes * o[5] / e2e_s / 1e9 * run.world, 4), "unit": "bed GB/s",
+           "h2d_bytes_per_step": int(bed_bytes + perm.nbytes), "d2h_bytes_per_step": int((N + M + 1) * cfg["k"] * 8),
+           "seconds_per_emu": round(e2e_s, 3)}
+    ctx.close()
+    cpu = cpu_baseline(args, cfg, prefix, wd, run)
+    run.close()
+    if run.rank != 0:
+        return
+    emit(args, cfg, run, value, "bed GB/s", sec * 1e3, prec, clocks, roofline, e2e, cpu, None,
+         {"samples": N, "snps": M, "k": cfg["k"], "windows": cfg["bands"], "em_iterations": it,
+          "epochs_total": epochs},
+         {"emu_seconds": round(sec, 4), "accuracy": acc,
+          "timing": "host clock around the EM loop (every library call synchronises)"})
+
+
+def run_pcangsd_cfg(args, cfg, run):
+    import pcaone_b200 as pb
+
+    wd, prefix = prepare(cfg, args.config, run)
+    N, M = cfg["n"], cfg["m"]
+    P = np.fromfile(prefix + ".gl.f32", dtype=np.float32).reshape(M, 2 * N)  # = 2N x M column-major
+    gl_bytes = P.nbytes
+    k, bands = cfg["k"], cfg["bands"]
+    ident = np.arange(M, dtype=np.int32)
+    ctx = pb.GpuContext(run.local)
+    ctx.load_gl(P.T)
+    log("likelihoods loaded")
+
+    def step():
+        F, it_maf = ctx.gl_freq(cfg["maxiter"], 1e-6)
+        ctx.gl_update()
+        out = pb._pcangsd_em(ctx, ident, F, k, 2, bands, cfg["maxp"], 10, cfg["tol"], cfg["maxiter"],
+                             cfg["tolem"], 101, 1, True, False)
+        return out, it_maf
+
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        out, itm = step()
+        log(f"warm-up PCAngsd: {time.perf_counter() - t0:.2f} s, {out[4]} EM iterations, {itm} MAF sweeps")
+    run.barrier()
+    times = []
+    with ClockSampler(run.local) as clk:
+        run.barrier()
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            out, itm = step()
+            times.append(time.perf_counter() - t0)
+        run.barrier()
+    clocks = clk.summary()
+    log(f"timed PCAngsd runs: {[round(t, 3) for t in times]} s")
+    sec = run.max_over_ranks(sum(times) / len(times))
+    # likelihood passes counted as for the reference: the initial posterior and one posterior
+    # per EM iteration (the allele-frequency EM sweeps are timed but not counted)
+    passes = 1 + out[4]
+    value = gl_bytes * passes / sec / 1e9 * run.world
+    # HBM roofline of the posterior kernel: P read (8 N bytes a site) + E write (4 Npad bytes)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ctx.gl_update(out[2], out[1], out[3])
+    upd_s = (time.perf_counter() - t0) / reps
+    npad = (N + 255) // 256 * 256
+    alg = M * (8 * N + 4 * npad)
+    pk, pk_kind = peaks()
+    roofline = {"bound": "hbm", "achieved": round(alg / upd_s / 1e9, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(alg / upd_s / 1e9 / pk["hbm_gbs"], 4), "traffic": None,
+                "peak_source": f"{pk_kind} hbm_gbs",
+                "kernel": "k_posterior_e (one pcaone_gpu_gl_update call, host clock incl. the factor upload)",
+                "algorithmic_bytes_per_launch": alg, "avg_call_ms": round(upd_s * 1e3, 3)}
+    pinned, keep = pinned_copy(P)
+    e2e_t = []
+    for i in range(2):
+        t0 = time.perf_counter()
+        ctx.load_gl(pinned.T)
+        o, _ = step()
+        if i > 0:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = run.max_over_ranks(e2e_t[0])
+    e2e = {"value": round(gl_bytes * passes / e2e_s / 1e9 * run.world, 4), "unit": "GL GB/s",
+           "h2d_bytes_per_step": int(gl_bytes), "d2h_bytes_per_step": int((N + M + 1) * k * 8),
+           "seconds_per_pcangsd": round(e2e_s, 3)}
+    ctx.close()
+    cpu = cpu_baseline(args, cfg, prefix, wd, run)
+    run.close()
+    if run.rank != 0:
+        return
+    emit(args, cfg, run, value, "GL GB/s", sec * 1e3, "fp32", clocks, roofline, e2e, cpu, None,
+         {"samples": N, "sites": M, "k": k, "windows": bands, "em_iterations": out[4], "maf_sweeps": itm,
+          "likelihood_passes": passes},
+         {"pcangsd_seconds": round(sec, 4),
+          "timing": "host clock around the EM loop (every library call synchronises)"}, metric=METRIC_GL)
+
+
+def cpu_baseline(args, cfg, prefix, wd, run):
+    if run.rank != 0 or run.world != 1 or args.skip_cpu:
+        return None
+    try:
+        runs = [reference_run(cfg, prefix, wd, s) for s in cfg["cpu_fit_snps"]]
+    except RuntimeError as e:
+        return {"value": None, "unavailable": str(e)}
+    value, sample = fitted_rate(cfg, runs)
+    cpu = {"value": round(value, 6), "unit": "GL GB/s" if cfg["kind"] == "pcangsd" else "bed GB/s",
+           "cores": runs[0]["cores"], "kind": "reference", "sample": sample}
+    log(f"cpu baseline: {cpu}")
+    return cpu
+
+
+def emit(args, cfg, run, value, unit, ms_per_step, prec, clocks, roofline, e2e, cpu, launches, conf, extra,
+         metric=METRIC):
     line = {
-        "metric": "top-k PCA bed GB/s (packed .bed bytes x epochs / s), mixed BF16 vs FP32 GPU path",
-        "value": round(value, 4), "unit": "bed GB/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
-        "pca_seconds": round(ms_per_step / 1e3, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if prec == "mixed" else prec,
-        "data": "synthetic (seeded Balding-Nichols simulator)",
-        "config": {"workload": cfg["workload"], "samples": N, "snps": M, "k": cfg["k"],
-                   "oversamples": max(10, cfg["k"]), "windows": cfg["bands"] if cfg["svd"] == 2 else 1,
-                   "svd": cfg["svd"], "epochs": epochs, "precision": prec,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs (2.5 GB packed) larger than L2; no flush needed"},
-        "fp32_path_ms": round(fp32_ms, 3) if fp32_ms else None,
-        "speedup_vs_fp32_path": round(fp32_ms / ms_per_step, 3) if fp32_ms else None,
-        "accuracy": acc, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
-        "gpu_launches": int(res[-1].kernel_launches), "clocks": clocks,
+        "metric": metric, "value": round(value, 4), "unit": unit, "n_gpus": run.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE.get(prec, prec),
+        "data": "synthetic (seeded simulator: " + " ".join(cfg["sim"]) + ")",
+        "config": dict({"workload": cfg["workload"]}, **conf, precision=prec,
+                       parallelism=f"replicas x{run.world}",
+                       l2="inputs larger than L2 (126 MB); no flush needed"),
     }
+    line.update(extra)
+    line.update({"roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks})
+    if launches is not None:
+        line["gpu_launches"] = launches
     print(json.dumps(line), flush=True)
 
 
 def run_reference_arm(args, cfg):
+    """The reference PCAone on the host cores, rank 0 only: W + K runs on slices of the
+    workload cycling through the configured sizes, the rate fitted over the K timed runs and
+    evaluated at the full size (one size: its own rate)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
-    os.makedirs(workdir, exist_ok=True)
-    prefix = os.path.join(workdir, args.config)
+    wd = workdir()
+    prefix = os.path.join(wd, args.config)
     make_data(cfg, prefix)
-    vals = []
-    info = None
+    sizes = list(cfg["cpu_fit_snps"])
+    runs = []
+    t_start = time.perf_counter()
     for i in range(args.warmup + args.steps):
-        cpu, why = run_reference_sample(cfg, prefix, workdir)
-        if cpu is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
+        try:
+            r = reference_run(cfg, prefix, wd, sizes[i % len(sizes)])
+        except RuntimeError as e:
+            print(json.dumps({"impl": "reference", "unavailable": str(e)}))
             return
         if i >= args.warmup:
-            vals.append(cpu["value"])
-            info = cpu
-        if args.warmup + args.steps > 2 and i == 0 and cpu["seconds"] > 60:
+            runs.append(r)
+        if time.perf_counter() - t_start > 240 and len(runs) >= len(sizes):
             break  # keep the arm within a few minutes
-    v = sum(vals) / len(vals) if vals else info["value"]
+    v, sample = fitted_rate(cfg, runs)
+    unit = "GL GB/s" if cfg["kind"] == "pcangsd" else "bed GB/s"
     print(json.dumps({
-        "impl": "reference", "metric": "top-k PCA bed GB/s (packed .bed bytes x epochs / s), "
-        "mixed BF16 vs FP32 GPU path", "value": round(v, 6), "unit": "bed GB/s", "n_gpus": world,
-        "steps": len(vals), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "dtype": "f64", "data": "synthetic (seeded Balding-Nichols simulator)",
-        "config": {"workload": cfg["workload"], "sample": info["sample"]},
-        "cpu_baseline": {"value": round(v, 6), "unit": "bed GB/s", "cores": info["cores"],
-                         "kind": "reference", "sample": info["sample"]},
-        "e2e": {"value": round(v, 6), "unit": "bed GB/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0}}), flush=True)
+        "impl": "reference", "metric": METRIC_GL if cfg["kind"] == "pcangsd" else METRIC, "value": round(v, 6),
+        "unit": unit, "n_gpus": world, "steps": len(runs), "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "dtype": "f64", "data": "synthetic (seeded simulator: " + " ".join(cfg["sim"]) + ")",
+        "config": {"workload": cfg["workload"], "sample": f"{len(runs)} timed runs; " + sample},
+        "cpu_baseline": {"value": round(v, 6), "unit": unit, "cores": runs[0]["cores"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(v, 6), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
 def run_profile_kernel(args, cfg):
     """Smallest command for ncu: one standardised product Z^T Omega through the C ABI on the
-    configured matrix (the mixed path launches the tcgen05 decode-GEMM once), then exit. No
+    configured matrix (the tensor-core paths launch their decode-GEMM once), then exit. No
     child processes, no torch."""
     import pcaone_b200 as pb
 
-    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
-    os.makedirs(workdir, exist_ok=True)
-    prefix = os.path.join(workdir, args.config)
+    prefix = os.path.join(workdir(), args.config)
     make_data(cfg, prefix)
     packed, N, M = pb.read_bed(prefix)
     l = cfg["k"] + max(10, cfg["k"])
@@ -433,9 +704,7 @@ def run_profile_step(args, cfg):
     (load, shuffle, then the full power iteration), then exit. No child processes, no torch."""
     import pcaone_b200 as pb
 
-    workdir = os.environ.get("PCAONE_BENCH_DIR", os.path.join(tempfile.gettempdir(), "pcaone_bench"))
-    os.makedirs(workdir, exist_ok=True)
-    prefix = os.path.join(workdir, args.config)
+    prefix = os.path.join(workdir(), args.config)
     make_data(cfg, prefix)
     packed, N, M = pb.read_bed(prefix)
     rs_kw = dict(k=cfg["k"], oversamples=10, maxp=cfg["maxp"], svd=cfg["svd"], bands=cfg["bands"],
@@ -457,7 +726,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "bf16", "fp32", "fp64"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-compare", action="store_true")
     ap.add_argument("--profile-kernel", action="store_true",
@@ -473,7 +742,8 @@ def main():
     elif args.impl == "reference":
         run_reference_arm(args, cfg)
     else:
-        run_ours(args, cfg)
+        run = Run()
+        {"rsvd": run_rsvd_cfg, "emu": run_emu_cfg, "pcangsd": run_pcangsd_cfg}[cfg["kind"]](args, cfg, run)
 
 
 if __name__ == "__main__":

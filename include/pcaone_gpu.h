@@ -137,6 +137,14 @@ int pcaone_gpu_rsvd(pcaone_ctx* ctx, const pcaone_rsvd_opts* opts, double* U, do
 int pcaone_gpu_product(pcaone_ctx* ctx, int precision, int transpose, int standardize,
                        int ploidy, const double* B, uint32_t ncols, double* out);
 
+/* Y = Z (Z^T X) for X (nsamples x ncols, column-major FP64 host), Y the same shape: the
+ * matrix operation of the IRAM solver, ArnoldiOpData::perform_op (src/Arnoldi.cpp:18-46),
+ * summed over the whole matrix as one block. Both decode-GEMMs and their centring/missing-
+ * entry epilogues run back to back on the device (Z^T X never leaves it); Z, precision,
+ * standardize and ploidy as for pcaone_gpu_product; ncols <= 64. */
+int pcaone_gpu_gram_product(pcaone_ctx* ctx, int precision, int standardize, int ploidy,
+                            const double* X, uint32_t ncols, double* Y);
+
 /* EMU imputation step, Data::fit_with_pi EMU branch (src/Data.cpp:272-287): every missing
  * genotype of the loaded matrix takes the centred value
  *   e_ij = clip(sum_t U_it S_t V_jt, -F_j, 1 - F_j)

@@ -30,7 +30,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
-           "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32"]
+           "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product"]
 
 
 class PcaoneError(RuntimeError):
@@ -89,6 +89,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
         L.pcaone_gpu_load_gl_f32.argtypes = [vp, vp, u64, u32]
+        L.pcaone_gpu_gram_product.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, u32, vp]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
@@ -234,6 +235,25 @@ GpuContext.product_t.__doc__ = "Z^T B (nsnps x ncols) for B nsamples x ncols."
 GpuContext.product = lambda self, B, precision=PREC_FP64, standardize=True, ploidy=2: \
     _product(self, B, 1, precision, standardize, ploidy)
 GpuContext.product.__doc__ = "Z B (nsamples x ncols) for B nsnps x ncols."
+
+
+def _gram_product(self, X, precision=PREC_FP64, standardize=True, ploidy=2):
+    """Z (Z^T X) (nsamples x ncols) for X nsamples x ncols, on the device in one call."""
+    if isinstance(precision, str):
+        precision = PRECISIONS[precision]
+    X = np.asarray(X, dtype=np.float64)
+    if X.ndim == 1:
+        X = X[:, None]
+    if X.shape[0] != self.N:
+        raise ValueError(f"X must have {self.N} rows")
+    Xc = np.asfortranarray(X)
+    Y = np.zeros(X.shape, order="F")
+    self._check(lib().pcaone_gpu_gram_product(self._h, precision, int(standardize), ploidy, _ptr(Xc),
+                                              X.shape[1], _ptr(Y)))
+    return np.ascontiguousarray(Y)
+
+
+GpuContext.gram_product = _gram_product
 
 
 def _fit_emu(self, U, S, V, reference_index=True):

@@ -516,6 +516,84 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
   }
 }
 
+// Y = Z (Z^T X) on the device: the first product and its epilogue give G = Z^T X and the
+// window operand s/2 G, which the second product and its epilogue turn into Z G, with no host
+// round trip between the two (the matrix operation of ArnoldiOpData::perform_op,
+// src/Arnoldi.cpp:18-46, over the whole matrix as one window).
+template <typename T>
+void gram_t(pcaone_ctx* c, GemmFnT<T> gemm, const double* X, int l, double* Y) {
+  const int N = (int)c->N;
+  const int64_t M = (int64_t)c->M, Npad = c->Npad;
+  auto d = [&](const char* name, size_t n) { return (double*)scratch(c, name, n * sizeof(double)); };
+  double* G = d("r_G", (size_t)c->Mpad * l);
+  double* H = d("r_H", Npad * l);
+  double* Bd = d("r_omg", Npad * l);
+  double* wsum = d("r_wsum", l);
+  double* h0 = d("r_h0", l);
+  T* B2 = (T*)scratch(c, "r_B2", (size_t)round_up(c->win.blocksize, 256) * l * sizeof(T));
+  std::vector<double> rm((size_t)Npad * l, 0.0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < l; ++j) rm[(size_t)i * l + j] = X[(size_t)j * N + i];
+  PG_CUDA(cudaMemcpyAsync(Bd, rm.data(), rm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  T* BT = std::is_same<T, double>::value ? reinterpret_cast<T*>(Bd) : (T*)scratch(c, "r_omgT", Npad * l * sizeof(T));
+  std::vector<float> f;
+  if (!std::is_same<T, double>::value) {
+    f.assign(rm.begin(), rm.end());
+    PG_CUDA(cudaMemcpyAsync(BT, f.data(), f.size() * 4, cudaMemcpyHostToDevice, c->stream));
+  }
+  colsum(c, Bd, l, N, wsum);
+  gemm.omega_changed(c, Bd, l, Npad);
+  const int ks1 = gemm.ksplit(c, M, N, l);
+  T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * M * l * sizeof(T));
+  gemm.p1(c, c->d_bed, c->pitch, 0, M, N, BT, l, ks1, D1);
+  EpiP1 p1;
+  p1.start = 0; p1.m = M; p1.l = l; p1.ksplit = ks1;
+  p1.F = c->d_F; p1.scale = c->d_scale; p1.wsum = wsum; p1.omega = Bd; p1.miss_ptr = c->d_miss_snp_ptr;
+  p1.miss_idx = c->d_miss_snp_idx; p1.miss_val = c->imputed ? c->d_miss_snp_val : nullptr; p1.G = G;
+  if (gemm.b2_bt) p1.bt2 = gemm.b2_bt(c, l, &p1.kpad2, &p1.bt_half);
+  if (gemm.b2_qmax) p1.qmax = gemm.b2_qmax(c, l);
+  launch_prep<T>(c, p1, D1, B2, h0);
+  if (!p1.bt2) gemm.b2_ready(c, B2, l, M);
+  const int ks2 = gemm.ksplit(c, N, M, l);
+  T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
+  gemm.p2(c, c->d_bedT, c->win.pitch, 0, N, M, B2, l, ks2, D2);
+  zero(c, H, Npad * l);
+  EpiP2 p2;
+  p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks2;
+  p2.F = c->d_F; p2.scale = c->d_scale; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
+  p2.miss_idx = c->d_miss_ws_idx; p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr; p2.H = H;
+  launch_accum<T>(c, p2, D2);
+  rm.resize((size_t)N * l);
+  PG_CUDA(cudaMemcpyAsync(rm.data(), H, rm.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  PG_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < l; ++j) Y[(size_t)j * N + i] = rm[(size_t)i * l + j];
+}
+
+void run_gram(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X, int l, double* Y) {
+  PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
+  PG_REQUIRE(X && Y && l >= 1 && l <= kLmax, PCAONE_EBADARG, "bad gram-product operands");
+  PG_REQUIRE(ploidy == 1 || ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
+  PG_REQUIRE(!c->dense, PCAONE_ESTATE, "products need packed genotypes (load_bed)");
+  build_transposed(c, 1);
+  build_missing_by_snp(c);
+  build_missing_by_window_sample(c);
+  if (c->imputed) compute_imputed_ws(c);
+  compute_scale(c, standardize, ploidy);
+  if (precision == PCAONE_PREC_FP64) {
+    gram_t<double>(c, gemm_simt_double(), X, l, Y);
+  } else if (precision == PCAONE_PREC_FP32) {
+    gram_t<float>(c, gemm_simt_float(), X, l, Y);
+  } else if (precision == PCAONE_PREC_MIXED || precision == PCAONE_PREC_BF16) {
+    PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
+    tc_clear_error(c);
+    gram_t<float>(c, precision == PCAONE_PREC_MIXED ? gemm_i8() : gemm_tc(), X, l, Y);
+    tc_check_error(c);
+  } else {
+    throw Error(PCAONE_EBADARG, "unknown precision");
+  }
+}
+
 void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
                  const double* B, int l, double* out) {
   PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");

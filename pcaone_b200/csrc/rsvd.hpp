@@ -52,6 +52,7 @@ void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);
 void jacobi_svd(int n, const double* A, double* U, double* s, double* V);
 void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
                  const double* B, int l, double* out);
+void run_gram(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X, int l, double* Y);
 void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, double* V,
               pcaone_rsvd_report* rep);
 

@@ -2,8 +2,9 @@
 // files as the reference CLI (src/Cmd.cpp:28-111, src/Main.cpp:44-165) for the modes this
 // build covers, with all compute going through the C ABI in include/pcaone_gpu.h.
 //
-// Covered: PLINK input (-b) with --svd 1 (Halko) and --svd 2 (winSVD, in-core shuffle unless
-// -S), -k, -p, -w/--batches/--windows, --oversamples, --seed, --rand, --tol-rsvd, --maf,
+// Covered: PLINK input (-b) with --svd 0 (IRAM: restarted Lanczos on the device gram
+// product, host/iram.hpp), --svd 1 (Halko) and --svd 2 (winSVD, in-core shuffle unless
+// -S), -k, -p, --ncv, --imaxiter, --itol, -w/--batches/--windows, --oversamples, --seed, --rand, --tol-rsvd, --maf,
 // -C/--scale 0 (no standardisation), --haploid, -V, -o, -v; outputs .sigvals .eigvals
 // .eigvecs [.loadings .mbim] .eigvecs2 and .log. Options of the reference that belong to
 // modes outside this build are recognised and rejected with a clear message and exit 1.
@@ -29,6 +30,7 @@
 #include <zlib.h>
 
 #include "../../include/pcaone_gpu.h"
+#include "iram.hpp"
 
 namespace {
 
@@ -74,11 +76,15 @@ struct Params {
   bool noshuffle = false, printv = false, haploid = false, emu = false, pcangsd = false;
   double tol = 1e-4, maf = 0.0, memory = 0.0, tolem = 1e-5;
   unsigned maxiter = 100;
+  unsigned ncv = 20, imaxiter = 1000;  // IRAM (--svd 0): ncv = max(20, 2k + 1) (src/Cmd.cpp:189)
+  double itol = 1e-6;
+  bool ncv_set = false;
   bool fix_index = false;
   bool print_r2 = false, fix_read_u = false;
   unsigned ld_bp = 0;
   std::string fileU, filebim;
   int precision = PCAONE_PREC_MIXED;
+  bool precision_set = false;
   int device = 0;
   std::string cmdline;
 };
@@ -88,7 +94,7 @@ const std::set<std::string> kUnsupported = {
     "-D", "--ld", "--ld-r2", "--ld-stats", "--clump",
     "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
     "--inbreed", "--USV", "--read-V", "--read-S", "--M", "--N",
-    "--scale-factor", "--buffer", "--imaxiter", "--itol", "--ncv"};
+    "--scale-factor", "--buffer"};
 
 void usage() {
   std::cout << "PCAone (B200 build)\n"
@@ -155,6 +161,11 @@ Params parse(int argc, char** argv) {
     else if (a == "-o" || a == "--out") p.fileout = next();
     else if (a == "-k" || a == "--pc") p.k = (unsigned)num(next());
     else if (a == "-d" || a == "--svd") p.svd = (int)num(next());
+    else if (a == "--ncv") {
+      p.ncv = (unsigned)num(next());
+      p.ncv_set = true;
+    } else if (a == "--imaxiter") p.imaxiter = (unsigned)num(next());
+    else if (a == "--itol") p.itol = num(next());
     else if (a == "-p" || a == "--maxp") p.maxp = (unsigned)num(next());
     else if (a == "-w" || a == "--batches" || a == "--windows") p.bands = (unsigned)num(next());
     else if (a == "-S" || a == "--no-shuffle") p.noshuffle = true;
@@ -180,6 +191,7 @@ Params parse(int argc, char** argv) {
     else if (a == "-m" || a == "--memory") p.memory = num(next());
     else if (a == "--device") p.device = (int)num(next());
     else if (a == "--precision") {
+      p.precision_set = true;
       std::string v = next();
       if (v == "mixed" || v == "int8") p.precision = PCAONE_PREC_MIXED;
       else if (v == "bf16") p.precision = PCAONE_PREC_BF16;
@@ -194,7 +206,10 @@ Params parse(int argc, char** argv) {
     }
   }
   if (p.bfile.empty() && p.beagle.empty()) fail("no input: use -b/--bfile or -G/--beagle");
-  if (p.svd != 1 && p.svd != 2) fail("--svd must be 1 or 2 in this build");
+  if (p.svd != 0 && p.svd != 1 && p.svd != 2) fail("--svd must be 0, 1 or 2 in this build");
+  if (!p.ncv_set) p.ncv = std::max(20u, 2 * p.k + 1);
+  // the reference's EM modes with --svd 0 fail (src/Data.cpp:277 reads an empty permutation)
+  if (p.svd == 0 && (p.emu || p.pcangsd)) fail("--emu / --pcangsd need --svd 1 or 2 in this build");
   if (p.bands < 4 || p.bands % 2 != 0) fail("the -w/--batches must be a power of 2 and the minimun is 4.");
   if (p.maf > 0.5) {
     std::cerr << "warning: '--maf' with a value greater than 0.5 will be converted to 1 - maf.\n";
@@ -671,8 +686,9 @@ int main(int argc, char** argv) {
     g_log.print(date(), "permuting data matrix by columns in place");
     check(ctx, pcaone_gpu_permute(ctx, perm.data()), "permute");
   }
-  g_log.print(date(), p.svd == 2 ? "initialize window-based RSVD (winSVD) with in-core"
-                                 : "initialize single-pass RSVD (sSVD) with in-core");
+  if (p.svd != 0)
+    g_log.print(date(), p.svd == 2 ? "initialize window-based RSVD (winSVD) with in-core"
+                                   : "initialize single-pass RSVD (sSVD) with in-core");
   pcaone_rsvd_opts o{};
   o.k = (int)p.k;
   o.oversamples = (int)p.oversamples;
@@ -689,7 +705,38 @@ int main(int argc, char** argv) {
   std::vector<double> U(N * p.k), S(p.k), V(M * p.k);
   pcaone_rsvd_report rep{};
   double gpu_s = 0;
-  if (p.pcangsd) {
+  if (p.svd == 0) {
+    // IRAM (run_pca_with_arnoldi in-core, src/Arnoldi.cpp:48-87): the largest k eigenpairs of
+    // Z Z^T by restarted Lanczos, each operator application one device gram product; then
+    // S = sqrt(eigenvalues), U = eigenvectors, V = Z^T U / S. FP64 products unless --precision
+    // is given (the Lanczos residuals need the operator to full precision).
+    g_log.print(date(), "running IRAM SVD with in-core mode.");
+    const int prec = p.precision_set ? p.precision : PCAONE_PREC_FP64;
+    const int stdz = p.scale == 0 ? 0 : 1, ploidy = p.haploid ? 1 : 2;
+    auto op = [&](const double* x, double* y) {
+      if (N <= M) {
+        check(ctx, pcaone_gpu_gram_product(ctx, prec, stdz, ploidy, x, 1, y), "gram_product");
+      } else {  // tall matrix: Z^T Z x on the SNP side
+        std::vector<double> t(N);
+        check(ctx, pcaone_gpu_product(ctx, prec, 1, stdz, ploidy, x, 1, t.data()), "product");
+        check(ctx, pcaone_gpu_product(ctx, prec, 0, stdz, ploidy, t.data(), 1, y), "product");
+      }
+    };
+    const size_t n = N <= M ? N : M;
+    auto res = iram::largest(op, n, (int)p.k, (int)p.ncv, (int)p.imaxiter, p.itol);
+    if (!res.converged) fail("the nconv is not equal to k.");
+    g_log.print(date(), "IRAM converged after", res.restarts, "restarts and", res.matvecs, "operator applications");
+    for (unsigned c = 0; c < p.k; ++c) S[c] = std::sqrt(std::max(res.evals[c], 0.0));
+    std::vector<double>& small = N <= M ? U : V;  // eigenvectors live on the smaller side
+    std::vector<double>& big = N <= M ? V : U;
+    small = res.evecs;
+    check(ctx, pcaone_gpu_product(ctx, prec, N <= M ? 0 : 1, stdz, ploidy, small.data(), p.k, big.data()),
+          "product");
+    const size_t nb = N <= M ? M : N;
+    for (unsigned c = 0; c < p.k; ++c)
+      for (size_t j = 0; j < nb; ++j) big[c * nb + j] /= S[c];
+    g_log.print(date(), "PCAone - IRAM SVD done");
+  } else if (p.pcangsd) {
     // PCAngsd on PLINK input (src/FilePlink.cpp:89-115, src/Halko.cpp:294-316): pseudo-
     // likelihoods from the genotypes, F from the genotype counts, the first RSVD on the
     // centred unstandardised genotypes; no GRM stage (Beagle input only)

@@ -63,3 +63,12 @@ def test_c1_cli_matches_reference(c1_prefix, tmp_path):
                     "--tol-rsvd", "0", "-V", "-o", out], check=True, stdout=subprocess.DEVNULL)
     assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_eigvals("c1_halko"), 1e-5)
     assert_cols_close(O.read_table(out + ".eigvecs")[:, :2], ref_table("c1_halko", ".eigvecs")[:, :2], 5e-4)
+
+
+def test_c1_iram_cli_matches_reference(c1_prefix, tmp_path):
+    """Config 1 with --svd 0 (IRAM, k = 10): every eigenvalue to 1e-5 of the reference's."""
+    out = str(tmp_path / "c1_iram")
+    cli = os.path.join(ROOT, "pcaone_b200", "bin", "PCAone")
+    subprocess.run([cli, "-b", c1_prefix, "-d", "0", "-k", "10", "-o", out], check=True, stdout=subprocess.DEVNULL)
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_eigvals("c1_iram"), 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs")[:, :2], ref_table("c1_iram", ".eigvecs")[:, :2], 5e-4)

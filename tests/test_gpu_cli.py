@@ -62,6 +62,16 @@ def test_cli_pcangsd_on_plink_matches_reference_outputs(tmp_path, name):
 
 
 @pytest.mark.gpu
+def test_cli_iram_matches_reference_outputs(tmp_path):
+    """--svd 0: restarted Lanczos on the device gram product against the reference's IRAM."""
+    run_cli(golden_args("g1_iram", tmp_path), tmp_path)
+    out = str(tmp_path / "g1_iram")
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table("g1_iram", ".eigvals")[:, 0], 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table("g1_iram", ".eigvecs"), 5e-4)
+    assert_cols_close(O.read_table(out + ".loadings"), ref_table("g1_iram", ".loadings"), 5e-4)
+
+
+@pytest.mark.gpu
 def test_cli_emu_matches_reference_outputs(tmp_path):
     run_cli(golden_args("g2_emu", tmp_path), tmp_path)
     out = str(tmp_path / "g2_emu")

@@ -45,3 +45,14 @@ def test_products_unstandardised_haploid(gpu, prec):
     assert rel_col_err(gpu.product_t(B, precision=prec, standardize=False), Zc.T @ B) <= TOL[prec]
     Zh = O.standardize(Zc, F, ploidy=1)
     assert rel_col_err(gpu.product_t(B, precision=prec, ploidy=1), Zh.T @ B) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed", "bf16"])
+def test_gram_product_matches_dense(gpu, prec):
+    """The IRAM operator Z (Z^T X) in one device call against the oracle's Z."""
+    bed = random_bed(777, 3001, seed=21, miss=0.02)
+    Z, F = O.standardized_from_bed(bed)
+    gpu.load_bed(bed.packed, bed.N)
+    X = np.random.default_rng(3).standard_normal((bed.N, 5))
+    got = gpu.gram_product(X, precision=prec)
+    assert rel_col_err(got, Z @ (Z.T @ X)) <= 2 * TOL[prec]

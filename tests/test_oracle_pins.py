@@ -158,3 +158,12 @@ def test_oracle_pcangsd_on_plink_matches_reference(name, shuffle):
     assert_eig_close(eig, ref_eigvals(name), 1e-5)
     assert_cols_close(U, ref_table(name, ".eigvecs"), 2e-6)
     assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)
+
+
+def test_oracle_dense_eig_matches_reference_iram():
+    """--svd 0 (IRAM, converged to --itol 1e-6) gives the exact leading eigenpairs: the oracle's
+    dense FP64 SVD of Z matches the reference's -d 0 outputs."""
+    eig, S, U, V = O.dense_eig(g("g1"), 4)
+    assert_eig_close(eig, ref_eigvals("g1_iram"), 1e-5)
+    assert_cols_close(U, ref_table("g1_iram", ".eigvecs"), 2e-5)
+    assert_cols_close(V, ref_table("g1_iram", ".loadings"), 2e-5)

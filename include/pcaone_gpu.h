@@ -170,6 +170,22 @@ int pcaone_gpu_clear_imputed(pcaone_ctx* ctx);
 int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
                      const int32_t* we, uint64_t nwin, float* r2);
 
+/* LD flow B, first half: the residual matrix of Data::write_residuals (src/Data.cpp:196-245)
+ * for the SNPs snp0 .. snp0 + nsnp - 1 of the current order. R_ij = Gc_ij - sum_t U_it S_t
+ * V_jt with Gc the centred genotypes (BED2GENO - F_j, missing -> 0; not standardised), or Gc
+ * itself when U is NULL (--ld-stats 1); every SNP's residuals are then centred over the
+ * samples (FP64) and stored as float. U (nsamples x k), S (k) and V (nsnp x k, the loadings
+ * of those SNPs) are column-major host matrices; out (host) receives nsnp rows of nsamples
+ * floats, the layout of the .residuals body. */
+int pcaone_gpu_residuals(pcaone_ctx* ctx, const double* U, const double* S, const double* V, uint32_t k,
+                         uint64_t snp0, uint64_t nsnp, float* out);
+
+/* LD flow B, second half: load a dense SNP-major float matrix (nsnps rows of nsamples, the
+ * .residuals body after its 8-byte header) and centre every row in FP64 as FileBin::read_all
+ * does (src/FileBinary.cpp:21-30). pcaone_gpu_ld_r2 with U = NULL then gives the r2 of
+ * ld_r2_big (src/LD.cpp:419-442) on it. */
+int pcaone_gpu_load_dense(pcaone_ctx* ctx, const float* X, uint64_t nsnps, uint32_t nsamples);
+
 /* PCAngsd on genotype likelihoods (Beagle input). Load the likelihood pairs: P is the
  * reference's 2N x M column-major FP64 matrix of the first two likelihoods per sample and
  * site (FileBeagle::read_all, src/FileBeagle.cpp:121-143; the third is implied as

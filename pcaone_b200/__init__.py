@@ -30,7 +30,8 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_product", "pcaone_gpu_fit_emu", "pcaone_gpu_clear_imputed",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
-           "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product"]
+           "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
+           "pcaone_gpu_residuals", "pcaone_gpu_load_dense"]
 
 
 class PcaoneError(RuntimeError):
@@ -90,6 +91,8 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
         L.pcaone_gpu_load_gl_f32.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gram_product.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, u32, vp]
+        L.pcaone_gpu_residuals.argtypes = [vp, vp, vp, vp, u32, u64, u64, vp]
+        L.pcaone_gpu_load_dense.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
@@ -254,6 +257,32 @@ def _gram_product(self, X, precision=PREC_FP64, standardize=True, ploidy=2):
 
 
 GpuContext.gram_product = _gram_product
+
+
+def _residuals(self, U=None, S=None, V=None, snp0=0, nsnp=None):
+    """Residual rows (nsnp x nsamples float32) of pcaone_gpu_residuals; V holds the loadings of
+    the nsnp SNPs from snp0 (current SNP order); no factors gives the centred genotypes."""
+    nsnp = self.M - snp0 if nsnp is None else nsnp
+    out = np.zeros((nsnp, self.N), dtype=np.float32)
+    if U is None:
+        self._check(lib().pcaone_gpu_residuals(self._h, None, None, None, 0, snp0, nsnp, _ptr(out)))
+    else:
+        Uf, Vf = np.asfortranarray(U, dtype=np.float64), np.asfortranarray(V, dtype=np.float64)
+        Sf = np.ascontiguousarray(S, dtype=np.float64)
+        self._check(lib().pcaone_gpu_residuals(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(Sf), snp0, nsnp,
+                                               _ptr(out)))
+    return out
+
+
+def _load_dense(self, X):
+    """X: nsnps x nsamples float32 (the .residuals body), centred per row on the device."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    self._check(lib().pcaone_gpu_load_dense(self._h, _ptr(X), X.shape[0], X.shape[1]))
+    self.M, self.N = X.shape
+
+
+GpuContext.residuals = _residuals
+GpuContext.load_dense = _load_dense
 
 
 def _fit_emu(self, U, S, V, reference_index=True):

@@ -32,6 +32,7 @@ static void free_ptr(void* p) {
 void free_data(pcaone_ctx* c) {
   c->d_P = nullptr;
   c->d_E = nullptr;
+  c->d_dense_norm = nullptr;
   c->d_zero = nullptr;
   c->dense = false;
   c->win = WindowLayout();
@@ -299,6 +300,38 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
                  "window " + std::to_string(w) + " out of range");
       off[w + 1] = off[w] + (we[w] - 1);
     }
+    if (c->dense) {
+      // LD flow B: r2 on the centred dense matrix of pcaone_gpu_load_dense
+      PG_REQUIRE(!U && c->d_dense_norm, PCAONE_ESTATE,
+                 "LD on a dense matrix needs pcaone_gpu_load_dense and no U (the residuals are already adjusted)");
+      std::vector<int64_t> win_of(c->M, -1);
+      const uint64_t blocks = (c->M + 31) / 32;
+      std::vector<int32_t> span(blocks, -1);
+      int max_span = 0;
+      for (uint64_t w = 0; w < nwin; ++w) {
+        win_of[ws[w]] = (int64_t)w;
+        const uint64_t b = (uint64_t)ws[w] / 32;
+        const int s = (int)((uint64_t)ws[w] - b * 32) + we[w] - 1;
+        span[b] = std::max(span[b], s);
+        max_span = std::max(max_span, s);
+      }
+      int64_t* d_win_of = (int64_t*)scratch(c, "ld_win_of", c->M * 8);
+      int32_t* d_span = (int32_t*)scratch(c, "ld_span", blocks * 4);
+      int32_t* d_we = (int32_t*)scratch(c, "ld_we", std::max<uint64_t>(nwin, 1) * 4);
+      int64_t* d_off = (int64_t*)scratch(c, "ld_off", (nwin + 1) * 8);
+      float* d_r2 = (float*)scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * 4);
+      PG_CUDA(cudaMemcpyAsync(d_win_of, win_of.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(d_span, span.data(), blocks * 4, cudaMemcpyHostToDevice, c->stream));
+      if (nwin) {
+        PG_CUDA(cudaMemcpyAsync(d_we, we, nwin * 4, cudaMemcpyHostToDevice, c->stream));
+        PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (nwin + 1) * 8, cudaMemcpyHostToDevice, c->stream));
+        ld_r2_dense(c, c->d_dense_norm, d_win_of, d_we, d_off, d_span, max_span, d_r2);
+      }
+      if (off[nwin] > 0)
+        PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * 4, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+      return;
+    }
     double *dW = nullptr, *dY = nullptr;
     if (U) {
       // W = Gc^T U (M x k) through the FP64 product path; Y = (2I - U^T U) W on the host
@@ -387,6 +420,60 @@ int pcaone_gpu_load_gl(pcaone_ctx* c, const double* P, uint64_t nsnps, uint32_t 
 
 int pcaone_gpu_load_gl_f32(pcaone_ctx* c, const float* P, uint64_t nsnps, uint32_t nsamples) {
   return guarded(c, [&] { load_gl_impl<float>(c, P, nsnps, nsamples); });
+}
+
+int pcaone_gpu_load_dense(pcaone_ctx* c, const float* X, uint64_t nsnps, uint32_t nsamples) {
+  return guarded(c, [&] {
+    PG_REQUIRE(X && nsnps > 0 && nsamples > 1, PCAONE_EBADARG, "empty dense matrix");
+    PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 29), PCAONE_EBADARG, "dense matrix too large");
+    free_data(c);
+    c->generation++;
+    c->dense = true;
+    c->N = nsamples;
+    c->M = nsnps;
+    c->Npad = (uint32_t)round_up(nsamples, kRowPad);
+    c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
+    c->pitch = 1;
+    c->d_E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
+    PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
+    PG_CUDA(cudaMemcpy2DAsync(c->d_E, (size_t)c->Npad * 4, X, (size_t)nsamples * 4, (size_t)nsamples * 4, nsnps,
+                              cudaMemcpyHostToDevice, c->stream));
+    c->d_dense_norm = (double*)scratch(c, "d_dense_norm", c->M * 8);
+    dense_center(c, c->d_dense_norm);
+    c->d_F = (double*)scratch(c, "d_F", c->M * 8);
+    c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
+    c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
+    c->d_zero = (double*)scratch(c, "d_zero", c->M * 8);
+    PG_CUDA(cudaMemsetAsync(c->d_zero, 0, c->M * 8, c->stream));
+    PG_CUDA(cudaMemsetAsync(c->d_F, 0, c->M * 8, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    c->loaded = true;
+  });
+}
+
+int pcaone_gpu_residuals(pcaone_ctx* c, const double* U, const double* S, const double* V, uint32_t k,
+                         uint64_t snp0, uint64_t nsnp, float* out) {
+  return guarded(c, [&] {
+    PG_REQUIRE(c->loaded && !c->dense, PCAONE_ESTATE, "residuals need packed genotypes (load_bed)");
+    PG_REQUIRE(out && snp0 + nsnp <= c->M, PCAONE_EBADARG, "residual rows out of range");
+    PG_REQUIRE(!U || (S && V && k >= 1 && k <= (uint32_t)kLmax), PCAONE_EBADARG, "bad factors");
+    double *dUS = nullptr, *dV = nullptr;
+    if (U) {
+      std::vector<double> us((size_t)c->N * k), v((size_t)nsnp * k);
+      for (uint32_t i = 0; i < c->N; ++i)
+        for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+      for (uint64_t j = 0; j < nsnp; ++j)
+        for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * nsnp + j];
+      dUS = (double*)scratch(c, "res_US", us.size() * 8);
+      dV = (double*)scratch(c, "res_V", std::max<size_t>(v.size(), 1) * 8);
+      PG_CUDA(cudaMemcpyAsync(dUS, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      PG_CUDA(cudaMemcpyAsync(dV, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    }
+    float* d_out = (float*)scratch(c, "res_out", std::max<uint64_t>(nsnp, 1) * c->N * 4);
+    if (nsnp) residuals(c, dUS, dV, U ? (int)k : 0, snp0, nsnp, d_out);
+    if (nsnp) PG_CUDA(cudaMemcpyAsync(out, d_out, nsnp * c->N * 4, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+  });
 }
 
 int pcaone_gpu_bed_to_gl(pcaone_ctx* c) {

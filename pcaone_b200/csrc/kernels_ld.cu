@@ -114,7 +114,135 @@ __global__ void k_ld_pairs(const uint32_t* __restrict__ ph, const uint32_t* __re
   }
 }
 
+// ---------------------------------------------------------------- LD flow B
+// Residual matrix of Data::write_residuals (src/Data.cpp:196-245): R_ij = Gc_ij - sum_t US_it
+// V_jt with Gc the centred genotypes (BED2GENO - F_j, missing -> 0; ld_stats 0) or Gc itself
+// without factors (ld_stats 1), then every SNP column centred over the samples (FP64), stored
+// as float, SNP-major (row jj = SNP snp0 + jj of the current order). Warp per SNP; the
+// residual is recomputed in the second pass instead of being stored.
+__global__ void k_residuals(const uint8_t* __restrict__ bed, uint32_t pitch, uint64_t snp0, uint64_t nsnp,
+                            uint32_t N, const double* __restrict__ F, const double* __restrict__ US,
+                            const double* __restrict__ V, int k, float* __restrict__ out) {
+  __shared__ double vs[8][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t jj = (uint64_t)blockIdx.x * 8 + warp;
+  if (jj >= nsnp) return;
+  const uint64_t j = snp0 + jj;
+  const double f = F[j];
+  if (V)
+    for (int t = lane; t < k; t += 32) vs[warp][t] = V[jj * k + t];
+  __syncwarp();
+  const uint8_t* rec = bed + j * pitch;
+  auto resid = [&](uint32_t i) {
+    const int code = (rec[i >> 2] >> (2 * (i & 3))) & 3;
+    double g = code == 1 ? 0.0 : (code == 0 ? 1.0 : (code == 2 ? 0.5 : 0.0)) - f;
+    if (V)
+      for (int t = 0; t < k; ++t) g -= US[(uint64_t)i * k + t] * vs[warp][t];
+    return g;
+  };
+  double s = 0.0;
+  for (uint32_t i = lane; i < N; i += 32) s += resid(i);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const double mean = s / N;
+  for (uint32_t i = lane; i < N; i += 32) out[jj * N + i] = (float)(resid(i) - mean);
+}
+
+// Dense matrix X (SNP-major floats, row stride ldx) -> column-centred copy in place (FP64
+// mean, FileBin::read_all, src/FileBinary.cpp:21-30) and the squared norms d_j of the centred
+// columns (calc_sds, src/LD.cpp:20-23, without the common 1/(N-1)). Warp per SNP.
+__global__ void k_dense_center(float* __restrict__ X, uint32_t ldx, uint64_t M, uint32_t N, double* __restrict__ d) {
+  const uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= M) return;
+  float* row = X + j * ldx;
+  double s = 0.0;
+  for (uint32_t i = lane; i < N; i += 32) s += (double)row[i];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const double mean = s / N;
+  double q = 0.0;
+  for (uint32_t i = lane; i < N; i += 32) {
+    const double v = (double)row[i] - mean;
+    row[i] = (float)v;
+    q += (double)row[i] * (double)row[i];
+  }
+  for (int o = 16; o; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+  if (lane == 0) d[j] = q;
+}
+
+// Band Gram of the centred dense matrix for LD flow B (ld_r2_big, src/LD.cpp:419-442): CTA
+// (lead block b of 32 SNPs, partner tile q of 32 SNPs starting at 32 b + 32 q); the 32 x 32
+// dot products are accumulated in FP64 from the float values (each product exact in FP64),
+// over sample chunks of 64 staged in shared memory; thread t owns lead row t / 8 and four
+// partner columns. Pairs (i, k) with 1 <= k - i < we[w] of the lead's window w are written
+// as r^2 = (X_i.X_k)^2 / (d_i d_k) to r2[off[w] + k - i - 1].
+constexpr int kLdTile = 32, kLdChunk = 64;
+__global__ void __launch_bounds__(256) k_ld_dense(const float* __restrict__ X, uint32_t ldx, uint64_t M, uint32_t N,
+                                                  const double* __restrict__ d, const int64_t* __restrict__ win_of,
+                                                  const int32_t* __restrict__ we, const int64_t* __restrict__ off,
+                                                  const int32_t* __restrict__ span, float* __restrict__ r2) {
+  __shared__ double A[kLdTile][kLdChunk + 1], B[kLdTile][kLdChunk + 1];
+  const uint64_t i0 = (uint64_t)blockIdx.x * kLdTile;
+  const uint64_t k0 = i0 + (uint64_t)blockIdx.y * kLdTile;
+  if (k0 >= M || (int64_t)blockIdx.y * kLdTile > span[blockIdx.x]) return;
+  const int t = threadIdx.x, r = t >> 3, c0 = (t & 7) * 4;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t s0 = 0; s0 < N; s0 += kLdChunk) {
+    __syncthreads();
+    for (int e = t; e < kLdTile * kLdChunk; e += 256) {
+      const int rr = e / kLdChunk, ss = e - rr * kLdChunk;
+      const uint64_t ia = i0 + rr, ib = k0 + rr;
+      const uint32_t s = s0 + ss;
+      A[rr][ss] = (ia < M && s < N) ? (double)X[ia * ldx + s] : 0.0;
+      B[rr][ss] = (ib < M && s < N) ? (double)X[ib * ldx + s] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int ss = 0; ss < kLdChunk; ++ss) {
+      const double a = A[r][ss];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(a, B[c0 + q][ss], acc[q]);
+    }
+  }
+  const uint64_t i = i0 + r;
+  if (i >= M) return;
+  const int64_t w = win_of[i];
+  if (w < 0) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint64_t kk = k0 + c0 + q;
+    const int64_t dist = (int64_t)kk - (int64_t)i;
+    if (kk < M && dist >= 1 && dist < we[w]) {
+      const double rr = acc[q] / sqrt(d[i] * d[kk]);
+      r2[off[w] + dist - 1] = (float)(rr * rr);
+    }
+  }
+}
+
 }  // namespace
+
+void residuals(pcaone_ctx* c, const double* US, const double* V, int k, uint64_t snp0, uint64_t nsnp, float* out) {
+  k_residuals<<<(unsigned)((nsnp + 7) / 8), 256, 0, c->stream>>>(c->d_bed, c->pitch, snp0, nsnp, c->N, c->d_F, US,
+                                                                  V, k, out);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void dense_center(pcaone_ctx* c, double* d) {
+  k_dense_center<<<(unsigned)((c->M * 32 + 255) / 256), 256, 0, c->stream>>>(c->d_E, c->Npad, c->M, c->N, d);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void ld_r2_dense(pcaone_ctx* c, const double* d, const int64_t* d_win_of, const int32_t* d_we, const int64_t* d_off,
+                 const int32_t* d_span, int max_span, float* d_r2) {
+  const uint64_t blocks = (c->M + kLdTile - 1) / kLdTile;
+  const unsigned tiles = (unsigned)((max_span + kLdTile) / kLdTile);
+  PG_REQUIRE(blocks < (1ull << 31) && tiles < 65536, PCAONE_EBADARG, "LD band too large");
+  k_ld_dense<<<dim3((unsigned)blocks, tiles), 256, 0, c->stream>>>(c->d_E, c->Npad, c->M, c->N, d, d_win_of, d_we,
+                                                                   d_off, d_span, d_r2);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
 
 void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,
            const int32_t* d_we, const int64_t* d_off, int64_t nwin, float* d_r2) {

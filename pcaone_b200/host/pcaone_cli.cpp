@@ -83,6 +83,9 @@ struct Params {
   bool print_r2 = false, fix_read_u = false;
   unsigned ld_bp = 0;
   std::string fileU, filebim;
+  std::string binfile;  // -B/--binary: float32 .residuals matrix (LD flow B input)
+  bool ld_write = false;  // -D/--ld: write the .residuals matrix after the PCA
+  int ld_stats = 0;       // --ld-stats: 0 ancestry-adjusted residuals, 1 centred genotypes
   int precision = PCAONE_PREC_MIXED;
   bool precision_set = false;
   int device = 0;
@@ -90,8 +93,7 @@ struct Params {
 };
 
 const std::set<std::string> kUnsupported = {
-    "-c", "--csv", "-g", "--bgen", "-B", "--binary",
-    "-D", "--ld", "--ld-r2", "--ld-stats", "--clump",
+    "-c", "--csv", "-g", "--bgen", "--ld-r2", "--clump",
     "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
     "--inbreed", "--USV", "--read-V", "--read-S", "--M", "--N",
     "--scale-factor", "--buffer"};
@@ -110,6 +112,8 @@ void usage() {
                "      --fix-perm-index  EM steps read each SNP's own F after the shuffle\n"
                "  -C, --scale      0: centre only, 1: standardise (default for PLINK)\n"
                "  LD r2 (flow A): -b plink --read-U pcs.eigvecs -f pcs.mbim --ld-bp BP -R\n"
+               "  LD r2 (flow B): -b plink -k K -D (writes .residuals), then\n"
+               "                  -B out.residuals -f out.mbim --ld-bp BP -R\n"
                "      --fix-read-u read U row by row (the reference views it column-major)\n"
                "  -V, --printv     write .loadings and .mbim\n"
                "  -o, --out        output prefix [pcaone]\n"
@@ -183,6 +187,9 @@ Params parse(int argc, char** argv) {
     else if (a == "-R" || a == "--print-r2") p.print_r2 = true;
     else if (a == "--ld-bp") p.ld_bp = (unsigned)num(next());
     else if (a == "--read-U") p.fileU = next();
+    else if (a == "-B" || a == "--binary") p.binfile = next();
+    else if (a == "-D" || a == "--ld") p.ld_write = true;
+    else if (a == "--ld-stats") p.ld_stats = (int)num(next());
     else if (a == "-f" || a == "--match-bim") p.filebim = next();
     else if (a == "--fix-read-u") p.fix_read_u = true;
     else if (a == "-V" || a == "--printv") p.printv = true;
@@ -205,7 +212,10 @@ Params parse(int argc, char** argv) {
       std::exit(EXIT_FAILURE);
     }
   }
-  if (p.bfile.empty() && p.beagle.empty()) fail("no input: use -b/--bfile or -G/--beagle");
+  if (p.bfile.empty() && p.beagle.empty() && p.binfile.empty())
+    fail("no input: use -b/--bfile, -G/--beagle or -B/--binary");
+  if (p.ld_write && (p.emu || p.pcangsd || p.bfile.empty()))
+    fail("-D/--ld writes residuals of a plain PCA of PLINK input in this build");
   if (p.svd != 0 && p.svd != 1 && p.svd != 2) fail("--svd must be 0, 1 or 2 in this build");
   if (!p.ncv_set) p.ncv = std::max(20u, 2 * p.k + 1);
   // the reference's EM modes with --svd 0 fail (src/Data.cpp:277 reads an empty permutation)
@@ -340,8 +350,10 @@ std::vector<std::string> beagle_samples(const std::string& path) {
 // ---------------------------------------------------------------- LD r2 output
 // get_snp_pos_bim + divide_pos_by_window (src/LD.cpp:51-74, 125-139) and the .ld.gz text of
 // ld_r2_big (src/LD.cpp:419-442): "chr\tpos\tid" pairs and std::to_string(r2).
-int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M) {
-  const std::string filebim = p.filebim.empty() ? p.bfile + ".bim" : p.filebim;
+// LD r2 of every window pair, written as .ld.gz: flow A on packed genotypes projected off
+// the --read-U factors, or flow B (dense) on the .residuals matrix loaded into ctx.
+int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M, bool dense) {
+  const std::string filebim = !p.filebim.empty() ? p.filebim : (dense ? p.binfile : p.bfile) + ".bim";
   std::ifstream fb(filebim);
   if (!fb.is_open()) fail("can not open " + filebim);
   std::vector<long> pos;
@@ -372,13 +384,18 @@ int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M) {
     we.push_back((int32_t)(j - i));
   }
   size_t ur = 0, uc = 0;
-  std::vector<double> U = read_usv(p.fileU, ur, uc, p.fix_read_u);
-  if (ur != N) fail("the number of rows of --read-U differs from the samples");
+  std::vector<double> U;
+  if (!dense) {
+    U = read_usv(p.fileU, ur, uc, p.fix_read_u);
+    if (ur != N) fail("the number of rows of --read-U differs from the samples");
+  }
   std::vector<int64_t> off(ws.size() + 1, 0);
   for (size_t w = 0; w < ws.size(); ++w) off[w + 1] = off[w] + (we[w] - 1);
   std::vector<float> r2(std::max<int64_t>(off.back(), 1));
   auto t0 = std::chrono::steady_clock::now();
-  check(ctx, pcaone_gpu_ld_r2(ctx, U.data(), (uint32_t)uc, ws.data(), we.data(), ws.size(), r2.data()), "ld_r2");
+  check(ctx, pcaone_gpu_ld_r2(ctx, dense ? nullptr : U.data(), (uint32_t)uc, ws.data(), we.data(), ws.size(),
+                              r2.data()),
+        "ld_r2");
   double gpu_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   g_log.print(date(), "LD r2 of", off.back(), "pairs computed in", gpu_s, "seconds");
   // format and deflate chunks of windows in parallel; concatenated gzip members are one file
@@ -600,6 +617,30 @@ int run_pcangsd(const Params& p, std::chrono::steady_clock::time_point t_start) 
   return 0;
 }
 
+// -B/--binary input (FileBin, src/FileBinary.cpp): the float32 matrix written by -D (header:
+// uint32 nsnps, uint32 nsamples; then nsnps rows of nsamples floats), LD r2 only.
+int run_binary(const Params& p, std::chrono::steady_clock::time_point t_start) {
+  std::ifstream f(p.binfile, std::ios::binary);
+  if (!f.is_open()) fail("Cannot open " + p.binfile);
+  uint32_t hdr[2] = {0, 0};
+  f.read((char*)hdr, 8);
+  const size_t M = hdr[0], N = hdr[1];
+  g_log.print(date(), "shape of input matrix (features x samples) is", M, "x", N);
+  if (!(p.print_r2 || p.ld_bp > 0)) fail("-B/--binary input supports the LD r2 mode (-R, --ld-bp) in this build");
+  std::vector<float> X(M * N);
+  f.read((char*)X.data(), (std::streamsize)(X.size() * 4));
+  if ((size_t)f.gcount() != X.size() * 4) fail("the binary file is shorter than its header implies");
+  pcaone_ctx* ctx = nullptr;
+  if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
+  check(ctx, pcaone_gpu_load_dense(ctx, X.data(), M, (uint32_t)N), "load_dense");
+  g_log.print(date(), "run LD stuff");
+  run_ld(p, ctx, N, M, true);
+  pcaone_gpu_destroy(ctx);
+  double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  g_log.print(date(), "total elapsed wall time:", wall, " seconds");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   Params p = parse(argc, argv);
   auto t_start = std::chrono::steady_clock::now();
@@ -614,6 +655,7 @@ int main(int argc, char** argv) {
   }
   g_log.print(date(), "program started");
   if (!p.beagle.empty()) return run_pcangsd(p, t_start);
+  if (!p.binfile.empty()) return run_binary(p, t_start);
   g_log.print(date(), "start parsing PLINK format");
   const size_t N = count_lines(p.bfile + ".fam"), M0 = count_lines(p.bfile + ".bim");
   g_log.print(date(), "N (# samples):", N, ", M (# SNPs):", M0);
@@ -671,7 +713,7 @@ int main(int argc, char** argv) {
   if (p.print_r2 || p.ld_bp > 0) {  // LD mode (src/Main.cpp:64-77)
     if (p.fileU.empty()) fail("LD r2 from PLINK input needs --read-U (flow A)");
     g_log.print(date(), "run LD stuff");
-    run_ld(p, ctx, N, M);
+    run_ld(p, ctx, N, M, false);
     pcaone_gpu_destroy(ctx);
     double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     g_log.print(date(), "total elapsed wall time:", wall, " seconds");
@@ -696,7 +738,9 @@ int main(int argc, char** argv) {
   o.svd = p.svd;
   o.bands = (int)p.bands;
   o.precision = p.precision;
-  o.standardize = p.scale == 0 ? 0 : 1;
+  // with -D the reference runs the PCA on the centred, unstandardised genotypes
+  // (src/Halko.cpp:285-288)
+  o.standardize = (p.scale == 0 || p.ld_write) ? 0 : 1;
   o.ploidy = p.haploid ? 1 : 2;
   o.seed = p.seed;
   o.rand = (int)p.rand;
@@ -712,7 +756,7 @@ int main(int argc, char** argv) {
     // is given (the Lanczos residuals need the operator to full precision).
     g_log.print(date(), "running IRAM SVD with in-core mode.");
     const int prec = p.precision_set ? p.precision : PCAONE_PREC_FP64;
-    const int stdz = p.scale == 0 ? 0 : 1, ploidy = p.haploid ? 1 : 2;
+    const int stdz = (p.scale == 0 || p.ld_write) ? 0 : 1, ploidy = p.haploid ? 1 : 2;
     auto op = [&](const double* x, double* y) {
       if (N <= M) {
         check(ctx, pcaone_gpu_gram_product(ctx, prec, stdz, ploidy, x, 1, y), "gram_product");
@@ -791,6 +835,37 @@ int main(int argc, char** argv) {
     gpu_s += rep.gpu_ms / 1e3;
   }
   g_log.print(date(), "PCAone - Randomized SVD done; GPU time", gpu_s, "seconds");
+  if (p.ld_write) {
+    // Data::write_residuals (src/Data.cpp:196-245): header uint32 nsnps, uint32 nsamples, then
+    // each SNP's centred residuals as float at its input position (perm undoes the shuffle);
+    // rows are computed on the device in chunks of the current SNP order
+    g_log.print(date(), p.ld_stats == 1 ? "ld-stats=1: calculate standardized genotype matrix!"
+                                        : "ld-stats=0: calculate the ancestry adjusted LD matrix!");
+    std::FILE* fr = std::fopen((p.fileout + ".residuals").c_str(), "wb");
+    if (!fr) fail("cannot write " + p.fileout + ".residuals");
+    const uint32_t hdr[2] = {(uint32_t)M, (uint32_t)N};
+    std::fwrite(hdr, 4, 2, fr);
+    const size_t chunk = std::max<size_t>(1, ((size_t)1 << 28) / (N * 4));
+    std::vector<float> rows;
+    std::vector<double> Vc;
+    for (size_t s0 = 0; s0 < M; s0 += chunk) {
+      const size_t n = std::min(chunk, M - s0);
+      rows.resize(n * N);
+      Vc.resize(n * p.k);
+      for (unsigned c = 0; c < p.k; ++c)
+        for (size_t j = 0; j < n; ++j) Vc[c * n + j] = V[c * M + s0 + j];
+      if (p.ld_stats == 1)
+        check(ctx, pcaone_gpu_residuals(ctx, nullptr, nullptr, nullptr, 0, s0, n, rows.data()), "residuals");
+      else
+        check(ctx, pcaone_gpu_residuals(ctx, U.data(), S.data(), Vc.data(), p.k, s0, n, rows.data()), "residuals");
+      for (size_t j = 0; j < n; ++j) {
+        const size_t dst = perm_on ? (size_t)perm[s0 + j] : s0 + j;
+        std::fseek(fr, (long)(8 + dst * N * 4), SEEK_SET);
+        std::fwrite(rows.data() + j * N, 4, N, fr);
+      }
+    }
+    std::fclose(fr);
+  }
   pcaone_gpu_destroy(ctx);
 
   // loadings back to the input SNP order (data->perm * V, src/Halko.cpp:340)
@@ -814,8 +889,8 @@ int main(int argc, char** argv) {
     write_matrix(outu, U.data(), N, p.k);
     outu << '\n';
   }
-  if (p.printv) {
-    // .mbim: .bim line + tab + F (src/Data.cpp:96-136)
+  if (p.printv || p.ld_write) {
+    // .mbim: .bim line + tab + F (src/Data.cpp:96-136); -D saves it too (write_residuals)
     g_log.print(date(), "save matched sites in .mbim file and permutation mode is", perm_on ? 1 : 0);
     std::ifstream ib(p.bfile + ".bim");
     std::ofstream ob(p.fileout + ".mbim");
@@ -832,6 +907,8 @@ int main(int argc, char** argv) {
       }
       ++j;
     }
+  }
+  if (p.printv) {
     std::ofstream ov(p.fileout + ".loadings");
     write_matrix(ov, V.data(), M, p.k);
     ov << '\n';

@@ -134,6 +134,30 @@ def test_cli_ld_flow_a_matches_reference(tmp_path):
 
 
 @pytest.mark.gpu
+def test_cli_ld_flow_b_matches_reference(tmp_path):
+    """Flow B end to end: -D writes the .residuals matrix and .mbim (compared with the
+    reference's), then -B reads it back for the windowed r2 (.ld.gz)."""
+    run_cli(golden_args("g4_adj", tmp_path), tmp_path)
+    out = str(tmp_path / "g4_adj")
+    assert open(out + ".mbim").read() == open(ref_out("g4_adj", ".mbim")).read()
+    got = np.fromfile(out + ".residuals", dtype=np.uint8)
+    ref = np.fromfile(ref_out("g4_adj", ".residuals"), dtype=np.uint8)
+    assert got.size == ref.size and np.array_equal(got[:8], ref[:8])  # header: nsnps, nsamples
+    diff = np.abs(got[8:].view(np.float32) - ref[8:].view(np.float32))
+    assert diff.max() <= 1e-5
+    c = case("g4_ldB")
+    args = [a.format(d=os.path.join(GOLDEN, c["dataset"]), g=GOLDEN) for a in c["args"]]
+    args[args.index("-B") + 1] = out + ".residuals"
+    args[args.index("-f") + 1] = out + ".mbim"
+    run_cli(args + ["-o", str(tmp_path / "g4_ldB")], tmp_path)
+    head, got = O.read_ld_gz(str(tmp_path / "g4_ldB.ld.gz"))
+    rhead, ref = O.read_ld_gz(ref_out("g4_ldB", ".ld.gz"))
+    assert head == rhead and [x[:6] for x in got] == [x[:6] for x in ref]
+    d = np.abs(np.array([float(x[6]) for x in got]) - np.array([float(x[6]) for x in ref]))
+    assert d.max() <= 1e-5
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["g3_pcangsd", "g3_pcangsd_shuf"])
 def test_cli_pcangsd_matches_reference_outputs(tmp_path, name):
     run_cli(golden_args(name, tmp_path), tmp_path)

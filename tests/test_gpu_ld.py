@@ -40,3 +40,56 @@ def test_ld_matches_oracle(gpu, N, M, with_u):
         G = G - U @ (U.T @ G)
     i, k, r = O.ld_pairs(G, snp)
     assert np.abs(r2 - r * r).max() <= 1e-6
+
+
+def test_ld_flow_b_matches_reference(gpu):
+    """Flow B: r2 on the reference's own .residuals matrix (loaded and re-centred on the
+    device) against the reference's .ld.gz of -B g4_adj.residuals -f g4_adj.mbim."""
+    path = os.path.join(GOLDEN, "ref", "g4_adj.residuals")
+    with open(path, "rb") as f:
+        M, N = (int(x) for x in np.frombuffer(f.read(8), dtype=np.uint32))
+        X = np.frombuffer(f.read(4 * M * N), dtype=np.float32).reshape(M, N)
+    snp = O.read_snp_pos(os.path.join(GOLDEN, "ref", "g4_adj.mbim"))
+    O.divide_pos_by_window(snp, 5000)
+    gpu.load_dense(X)
+    r2 = gpu.ld_r2(snp.ws, snp.we)
+    head, ref = O.read_ld_gz(os.path.join(GOLDEN, "ref", "g4_ldB.ld.gz"))
+    rr = np.array([float(x[6]) for x in ref])
+    assert len(r2) == len(rr)
+    assert np.abs(r2 - rr).max() <= 1e-5
+    i, k, r = O.ld_pairs(O.read_residuals(path), snp)
+    assert np.abs(r2 - r * r).max() <= 1e-6
+
+
+@pytest.mark.parametrize("N,M", [(517, 900), (64, 2000)])
+def test_ld_dense_matches_oracle(gpu, N, M):
+    """Dense r2 on an arbitrary float matrix with long windows (tiles across block edges)."""
+    rng = np.random.default_rng(N)
+    X = rng.standard_normal((M, N)).astype(np.float32) + 3.0
+    snp = O.SnpLD(["1"], np.cumsum(rng.integers(1, 50, M)), [M - 1], [""] * M)
+    O.divide_pos_by_window(snp, 3000)
+    gpu.load_dense(X)
+    r2 = gpu.ld_r2(snp.ws, snp.we)
+    G = X.T.astype(np.float64)
+    G = G - G.mean(axis=0, keepdims=True)
+    i, k, r = O.ld_pairs(G, snp)
+    assert np.abs(r2 - r * r).max() <= 1e-6
+
+
+def test_residuals_match_reference(gpu):
+    """The -D writer's rows (Data::write_residuals) from the reference's own factors of the
+    g4_adj run against the reference's .residuals file."""
+    bed = O.read_bed(os.path.join(GOLDEN, "g4"))
+    gpu.load_bed(bed.packed, bed.N)
+    with open(os.path.join(GOLDEN, "ref", "g4_adj.residuals"), "rb") as f:
+        M, N = (int(x) for x in np.frombuffer(f.read(8), dtype=np.uint32))
+        ref = np.frombuffer(f.read(4 * M * N), dtype=np.float32).reshape(M, N)
+    # the centred genotypes (ld-stats 1) are independent of the factors: exact up to float rounding
+    G = O.centered_matrix(O.decode_codes(bed), O.allele_freq(O.decode_codes(bed)))
+    G = G - G.mean(axis=0, keepdims=True)
+    got = gpu.residuals()
+    np.testing.assert_allclose(got, G.T.astype(np.float32), atol=2e-7)
+    # with factors: U S V^T from an FP64 GPU Halko run of the same flags (-d 1 -k 3 -p 7, unstandardised)
+    r = gpu.rsvd(k=3, maxp=7, svd=1, tol=0.0, precision="fp64", standardize=False)
+    res = gpu.residuals(r.U, r.S, r.V)
+    assert np.abs(res - ref).max() <= 1e-5

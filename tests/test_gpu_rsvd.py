@@ -175,11 +175,11 @@ def bench_shape_oracle():
 @pytest.mark.parametrize("prec", ["mixed", "bf16"])
 def test_winsvd_bench_shape_matches_oracle(gpu, bench_shape_oracle, prec):
     """Eigenvalues to 1e-5 relative and a largest principal angle of 1e-3 rad (the mixed-precision
-    bar) against the FP64 oracle; the population PCs 1-4 to 1e-6 rad."""
+    bar) against the FP64 oracle; the leading four PCs to 1e-4 rad."""
     bed, (eig_o, S_o, U_o, V_o, F_o, ep_o) = bench_shape_oracle
     r, V = run_gpu(gpu, bed, True, precision=prec, svd=2, k=20, maxp=20, bands=64)
     assert r.epochs == ep_o
     assert_eig_close(r.S ** 2 / bed.M * 2, eig_o, 1e-5)
     assert max_angle(r.U, U_o) <= 1e-3
     assert max_angle(V, V_o) <= 1e-3
-    assert max_angle(r.U[:, :4], U_o[:, :4]) <= 1e-6
+    assert max_angle(r.U[:, :4], U_o[:, :4]) <= 1e-4

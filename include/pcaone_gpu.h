@@ -80,6 +80,12 @@ int pcaone_gpu_permute(pcaone_ctx* ctx, const int32_t* perm);
  * std::default_random_engine, src/RSVD.hpp:67-70), written to perm (host, n int32). */
 int pcaone_shuffle_perm(uint64_t n, int32_t* perm);
 
+/* The structured SNP order of the reference's out-of-core winSVD (-m with --svd 2 without -S):
+ * permute_plink (src/FilePlink.cpp:298-405) deals the SNPs of each read buffer (buffer_gb GB,
+ * --buffer, default 2) round-robin to nbands contiguous bands. perm[new] = old, n int32, for
+ * pcaone_gpu_permute. */
+int pcaone_plink_perm(uint64_t nsnps, uint32_t nsamples, uint32_t buffer_gb, uint32_t nbands, int32_t* perm);
+
 /* The reference's sketch Omega (nrow x ncol, column-major FP64) drawn from
  * std::default_random_engine seeded with `seed` through std::normal_distribution (rand=1)
  * or uniform(-1,1) (rand=0), as RsvdOpData::initOmg (src/Halko.cpp:14-22). */
@@ -103,7 +109,11 @@ typedef struct {
                                  this context, as successive computeUSV calls on one
                                  FancyRsvdOpData do (src/Halko.hpp:68, src/Halko.cpp:159-163);
                                  0 starts from zero like a fresh process */
-  int32_t reserved;
+  int32_t block_snps;   /* winSVD with the out-of-core block plan of -m (src/Data.cpp:27-71):
+                           windows of block_snps SNPs (the reference's blocks) and band_factor
+                           blocks per band (FancyRsvdOpData::computeGandH out-of-core,
+                           src/Halko.cpp:228-269); 0 = the in-core windows of ceil(M / bands) */
+  int32_t band_factor;
 } pcaone_rsvd_opts;
 
 typedef struct {

@@ -241,15 +241,64 @@ def halko(Z: np.ndarray, k: int, os_: int, p: int, tol: float, seed: int = 101,
     return compute_usv(Z, k, os_, p, tol, gandh, st)
 
 
+def plink_perm(nsnps: int, nsamples: int, nbands: int, gb: int = 2) -> np.ndarray:
+    """permute_plink (src/FilePlink.cpp:298-405): the out-of-core SNP order. Each read buffer (a
+    multiple of nbands SNPs, gb GB at most) deals its SNPs round-robin to nbands contiguous
+    bands; perm[new] = old."""
+    M, bpr = nsnps, (nsamples + 3) >> 2
+    two = min(int(np.floor(1073741824 * gb / bpr)), M)
+    bufsize = two // nbands
+    two = bufsize * nbands
+    nblocks = (M + two - 1) // two
+    modr2 = M % two
+    bufidx = bufsize
+    modr, bandsize = M % nbands, (M + nbands - 1) // nbands
+    bandidx = [b * bandsize if (modr == 0 or b < modr) else modr * bandsize + (bandsize - 1) * (b - modr)
+               for b in range(nbands)]
+    perm = np.full(M, -1, dtype=np.int64)
+    for i in range(nblocks):
+        if i == nblocks - 1 and modr2 != 0:
+            two2 = M - (nblocks - 1) * two
+            bufsize = (two2 + nbands - 1) // nbands
+            modr2 = two2 % nbands
+        for b in range(nbands):
+            last = [bufsize - 1] if (i != nblocks - 1 or b < modr2 or modr2 == 0) else []
+            for j in list(range(bufsize - 1)) + last:
+                perm[i * bufidx + bandidx[b] + j] = i * two + j * nbands + b
+    assert (perm >= 0).all()
+    return perm.astype(np.int32)
+
+
+def block_plan(nsamples: int, nsnps: int, k: int, os_: int, memory_gb: float, bands: int):
+    """Data::prepare for the out-of-core winSVD (src/Data.cpp:27-71): (blocksize, band_factor)."""
+    l = k + os_
+    m = (3 * nsamples * l + 2 * nsnps * l + 5 * nsnps) / 134217728
+    m = 0 if memory_gb > 1.1 * m else m
+    bs = int(np.ceil(((m + memory_gb) * 134217728 - 3 * nsamples * l - 2 * nsnps * l - 5 * nsnps) / nsamples))
+    nblocks = int(np.ceil(nsnps / bs))
+    factor = 1
+    if nblocks < bands:
+        bs = int(np.ceil(nsnps / bands))
+    else:
+        factor = int(np.ceil(nblocks / bands))
+        bs = int(np.ceil(nsnps / (bands * factor)))
+    return bs, factor
+
+
 def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed: int = 101,
-           rand: int = 1, update_hook=None, state: dict | None = None) -> RsvdResult:
+           rand: int = 1, update_hook=None, state: dict | None = None, blocksize: int = 0,
+           band_factor: int = 1) -> RsvdResult:
     """Window-based RSVD, FancyRsvdOpData::computeGandH in-core (src/Halko.cpp:153-226).
     Z must already be column-permuted when the reference permutes (src/Halko.cpp:181-184).
 
     `state` carries the window sums H1/H2 between successive calls: FancyRsvdOpData keeps
     them as members (src/Halko.hpp:68) and only zeroes them when 2^pi >= bands
     (src/Halko.cpp:159-163), so a second computeUSV on the same operator (the EM loops,
-    src/Halko.cpp:301-336) starts from the previous call's leftover H2."""
+    src/Halko.cpp:301-336) starts from the previous call's leftover H2.
+
+    blocksize > 0 gives the out-of-core schedule (src/Halko.cpp:228-269): the windows are the
+    ceil(M / blocksize) blocks of the -m plan, bands start at band_factor blocks and the
+    "adjacent" update falls on block 2^(pi-1) * band_factor."""
     N, M = Z.shape
     l = k + os_
     st = _HalkoState(N, l, seed, rand)
@@ -261,7 +310,9 @@ def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed
     if state is not None:
         state["H1"], state["H2"] = H1, H2
     sched = {"bandsize": 1}
-    blocksize = int(np.ceil(M / bands))
+    bf = band_factor if blocksize > 0 else 1
+    blocksize = blocksize if blocksize > 0 else int(np.ceil(M / bands))
+    nwin = int(np.ceil(M / blocksize))
 
     def gandh(pi):
         nonlocal H1, H2
@@ -271,13 +322,13 @@ def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed
             H1[:] = 0
             H2[:] = 0
         if pi == 0:
-            sched["bandsize"] = 1
-        sched["bandsize"] = min(sched["bandsize"] * 2, bands)
+            sched["bandsize"] = bf
+        sched["bandsize"] = min(sched["bandsize"] * 2, nwin)
         bandsize = sched["bandsize"]
         G = np.zeros((M, l))
         H = None
         i = 1
-        for b in range(bands):
+        for b in range(nwin):
             s0 = b * blocksize
             s1 = M if (b + 1) * blocksize >= M else (b + 1) * blocksize
             if s0 < M:
@@ -287,7 +338,7 @@ def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed
                     H1 += Z[:, s0:s1] @ Gb
                 else:
                     H2 += Z[:, s0:s1] @ Gb
-            adjacent = pi > 0 and (b + 1) == 2 ** (pi - 1) and 2 ** pi < bands
+            adjacent = pi > 0 and (b + 1) == 2 ** (pi - 1) * bf and 2 ** pi < bands
             if (b + 1) < bandsize and not adjacent:
                 i += 1
                 continue
@@ -312,7 +363,7 @@ def winsvd(Z: np.ndarray, k: int, os_: int, p: int, tol: float, bands: int, seed
 
 def run_pca(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: int = 10,
             bands: int = 64, tol: float = 1e-4, seed: int = 101, rand: int = 1,
-            shuffle: bool = True, standardize_geno: bool = True):
+            shuffle: bool = True, standardize_geno: bool = True, memory: float = 0.0):
     """Plain (no EM) PLINK PCA, run_pca_with_halko (src/Halko.cpp:272-293, 338-342).
     Returns (eigvals, sigvals, U, V, F, epochs) with V in original SNP order."""
     os_ = max(oversamples, k)  # src/Cmd.cpp:190
@@ -320,6 +371,12 @@ def run_pca(bed: Bed, k: int = 10, svd: int = 2, maxp: int = 20, oversamples: in
     if svd == 1:
         res = halko(Z, k, os_, maxp, tol, seed, rand)
         V = res.V
+    elif svd == 2 and memory > 0:  # out-of-core: permute_plink order and the block plan
+        perm = plink_perm(bed.M, bed.N, bands) if shuffle else np.arange(bed.M, dtype=np.int32)
+        bs, bf = block_plan(bed.N, bed.M, k, os_, memory, bands)
+        res = winsvd(Z[:, perm], k, os_, maxp, tol, bands, seed, rand, blocksize=bs, band_factor=bf)
+        V = np.empty_like(res.V)
+        V[perm] = res.V
     elif svd == 2:
         perm = shuffle_perm(bed.M) if shuffle else np.arange(bed.M, dtype=np.int32)
         res = winsvd(Z[:, perm], k, os_, maxp, tol, bands, seed, rand)

@@ -31,7 +31,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
            "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
-           "pcaone_gpu_residuals", "pcaone_gpu_load_dense"]
+           "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm"]
 
 
 class PcaoneError(RuntimeError):
@@ -47,7 +47,7 @@ class RsvdOpts(ctypes.Structure):
                 ("ploidy", ctypes.c_int32), ("seed", ctypes.c_int32), ("rand", ctypes.c_int32),
                 ("tol", ctypes.c_double), ("verbose", ctypes.c_int32),
                 ("profile", ctypes.c_int32), ("carry_window_state", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("block_snps", ctypes.c_int32), ("band_factor", ctypes.c_int32)]
 
 
 class RsvdReport(ctypes.Structure):
@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_gram_product.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, u32, vp]
         L.pcaone_gpu_residuals.argtypes = [vp, vp, vp, vp, u32, u64, u64, vp]
         L.pcaone_gpu_load_dense.argtypes = [vp, vp, u64, u32]
+        L.pcaone_plink_perm.argtypes = [u64, u32, u32, u32, vp]
         L.pcaone_gpu_gl_update.argtypes = [vp, vp, vp, vp, u32]
         L.pcaone_gpu_gl_grm.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp]
         L.pcaone_gpu_product_t_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, u32, vp]
@@ -111,6 +112,33 @@ def shuffle_perm(n: int) -> np.ndarray:
     out = np.zeros(n, dtype=np.int32)
     lib().pcaone_shuffle_perm(n, _ptr(out))
     return out
+
+
+def plink_perm(nsnps: int, nsamples: int, nbands: int, buffer_gb: int = 2) -> np.ndarray:
+    """The reference's out-of-core SNP order (permute_plink, src/FilePlink.cpp:298-405)."""
+    out = np.zeros(nsnps, dtype=np.int32)
+    st = lib().pcaone_plink_perm(nsnps, nsamples, buffer_gb, nbands, _ptr(out))
+    if st != 0:
+        raise PcaoneError(st, "pcaone_plink_perm failed")
+    return out
+
+
+def block_plan(nsamples: int, nsnps: int, k: int, oversamples: int, memory_gb: float, bands: int):
+    """Data::prepare's out-of-core plan for the winSVD (src/Data.cpp:27-71): (blocksize,
+    nblocks, band_factor) for -m memory_gb, l = k + max(oversamples, k)."""
+    import math
+    l = k + max(oversamples, k)
+    m = (3 * nsamples * l + 2 * nsnps * l + 5 * nsnps) / 134217728
+    m = 0 if memory_gb > 1.1 * m else m
+    bs = math.ceil(((m + memory_gb) * 134217728 - 3 * nsamples * l - 2 * nsnps * l - 5 * nsnps) / nsamples)
+    nblocks = math.ceil(nsnps / bs)
+    factor = 1
+    if nblocks < bands:
+        bs = math.ceil(nsnps / bands)
+    else:
+        factor = math.ceil(nblocks / bands)
+        bs = math.ceil(nsnps / (bands * factor))
+    return bs, math.ceil(nsnps / bs), factor
 
 
 def omega(seed: int, nrow: int, ncol: int, rand: int = 1) -> np.ndarray:
@@ -198,12 +226,12 @@ class GpuContext:
              bands: int = 64, precision: int | str = PREC_FP32, standardize: bool = True,
              ploidy: int = 2, seed: int = 101, rand: int = 1, tol: float = 1e-4,
              verbose: bool = False, profile: bool = False, want_v: bool = True,
-             carry: bool = False) -> RsvdResult:
+             carry: bool = False, block_snps: int = 0, band_factor: int = 0) -> RsvdResult:
         if isinstance(precision, str):
             precision = PRECISIONS[precision]
         os_ = max(oversamples, k)  # src/Cmd.cpp:190
         o = RsvdOpts(k, os_, maxp, svd, bands, precision, int(standardize), ploidy, seed,
-                     rand, tol, int(verbose), int(profile), int(carry), 0)
+                     rand, tol, int(verbose), int(profile), int(carry), block_snps, band_factor)
         U = np.zeros((k, self.N))
         S = np.zeros(k)
         V = np.zeros((k, self.M)) if want_v else None

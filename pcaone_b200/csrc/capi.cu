@@ -233,6 +233,51 @@ int pcaone_shuffle_perm(uint64_t n, int32_t* perm) {
   return PCAONE_OK;
 }
 
+int pcaone_plink_perm(uint64_t nsnps, uint32_t nsamples, uint32_t buffer_gb, uint32_t nbands, int32_t* perm) {
+  // permute_plink (src/FilePlink.cpp:298-405) without its file copies: the input is read in
+  // buffers of a multiple of nbands SNPs (buffer_gb GB at most); within a buffer SNP
+  // j * nbands + b goes to band b, whose SNPs are stored contiguously from bandidx[b]
+  // (bands as equal as possible, the first M % nbands one SNP longer); the last, shorter
+  // buffer deals its SNPs round-robin to the first bands. perm[new] = old.
+  if (!perm || nsnps == 0 || nbands == 0 || nsamples == 0) return PCAONE_EBADARG;
+  const uint64_t M = nsnps, bpr = (nsamples + 3) >> 2, nb = nbands;
+  uint64_t two = (uint64_t)std::floor(1073741824.0 * buffer_gb / (double)bpr);
+  if (two > M) two = M;
+  uint64_t bufsize = two / nb;
+  if (bufsize == 0) return PCAONE_EBADARG;
+  two = bufsize * nb;
+  const uint64_t nblocks = (M + two - 1) / two;
+  uint64_t modr2 = M % two;
+  const uint64_t bufidx = bufsize;
+  std::vector<uint64_t> bandidx(nb);
+  const uint64_t modr = M % nb, bandsize = (M + nb - 1) / nb;
+  for (uint64_t b = 0; b < nb; ++b)
+    bandidx[b] = (modr == 0 || b < modr) ? b * bandsize : modr * bandsize + (bandsize - 1) * (b - modr);
+  std::vector<char> seen(M, 0);
+  for (uint64_t i = 0; i < nblocks; ++i) {
+    if (i == nblocks - 1 && modr2 != 0) {
+      const uint64_t two2 = M - (nblocks - 1) * two;
+      bufsize = (two2 + nb - 1) / nb;
+      modr2 = two2 % nb;
+    }
+    for (uint64_t b = 0; b < nb; ++b) {
+      uint64_t j = 0;
+      auto put = [&](uint64_t jj) {
+        const uint64_t ia = i * two + jj * nb + b, ib = i * bufidx + bandidx[b] + jj;
+        if (ia < M && ib < M) {
+          perm[ib] = (int32_t)ia;
+          seen[ib] = 1;
+        }
+      };
+      for (; j + 1 < bufsize; ++j) put(j);
+      if (i != nblocks - 1 || b < modr2 || modr2 == 0) put(j);
+    }
+  }
+  for (uint64_t t = 0; t < M; ++t)
+    if (!seen[t]) return PCAONE_EBADARG;
+  return PCAONE_OK;
+}
+
 int pcaone_omega(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out) {
   if (!out) return PCAONE_EBADARG;
   omega_host(seed, rand, nrow, ncol, out);

@@ -163,8 +163,10 @@ void free_all(pcaone_ctx* c);
 void launch_fix_padding(pcaone_ctx* c);
 void launch_counts(pcaone_ctx* c);
 void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out);
-void build_transposed(pcaone_ctx* c, int bands);
-void set_window_layout(pcaone_ctx* c, int bands);  // layout only (dense mode)
+// Window layout: bands windows of ceil(M / bands) SNPs, or of blocksize SNPs when it is set
+// (the out-of-core block plan); the transposed copy is built per window.
+void build_transposed(pcaone_ctx* c, int bands, uint64_t blocksize = 0);
+void set_window_layout(pcaone_ctx* c, int bands, uint64_t blocksize = 0);  // layout only (dense mode)
 void build_empty_missing(pcaone_ctx* c);           // dense mode: no missing entries
 void build_missing_by_snp(pcaone_ctx* c);
 void build_missing_by_window_sample(pcaone_ctx* c);

@@ -250,10 +250,12 @@ void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out) {
   c->launches++;
 }
 
-static WindowLayout make_layout(pcaone_ctx* c, int bands) {
+// bands windows of blocksize SNPs; blocksize 0 = ceil(M / bands) (src/Halko.cpp:178), else the
+// blocks of the out-of-core plan (src/Data.cpp:56-71, bands = ceil(M / blocksize)).
+static WindowLayout make_layout(pcaone_ctx* c, int bands, uint64_t blocksize) {
   WindowLayout w;
   w.bands = bands;
-  w.blocksize = (uint64_t)std::ceil((double)c->M / bands);  // src/Halko.cpp:178
+  w.blocksize = blocksize ? blocksize : (uint64_t)std::ceil((double)c->M / bands);
   PG_REQUIRE(w.blocksize > 0, PCAONE_EBADARG, "empty windows");
   w.pitch = (uint32_t)round_up((w.blocksize + 3) / 4, kPitchAlign);
   for (int b = 0; b < bands; ++b) {
@@ -267,9 +269,10 @@ static WindowLayout make_layout(pcaone_ctx* c, int bands) {
   return w;
 }
 
-void set_window_layout(pcaone_ctx* c, int bands) {
-  if (c->win.bands == bands && !c->win.start.empty()) return;
-  c->win = make_layout(c, bands);
+void set_window_layout(pcaone_ctx* c, int bands, uint64_t blocksize) {
+  const uint64_t bs = blocksize ? blocksize : (uint64_t)std::ceil((double)c->M / bands);
+  if (c->win.bands == bands && c->win.blocksize == bs && !c->win.start.empty()) return;
+  c->win = make_layout(c, bands, blocksize);
   c->miss_ws_valid = false;
 }
 
@@ -290,9 +293,10 @@ void build_empty_missing(pcaone_ctx* c) {
   }
 }
 
-void build_transposed(pcaone_ctx* c, int bands) {
-  if (c->bedT_valid && c->win.bands == bands) return;
-  WindowLayout w = make_layout(c, bands);
+void build_transposed(pcaone_ctx* c, int bands, uint64_t blocksize) {
+  const uint64_t bs = blocksize ? blocksize : (uint64_t)std::ceil((double)c->M / bands);
+  if (c->bedT_valid && c->win.bands == bands && c->win.blocksize == bs) return;
+  WindowLayout w = make_layout(c, bands, blocksize);
   size_t bytes = (size_t)bands * c->Npad * w.pitch;
   c->d_bedT = (uint8_t*)scratch(c, "d_bedT", bytes);
   PG_CUDA(cudaMemsetAsync(c->d_bedT, 0xFF, bytes, c->stream));

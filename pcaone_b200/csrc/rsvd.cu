@@ -321,18 +321,21 @@ struct Engine {
     process_window(0, H);
   }
 
+  // The in-core schedule runs over the o.bands windows; with the out-of-core block plan the
+  // windows are the nblocks blocks and bands start at band_factor blocks (src/Halko.cpp:228-
+  // 269); the two coincide for band_factor = 1 and nblocks = bands.
   void epoch_winsvd(int pi) {
-    const int bands = o.bands;
+    const int bands = o.bands, nwin = c->win.bands, bf = o.block_snps > 0 ? std::max(1, o.band_factor) : 1;
     if (pi == 0) init_omega();
     if (std::pow(2.0, pi) >= bands) {
       zero(c, H1, Npad * l);
       zero(c, H2, Npad * l);
     }
-    if (pi == 0) bandsize = 1;
-    bandsize = std::min(bandsize * 2, bands);
-    for (int b = 0, i = 1; b < bands; ++b, ++i) {
+    if (pi == 0) bandsize = bf;
+    bandsize = std::min(bandsize * 2, nwin);
+    for (int b = 0, i = 1; b < nwin; ++b, ++i) {
       process_window(b, i <= bandsize / 2 ? H1 : H2);
-      const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) && std::pow(2.0, pi) < bands;
+      const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) * bf && std::pow(2.0, pi) < bands;
       if ((b + 1) < bandsize && !adjacent) continue;
       if (!((i == bandsize) || (i == bandsize / 2) || adjacent)) continue;
       timed([&] { update_omega(H1, H2); }, 2);
@@ -358,7 +361,8 @@ struct Engine {
   void run(double* U, double* S, double* V, pcaone_rsvd_report* rep) {
     // zero the FP64 work buffers once so padded rows stay zero; the winSVD window sums are
     // kept from the previous call when asked to and still valid for this shape and data
-    const uint64_t key = ((uint64_t)N * 131 + (uint64_t)l) * 1031 + (uint64_t)o.bands + (c->generation << 40);
+    const uint64_t key = ((uint64_t)N * 131 + (uint64_t)l) * 1031 + (uint64_t)o.bands + ((uint64_t)o.block_snps << 20) +
+                         (c->generation << 40);
     zero(c, H, Npad * l);
     if (!(o.svd == 2 && o.carry_window_state && c->h12_key == key)) {
       zero(c, H1, Npad * l);
@@ -633,18 +637,23 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
              "the -w/--batches must be a power of 2 and the minimun is 4.");
   PG_REQUIRE(o.maxp >= 0, PCAONE_EBADARG, "maxp must be >= 0");
   PG_REQUIRE(o.ploidy == 1 || o.ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
-  const int bands = o.svd == 1 ? 1 : o.bands;
+  PG_REQUIRE(o.block_snps >= 0 && o.band_factor >= 0, PCAONE_EBADARG, "bad block plan");
+  // the out-of-core block plan changes only the winSVD windows; Halko's result does not depend
+  // on the blocks
+  const bool blocks = o.svd == 2 && o.block_snps > 0;
+  const int bands = o.svd == 1 ? 1 : (blocks ? (int)((c->M + o.block_snps - 1) / o.block_snps) : o.bands);
+  const uint64_t blocksize = blocks ? (uint64_t)o.block_snps : 0;
   if (c->dense) {
     // dense posterior matrix: already centred and not standardised in the EM steps; the
     // epilogues see F = 0 and s = 2 so that G = E^T Omega and B2 = G exactly
-    set_window_layout(c, bands);
+    set_window_layout(c, bands, blocksize);
     build_empty_missing(c);
     std::vector<double> two(c->M, 2.0);
     PG_CUDA(cudaMemcpyAsync(c->d_scale, two.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
     PG_REQUIRE(o.precision != PCAONE_PREC_FP64, PCAONE_EBADARG, "the PCAngsd matrix is FP32");
   } else {
-    build_transposed(c, bands);
+    build_transposed(c, bands, blocksize);
     build_missing_by_snp(c);
     build_missing_by_window_sample(c);
     if (c->imputed) compute_imputed_ws(c);

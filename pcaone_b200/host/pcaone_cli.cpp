@@ -75,6 +75,7 @@ struct Params {
   int seed = 101, scale = -1;
   bool noshuffle = false, printv = false, haploid = false, emu = false, pcangsd = false;
   double tol = 1e-4, maf = 0.0, memory = 0.0, tolem = 1e-5;
+  unsigned buffer = 2;  // --buffer: GB per read buffer of the out-of-core permutation
   unsigned maxiter = 100;
   unsigned ncv = 20, imaxiter = 1000;  // IRAM (--svd 0): ncv = max(20, 2k + 1) (src/Cmd.cpp:189)
   double itol = 1e-6;
@@ -196,6 +197,7 @@ Params parse(int argc, char** argv) {
     else if (a == "-v" || a == "--verbose") p.verbose = (unsigned)num(next());
     else if (a == "-n" || a == "--threads") p.threads = (unsigned)num(next());
     else if (a == "-m" || a == "--memory") p.memory = num(next());
+    else if (a == "--buffer") p.buffer = (unsigned)num(next());
     else if (a == "--device") p.device = (int)num(next());
     else if (a == "--precision") {
       p.precision_set = true;
@@ -226,7 +228,12 @@ Params parse(int argc, char** argv) {
     p.maf = 1 - p.maf;
   }
   p.oversamples = std::max(p.oversamples, p.k);  // src/Cmd.cpp:190
-  if (p.memory > 0) fail("-m/--memory (out-of-core mode) is not provided by this build: inputs are kept in HBM");
+  // -m/--memory: the reference's out-of-core mode. The packed genotypes stay in device memory;
+  // what -m changes in the results (the permute_plink SNP order and the block-granular winSVD
+  // windows) is reproduced. The reference's own restrictions apply (src/Cmd.cpp:201-212).
+  if (p.memory > 0 && p.maf > 0) fail("does not support --maf filters for out-of-core mode yet! ");
+  if (p.memory > 0 && (p.emu || p.pcangsd || p.bfile.empty()))
+    fail("-m/--memory applies to a plain PCA of PLINK input in this build");
   return p;
 }
 
@@ -721,11 +728,63 @@ int main(int argc, char** argv) {
   }
 
   const bool perm_on = p.svd == 2 && !p.noshuffle;  // src/Cmd.cpp:216
+  // out-of-core plan (Data::prepare, src/Data.cpp:27-71): blocks of blocksize SNPs and, for the
+  // winSVD, band_factor blocks per band
+  int block_snps = 0, band_factor = 0;
+  if (p.memory > 0) {
+    const double l = p.k + p.oversamples;
+    double bs;
+    if (p.svd == 0) {
+      bs = std::ceil(p.memory * 134217728 / N);
+    } else {
+      double m = (3 * N * l + 2 * M * l + 5 * M) / 134217728;
+      if (p.memory > 1.1 * m) m = 0;
+      else std::cout << "\x1B[33m" << "minimum RAM required is " << m << " GB. trying to allocate more RAM." << "\033[0m\n";
+      bs = std::ceil(((m + p.memory) * 134217728 - 3 * N * l - 2 * M * l - 5 * M) / N);
+    }
+    long nblocks = (long)std::ceil((double)M / bs);
+    int factor = 1;
+    g_log.print(date(), "initial setting by -m/--memory: blocksize =", (long)bs, ", nblocks =", nblocks,
+                ", factor =", factor);
+    if (nblocks == 1) fail("only one block exists. please remove -m option");
+    if (p.svd == 2) {
+      if (nblocks < (long)p.bands) {
+        bs = std::ceil((double)M / p.bands);
+      } else {
+        factor = (int)std::ceil((double)nblocks / p.bands);
+        bs = std::ceil((double)M / (p.bands * factor));
+      }
+      nblocks = (long)std::ceil((double)M / bs);
+      g_log.print(date(), "after adjustment by PCAone: -w =", p.bands, ", blocksize =", (long)bs, ", nblocks =",
+                  nblocks, ", factor =", factor);
+      block_snps = (int)bs;
+      band_factor = factor;
+    }
+  }
   std::vector<int32_t> perm;
   if (perm_on) {
     perm.resize(M);
-    pcaone_shuffle_perm(M, perm.data());
-    g_log.print(date(), "permuting data matrix by columns in place");
+    if (p.memory > 0) {  // the structured order of permute_plink (src/FilePlink.cpp:298-405)
+      g_log.print(date(), "permute plink files. nsnps:", M, ", nsamples:", N);
+      if (pcaone_plink_perm(M, (uint32_t)N, p.buffer, p.bands, perm.data()) != PCAONE_OK)
+        fail("cannot plan the out-of-core permutation");
+      // the reference leaves the permuted fileset beside its outputs (src/FilePlink.cpp:339-403)
+      std::ofstream ob(p.fileout + ".perm.bed", std::ios::binary);
+      const char magic[3] = {0x6c, 0x1b, 0x01};
+      ob.write(magic, 3);
+      for (size_t i = 0; i < M; ++i) ob.write((const char*)&packed[(size_t)perm[i] * bpr], (std::streamsize)bpr);
+      std::vector<std::string> bims;
+      std::ifstream ib(p.bfile + ".bim");
+      for (std::string line; std::getline(ib, line);) bims.push_back(line);
+      std::ofstream obim(p.fileout + ".perm.bim");
+      for (size_t i = 0; i < M; ++i) obim << bims[perm[i]] << "\n";
+      std::ifstream ifam(p.bfile + ".fam");
+      std::ofstream ofam(p.fileout + ".perm.fam");
+      ofam << ifam.rdbuf();
+    } else {
+      pcaone_shuffle_perm(M, perm.data());
+      g_log.print(date(), "permuting data matrix by columns in place");
+    }
     check(ctx, pcaone_gpu_permute(ctx, perm.data()), "permute");
   }
   if (p.svd != 0)
@@ -746,6 +805,8 @@ int main(int argc, char** argv) {
   o.rand = (int)p.rand;
   o.tol = p.tol;
   o.verbose = p.verbose > 0;
+  o.block_snps = block_snps;
+  o.band_factor = band_factor;
   std::vector<double> U(N * p.k), S(p.k), V(M * p.k);
   pcaone_rsvd_report rep{};
   double gpu_s = 0;

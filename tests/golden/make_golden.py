@@ -89,6 +89,12 @@ CASES = [
                               "-V"], EIG + [".loadings"]),
     ("g1_pcangsd_bedS", "g1", ["-b", "{d}", "--pcangsd", "-k", "3", "-w", "8", "-S",
                                "--maxiter", "30", "-V"], EIG + [".loadings"]),
+    # out-of-core winSVD (-m): permute_plink order and the block plan (24 blocks, band factor 3;
+    # 8 blocks, band factor 1); -v 3 keeps the permuted .bim for the order's pin
+    ("g1_win_m", "g1", ["-b", "{d}", "-d", "2", "-k", "4", "-w", "8", "-m", "0.0001", "-V", "-v", "3"],
+     EIG + [".loadings", ".perm.bim"]),
+    ("g1_win_m8", "g1", ["-b", "{d}", "-d", "2", "-k", "4", "-w", "8", "-m", "0.0003", "-V"],
+     EIG + [".loadings"]),
     # IRAM (--svd 0): Spectra's restarted Lanczos on Z Z^T, converged to --itol 1e-6
     ("g1_iram", "g1", ["-b", "{d}", "-d", "0", "-k", "4", "-V"], EIG + [".loadings"]),
     # config 1 at its full shape: Halko k=10, oversampling 10, 8 epochs
@@ -130,7 +136,8 @@ def main() -> int:
             dpath = os.path.join(large_dir if ds in LARGE else HERE, ds)
             argv = [a.format(d=dpath, g=HERE) for a in args]
             out = os.path.join(tmp, name)
-            subprocess.run([REF] + argv + ["-o", out, "-v", "0"], check=True, env=env,
+            verb = [] if "-v" in argv else ["-v", "0"]
+            subprocess.run([REF] + argv + ["-o", out] + verb, check=True, env=env,
                            stdout=subprocess.DEVNULL)
             for suf in keep:
                 if ds in LARGE and suf == ".loadings":

@@ -32,6 +32,21 @@ def test_omega_and_shuffle_match_oracle():
     np.testing.assert_array_equal(pb.shuffle_perm(10007), O.shuffle_perm(10007))
 
 
+def test_plink_perm_and_block_plan_match_oracle():
+    # single read buffer (g1-like sizes) and many buffers (1e8 samples -> 40 SNPs per 1 GB
+    # buffer with 4 bands), with and without a ragged last buffer and ragged bands
+    for M, N, nb, gb in [(1000, 100, 8, 2), (1013, 100, 8, 2), (1000, 100_000_000, 4, 1),
+                         (1013, 100_000_000, 4, 1), (997, 100_000_000, 8, 1), (64, 7, 64, 2)]:
+        p = pb.plink_perm(M, N, nb, gb)
+        np.testing.assert_array_equal(p, O.plink_perm(M, N, nb, gb))
+        assert np.array_equal(np.sort(p), np.arange(M))
+    for N, M, k, os_, mem, nb in [(100, 1000, 4, 10, 0.0001, 8), (100, 1000, 4, 10, 0.0003, 8),
+                                  (2000, 50000, 10, 10, 0.05, 64)]:
+        bs, nblocks, bf = pb.block_plan(N, M, k, os_, mem, nb)
+        assert (bs, bf) == O.block_plan(N, M, k, max(os_, k), mem, nb)
+        assert nblocks == -(-M // bs)
+
+
 def test_create_without_device_fails_cleanly():
     import subprocess
     import sys

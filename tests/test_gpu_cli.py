@@ -31,7 +31,8 @@ def golden_args(name, tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
-@pytest.mark.parametrize("name", ["g1_halko", "g1_win", "g1_winS", "g1_nostd", "g1_win_unif"])
+@pytest.mark.parametrize("name", ["g1_halko", "g1_win", "g1_winS", "g1_nostd", "g1_win_unif", "g1_win_m",
+                                  "g1_win_m8"])
 def test_cli_matches_reference_outputs(tmp_path, prec, name):
     run_cli(golden_args(name, tmp_path) + ["--precision", prec], tmp_path)
     out = str(tmp_path / name)
@@ -48,6 +49,25 @@ def test_cli_matches_reference_outputs(tmp_path, prec, name):
     lines = open(out + ".eigvecs2").read().splitlines()
     assert lines[0].startswith("#FID\tIID\tPC1")
     assert len(lines) == 1 + O.count_lines(os.path.join(GOLDEN, "g1.fam"))
+
+
+@pytest.mark.gpu
+def test_cli_out_of_core_writes_permuted_fileset(tmp_path):
+    """-m leaves the permute_plink fileset (src/FilePlink.cpp:339-403) beside the outputs."""
+    run_cli(golden_args("g1_win_m", tmp_path), tmp_path)
+    out = str(tmp_path / "g1_win_m")
+    assert open(out + ".perm.bim").read() == open(ref_out("g1_win_m", ".perm.bim")).read()
+    bed = O.read_bed(os.path.join(GOLDEN, "g1"))
+    perm = O.plink_perm(bed.M, bed.N, 8)
+    raw = open(out + ".perm.bed", "rb").read()
+    assert raw[:3] == bytes([0x6C, 0x1B, 0x01])
+    bpr = (bed.N + 3) // 4
+    assert np.array_equal(np.frombuffer(raw[3:], np.uint8).reshape(bed.M, bpr), bed.packed.reshape(bed.M, bpr)[perm])
+    assert open(out + ".perm.fam").read() == open(os.path.join(GOLDEN, "g1.fam")).read()
+    # one block only: the reference refuses -m (src/Data.cpp:51)
+    r = run_cli(["-b", os.path.join(GOLDEN, "g1"), "-k", "4", "-m", "8", "-o", str(tmp_path / "one")], tmp_path,
+                check=False)
+    assert r.returncode != 0 and "only one block" in r.stdout + r.stderr
 
 
 @pytest.mark.gpu

@@ -101,6 +101,27 @@ def test_rsvd_matches_reference_golden(gpu, prec, name, kw, shuffle):
         assert r.gemm_launches > 0
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name,mem", [("g1_win_m", 0.0001), ("g1_win_m8", 0.0003)])
+def test_rsvd_out_of_core_plan_matches_reference_golden(gpu, prec, name, mem):
+    """-m: permute_plink order and winSVD windows of the -m block plan (src/Data.cpp:27-71,
+    src/Halko.cpp:228-269); three blocks per band for g1_win_m, one for g1_win_m8."""
+    bed = O.read_bed(os.path.join(GOLDEN, "g1"))
+    bs, nblocks, bf = pb.block_plan(bed.N, bed.M, 4, 10, mem, 8)
+    perm = pb.plink_perm(bed.M, bed.N, 8)
+    gpu.load_bed(bed.packed, bed.N)
+    gpu.permute(perm)
+    r = gpu.rsvd(svd=2, k=4, bands=8, precision=prec, block_snps=bs, band_factor=bf)
+    V = np.empty_like(r.V)
+    V[perm] = r.V
+    assert_eig_close(r.S ** 2 / bed.M * 2, ref_eigvals(name), 1e-5)
+    tol = 2e-6 if prec == "fp64" else 5e-4
+    assert_cols_close(r.U, ref_table(name, ".eigvecs"), tol)
+    assert_cols_close(V, O.read_table(os.path.join(GOLDEN, "ref", name + ".loadings")), tol)
+    eig_o, S_o, U_o, V_o, F_o, ep_o = O.run_pca(bed, k=4, bands=8, memory=mem)
+    assert r.epochs == ep_o
+
+
 @pytest.mark.parametrize("svd,bands", [(1, 0), (2, 16), (2, 64)])
 def test_rsvd_matches_oracle_larger(gpu, svd, bands):
     bed = random_bed(1502, 9001, seed=5, miss=0.01)

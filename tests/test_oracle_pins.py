@@ -31,6 +31,8 @@ def test_allele_freq_matches_reference_mbim():
     ("g1_winS", 2, dict(k=4, bands=8, shuffle=False)),
     ("g1_win_unif", 2, dict(k=3, bands=4, rand=0, seed=3, maxp=5)),
     ("g1_nostd", 1, dict(k=3, maxp=5, tol=0.0, standardize_geno=False)),
+    ("g1_win_m", 2, dict(k=4, bands=8, memory=0.0001)),
+    ("g1_win_m8", 2, dict(k=4, bands=8, memory=0.0003)),
 ])
 def test_oracle_rsvd_matches_reference(name, svd, kw):
     bed = g("g1")
@@ -167,3 +169,20 @@ def test_oracle_dense_eig_matches_reference_iram():
     assert_eig_close(eig, ref_eigvals("g1_iram"), 1e-5)
     assert_cols_close(U, ref_table("g1_iram", ".eigvecs"), 2e-5)
     assert_cols_close(V, ref_table("g1_iram", ".loadings"), 2e-5)
+
+
+def test_oracle_plink_perm_matches_reference_perm_bim():
+    # -m writes the permuted .bim (src/FilePlink.cpp:298-405); row i of it is SNP perm[i]
+    bed = g("g1")
+    ids = [line.split()[1] for line in open(os.path.join(GOLDEN, "g1.bim"))]
+    ref = [line.split()[1] for line in open(os.path.join(GOLDEN, "ref", "g1_win_m.perm.bim"))]
+    perm = O.plink_perm(bed.M, bed.N, 8)
+    assert [ids[j] for j in perm] == ref
+
+
+def test_oracle_block_plan_windows():
+    # the plans behind the two -m fixtures (203 samples, 1500 SNPs, -w 8): three blocks of 63
+    # SNPs per band, and one block of 188 SNPs per band
+    bed = g("g1")
+    assert O.block_plan(bed.N, bed.M, 4, 10, 0.0001, 8) == (63, 3)
+    assert O.block_plan(bed.N, bed.M, 4, 10, 0.0003, 8) == (188, 1)

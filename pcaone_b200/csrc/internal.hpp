@@ -101,7 +101,7 @@ struct pcaone_ctx {
   int64_t n_missing = 0;
   int64_t* d_miss_snp_ptr = nullptr;   // M + 1
   int32_t* d_miss_snp_idx = nullptr;   // sample index per entry
-  int64_t* d_miss_ws_ptr = nullptr;    // bands * N + 1
+  int64_t* d_miss_ws_ptr = nullptr;    // bands * Npad + 1, sample-major: row i * bands + b
   int32_t* d_miss_ws_idx = nullptr;    // SNP index (global, current order) per entry
   bool miss_snp_valid = false, miss_ws_valid = false;
 

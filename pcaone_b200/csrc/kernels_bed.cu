@@ -100,8 +100,15 @@ __global__ void k_transpose(const uint8_t* __restrict__ bed, uint32_t pitch, uin
 }
 
 // Warp per packed row: count missing codes (01) in a row of `nbytes` bytes.
-__global__ void k_count_missing_rows(const uint8_t* __restrict__ base, uint32_t pitch,
-                                     uint64_t nrows, uint32_t nwords, int64_t* __restrict__ cnt) {
+// CSR row of packed row r: r itself (by-SNP list, nwin = 0), or for the (window, sample)
+// list, where packed row r = b * npad + i, the sample-major row i * nwin + b, so that the
+// entries of sample i over a run of consecutive windows [b0, b1) are one contiguous range.
+__device__ __forceinline__ uint64_t csr_row(uint64_t r, uint32_t npad, uint32_t nwin) {
+  return nwin ? (r % npad) * nwin + r / npad : r;
+}
+
+__global__ void k_count_missing_rows(const uint8_t* __restrict__ base, uint32_t pitch, uint64_t nrows,
+                                     uint32_t nwords, uint32_t npad, uint32_t nwin, int64_t* __restrict__ cnt) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (r >= nrows) return;
@@ -112,7 +119,7 @@ __global__ void k_count_missing_rows(const uint8_t* __restrict__ base, uint32_t 
     n += __popc((x & 0x55555555u) & ~((x >> 1) & 0x55555555u));
   }
   for (int o = 16; o; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-  if (lane == 0) cnt[r] = n;
+  if (lane == 0) cnt[csr_row(r, npad, nwin)] = n;
 }
 
 // ---- exclusive prefix sum of int64 counts on the device (CSR row pointers): per 1024-element
@@ -187,17 +194,19 @@ __global__ void k_missing_counts(const uint32_t* __restrict__ nonmiss, uint64_t 
 }
 
 // Warp per packed row: write the positions of missing codes in increasing order.
-// idx_out[ptr[r] + t] = pos_offset(r) + position. pos_base is added to every position;
-// for the (window, sample) lists, row r = b * Npad + i and pos_base = window start of b.
+// idx_out[ptr[csr_row(r)] + t] = pos_offset(r) + position. pos_base is added to every
+// position; for the (window, sample) lists, row r = b * Npad + i and pos_base = window start
+// of b (rows_per_base = npad).
 __global__ void k_fill_missing_rows(const uint8_t* __restrict__ base, uint32_t pitch,
                                     uint64_t nrows, uint32_t nwords,
                                     const int64_t* __restrict__ ptr, int32_t* __restrict__ idx,
-                                    const uint64_t* __restrict__ row_pos_base, uint32_t rows_per_base) {
+                                    const uint64_t* __restrict__ row_pos_base, uint32_t rows_per_base,
+                                    uint32_t nwin) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (r >= nrows) return;
   const uint32_t* row = reinterpret_cast<const uint32_t*>(base + r * pitch);
-  int64_t out = ptr[r];
+  int64_t out = ptr[csr_row(r, rows_per_base, nwin)];
   uint64_t pbase = row_pos_base ? row_pos_base[r / rows_per_base] : 0;
   for (uint32_t w0 = 0; w0 < nwords; w0 += 32) {
     uint32_t w = w0 + lane;
@@ -337,7 +346,7 @@ void build_missing_by_snp(pcaone_ctx* c) {
   c->d_miss_snp_idx = (int32_t*)scratch(c, "d_miss_snp_idx", std::max<int64_t>(c->n_missing, 1) * 4);
   uint64_t threads = c->M * 32;
   k_fill_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-      c->d_bed, c->pitch, c->M, c->pitch / 4, c->d_miss_snp_ptr, c->d_miss_snp_idx, nullptr, 1);
+      c->d_bed, c->pitch, c->M, c->pitch / 4, c->d_miss_snp_ptr, c->d_miss_snp_idx, nullptr, 1, 0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
   c->miss_snp_valid = true;
@@ -350,7 +359,7 @@ void build_missing_by_window_sample(pcaone_ctx* c) {
   int64_t* d_cnt = (int64_t*)scratch(c, "miss_ws_cnt", rows * 8);
   uint64_t threads = rows * 32;
   k_count_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-      c->d_bedT, c->win.pitch, rows, c->win.pitch / 4, d_cnt);
+      c->d_bedT, c->win.pitch, rows, c->win.pitch / 4, c->Npad, (uint32_t)c->win.bands, d_cnt);
   PG_CHECK_LAUNCH();
   c->d_miss_ws_ptr = (int64_t*)scratch(c, "d_miss_ws_ptr", (rows + 1) * 8);
   const int64_t total = device_exclusive_scan(c, d_cnt, rows, c->d_miss_ws_ptr);
@@ -360,7 +369,7 @@ void build_missing_by_window_sample(pcaone_ctx* c) {
                           c->stream));
   k_fill_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
       c->d_bedT, c->win.pitch, rows, c->win.pitch / 4, c->d_miss_ws_ptr, c->d_miss_ws_idx, d_base,
-      c->Npad);
+      c->Npad, (uint32_t)c->win.bands);
   PG_CHECK_LAUNCH();
   PG_CUDA(cudaStreamSynchronize(c->stream));
   c->launches += 2;

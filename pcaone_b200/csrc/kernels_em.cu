@@ -43,14 +43,14 @@ __global__ void k_impute_snp(const int64_t* __restrict__ ptr, const int32_t* __r
     val[e] = imputed_value(US, V, k, idx[e], (int64_t)j, Fc[j]);
 }
 
-// (window, sample) list: row r = b * Npad + i holds the SNPs of window b missing in sample i
+// (window, sample) list: CSR row r = i * nwin + b holds the SNPs of window b missing in sample i
 __global__ void k_impute_ws(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, uint64_t rows,
-                            uint32_t npad, const double* __restrict__ US, const double* __restrict__ V,
+                            uint32_t nwin, const double* __restrict__ US, const double* __restrict__ V,
                             int k, const double* __restrict__ Fc, double* __restrict__ val) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (r >= rows) return;
-  const int64_t i = (int64_t)(r % npad);
+  const int64_t i = (int64_t)(r / nwin);
   for (int64_t e = ptr[r] + lane; e < ptr[r + 1]; e += 32) {
     const int64_t j = idx[e];
     val[e] = imputed_value(US, V, k, i, j, Fc[j]);
@@ -86,7 +86,7 @@ void compute_imputed_ws(pcaone_ctx* c) {
   const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
   uint64_t threads = rows * 32;
   k_impute_ws<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-      c->d_miss_ws_ptr, c->d_miss_ws_idx, rows, c->Npad, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
+      c->d_miss_ws_ptr, c->d_miss_ws_idx, rows, (uint32_t)c->win.bands, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
       c->d_miss_ws_val);
   PG_CHECK_LAUNCH();
   c->launches++;

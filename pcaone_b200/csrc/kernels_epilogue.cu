@@ -81,10 +81,64 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
   __syncwarp();
 }
 
+// Unweighted warp-cooperative gather for rows of l = 4 G FP32 values (16-byte aligned rows):
+// out[c] = sum_{e in [e0, e1)} rows[idx_e - row0][c]. The warp takes 32 entries at a time
+// (lane t loads the index of entry t); the rows of the batch are then split over R = 32 / G
+// row groups of G lanes, lane g of a group owning columns 4g .. 4g + 3, and each lane issues
+// all its float4 loads of the batch (ceil(32 / R) rows) before it adds them, so up to 32 rows
+// are in flight per warp. FP64 sums; the row groups are combined in a fixed order
+// (deterministic) into out (shared memory of this warp).
+template <int G>
+__device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
+                                          const float* __restrict__ rows, int64_t row0, double* out) {
+  constexpr int R = 32 / G, T = (32 + R - 1) / R;
+  const int lane = threadIdx.x & 31, grp = lane / G, cg = lane - grp * G;
+  const bool active = grp < R;
+  const float4* rows4 = reinterpret_cast<const float4*>(rows);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int cnt = (int)(e1 - base < 32 ? e1 - base : 32);
+    const int64_t my = lane < cnt ? (int64_t)idx[base + lane] - row0 : 0;
+    float4 v[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int src = grp + R * t;
+      const int64_t ii = __shfl_sync(0xffffffffu, my, src & 31);
+      v[t] = (active && src < cnt) ? __ldg(rows4 + ii * G + cg) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      acc[0] += (double)v[t].x;
+      acc[1] += (double)v[t].y;
+      acc[2] += (double)v[t].z;
+      acc[3] += (double)v[t].w;
+    }
+  }
+  for (int g = 0; g < R; ++g) {
+    if (active && grp == g)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) out[4 * cg + j] = (g == 0 ? 0.0 : out[4 * cg + j]) + acc[j];
+    __syncwarp();
+  }
+}
+
+// out = sum of the rows for l % 4 == 0 and ceil(l / 8) = CPL, i.e. G = l / 4 = 2 CPL - 1 or
+// 2 CPL (the two instantiations a kernel of that CPL can meet).
+template <int CPL>
+__device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
+                                         const float* __restrict__ rows, int64_t row0, int l, double* out) {
+  if ((l >> 2) == 2 * CPL)
+    sum_rows4<2 * CPL>(e0, e1, idx, rows, row0, out);
+  else
+    sum_rows4<(2 * CPL - 1 > 0 ? 2 * CPL - 1 : 1)>(e0, e1, idx, rows, row0, out);
+}
+
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
-// per-CTA partials of h0; with p.Gf also the FP32 copy of G the second gather reads, with
-// p.qmax the column maxima of |B2| the int8 quantiser needs. The sparse gather reads the
-// FP32 copy of Omega when p.omega_f is set (half the L2 bytes of the FP64 rows).
+// per-CTA partials of h0; with p.Gf also the FP32 rows the second gather reads (G, or
+// s F G when no imputed values are set, which makes that gather unweighted), with p.qmax the
+// column maxima of |B2| the int8 quantiser needs. The sparse gather reads the FP32 copy of
+// Omega when p.omega_f is set (half the L2 bytes of the FP64 rows); without imputed values
+// its weight is F_j for every entry, so it sums the rows unweighted (sum_rows, l % 4 == 0).
 template <typename T, int CPL>
 __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
@@ -97,24 +151,30 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
     for (int c = threadIdx.x; c < p.l; c += blockDim.x) smax[c] = 0ull;
     __syncthreads();
   }
+  const int64_t wl = p.wlen ? p.wlen : p.m, d1ws = p.d1_ws ? p.d1_ws : p.m, b2ws = p.b2_ws ? p.b2_ws : p.m;
+  const int64_t d1rows = p.d1_rows ? p.d1_rows : p.m;
   for (int64_t jl = (int64_t)blockIdx.x * nwarps + warp; jl < p.m; jl += (int64_t)gridDim.x * nwarps) {
     const int64_t j = p.start + jl;
+    const int64_t wi = jl / wl, r = jl - wi * wl, d1row = wi * d1ws + r, b2row = wi * b2ws + r;
     const double F = p.F[j];
     const double s = p.scale[j];
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
     const double* mv = p.miss_val;
     auto w = [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; };
-    if (p.omega_f)
+    const bool plain = !mv && p.omega_f && (p.l & 3) == 0;
+    if (plain)
+      sum_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp);
+    else if (p.omega_f)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, w, ssp);
     else
       gather_rows<CPL>(e0, e1, p.miss_idx, p.omega, 0, p.l, w, ssp);
     for (int c = lane; c < p.l; c += 32) {
       double d = 0.0;
-      for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * p.m + jl) * p.l + c];
-      const double sparse = ssp[c];
+      for (int sp = 0; sp < p.ksplit; ++sp) d += (double)D1[((int64_t)sp * d1rows + d1row) * p.l + c];
+      const double sparse = plain ? F * ssp[c] : ssp[c];
       double g = s * (0.5 * d - F * p.wsum[c] + sparse);
       p.G[j * p.l + c] = g;
-      if (p.Gf) p.Gf[jl * p.l + c] = (float)g;
+      if (p.Gf) p.Gf[jl * p.l + c] = (float)(mv ? g : s * F * g);
       const T b2 = (T)(0.5 * s * g);
       if (p.qmax) atomicMax(&smax[c], (unsigned long long)__double_as_longlong(fabs((double)b2)));
       if (p.bt2) {
@@ -125,7 +185,7 @@ __global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
         p.bt2[bt_elem(c, kp, np)] = hi;
         p.bt2[bt_elem(p.bt_half + c, kp, np)] = __float2bfloat16_rn(x - __bfloat162float(hi));
       } else {
-        B2[jl * p.l + c] = b2;
+        B2[b2row * p.l + c] = b2;
       }
       sh0[warp * p.l + c] += s * F * g;
     }
@@ -201,19 +261,23 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __res
   }
 }
 
-// Warp per sample: H[i] += sum_split D2 - h0 + sparse.
+// Warp per sample: H[i] += sum_split D2 - h0 + sparse, the sparse term over the sample's
+// missing entries in the windows [b0, b1).
 template <typename T, int CPL>
 __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
   extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = ssm + warp * p.l;
   for (int64_t i = (int64_t)blockIdx.x * nwarps + warp; i < p.n; i += (int64_t)gridDim.x * nwarps) {
-    const int64_t row = (int64_t)p.window * p.npad + i;
-    const int64_t e0 = p.miss_ptr[row], e1 = p.miss_ptr[row + 1];
+    const int64_t e0 = p.miss_ptr[i * p.nwin + p.b0], e1 = p.miss_ptr[i * p.nwin + p.b1];
     const double* mv = p.miss_val;
     const double *sc = p.scale, *F = p.F;
     auto w = [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); };
-    if (p.Gf)
+    if (p.Gf && !mv && (p.l & 3) == 0)  // Gf holds s F G: the sparse term is a plain row sum
+      sum_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp);
+    else if (p.Gf && !mv)
+      gather_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, [](int64_t, int) { return 1.0; }, ssp);
+    else if (p.Gf)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, w, ssp);
     else
       gather_rows<CPL>(e0, e1, p.miss_idx, p.G, 0, p.l, w, ssp);
@@ -227,26 +291,42 @@ __global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
   }
 }
 
+// CTAs of `threads` threads that fit on one SM at once for kernel fn with `smem` dynamic
+// shared memory (at least 1): the grid-stride epilogues launch exactly one resident wave.
+int resident_ctas(const void* fn, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    n = 1;
+  }
+  return std::max(1, n);
+}
+
 }  // namespace
 
 template <typename T>
 void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) {
   const int threads = 256, nwarps = threads / 32;
-  int nblk = (int)std::min<int64_t>(4 * c->sm_count, std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
-  double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
   const size_t smem = (size_t)2 * nwarps * p.l * 8 + (size_t)p.l * 8;
+  auto go = [&](auto kern) {
+    const int per_sm = resident_ctas((const void*)kern, threads, smem);
+    const int nblk = (int)std::min<int64_t>((int64_t)per_sm * c->sm_count,
+                                            std::max<int64_t>(1, (p.m + nwarps - 1) / nwarps));
+    double* part = (double*)scratch(c, "h0_part", (size_t)nblk * p.l * 8);
+    kern<<<nblk, threads, smem, c->stream>>>(p, D1, B2, part);
+    PG_CHECK_LAUNCH();
+    k_reduce_cols<<<p.l, kRedThreads, 0, c->stream>>>(part, nblk, p.l, h0);
+  };
   switch ((p.l + 7) / 8) {
-    case 1: k_prep<T, 1><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 2: k_prep<T, 2><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 3: k_prep<T, 3><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 4: k_prep<T, 4><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 5: k_prep<T, 5><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 6: k_prep<T, 6><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    case 7: k_prep<T, 7><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
-    default: k_prep<T, 8><<<nblk, threads, smem, c->stream>>>(p, D1, B2, part); break;
+    case 1: go(k_prep<T, 1>); break;
+    case 2: go(k_prep<T, 2>); break;
+    case 3: go(k_prep<T, 3>); break;
+    case 4: go(k_prep<T, 4>); break;
+    case 5: go(k_prep<T, 5>); break;
+    case 6: go(k_prep<T, 6>); break;
+    case 7: go(k_prep<T, 7>); break;
+    default: go(k_prep<T, 8>); break;
   }
-  PG_CHECK_LAUNCH();
-  k_reduce_cols<<<p.l, kRedThreads, 0, c->stream>>>(part, nblk, p.l, h0);
   PG_CHECK_LAUNCH();
   c->launches += 2;
 }
@@ -254,17 +334,21 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
 template <typename T>
 void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
   const int threads = 256, nwarps = threads / 32;
-  int nblk = (int)std::min<int64_t>(4 * c->sm_count, (p.n + nwarps - 1) / nwarps);
   const size_t smem = (size_t)nwarps * p.l * 8;
+  auto go = [&](auto kern) {
+    const int per_sm = resident_ctas((const void*)kern, threads, smem);
+    const int nblk = (int)std::min<int64_t>((int64_t)per_sm * c->sm_count, (p.n + nwarps - 1) / nwarps);
+    kern<<<nblk, threads, smem, c->stream>>>(p, D2);
+  };
   switch ((p.l + 7) / 8) {
-    case 1: k_accum<T, 1><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 2: k_accum<T, 2><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 3: k_accum<T, 3><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 4: k_accum<T, 4><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 5: k_accum<T, 5><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 6: k_accum<T, 6><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    case 7: k_accum<T, 7><<<nblk, threads, smem, c->stream>>>(p, D2); break;
-    default: k_accum<T, 8><<<nblk, threads, smem, c->stream>>>(p, D2); break;
+    case 1: go(k_accum<T, 1>); break;
+    case 2: go(k_accum<T, 2>); break;
+    case 3: go(k_accum<T, 3>); break;
+    case 4: go(k_accum<T, 4>); break;
+    case 5: go(k_accum<T, 5>); break;
+    case 6: go(k_accum<T, 6>); break;
+    case 7: go(k_accum<T, 7>); break;
+    default: go(k_accum<T, 8>); break;
   }
   PG_CHECK_LAUNCH();
   c->launches++;

@@ -105,7 +105,9 @@ struct I8Args {
   const uint8_t* a_tiles;  // tiled codes: block (pair, chunk) of 8192 bytes, chunk-fastest
   const int8_t* bq;        // quantised B, per chunk NP rows x 128 bytes (swizzled)
   const float* sig;        // 3 x LP piece scales
-  int64_t a_stride;        // chunks per pair in a_tiles (>= chunks)
+  int64_t a_stride;        // chunks per pair in a_tiles (>= cpw)
+  int64_t cpw;             // K chunks per window: chunk g lies in window g / cpw of a_tiles
+  int64_t win_bytes;       // bytes per window of a_tiles (0 for a single window)
   int64_t rows;            // valid rows (outputs written for r < rows)
   int64_t chunks;          // K chunks (C)
   int64_t upp;             // units per pair (P = ceil(C / UC))
@@ -218,8 +220,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_con
         const uint32_t bar = smem_u32(&full[s]);
         if (lane == 0) {
           mbar_arrive_tx(bar, nch * (kPairChunkBytes + C::SB));
-          bulk_load(smem_u32(sA + s * kStageA), args.a_tiles + (pair * args.a_stride + kc) * kPairChunkBytes,
-                    nch * kPairChunkBytes, bar);
+          for (uint32_t ch = 0; ch < nch; ++ch) {  // chunk by chunk: a unit may straddle two windows
+            const int64_t g = kc + ch, w = g / args.cpw;
+            bulk_load(smem_u32(sA + s * kStageA + ch * kPairChunkBytes),
+                      args.a_tiles + w * args.win_bytes + (pair * args.a_stride + (g - w * args.cpw)) * kPairChunkBytes,
+                      kPairChunkBytes, bar);
+          }
         } else {
           bulk_load(smem_u32(sB + s * kStageB), args.bq + kc * C::SB, nch * C::SB, bar);
         }
@@ -383,49 +389,55 @@ __device__ __forceinline__ void piece_scales(unsigned long long bits, float* s) 
   s[2] = s[1] / 254.0f;
 }
 
-__device__ __forceinline__ int8_t quant_piece(double x, const float* s, int p) {
-  double r = x, q = 0.0;
-  for (int i = 0; i <= p; ++i) {
-    q = fmin(127.0, fmax(-127.0, rint(r / (double)s[i])));
-    r -= q * (double)s[i];
-  }
-  return (int8_t)(int)q;
-}
-
 // Quantised B of one chunk per CTA: every byte of the chunk's NP x 128 image is written
-// (piece rows, zero rows past 3 LP and past l, zero K positions past K). Thread task (n, u)
-// = the 16-byte unit u (K positions 16u..16u+15 in decode order) of row n; position pp of
-// the unit holds code 16u + 2 (pp & 7) + (pp >> 3) (inverse of decode_word_i8). CTA 0
-// also writes the 3 x LP scales.
+// (piece rows, zero rows past 3 LP and past l, zero K positions that hold no operand row).
+// The image is assembled in shared memory: thread task = one (K position kk, column c)
+// element, whose three pieces (each the rounded residual of the previous ones, |q| <= 127) go
+// to rows c, LP + c, 2 LP + c at the byte that the decoder's order gives code kk (16-byte
+// unit u = kk / 16, byte 8 (o & 1) + (o >> 1) for o = kk % 16, units 128-byte swizzled); the
+// image then leaves as 16-byte stores. Operand row k is present when it lies in the first
+// wlen rows of its window of kpw rows (windows w = k / kpw) and w * wlen + (k % kpw) < mtot.
+// CTA 0 also writes the 3 x LP scales.
 template <typename T>
-__global__ void k_quant(const T* __restrict__ X, int64_t K, int l, int lp, int np,
-                        const unsigned long long* __restrict__ qmax, int8_t* __restrict__ bq, float* __restrict__ sig) {
+__global__ void __launch_bounds__(256) k_quant(const T* __restrict__ X, int64_t kpw, int64_t wlen, int64_t mtot,
+                                               int l, int lp, int np, const unsigned long long* __restrict__ qmax,
+                                               int8_t* __restrict__ bq, float* __restrict__ sig) {
+  __shared__ __align__(16) uint8_t img[192 * 128];
+  __shared__ float sc[3][64];
   const int64_t kc = blockIdx.x;
-  if (kc == 0)
-    for (int n = threadIdx.x; n < 3 * lp; n += blockDim.x) {
-      const int p = n / lp, c = n - p * lp;
-      float s[3] = {1.0f, 1.0f, 1.0f};
-      if (c < l) piece_scales(qmax[c], s);
-      sig[n] = s[p];
+  for (int c = threadIdx.x; c < lp; c += blockDim.x) {
+    float s[3] = {1.0f, 1.0f, 1.0f};
+    if (c < l) piece_scales(qmax[c], s);
+    sc[0][c] = s[0];
+    sc[1][c] = s[1];
+    sc[2][c] = s[2];
+    if (kc == 0) {
+      sig[c] = s[0];
+      sig[lp + c] = s[1];
+      sig[2 * lp + c] = s[2];
     }
-  for (int task = threadIdx.x; task < np * 8; task += blockDim.x) {
-    const int nrow = task >> 3, u = task & 7;
-    const int p = nrow / lp, c = nrow - p * lp;
-    uint32_t w[4] = {0u, 0u, 0u, 0u};
-    if (p < 3 && c < l) {
-      float s[3];
-      piece_scales(qmax[c], s);
-#pragma unroll
-      for (int pp = 0; pp < 16; ++pp) {
-        const int64_t k = kc * kChunk + 16 * u + 2 * (pp & 7) + (pp >> 3);
-        const double x = k < K ? (double)X[k * l + c] : 0.0;
-        const uint32_t b = (uint32_t)(uint8_t)quant_piece(x, s, p);
-        w[pp >> 2] |= b << (8 * (pp & 3));
-      }
-    }
-    *reinterpret_cast<uint4*>(bq + kc * (int64_t)np * 128 + (int64_t)nrow * 128 + ((u ^ (nrow & 7)) << 4)) =
-        make_uint4(w[0], w[1], w[2], w[3]);
   }
+  uint4* img4 = reinterpret_cast<uint4*>(img);
+  for (int t = threadIdx.x; t < np * 8; t += blockDim.x) img4[t] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  for (int e = threadIdx.x; e < kChunk * l; e += blockDim.x) {
+    const int kk = e / l, c = e - kk * l;
+    const int64_t k = kc * kChunk + kk, w = k / kpw, r = k - w * kpw;
+    if (r >= wlen || w * wlen + r >= mtot) continue;
+    double x = (double)X[k * l + c];
+    const int u = kk >> 4, o = kk & 15, pp = 8 * (o & 1) + (o >> 1);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const double s = (double)sc[p][c];
+      const double q = fmin(127.0, fmax(-127.0, rint(x / s)));
+      x -= q * s;
+      const int n = p * lp + c;
+      img[n * 128 + ((u ^ (n & 7)) << 4) + pp] = (uint8_t)(int8_t)(int)q;
+    }
+  }
+  __syncthreads();
+  uint4* dst = reinterpret_cast<uint4*>(bq + kc * (int64_t)np * 128);
+  for (int t = threadIdx.x; t < np * 8; t += blockDim.x) dst[t] = img4[t];
 }
 
 // ------------------------------------------------------------------ host side
@@ -473,11 +485,12 @@ void launch_np(pcaone_ctx* c, const I8Args& a) {
   PG_CHECK_LAUNCH();
 }
 
-// One product over the tiled codes of one window (a_stride chunks per pair row, rows valid,
-// K codes) and the quantised B (kpad K positions); out holds ks = make_plan(rows, K).ks
-// slots of rows x l partial sums.
+// One product over tiled codes (a_stride chunks per pair row, rows valid, K codes) and the
+// quantised B (kpad K positions); out holds ks = make_plan(rows, K).ks slots of rows x l
+// partial sums. With cpw > 0 the K chunks run over consecutive windows of a_tiles, cpw chunks
+// and win_bytes bytes per window (a run of windows as one product).
 void run_i8(pcaone_ctx* c, const uint8_t* a_tiles, int64_t a_stride, int64_t rows, int64_t K, const int8_t* bq,
-            const float* sig, int64_t kpad, int l, int ks, float* out) {
+            const float* sig, int64_t kpad, int l, int ks, float* out, int64_t cpw = 0, int64_t win_bytes = 0) {
   const int np = np_of(l);
   PG_REQUIRE(np <= 192, PCAONE_EBADARG, "sketch width too large for the int8 tensor-core path");
   const I8Plan p = make_plan(c, rows, K, np);
@@ -486,7 +499,11 @@ void run_i8(pcaone_ctx* c, const uint8_t* a_tiles, int64_t a_stride, int64_t row
     PG_CUDA(cudaMemsetAsync(out, 0, (size_t)ks * rows * l * sizeof(float), c->stream));
     return;
   }
-  PG_REQUIRE(p.chunks <= a_stride && p.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
+  if (cpw <= 0) {
+    cpw = p.chunks;
+    win_bytes = 0;
+  }
+  PG_REQUIRE(cpw <= a_stride && p.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
   PG_REQUIRE(((uintptr_t)a_tiles & 15) == 0 && ((uintptr_t)bq & 15) == 0, PCAONE_EBADARG,
              "operands not 16-byte aligned");
   I8Args a;
@@ -494,6 +511,8 @@ void run_i8(pcaone_ctx* c, const uint8_t* a_tiles, int64_t a_stride, int64_t row
   a.bq = bq;
   a.sig = sig;
   a.a_stride = a_stride;
+  a.cpw = cpw;
+  a.win_bytes = win_bytes;
   a.rows = rows;
   a.chunks = p.chunks;
   a.upp = p.upp;
@@ -559,11 +578,13 @@ void ensure_tiles(pcaone_ctx* c) {
   c->tile82_ptr = d2;
 }
 
-// Quantise a row-major K x l operand into the chunked piece layout (kpad / 128 chunks).
-// have_max: the column maxima in "i8_qmax<tag>" were already accumulated (by the first
-// epilogue); otherwise they are computed here.
+// Quantise a row-major operand of kpad rows x l into the chunked piece layout (kpad / 128
+// chunks); rows that hold no operand (see k_quant: windows of kpw rows with wlen present, mtot
+// in all) quantise to zero. have_max: the column maxima in "i8_qmax<tag>" were already
+// accumulated (by the first epilogue); otherwise they are computed here over the first K rows.
 template <typename T>
-void quantize(pcaone_ctx* c, const T* X, int64_t K, int l, int64_t kpad, const char* tag, bool have_max) {
+void quantize(pcaone_ctx* c, const T* X, int64_t K, int l, int64_t kpad, const char* tag, bool have_max,
+              int64_t kpw = 0, int64_t wlen = 0, int64_t mtot = 0) {
   const int np = np_of(l), lp = lp_of(l);
   const std::string t(tag);
   auto* qmax = (unsigned long long*)scratch(c, "i8_qmax" + t, 64 * sizeof(unsigned long long));
@@ -577,7 +598,11 @@ void quantize(pcaone_ctx* c, const T* X, int64_t K, int l, int64_t kpad, const c
     PG_CHECK_LAUNCH();
     c->launches++;
   }
-  k_quant<T><<<(unsigned)(kpad / kChunk), 256, 0, c->stream>>>(X, K, l, lp, np, qmax, bq, sig);
+  if (kpw <= 0) {
+    kpw = kpad;
+    wlen = mtot = K;
+  }
+  k_quant<T><<<(unsigned)(kpad / kChunk), 256, 0, c->stream>>>(X, kpw, wlen, mtot, l, lp, np, qmax, bq, sig);
   PG_CHECK_LAUNCH();
   c->launches++;
 }
@@ -627,10 +652,62 @@ void i8_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t rows
          kpad, l, ks, out);
 }
 
+// ---- runs of consecutive windows [b0, b1) as one product each (the tiled copies of the
+// windows are contiguous): the first product's rows are the windows' SNP pairs, each window
+// padded to p1 pairs (padding rows decode to zero); the second product's K runs over the
+// windows' chunks, each window padded to c2 chunks, with B2 in the same padded row layout.
+int64_t i8_seg_rows1(pcaone_ctx* c) { return tile_geom(c).p1 * 2 * kRows; }
+int64_t i8_seg_k2(pcaone_ctx* c) { return tile_geom(c).c2 * kChunk; }
+
+int i8_ksplit_seg(pcaone_ctx* c, int which, int nw, int l) {
+  const TileGeom g = tile_geom(c);
+  return which == 1 ? make_plan(c, (int64_t)nw * g.p1 * 2 * kRows, (int64_t)c->N, np_of(l)).ks
+                    : make_plan(c, (int64_t)c->N, (int64_t)nw * g.c2 * kChunk, np_of(l)).ks;
+}
+
+void i8_p1_seg(pcaone_ctx* c, int b0, int b1, int l, int ks, float* out) {
+  ensure_tiles(c);
+  const TileGeom g = tile_geom(c);
+  PG_REQUIRE(b0 >= 0 && b0 < b1 && b1 <= c->win.bands, PCAONE_EBADARG, "bad window run");
+  const int np = np_of(l);
+  auto* bq = (const int8_t*)scratch(c, "i8_bq1", (size_t)c->Npad * np);
+  auto* sig = (const float*)scratch(c, "i8_sig1", 3 * 64 * sizeof(float));
+  run_i8(c, (const uint8_t*)c->tile81_ptr + (size_t)b0 * g.p1 * g.c1 * kPairChunkBytes, g.c1,
+         (int64_t)(b1 - b0) * g.p1 * 2 * kRows, (int64_t)c->N, bq, sig, c->Npad, l, ks, out);
+}
+
+void i8_b2_seg(pcaone_ctx* c, const float* B2, int l, int b0, int b1) {
+  const TileGeom g = tile_geom(c);
+  const int64_t kpw = g.c2 * kChunk, kpad = (int64_t)(b1 - b0) * kpw;
+  const int64_t mtot = (int64_t)(c->win.stop[b1 - 1] - c->win.start[b0]);
+  PG_REQUIRE(c->i8_b2_max_ready, PCAONE_ESTATE, "column maxima of the window operand not gathered");
+  quantize<float>(c, B2, kpad, l, kpad, "2", c->i8_b2_max_ready, kpw, (int64_t)c->win.blocksize, mtot);
+  c->i8_b2_max_ready = false;
+}
+
+void i8_p2_seg(pcaone_ctx* c, int b0, int b1, int l, int ks, float* out) {
+  ensure_tiles(c);
+  const TileGeom g = tile_geom(c);
+  PG_REQUIRE(b0 >= 0 && b0 < b1 && b1 <= c->win.bands, PCAONE_EBADARG, "bad window run");
+  const int64_t kpad = (int64_t)(b1 - b0) * g.c2 * kChunk;
+  const int np = np_of(l);
+  auto* bq = (const int8_t*)scratch(c, "i8_bq2", (size_t)kpad * np);
+  auto* sig = (const float*)scratch(c, "i8_sig2", 3 * 64 * sizeof(float));
+  run_i8(c, (const uint8_t*)c->tile82_ptr + (size_t)b0 * g.p2 * g.c2 * kPairChunkBytes, g.c2, (int64_t)c->N, kpad,
+         bq, sig, kpad, l, ks, out, g.c2, g.p2 * g.c2 * kPairChunkBytes);
+}
+
 }  // namespace
 
 GemmFnT<float> gemm_i8() {
-  return GemmFnT<float>{i8_ksplit, i8_p1, i8_p2, i8_omega, i8_b2, nullptr, nullptr, i8_b2_qmax};
+  GemmFnT<float> f{i8_ksplit, i8_p1, i8_p2, i8_omega, i8_b2, nullptr, nullptr, i8_b2_qmax};
+  f.seg_rows1 = i8_seg_rows1;
+  f.seg_k2 = i8_seg_k2;
+  f.ksplit_seg = i8_ksplit_seg;
+  f.p1_seg = i8_p1_seg;
+  f.b2_seg = i8_b2_seg;
+  f.p2_seg = i8_p2_seg;
+  return f;
 }
 
 }  // namespace pg

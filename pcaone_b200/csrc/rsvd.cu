@@ -246,7 +246,9 @@ struct Engine {
     const uint8_t* codesT = c->dense ? nullptr : c->d_bedT + (int64_t)b * Npad * c->win.pitch;
     timed([&] { gemm.p2(c, codesT, c->win.pitch, b, N, m, B2, l, ks2, D2); });
     EpiP2 p2;
-    p2.window = b;
+    p2.b0 = b;
+    p2.b1 = b + 1;
+    p2.nwin = c->win.bands;
     p2.n = N;
     p2.npad = Npad;
     p2.l = l;
@@ -262,6 +264,80 @@ struct Engine {
     p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
     p2.H = Ht;
     timed([&] { launch_accum<T>(c, p2, D2); }, 1);
+  }
+
+  // Windows [b0, b1) into Ht as one pair of products (back ends with window runs): the
+  // first product covers the run's SNPs, its epilogue writes G, the FP32 rows of the second
+  // gather and the run's window operand B2 in the padded layout of the second product, whose
+  // K then runs over all the run's SNPs. The same sums as window by window, in another order.
+  void process_run(int b0, int b1, double* Ht) {
+    const int64_t s = (int64_t)c->win.start[b0], e = (int64_t)c->win.stop[b1 - 1], m = e - s;
+    const int nw = b1 - b0;
+    const int64_t rows1 = gemm.seg_rows1(c), k2 = gemm.seg_k2(c);
+    const int ks1 = gemm.ksplit_seg(c, 1, nw, l);
+    T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * nw * rows1 * l * sizeof(T));
+    timed([&] { gemm.p1_seg(c, b0, b1, l, ks1, D1); });
+    EpiP1 p1;
+    p1.start = s;
+    p1.m = m;
+    p1.l = l;
+    p1.ksplit = ks1;
+    p1.wlen = (int64_t)c->win.blocksize;
+    p1.d1_ws = rows1;
+    p1.b2_ws = k2;
+    p1.d1_rows = nw * rows1;
+    p1.F = Fcent;
+    p1.scale = c->d_scale;
+    p1.wsum = wsum;
+    p1.omega = Omg;
+    p1.omega_f = omg_float();
+    p1.miss_ptr = c->d_miss_snp_ptr;
+    p1.miss_idx = c->d_miss_snp_idx;
+    p1.miss_val = c->imputed ? c->d_miss_snp_val : nullptr;
+    p1.G = G;
+    T* B2 = (T*)scratch(c, "r_B2", (size_t)nw * k2 * l * sizeof(T));
+    double* h0 = (double*)scratch(c, "r_h0", l * 8);
+    p1.qmax = gemm.b2_qmax(c, l);
+    float* Gf = (float*)scratch(c, "r_Gf", (size_t)round_up(m, 256) * l * sizeof(float));
+    p1.Gf = Gf;
+    timed([&] {
+      launch_prep<T>(c, p1, D1, B2, h0);
+      gemm.b2_seg(c, B2, l, b0, b1);
+    }, 1);
+    const int ks2 = gemm.ksplit_seg(c, 2, nw, l);
+    T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
+    timed([&] { gemm.p2_seg(c, b0, b1, l, ks2, D2); });
+    EpiP2 p2;
+    p2.b0 = b0;
+    p2.b1 = b1;
+    p2.nwin = c->win.bands;
+    p2.n = N;
+    p2.npad = Npad;
+    p2.l = l;
+    p2.ksplit = ks2;
+    p2.F = Fcent;
+    p2.scale = c->d_scale;
+    p2.G = G;
+    p2.Gf = Gf;
+    p2.g_start = s;
+    p2.h0 = h0;
+    p2.miss_ptr = c->d_miss_ws_ptr;
+    p2.miss_idx = c->d_miss_ws_idx;
+    p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
+    p2.H = Ht;
+    timed([&] { launch_accum<T>(c, p2, D2); }, 1);
+  }
+
+  // Windows [b0, b1) into Ht: as runs of at most kRunRows padded rows of the first product
+  // when the back end batches windows, else one window at a time.
+  static constexpr int64_t kRunRows = int64_t(1) << 22;
+  void process_windows(int b0, int b1, double* Ht) {
+    if (!gemm.p1_seg || c->dense) {
+      for (int b = b0; b < b1; ++b) process_window(b, Ht);
+      return;
+    }
+    const int per = (int)std::max<int64_t>(1, kRunRows / gemm.seg_rows1(c));
+    for (int b = b0; b < b1; b += per) process_run(b, std::min(b1, b + per), Ht);
   }
 
   int bandsize = 1;
@@ -318,7 +394,7 @@ struct Engine {
       updates++;
     }
     zero(c, H, Npad * l);
-    process_window(0, H);
+    process_windows(0, 1, H);
   }
 
   // The in-core schedule runs over the o.bands windows; with the out-of-core block plan the
@@ -333,11 +409,22 @@ struct Engine {
     }
     if (pi == 0) bandsize = bf;
     bandsize = std::min(bandsize * 2, nwin);
+    // windows are gathered into runs that share the target sum and end at the next Omega
+    // update; each run is processed as a whole before the update reads H1 / H2
+    int run0 = 0;
+    double* run_target = nullptr;
     for (int b = 0, i = 1; b < nwin; ++b, ++i) {
-      process_window(b, i <= bandsize / 2 ? H1 : H2);
+      double* target = i <= bandsize / 2 ? H1 : H2;
+      if (b > run0 && target != run_target) {
+        process_windows(run0, b, run_target);
+        run0 = b;
+      }
+      run_target = target;
       const bool adjacent = pi > 0 && (b + 1) == (int)std::pow(2.0, pi - 1) * bf && std::pow(2.0, pi) < bands;
       if ((b + 1) < bandsize && !adjacent) continue;
       if (!((i == bandsize) || (i == bandsize / 2) || adjacent)) continue;
+      process_windows(run0, b + 1, run_target);
+      run0 = b + 1;
       timed([&] { update_omega(H1, H2); }, 2);
       updates++;
       if (i == bandsize) {
@@ -347,6 +434,7 @@ struct Engine {
         zero(c, H2, Npad * l);
       }
     }
+    if (run0 < nwin) process_windows(run0, nwin, run_target);
   }
 
   void check_status() {
@@ -508,7 +596,7 @@ void product_t(pcaone_ctx* c, GemmFnT<T> gemm, int transpose, int standardize, i
     gemm.p2(c, c->d_bedT, c->win.pitch, 0, N, M, B2, l, ks, D2);
     zero(c, H, Npad * l);
     EpiP2 p2;
-    p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks;
+    p2.b0 = 0; p2.b1 = 1; p2.nwin = c->win.bands; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks;
     p2.F = c->d_F; p2.scale = c->d_scale; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
     p2.miss_idx = c->d_miss_ws_idx; p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr; p2.H = H;
     launch_accum<T>(c, p2, D2);
@@ -563,7 +651,7 @@ void gram_t(pcaone_ctx* c, GemmFnT<T> gemm, const double* X, int l, double* Y) {
   gemm.p2(c, c->d_bedT, c->win.pitch, 0, N, M, B2, l, ks2, D2);
   zero(c, H, Npad * l);
   EpiP2 p2;
-  p2.window = 0; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks2;
+  p2.b0 = 0; p2.b1 = 1; p2.nwin = c->win.bands; p2.n = N; p2.npad = Npad; p2.l = l; p2.ksplit = ks2;
   p2.F = c->d_F; p2.scale = c->d_scale; p2.G = G; p2.h0 = h0; p2.miss_ptr = c->d_miss_ws_ptr;
   p2.miss_idx = c->d_miss_ws_idx; p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr; p2.H = H;
   launch_accum<T>(c, p2, D2);

@@ -28,6 +28,16 @@ struct GemmFnT {
   __nv_bfloat16* (*b2_bt)(pcaone_ctx* c, int l, int64_t* kpad, int* half) = nullptr;
   // Zeroed per-column maxima of |B2| for the first epilogue to fill (int8 back end), or null.
   unsigned long long* (*b2_qmax)(pcaone_ctx* c, int l) = nullptr;
+  // Runs of consecutive windows [b0, b1) as one product each (null: one window at a time).
+  // The first product writes seg_rows1 rows per window (SNP rows, zero padding rows); the
+  // second reads B2 with seg_k2 rows per window (window SNPs first, zero rows after);
+  // ksplit_seg(which = 1 or 2, windows, l) is the split count of either product.
+  int64_t (*seg_rows1)(pcaone_ctx* c) = nullptr;
+  int64_t (*seg_k2)(pcaone_ctx* c) = nullptr;
+  int (*ksplit_seg)(pcaone_ctx* c, int which, int nw, int l) = nullptr;
+  void (*p1_seg)(pcaone_ctx* c, int b0, int b1, int l, int ks, T* out) = nullptr;
+  void (*b2_seg)(pcaone_ctx* c, const T* B2, int l, int b0, int b1) = nullptr;
+  void (*p2_seg)(pcaone_ctx* c, int b0, int b1, int l, int ks, T* out) = nullptr;
 };
 
 GemmFnT<float> gemm_simt_float();

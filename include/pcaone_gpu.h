@@ -180,6 +180,13 @@ int pcaone_gpu_clear_imputed(pcaone_ctx* ctx);
 int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
                      const int32_t* we, uint64_t nwin, float* r2);
 
+/* The same pairs as pcaone_gpu_ld_r2 with r2 in FP64: the values the pruning
+ * (ld_prune_big / ld_prune_small, src/LD.cpp:141-242: r2 > --ld-r2) and clumping
+ * (ld_clump_single_pheno, src/LD.cpp:299-367: r2 >= --clump-r2, on the unprojected matrix,
+ * U = NULL) decisions compare. */
+int pcaone_gpu_ld_r2_f64(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
+                         const int32_t* we, uint64_t nwin, double* r2);
+
 /* LD flow B, first half: the residual matrix of Data::write_residuals (src/Data.cpp:196-245)
  * for the SNPs snp0 .. snp0 + nsnp - 1 of the current order. R_ij = Gc_ij - sum_t U_it S_t
  * V_jt with Gc the centred genotypes (BED2GENO - F_j, missing -> 0; not standardised), or Gc

@@ -565,13 +565,14 @@ def ld_pairs(G: np.ndarray, snp: SnpLD):
     return np.concatenate(out_i), np.concatenate(out_k), np.concatenate(out_r)
 
 
-def ld_flow_a(bed: Bed, U: np.ndarray):
+def ld_flow_a(bed: Bed, U: np.ndarray | None):
     """run_ld_stuff with PLINK + --read-U (src/LD.cpp:444-468): centred G (not standardised,
-    pca is off for LD, src/Cmd.cpp:166-169) projected off U: G = (I - U U^T) G."""
+    pca is off for LD, src/Cmd.cpp:166-169) projected off U: G = (I - U U^T) G. Clumping
+    (src/LD.cpp:474-505) skips the projection and reads the centred G itself (U = None)."""
     codes = decode_codes(bed)
     F = allele_freq(codes)
     G = centered_matrix(codes, F)
-    return G - U @ (U.T @ G)
+    return G if U is None else G - U @ (U.T @ G)
 
 
 def read_residuals(path: str) -> np.ndarray:
@@ -587,6 +588,165 @@ def read_residuals(path: str) -> np.ndarray:
 def ld_lines(snp: SnpLD, i, k, r) -> list:
     """Text lines of the .ld.gz output: bims[i] \\t bims[k] \\t std::to_string(r*r)."""
     return [f"{snp.bims[a]}\t{snp.bims[b]}\t{x * x:.6f}" for a, b, x in zip(i, k, r)]
+
+
+def _maf(a: float) -> float:
+    return 1 - a if a > 0.5 else a  # MAF (src/Common.hpp:25)
+
+
+def read_bim_af(filebim: str) -> list:
+    """The allele frequencies get_snp_pos_bim reads from a 7-column (.mbim) file, else []
+    (src/LD.cpp:61)."""
+    af = []
+    with open(filebim) as f:
+        for line in f:
+            tok = [t for t in line.rstrip("\n").replace(" ", "\t").split("\t")]
+            if len(tok) == 7:
+                af.append(float(tok[6]))
+    return af
+
+
+def ld_prune(snp: SnpLD, r2: dict, r2_tol: float, af: list) -> np.ndarray:
+    """ld_prune_big / ld_prune_small (src/LD.cpp:141-242): windows in order; a lead SNP i that
+    is still kept compares every kept follower k of its window; r^2 > r2_tol drops k, or i
+    when the .mbim frequencies give k the larger MAF. r2[(i, k)] holds the pair's r^2."""
+    keep = np.ones(len(snp.pos), dtype=bool)
+    pick_random = len(af) == 0
+    for i, w in zip(snp.ws, snp.we):
+        if not keep[i]:
+            continue
+        for j in range(1, int(w)):
+            k = i + j
+            if not keep[k]:
+                continue
+            if r2[(int(i), int(k))] > r2_tol:
+                o = k
+                if not pick_random:
+                    o = i if _maf(af[k]) > _maf(af[i]) else k
+                keep[o] = False
+    return keep
+
+
+def read_assoc(path: str, colnames: str = "CHR,BP,P"):
+    """valid_assoc_file, get_snp_pos_bim(header) and map_index_snps (src/LD.cpp:245-300) for
+    one assoc-like file: (header line, column indices, per-chromosome target positions,
+    per-chromosome {bp: (p, line)} of the SNPs with p <= p2 built later). Returns the header,
+    the column indices, the SnpLD of the targets and the raw lines."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    head = lines[0]
+    fields = head.split("\t")
+    want = colnames.split(",")
+    idx = [-1, -1, -1]
+    for j, col in enumerate(fields):
+        for t in range(3):
+            if col == want[t]:
+                idx[t] = j
+    if min(idx) < 0:
+        raise ValueError("the assoc-like file has no " + want[idx.index(-1)] + " column")
+    chrs, pos, end_pos = [], [], []
+    prev = None
+    for i, line in enumerate(lines[1:]):
+        tok = line.replace(" ", "\t").split("\t")
+        cur = tok[idx[0]]
+        if prev is None:
+            chrs.append(cur)
+        elif prev != cur:
+            end_pos.append(i - 1)
+            chrs.append(cur)
+        prev = cur
+        pos.append(int(tok[idx[1]]))
+    end_pos.append(len(pos) - 1)
+    return head, idx, SnpLD(chrs, np.array(pos, dtype=np.int64), end_pos, []), lines[1:]
+
+
+def assoc_pvals(lines: list, idx: list, clump_p2: float) -> list:
+    """map_index_snps (src/LD.cpp:272-297): per chromosome, {bp: (p, line)} of the lines with
+    p <= clump_p2. The first line of a new chromosome is inserted before the switch, so it
+    lands in the previous chromosome's map (the reference's order of operations); the first
+    insert of a bp wins."""
+    vm, m = [], {}
+    prev = None
+    for line in lines:
+        tok = line.split("\t")
+        cur = tok[idx[0]]
+        bp = int(tok[idx[1]])
+        p = float(tok[idx[2]])
+        if p <= clump_p2 and bp not in m:
+            m[bp] = (p, line)
+        if prev is not None and prev != cur:
+            vm.append(m)
+            m = {}
+        prev = cur
+    vm.append(m)
+    return vm
+
+
+def target_snp_idx(snp_t: SnpLD, snp: SnpLD):
+    """get_target_snp_idx (src/LD.cpp:79-123): per target chromosome, the indices in the LD
+    matrix of the target SNPs whose position occurs on that chromosome, and their positions."""
+    idx_per_chr, bp_per_chr = [], []
+    for tc, ch in enumerate(snp_t.chr):
+        c = snp.chr.index(ch)
+        e = snp.end_pos[c]
+        s = snp.end_pos[c - 1] if c > 0 else 0
+        mpos = {int(snp.pos[i]): i for i in range(s, e + 1)}
+        e = snp_t.end_pos[tc]
+        s = snp_t.end_pos[tc - 1] if tc > 0 else 0
+        idx, bp = [], []
+        for i in range(s, e + 1):
+            p = int(snp_t.pos[i])
+            if p in mpos:
+                bp.append(p)
+                idx.append(mpos[p])
+        idx_per_chr.append(idx)
+        bp_per_chr.append(bp)
+    return idx_per_chr, bp_per_chr
+
+
+def ld_clump(head: str, clump_bp: int, clump_r2: float, clump_p1: float, r2_of, idx_per_chr,
+             bp_per_chr, pvals_per_chr) -> list:
+    """ld_clump_single_pheno (src/LD.cpp:299-367): index SNPs (p <= clump_p1) in increasing p;
+    each takes the still unclumped targets within clump_bp on either side (backward first)
+    with r^2 >= clump_r2; output lines = the index SNP's assoc line + tab + the clumped
+    positions by increasing p, comma-separated, or NONE. r2_of(a, b) gives r^2 of matrix
+    columns a < b."""
+    out = [head + "\tSP2"]
+    for c in range(len(bp_per_chr)):
+        idx, bp = idx_per_chr[c], bp_per_chr[c]
+        mbp = {}
+        for j, b in enumerate(bp):
+            mbp.setdefault(b, j)
+        mpp = dict(pvals_per_chr[c])
+        cand = sorted([(v[0], b) for b, v in mpp.items() if v[0] <= clump_p1])
+        for _, p in cand:
+            if p not in mpp or p not in mbp:
+                continue
+            j = mbp[p]
+            clumped = []
+            for direction in (-1, 1):
+                k = j
+                while True:
+                    k += direction
+                    if k < 0 or k >= len(bp):
+                        break
+                    if (direction < 0 and bp[k] < p - clump_bp) or (direction > 0 and bp[k] > p + clump_bp):
+                        break
+                    p2 = bp[k]
+                    if p2 not in mpp:
+                        continue
+                    a, b = sorted((idx[j], idx[k]))
+                    if r2_of(a, b) >= clump_r2:
+                        clumped.append(p2)
+                        del mpp[p2]
+            line = pvals_per_chr[c][p][1] + "\t"
+            if not clumped:
+                line += "NONE"
+            else:
+                order = sorted(range(len(clumped)), key=lambda t: pvals_per_chr[c][clumped[t]][0])
+                line += ",".join(str(clumped[t]) for t in order)
+            out.append(line)
+    return out
 
 
 def read_usv(path: str) -> np.ndarray:

@@ -31,7 +31,8 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_ld_r2", "pcaone_gpu_load_gl", "pcaone_gpu_gl_freq",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
            "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
-           "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm"]
+           "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm",
+           "pcaone_gpu_ld_r2_f64"]
 
 
 class PcaoneError(RuntimeError):
@@ -86,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_fit_emu.argtypes = [vp, vp, vp, vp, u32, ctypes.c_int]
         L.pcaone_gpu_clear_imputed.argtypes = [vp]
         L.pcaone_gpu_ld_r2.argtypes = [vp, vp, u32, vp, vp, u64, vp]
+        L.pcaone_gpu_ld_r2_f64.argtypes = [vp, vp, u32, vp, vp, u64, vp]
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
@@ -327,15 +329,16 @@ def _clear_imputed(self):
     self._check(lib().pcaone_gpu_clear_imputed(self._h))
 
 
-def _ld_r2(self, ws, we, U=None):
-    """r2 of every window pair (see pcaone_gpu_ld_r2); ws, we as divide_pos_by_window."""
+def _ld_r2(self, ws, we, U=None, f64=False):
+    """r2 of every window pair (see pcaone_gpu_ld_r2, pcaone_gpu_ld_r2_f64 with f64); ws, we
+    as divide_pos_by_window."""
     ws = np.ascontiguousarray(ws, dtype=np.int64)
     we = np.ascontiguousarray(we, dtype=np.int32)
-    out = np.zeros(int(np.maximum(we - 1, 0).sum()), dtype=np.float32)
+    out = np.zeros(int(np.maximum(we - 1, 0).sum()), dtype=np.float64 if f64 else np.float32)
     Uf = None if U is None else np.asfortranarray(U, dtype=np.float64)
     k = 0 if U is None else U.shape[1]
-    self._check(lib().pcaone_gpu_ld_r2(self._h, _ptr(Uf), k, _ptr(ws), _ptr(we), len(ws),
-                                       _ptr(out)))
+    fn = lib().pcaone_gpu_ld_r2_f64 if f64 else lib().pcaone_gpu_ld_r2
+    self._check(fn(self._h, _ptr(Uf), k, _ptr(ws), _ptr(we), len(ws), _ptr(out)))
     return out
 
 

@@ -332,9 +332,14 @@ int pcaone_gpu_clear_imputed(pcaone_ctx* c) {
   return guarded(c, [&] { c->imputed = false; });
 }
 
-int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
-                     uint64_t nwin, float* r2) {
-  return guarded(c, [&] {
+}  // extern "C"
+
+namespace {
+// r2 of the window pairs into the host array r2 (float, or double with f64).
+void ld_r2_impl(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we, uint64_t nwin,
+                void* r2, bool f64) {
+  {
+    const size_t esz = f64 ? 8 : 4;
     PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
     PG_REQUIRE(ws && we && (r2 || nwin == 0), PCAONE_EBADARG, "null window arrays");
     PG_REQUIRE(!U || (k >= 1 && k <= (uint32_t)kLmax), PCAONE_EBADARG, "bad U width");
@@ -364,16 +369,16 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
       int32_t* d_span = (int32_t*)scratch(c, "ld_span", blocks * 4);
       int32_t* d_we = (int32_t*)scratch(c, "ld_we", std::max<uint64_t>(nwin, 1) * 4);
       int64_t* d_off = (int64_t*)scratch(c, "ld_off", (nwin + 1) * 8);
-      float* d_r2 = (float*)scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * 4);
+      void* d_r2 = scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * esz);
       PG_CUDA(cudaMemcpyAsync(d_win_of, win_of.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
       PG_CUDA(cudaMemcpyAsync(d_span, span.data(), blocks * 4, cudaMemcpyHostToDevice, c->stream));
       if (nwin) {
         PG_CUDA(cudaMemcpyAsync(d_we, we, nwin * 4, cudaMemcpyHostToDevice, c->stream));
         PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (nwin + 1) * 8, cudaMemcpyHostToDevice, c->stream));
-        ld_r2_dense(c, c->d_dense_norm, d_win_of, d_we, d_off, d_span, max_span, d_r2);
+        ld_r2_dense(c, c->d_dense_norm, d_win_of, d_we, d_off, d_span, max_span, d_r2, f64);
       }
       if (off[nwin] > 0)
-        PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * 4, cudaMemcpyDeviceToHost, c->stream));
+        PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * esz, cudaMemcpyDeviceToHost, c->stream));
       PG_CUDA(cudaStreamSynchronize(c->stream));
       return;
     }
@@ -404,18 +409,32 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
     int64_t* d_ws = (int64_t*)scratch(c, "ld_ws", std::max<uint64_t>(nwin, 1) * 8);
     int32_t* d_we = (int32_t*)scratch(c, "ld_we", std::max<uint64_t>(nwin, 1) * 4);
     int64_t* d_off = (int64_t*)scratch(c, "ld_off", (nwin + 1) * 8);
-    float* d_r2 = (float*)scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * 4);
+    void* d_r2 = scratch(c, "ld_r2", std::max<int64_t>(off[nwin], 1) * esz);
     if (nwin) {
       PG_CUDA(cudaMemcpyAsync(d_ws, ws, nwin * 8, cudaMemcpyHostToDevice, c->stream));
       PG_CUDA(cudaMemcpyAsync(d_we, we, nwin * 4, cudaMemcpyHostToDevice, c->stream));
       PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (nwin + 1) * 8, cudaMemcpyHostToDevice, c->stream));
     }
-    ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2);
+    ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2, f64);
     if (off[nwin] > 0)
-      PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * 4, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * esz, cudaMemcpyDeviceToHost, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
-  });
+  }
 }
+}  // namespace
+
+extern "C" {
+
+int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
+                     uint64_t nwin, float* r2) {
+  return guarded(c, [&] { ld_r2_impl(c, U, k, ws, we, nwin, r2, false); });
+}
+
+int pcaone_gpu_ld_r2_f64(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
+                         uint64_t nwin, double* r2) {
+  return guarded(c, [&] { ld_r2_impl(c, U, k, ws, we, nwin, r2, true); });
+}
+
 
 }  // extern "C"
 

@@ -176,15 +176,16 @@ void build_missing_by_window_sample(pcaone_ctx* c);
 void compute_imputed_snp(pcaone_ctx* c);
 void compute_imputed_ws(pcaone_ctx* c);
 // LD r2 of every window pair (kernels_ld.cu). W, Y: M x k row-major device arrays (or null).
+// d_r2 holds float values, or double with f64.
 void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,
-           const int32_t* d_we, const int64_t* d_off, int64_t nwin, float* d_r2);
+           const int32_t* d_we, const int64_t* d_off, int64_t nwin, void* d_r2, bool f64);
 // LD flow B (kernels_ld.cu): residual rows of snp0..snp0+nsnp (US N x k, V nsnp x k
 // row-major device arrays, or null for the centred genotypes), the in-place centring of the
 // dense matrix with its squared column norms d, and r2 of the window pairs on it.
 void residuals(pcaone_ctx* c, const double* US, const double* V, int k, uint64_t snp0, uint64_t nsnp, float* out);
 void dense_center(pcaone_ctx* c, double* d);
 void ld_r2_dense(pcaone_ctx* c, const double* d, const int64_t* d_win_of, const int32_t* d_we, const int64_t* d_off,
-                 const int32_t* d_span, int max_span, float* d_r2);
+                 const int32_t* d_span, int max_span, void* d_r2, bool f64);
 // d_scale_j = 1/sqrt(ploidy Fs_j (1 - Fs_j)) (or 1 when not standardising / sd <= 1e-9).
 void compute_scale(pcaone_ctx* c, int standardize, int ploidy);
 

@@ -82,22 +82,24 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
 }
 
 // Unweighted warp-cooperative gather for rows of l = 4 G FP32 values (16-byte aligned rows):
-// out[c] = sum_{e in [e0, e1)} rows[idx_e - row0][c]. The warp takes 32 entries at a time
-// (lane t loads the index of entry t); the rows of the batch are then split over R = 32 / G
-// row groups of G lanes, lane g of a group owning columns 4g .. 4g + 3, and each lane issues
-// all its float4 loads of the batch (ceil(32 / R) rows) before it adds them, so up to 32 rows
-// are in flight per warp. FP64 sums; the row groups are combined in a fixed order
-// (deterministic) into out (shared memory of this warp).
+// out[c] = sum_{e in [e0, e1)} rows[idx_e - row0][c]. The warp takes kSumBatch entries at a
+// time (lane t loads the index of entry t); the rows of the batch are then split over
+// R = 32 / G row groups of G lanes, lane g of a group owning columns 4g .. 4g + 3, and each
+// lane issues all its float4 loads of the batch (ceil(kSumBatch / R) rows) before it adds
+// them. FP64 sums; the row groups are combined in a fixed order (deterministic) into out
+// (shared memory of this warp). The batch is sized so that the kernels keep three CTAs of
+// 256 threads per SM (registers) with 16 rows in flight per warp.
+constexpr int kSumBatch = 16;
 template <int G>
 __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                           const float* __restrict__ rows, int64_t row0, double* out) {
-  constexpr int R = 32 / G, T = (32 + R - 1) / R;
+  constexpr int R = 32 / G, T = (kSumBatch + R - 1) / R;
   const int lane = threadIdx.x & 31, grp = lane / G, cg = lane - grp * G;
   const bool active = grp < R;
   const float4* rows4 = reinterpret_cast<const float4*>(rows);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t base = e0; base < e1; base += 32) {
-    const int cnt = (int)(e1 - base < 32 ? e1 - base : 32);
+  for (int64_t base = e0; base < e1; base += kSumBatch) {
+    const int cnt = (int)(e1 - base < kSumBatch ? e1 - base : kSumBatch);
     const int64_t my = lane < cnt ? (int64_t)idx[base + lane] - row0 : 0;
     float4 v[T];
 #pragma unroll
@@ -140,7 +142,7 @@ __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* 
 // Omega when p.omega_f is set (half the L2 bytes of the FP64 rows); without imputed values
 // its weight is F_j for every entry, so it sums the rows unweighted (sum_rows, l % 4 == 0).
 template <typename T, int CPL>
-__global__ void k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
+__global__ void __launch_bounds__(256, 3) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
   extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __res
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse, the sparse term over the sample's
 // missing entries in the windows [b0, b1).
 template <typename T, int CPL>
-__global__ void k_accum(EpiP2 p, const T* __restrict__ D2) {
+__global__ void __launch_bounds__(256, 3) k_accum(EpiP2 p, const T* __restrict__ D2) {
   extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = ssm + warp * p.l;

@@ -87,13 +87,15 @@ __global__ void k_ld_diag(const uint32_t* __restrict__ ph, const uint32_t* __res
   if (lane == 0) d[i] = centred_dot(s, F[i], F[i], npad) - wy;
 }
 
-// CTA per window: warp per follower k of the lead SNP i; writes r^2 in pair order.
+// CTA per window: warp per follower k of the lead SNP i; writes r^2 in pair order (as float
+// for the .ld.gz text, or as double for the pruning and clumping decisions).
+template <typename OutT>
 __global__ void k_ld_pairs(const uint32_t* __restrict__ ph, const uint32_t* __restrict__ pe,
                            const uint32_t* __restrict__ pn, uint32_t nw, long long npad,
                            const double* __restrict__ F, const double* __restrict__ W,
                            const double* __restrict__ Y, int k, const double* __restrict__ d,
                            const int64_t* __restrict__ ws, const int32_t* __restrict__ we,
-                           const int64_t* __restrict__ off, float* __restrict__ r2) {
+                           const int64_t* __restrict__ off, OutT* __restrict__ r2) {
   const int64_t w = blockIdx.x;
   const int64_t i = ws[w];
   const int cnt = we[w];
@@ -109,7 +111,7 @@ __global__ void k_ld_pairs(const uint32_t* __restrict__ ph, const uint32_t* __re
     if (lane == 0) {
       const double num = centred_dot(s, F[i], F[kk], npad) - wy;
       const double r = num / sqrt(d[i] * d[kk]);
-      r2[off[w] + t - 1] = (float)(r * r);
+      r2[off[w] + t - 1] = (OutT)(r * r);
     }
   }
 }
@@ -176,10 +178,11 @@ __global__ void k_dense_center(float* __restrict__ X, uint32_t ldx, uint64_t M, 
 // partner columns. Pairs (i, k) with 1 <= k - i < we[w] of the lead's window w are written
 // as r^2 = (X_i.X_k)^2 / (d_i d_k) to r2[off[w] + k - i - 1].
 constexpr int kLdTile = 32, kLdChunk = 64;
+template <typename OutT>
 __global__ void __launch_bounds__(256) k_ld_dense(const float* __restrict__ X, uint32_t ldx, uint64_t M, uint32_t N,
                                                   const double* __restrict__ d, const int64_t* __restrict__ win_of,
                                                   const int32_t* __restrict__ we, const int64_t* __restrict__ off,
-                                                  const int32_t* __restrict__ span, float* __restrict__ r2) {
+                                                  const int32_t* __restrict__ span, OutT* __restrict__ r2) {
   __shared__ double A[kLdTile][kLdChunk + 1], B[kLdTile][kLdChunk + 1];
   const uint64_t i0 = (uint64_t)blockIdx.x * kLdTile;
   const uint64_t k0 = i0 + (uint64_t)blockIdx.y * kLdTile;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(256) k_ld_dense(const float* __restrict__ X, u
     const int64_t dist = (int64_t)kk - (int64_t)i;
     if (kk < M && dist >= 1 && dist < we[w]) {
       const double rr = acc[q] / sqrt(d[i] * d[kk]);
-      r2[off[w] + dist - 1] = (float)(rr * rr);
+      r2[off[w] + dist - 1] = (OutT)(rr * rr);
     }
   }
 }
@@ -234,18 +237,22 @@ void dense_center(pcaone_ctx* c, double* d) {
 }
 
 void ld_r2_dense(pcaone_ctx* c, const double* d, const int64_t* d_win_of, const int32_t* d_we, const int64_t* d_off,
-                 const int32_t* d_span, int max_span, float* d_r2) {
+                 const int32_t* d_span, int max_span, void* d_r2, bool f64) {
   const uint64_t blocks = (c->M + kLdTile - 1) / kLdTile;
   const unsigned tiles = (unsigned)((max_span + kLdTile) / kLdTile);
   PG_REQUIRE(blocks < (1ull << 31) && tiles < 65536, PCAONE_EBADARG, "LD band too large");
-  k_ld_dense<<<dim3((unsigned)blocks, tiles), 256, 0, c->stream>>>(c->d_E, c->Npad, c->M, c->N, d, d_win_of, d_we,
-                                                                   d_off, d_span, d_r2);
+  if (f64)
+    k_ld_dense<double><<<dim3((unsigned)blocks, tiles), 256, 0, c->stream>>>(c->d_E, c->Npad, c->M, c->N, d, d_win_of,
+                                                                             d_we, d_off, d_span, (double*)d_r2);
+  else
+    k_ld_dense<float><<<dim3((unsigned)blocks, tiles), 256, 0, c->stream>>>(c->d_E, c->Npad, c->M, c->N, d, d_win_of,
+                                                                            d_we, d_off, d_span, (float*)d_r2);
   PG_CHECK_LAUNCH();
   c->launches++;
 }
 
 void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,
-           const int32_t* d_we, const int64_t* d_off, int64_t nwin, float* d_r2) {
+           const int32_t* d_we, const int64_t* d_off, int64_t nwin, void* d_r2, bool f64) {
   const uint32_t nw = (c->N + 31) / 32;  // 32 samples per word; pitch covers ceil(N/32)*8 bytes
   PG_REQUIRE((uint64_t)nw * 8 <= c->pitch, PCAONE_EBADARG, "pitch too small for bit planes");
   const long long npad = (long long)nw * 32 - c->N;
@@ -260,8 +267,12 @@ void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t
                                                                          Y, k, d);
   PG_CHECK_LAUNCH();
   if (nwin > 0) {
-    k_ld_pairs<<<(unsigned)nwin, 256, 0, c->stream>>>(ph, pe, pn, nw, npad, c->d_F, W, Y, k, d, d_ws, d_we,
-                                                     d_off, d_r2);
+    if (f64)
+      k_ld_pairs<double><<<(unsigned)nwin, 256, 0, c->stream>>>(ph, pe, pn, nw, npad, c->d_F, W, Y, k, d, d_ws, d_we,
+                                                               d_off, (double*)d_r2);
+    else
+      k_ld_pairs<float><<<(unsigned)nwin, 256, 0, c->stream>>>(ph, pe, pn, nw, npad, c->d_F, W, Y, k, d, d_ws, d_we,
+                                                              d_off, (float*)d_r2);
     PG_CHECK_LAUNCH();
   }
   c->launches += 3;

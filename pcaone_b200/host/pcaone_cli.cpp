@@ -24,6 +24,7 @@
 #include <set>
 #include <sstream>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <omp.h>
@@ -83,6 +84,11 @@ struct Params {
   bool fix_index = false;
   bool print_r2 = false, fix_read_u = false;
   unsigned ld_bp = 0;
+  double ld_r2 = 0.0;  // --ld-r2: LD pruning threshold
+  // --clump (comma-separated assoc-like files) and its options (src/Cmd.hpp:57-66)
+  std::string clump, clump_names = "CHR,BP,P";
+  double clump_p1 = 0.0001, clump_p2 = 0.01, clump_r2 = 0.5;
+  unsigned clump_bp = 250000;
   std::string fileU, filebim;
   std::string binfile;  // -B/--binary: float32 .residuals matrix (LD flow B input)
   bool ld_write = false;  // -D/--ld: write the .residuals matrix after the PCA
@@ -94,8 +100,7 @@ struct Params {
 };
 
 const std::set<std::string> kUnsupported = {
-    "-c", "--csv", "-g", "--bgen", "--ld-r2", "--clump",
-    "--clump-names", "--clump-p1", "--clump-p2", "--clump-r2", "--clump-bp", "--project",
+    "-c", "--csv", "-g", "--bgen", "--project",
     "--inbreed", "--USV", "--read-V", "--read-S", "--M", "--N",
     "--scale-factor", "--buffer"};
 
@@ -115,6 +120,9 @@ void usage() {
                "  LD r2 (flow A): -b plink --read-U pcs.eigvecs -f pcs.mbim --ld-bp BP -R\n"
                "  LD r2 (flow B): -b plink -k K -D (writes .residuals), then\n"
                "                  -B out.residuals -f out.mbim --ld-bp BP -R\n"
+               "  LD pruning:     either flow with --ld-r2 R2 instead of -R (.ld.prune.in/.out)\n"
+               "  LD clumping:    either flow with --clump a.assoc[,b.assoc] (--clump-names,\n"
+               "                  --clump-p1, --clump-p2, --clump-r2, --clump-bp; .pN.clump)\n"
                "      --fix-read-u read U row by row (the reference views it column-major)\n"
                "  -V, --printv     write .loadings and .mbim\n"
                "  -o, --out        output prefix [pcaone]\n"
@@ -187,6 +195,13 @@ Params parse(int argc, char** argv) {
     else if (a == "--fix-perm-index") p.fix_index = true;
     else if (a == "-R" || a == "--print-r2") p.print_r2 = true;
     else if (a == "--ld-bp") p.ld_bp = (unsigned)num(next());
+    else if (a == "--ld-r2") p.ld_r2 = num(next());
+    else if (a == "--clump") p.clump = next();
+    else if (a == "--clump-names") p.clump_names = next();
+    else if (a == "--clump-p1") p.clump_p1 = num(next());
+    else if (a == "--clump-p2") p.clump_p2 = num(next());
+    else if (a == "--clump-r2") p.clump_r2 = num(next());
+    else if (a == "--clump-bp") p.clump_bp = (unsigned)num(next());
     else if (a == "--read-U") p.fileU = next();
     else if (a == "-B" || a == "--binary") p.binfile = next();
     else if (a == "-D" || a == "--ld") p.ld_write = true;
@@ -354,50 +369,314 @@ std::vector<std::string> beagle_samples(const std::string& path) {
 
 }  // namespace
 
-// ---------------------------------------------------------------- LD r2 output
-// get_snp_pos_bim + divide_pos_by_window (src/LD.cpp:51-74, 125-139) and the .ld.gz text of
-// ld_r2_big (src/LD.cpp:419-442): "chr\tpos\tid" pairs and std::to_string(r2).
-// LD r2 of every window pair, written as .ld.gz: flow A on packed genotypes projected off
-// the --read-U factors, or flow B (dense) on the .residuals matrix loaded into ctx.
-int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M, bool dense) {
-  const std::string filebim = !p.filebim.empty() ? p.filebim : (dense ? p.binfile : p.bfile) + ".bim";
-  std::ifstream fb(filebim);
-  if (!fb.is_open()) fail("can not open " + filebim);
+// ---------------------------------------------------------------- LD: r2, pruning, clumping
+// SNPld (src/LD.hpp:8-15) of a .bim / .mbim or of an assoc-like file, as get_snp_pos_bim
+// reads it (src/LD.cpp:51-77): chromosome runs, positions, the "chr\tpos\tid" strings of the
+// .ld.gz text, the raw lines and, from 7-column (.mbim) files, the allele frequencies.
+struct SnpLd {
   std::vector<long> pos;
   std::vector<int> end_pos;
-  std::vector<std::string> bims;
+  std::vector<std::string> chr, bims, lines;
+  std::vector<double> af;
+  std::vector<int64_t> ws;  // divide_pos_by_window: lead SNP of each window
+  std::vector<int32_t> we;  // and its SNP count (lead included)
+};
+
+SnpLd read_snp_ld(const std::string& file, bool header, int ic, int ip, std::string* head = nullptr) {
+  std::ifstream fb(file);
+  if (!fb.is_open()) fail("can not open " + file);
+  SnpLd s;
   std::string line, prev;
+  if (header) {
+    std::getline(fb, line);
+    if (head) *head = line;
+  }
   while (std::getline(fb, line)) {
     auto tok = split(line, " \t");
-    if (tok.size() < 4) fail("the input file is not valid!\n => " + filebim);
-    if (!prev.empty() && prev != tok[0]) end_pos.push_back((int)pos.size() - 1);
-    prev = tok[0];
-    pos.push_back(std::stol(tok[3]));
-    bims.push_back(tok[0] + "\t" + tok[3] + "\t" + tok[1]);
+    if ((int)tok.size() <= std::max(ic, ip)) fail("the input file is not valid!\n => " + file);
+    if (tok.size() == 7 && !header) s.af.push_back(std::stod(tok[6]));
+    if (prev.empty()) s.chr.push_back(tok[ic]);
+    if (!prev.empty() && prev != tok[ic]) {
+      s.end_pos.push_back((int)s.pos.size() - 1);
+      s.chr.push_back(tok[ic]);
+    }
+    prev = tok[ic];
+    s.pos.push_back(std::stol(tok[ip]));
+    if (!header) s.bims.push_back(tok[0] + "\t" + tok[3] + "\t" + tok[1]);
+    s.lines.push_back(line);
   }
-  end_pos.push_back((int)pos.size() - 1);
-  if (pos.size() != M) fail("The number of variants is not matching the LD matrix");
-  std::vector<int64_t> ws;
-  std::vector<int32_t> we;
-  for (size_t i = 0, c = 0; i < pos.size(); ++i) {
-    if (pos[i] == pos[end_pos[c]]) {
+  s.end_pos.push_back((int)s.pos.size() - 1);
+  return s;
+}
+
+// divide_pos_by_window (src/LD.cpp:125-139): for each SNP not at its chromosome's last
+// position, the window of the following SNPs of that chromosome within bp (lead included).
+void divide_by_window(SnpLd& s, long bp) {
+  s.ws.clear();
+  s.we.clear();
+  for (size_t i = 0, c = 0; i < s.pos.size(); ++i) {
+    if (s.pos[i] == s.pos[s.end_pos[c]]) {
       ++c;
       continue;
     }
     size_t j = i;
-    for (; j <= (size_t)end_pos[c]; ++j)
-      if (pos[j] - pos[i] > (long)p.ld_bp) break;
-    ws.push_back((int64_t)i);
-    we.push_back((int32_t)(j - i));
+    for (; j <= (size_t)s.end_pos[c]; ++j)
+      if (s.pos[j] - s.pos[i] > bp) break;
+    s.ws.push_back((int64_t)i);
+    s.we.push_back((int32_t)(j - i));
   }
+}
+
+std::vector<int64_t> pair_offsets(const std::vector<int32_t>& we) {
+  std::vector<int64_t> off(we.size() + 1, 0);
+  for (size_t w = 0; w < we.size(); ++w) off[w + 1] = off[w] + (we[w] - 1);
+  return off;
+}
+
+// r2 (FP64) of every window pair on the device: flow A (packed genotypes, projected off U when
+// given) or flow B (the dense matrix loaded into ctx).
+std::vector<double> device_r2_f64(pcaone_ctx* ctx, const std::vector<double>* U, size_t uc,
+                                  const std::vector<int64_t>& ws, const std::vector<int32_t>& we) {
+  const auto off = pair_offsets(we);
+  std::vector<double> r2(std::max<int64_t>(off.back(), 1));
+  auto t0 = std::chrono::steady_clock::now();
+  check(ctx, pcaone_gpu_ld_r2_f64(ctx, U ? U->data() : nullptr, (uint32_t)(U ? uc : 0), ws.data(), we.data(),
+                                  ws.size(), r2.data()),
+        "ld_r2_f64");
+  g_log.print(date(), "LD r2 of", off.back(), "pairs computed in",
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), "seconds");
+  return r2;
+}
+
+// ld_prune_big / ld_prune_small (src/LD.cpp:141-242): windows in order; a lead SNP that is
+// still kept compares every kept follower of its window; r2 > tol drops the follower, or the
+// lead when the .mbim frequencies give the follower the larger MAF.
+void ld_prune(const Params& p, const SnpLd& s, const std::vector<double>& r2) {
+  const bool pick_random_one = s.af.empty();
+  g_log.print(date(), "LD pruning, choose sites to be kept randomly or with high MAF? 1(random) : 0(high MAF). =>",
+              pick_random_one);
+  auto maf = [](double a) { return a > 0.5 ? 1 - a : a; };
+  std::vector<char> keep(s.pos.size(), 1);
+  const auto off = pair_offsets(s.we);
+  for (size_t w = 0; w < s.ws.size(); ++w) {
+    const int64_t i = s.ws[w];
+    if (!keep[i]) continue;
+    for (int j = 1; j < s.we[w]; ++j) {
+      const int64_t k = i + j;
+      if (!keep[k]) continue;
+      if (r2[off[w] + j - 1] > p.ld_r2) {
+        int64_t o = k;
+        if (!pick_random_one) o = maf(s.af[k]) > maf(s.af[i]) ? i : k;
+        keep[o] = 0;
+      }
+    }
+  }
+  std::ofstream out(p.fileout + ".ld.prune.out"), in(p.fileout + ".ld.prune.in");
+  for (size_t i = 0; i < s.lines.size(); ++i) (keep[i] ? in : out) << s.lines[i] << std::endl;
+}
+
+// std::sort of the indices by value (sortidx, src/Common.hpp:68-73): the same algorithm on
+// the same sequence gives the reference's order of ties.
+std::vector<size_t> sortidx(const std::vector<double>& v) {
+  std::vector<size_t> idx(v.size());
+  for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&v](size_t a, size_t b) { return v[a] < v[b]; });
+  return idx;
+}
+
+// LD clumping of each assoc-like file (src/LD.cpp:245-367, 474-505): the targets with
+// p <= clump_p2 per chromosome (map_index_snps, whose first line of a chromosome is filed
+// under the previous one), matched by position to the LD matrix (get_target_snp_idx); index
+// SNPs in increasing p take the unclumped targets within clump_bp (backward, then forward)
+// with r2 >= clump_r2. The r2 of every pair within clump_bp comes from one device call per
+// file (windows led by the matched targets).
+void ld_clump(const Params& p, pcaone_ctx* ctx, const SnpLd& snp, const std::vector<double>* U, size_t uc) {
+  using Pds = std::pair<double, std::string>;
+  const auto files = split(p.clump, ",");
+  const auto want = split(p.clump_names, ",");
+  if (want.size() != 3) fail("--clump-names needs three column names");
+  for (size_t fi = 0; fi < files.size(); ++fi) {
+    g_log.print(date(), "LD-based clumping for associated file:", files[fi]);
+    std::ifstream fa(files[fi]);
+    if (!fa.is_open()) fail("can not open " + files[fi]);
+    std::string line;
+    std::getline(fa, line);
+    const auto fields = split(line, "\t");
+    int colidx[3] = {-1, -1, -1};
+    for (size_t j = 0; j < fields.size(); ++j)
+      for (int t = 0; t < 3; ++t)
+        if (fields[j] == want[t]) colidx[t] = (int)j;
+    for (int t = 0; t < 3; ++t)
+      if (colidx[t] < 0) fail("the assoc-like file has no " + want[t] + " column");
+    std::string head;
+    const SnpLd tgt = read_snp_ld(files[fi], true, colidx[0], colidx[1], &head);
+    // map_index_snps
+    std::vector<std::unordered_map<int, Pds>> vm;
+    {
+      std::unordered_map<int, Pds> m;
+      std::string prev;
+      for (const auto& l : tgt.lines) {
+        const auto tok = split(l, "\t");
+        const std::string cur = tok[colidx[0]];
+        const int bp = std::stoi(tok[colidx[1]]);
+        const double pval = std::stod(tok[colidx[2]]);
+        if (pval <= p.clump_p2) m.insert({bp, {pval, l}});
+        if (!prev.empty() && prev != cur) {
+          vm.push_back(m);
+          m.clear();
+        }
+        prev = cur;
+      }
+      vm.push_back(m);
+    }
+    // get_target_snp_idx
+    std::vector<std::vector<int>> idx_per_chr(tgt.chr.size()), bp_per_chr(tgt.chr.size());
+    {
+      std::vector<size_t> ord;
+      for (const auto& ch : snp.chr) {
+        size_t i = 0;
+        while (i < tgt.chr.size() && tgt.chr[i] != ch) ++i;
+        ord.push_back(i);
+      }
+      if (!std::is_sorted(ord.begin(), ord.end()))
+        fail("the association file may be not sorted, hence not matching the bimfile ");
+      for (size_t tc = 0; tc < tgt.chr.size(); ++tc) {
+        size_t c = 0;
+        while (c < snp.chr.size() && snp.chr[c] != tgt.chr[tc]) ++c;
+        if (c == snp.chr.size()) continue;
+        std::unordered_map<long, int> mpos;
+        const int e = snp.end_pos[c], s0 = c > 0 ? snp.end_pos[c - 1] : 0;
+        for (int i = s0; i <= e; ++i) mpos[snp.pos[i]] = i;
+        const int te = tgt.end_pos[tc], ts = tc > 0 ? tgt.end_pos[tc - 1] : 0;
+        for (int i = ts; i <= te; ++i) {
+          auto it = mpos.find(tgt.pos[i]);
+          if (it != mpos.end()) {
+            bp_per_chr[tc].push_back((int)tgt.pos[i]);
+            idx_per_chr[tc].push_back(it->second);
+          }
+        }
+      }
+    }
+    // r2 of the pairs within clump_bp: one window per matched target, up to its farthest
+    // matched partner on the right
+    std::vector<int64_t> ws;
+    std::vector<int32_t> we;
+    std::unordered_map<int64_t, size_t> win_of;
+    for (size_t c = 0; c < idx_per_chr.size(); ++c) {
+      const auto& idx = idx_per_chr[c];
+      const auto& bp = bp_per_chr[c];
+      for (size_t j = 0; j < idx.size(); ++j) {
+        size_t kmax = j;
+        while (kmax + 1 < idx.size() && bp[kmax + 1] <= (long)bp[j] + (long)p.clump_bp) ++kmax;
+        const int64_t a = idx[j];
+        int32_t len = 1;
+        for (size_t k = j + 1; k <= kmax; ++k) len = std::max<int32_t>(len, (int32_t)(idx[k] - a + 1));
+        auto it = win_of.find(a);
+        if (it == win_of.end()) {
+          win_of[a] = ws.size();
+          ws.push_back(a);
+          we.push_back(len);
+        } else {
+          we[it->second] = std::max(we[it->second], len);
+        }
+      }
+    }
+    const auto off = pair_offsets(we);
+    const std::vector<double> r2 = ws.empty() ? std::vector<double>() : device_r2_f64(ctx, U, uc, ws, we);
+    auto r2_of = [&](int64_t a, int64_t b) {
+      if (a > b) std::swap(a, b);
+      const size_t w = win_of.at(a);
+      if (b - a >= we[w]) fail("internal error: clumping pair outside its window");
+      return r2[off[w] + (b - a) - 1];
+    };
+    // ld_clump_single_pheno
+    std::ofstream ofs(p.fileout + ".p" + std::to_string(fi) + ".clump");
+    ofs << head + "\tSP2" << std::endl;
+    for (size_t c = 0; c < bp_per_chr.size() && c < vm.size(); ++c) {
+      const auto& idx = idx_per_chr[c];
+      const auto& bp = bp_per_chr[c];
+      std::unordered_map<int, int> mbp;
+      for (size_t i = 0; i < bp.size(); ++i) mbp.insert({bp[i], (int)i});
+      auto mpp = vm[c];
+      std::vector<double> pp;
+      std::vector<int> ps;
+      for (auto it = mpp.begin(); it != mpp.end(); ++it)
+        if (it->second.first <= p.clump_p1) {
+          ps.push_back(it->first);
+          pp.push_back(it->second.first);
+        }
+      for (size_t oi : sortidx(pp)) {
+        const int pos = ps[oi];
+        if (mpp.count(pos) == 0) continue;
+        if (mbp.count(pos) == 0) continue;
+        std::vector<int> clumped;
+        const int j = mbp.at(pos);
+        int k = j;
+        bool backward = true;
+        while (true) {
+          if (backward) {
+            --k;
+            if (k < 0 || bp[k] < (long)pos - (long)p.clump_bp) {
+              backward = false;
+              k = j;
+              continue;
+            }
+          } else {
+            ++k;
+            if (k >= (int)bp.size() || bp[k] > (long)pos + (long)p.clump_bp) break;
+          }
+          const int p2 = bp[k];
+          if (mpp.count(p2) == 0) continue;
+          if (r2_of(idx[j], idx[k]) >= p.clump_r2) {
+            clumped.push_back(p2);
+            mpp.erase(p2);
+          }
+        }
+        ofs << vm[c].at(pos).second << "\t";
+        if (clumped.empty()) {
+          ofs << "NONE";
+        } else {
+          std::vector<double> opp;
+          for (int op : clumped) opp.push_back(vm[c].at(op).first);
+          size_t t = 0;
+          for (size_t q : sortidx(opp)) {
+            ofs << clumped[q] << (t + 1 == opp.size() ? "" : ",");
+            ++t;
+          }
+        }
+        ofs << std::endl;
+      }
+    }
+  }
+}
+
+// run_ld_stuff (src/LD.cpp:444-507): clumping when --clump is given, else the windows of
+// --ld-bp with -R (.ld.gz of every pair's r2) or --ld-r2 (pruning). Flow A: packed genotypes
+// projected off the --read-U factors (clumping reads them unprojected); flow B (dense): the
+// .residuals matrix loaded into ctx.
+int run_ld(const Params& p, pcaone_ctx* ctx, size_t N, size_t M, bool dense) {
+  const std::string filebim = !p.filebim.empty() ? p.filebim : (dense ? p.binfile : p.bfile) + ".bim";
+  SnpLd snp = read_snp_ld(filebim, false, 0, 3);
+  if (snp.pos.size() != M) fail("The number of variants is not matching the LD matrix");
   size_t ur = 0, uc = 0;
   std::vector<double> U;
   if (!dense) {
     U = read_usv(p.fileU, ur, uc, p.fix_read_u);
     if (ur != N) fail("the number of rows of --read-U differs from the samples");
   }
-  std::vector<int64_t> off(ws.size() + 1, 0);
-  for (size_t w = 0; w < ws.size(); ++w) off[w + 1] = off[w] + (we[w] - 1);
+  if (!p.clump.empty()) {
+    ld_clump(p, ctx, snp, nullptr, 0);
+    return 0;
+  }
+  divide_by_window(snp, (long)p.ld_bp);
+  const auto& ws = snp.ws;
+  const auto& we = snp.we;
+  if (!p.print_r2) {
+    ld_prune(p, snp, device_r2_f64(ctx, dense ? nullptr : &U, uc, ws, we));
+    return 0;
+  }
+  const auto off = pair_offsets(we);
+  const auto& bims = snp.bims;
   std::vector<float> r2(std::max<int64_t>(off.back(), 1));
   auto t0 = std::chrono::steady_clock::now();
   check(ctx, pcaone_gpu_ld_r2(ctx, dense ? nullptr : U.data(), (uint32_t)uc, ws.data(), we.data(), ws.size(),
@@ -633,7 +912,8 @@ int run_binary(const Params& p, std::chrono::steady_clock::time_point t_start) {
   f.read((char*)hdr, 8);
   const size_t M = hdr[0], N = hdr[1];
   g_log.print(date(), "shape of input matrix (features x samples) is", M, "x", N);
-  if (!(p.print_r2 || p.ld_bp > 0)) fail("-B/--binary input supports the LD r2 mode (-R, --ld-bp) in this build");
+  if (!(p.print_r2 || p.ld_r2 > 0 || !p.clump.empty()))
+    fail("-B/--binary input supports the LD modes (-R, --ld-r2, --clump) in this build");
   std::vector<float> X(M * N);
   f.read((char*)X.data(), (std::streamsize)(X.size() * 4));
   if ((size_t)f.gcount() != X.size() * 4) fail("the binary file is shorter than its header implies");
@@ -717,8 +997,8 @@ int main(int argc, char** argv) {
   }
   g_log.print(date(), "done reading all data");
 
-  if (p.print_r2 || p.ld_bp > 0) {  // LD mode (src/Main.cpp:64-77)
-    if (p.fileU.empty()) fail("LD r2 from PLINK input needs --read-U (flow A)");
+  if (p.print_r2 || p.ld_r2 > 0 || !p.clump.empty()) {  // LD mode (src/Main.cpp:64-77)
+    if (p.fileU.empty()) fail("LD from PLINK input needs --read-U (flow A)");
     g_log.print(date(), "run LD stuff");
     run_ld(p, ctx, N, M, false);
     pcaone_gpu_destroy(ctx);

@@ -6,7 +6,8 @@ v0.6.0 binary built from its own sources by ``oracle/ref.mk`` into ``oracle/_ref
 Run from the repository root in the container that has the reference sources:
 
     make -f oracle/ref.mk -j8            # REF defaults to $PCAONE_REF, else /root/reference
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             # every case
+    python tests/golden/make_golden.py g4_pruneA   # only the named cases (others kept)
 
 Each case in ``CASES`` is (name, dataset, reference arguments, output suffixes kept).
 ``cases.json`` records the exact commands so the tests can reproduce them.
@@ -56,6 +57,32 @@ LARGE = {
 
 LARGE_LOADING_ROWS = 5000
 
+# assoc-like files for clumping, drawn from the g4 .bim: (file, seed, fraction of SNPs kept,
+# fraction with a small p-value); columns CHR, SNP, BP, P (tab-separated, with a header);
+# every p-value is distinct
+ASSOC = {"g4_a.assoc": (21, 0.8, 0.15), "g4_b.assoc": (22, 0.6, 0.3)}
+
+
+def write_assoc(bim: str, path: str, seed: int, keep: float, small: float) -> None:
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    rows = [line.split() for line in open(bim)]
+    lines = ["CHR\tSNP\tBP\tP"]
+    used = set()
+    for r in rows:
+        if rng.random() >= keep:
+            continue
+        while True:
+            p = float(10 ** -rng.uniform(3, 6)) if rng.random() < small else float(rng.uniform(0.001, 1))
+            p = float(f"{p:.6g}")
+            if p not in used:
+                used.add(p)
+                break
+        lines.append(f"{r[0]}\t{r[1]}\t{r[3]}\t{p:.6g}")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
 EIG = [".eigvals", ".sigvals", ".eigvecs"]
 CASES = [
     ("g1_halko", "g1", ["-b", "{d}", "-d", "1", "-k", "4", "--oversamples", "10", "-p", "7",
@@ -84,6 +111,22 @@ CASES = [
      [".residuals", ".mbim"] + EIG),
     ("g4_ldB", "g4", ["-B", "{g}/ref/g4_adj.residuals", "-f", "{g}/ref/g4_adj.mbim",
                       "--ld-bp", "5000", "-R"], [".ld.gz"]),
+    # LD pruning: flow A keeping the higher-MAF SNP (.mbim frequencies), flow A with a plain
+    # .bim (the follower is dropped), flow B
+    ("g4_pruneA", "g4", ["-b", "{d}", "--read-U", "{g}/ref/g4_pcs.eigvecs", "-f", "{g}/ref/g4_pcs.mbim",
+                         "--ld-bp", "5000", "--ld-r2", "0.05"], [".ld.prune.in", ".ld.prune.out"]),
+    ("g4_pruneA_bim", "g4", ["-b", "{d}", "--read-U", "{g}/ref/g4_pcs.eigvecs", "--ld-bp", "5000",
+                             "--ld-r2", "0.05"], [".ld.prune.in", ".ld.prune.out"]),
+    ("g4_pruneB", "g4", ["-B", "{g}/ref/g4_adj.residuals", "-f", "{g}/ref/g4_adj.mbim", "--ld-bp", "5000",
+                         "--ld-r2", "0.05"], [".ld.prune.in", ".ld.prune.out"]),
+    # LD clumping of two assoc-like files (flow A) and of one with other thresholds (flow B)
+    ("g4_clumpA", "g4", ["-b", "{d}", "--read-U", "{g}/ref/g4_pcs.eigvecs", "-f", "{g}/ref/g4_pcs.mbim",
+                         "--clump", "{g}/g4_a.assoc,{g}/g4_b.assoc", "--clump-p1", "0.01",
+                         "--clump-p2", "0.2", "--clump-r2", "0.05", "--clump-bp", "5000"],
+     [".p0.clump", ".p1.clump"]),
+    ("g4_clumpB", "g4", ["-B", "{g}/ref/g4_adj.residuals", "-f", "{g}/ref/g4_adj.mbim",
+                         "--clump", "{g}/g4_a.assoc", "--clump-p1", "0.05", "--clump-p2", "0.5",
+                         "--clump-r2", "0.03", "--clump-bp", "3000"], [".p0.clump"]),
     # PCAngsd on PLINK input: pseudo-likelihoods from the genotypes (shuffled and -S)
     ("g1_pcangsd_bed", "g1", ["-b", "{d}", "--pcangsd", "-k", "3", "-w", "8", "--maxiter", "30",
                               "-V"], EIG + [".loadings"]),
@@ -123,15 +166,25 @@ def main() -> int:
     os.makedirs(refdir, exist_ok=True)
     for name, args in DATASETS.items():
         subprocess.check_call([SIM, "--out", os.path.join(HERE, name)] + args)
+    for fname, (seed, keep, small) in ASSOC.items():
+        write_assoc(os.path.join(HERE, "g4.bim"), os.path.join(HERE, fname), seed, keep, small)
     large_dir = tempfile.mkdtemp()
     large_sha = {}
     for name, args in LARGE.items():
         subprocess.check_call([SIM, "--out", os.path.join(large_dir, name)] + args)
         large_sha[name] = sha256(os.path.join(large_dir, name + ".bed"))
+    only = set(sys.argv[1:])
+    old = {}
+    if only and os.path.exists(os.path.join(HERE, "cases.json")):
+        with open(os.path.join(HERE, "cases.json")) as f:
+            old = {c["name"]: c for c in json.load(f)["cases"]}
     record = {"datasets": DATASETS, "large_datasets": LARGE, "large_bed_sha256": large_sha,
               "cases": []}
     env = dict(os.environ, OMP_NUM_THREADS="4")
     for name, ds, args, keep in CASES:
+        if only and name not in only and name in old:
+            record["cases"].append(old[name])
+            continue
         with tempfile.TemporaryDirectory() as tmp:
             dpath = os.path.join(large_dir if ds in LARGE else HERE, ds)
             argv = [a.format(d=dpath, g=HERE) for a in args]

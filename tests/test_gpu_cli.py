@@ -154,6 +154,42 @@ def test_cli_ld_flow_a_matches_reference(tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["g4_pruneA", "g4_pruneA_bim", "g4_pruneB"])
+def test_cli_ld_prune_matches_reference(tmp_path, name):
+    """--ld-r2: the kept and removed SNP lists are identical to the reference's (r2 from the
+    device in FP64, the greedy pass of src/LD.cpp:141-242 on the host)."""
+    run_cli(golden_args(name, tmp_path), tmp_path)
+    for suf in (".ld.prune.in", ".ld.prune.out"):
+        assert open(str(tmp_path / name) + suf).read() == open(ref_out(name, suf)).read()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,files", [("g4_clumpA", 2), ("g4_clumpB", 1)])
+def test_cli_ld_clump_matches_reference(tmp_path, name, files):
+    """--clump: one .pN.clump per assoc-like file, identical to the reference's."""
+    run_cli(golden_args(name, tmp_path), tmp_path)
+    for t in range(files):
+        suf = f".p{t}.clump"
+        assert open(str(tmp_path / name) + suf).read() == open(ref_out(name, suf)).read()
+
+
+@pytest.mark.gpu
+def test_ld_r2_f64_matches_oracle(tmp_path):
+    """pcaone_gpu_ld_r2_f64 on flow A (projected) and on the unprojected genotypes."""
+    import pcaone_b200 as pb
+    bed = O.read_bed(os.path.join(GOLDEN, "g4"))
+    snp = O.read_snp_pos(os.path.join(GOLDEN, "g4.bim"))
+    O.divide_pos_by_window(snp, 5000)
+    U = O.read_usv(os.path.join(GOLDEN, "ref", "g4_pcs.eigvecs"))
+    with pb.GpuContext(0) as ctx:
+        ctx.load_bed(bed.packed, bed.N)
+        for Uuse in (U, None):
+            got = ctx.ld_r2(snp.ws, snp.we, Uuse, f64=True)
+            i, k, r = O.ld_pairs(O.ld_flow_a(bed, Uuse), snp)
+            np.testing.assert_allclose(got, r * r, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.gpu
 def test_cli_ld_flow_b_matches_reference(tmp_path):
     """Flow B end to end: -D writes the .residuals matrix and .mbim (compared with the
     reference's), then -B reads it back for the windowed r2 (.ld.gz)."""

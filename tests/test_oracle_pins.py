@@ -103,6 +103,57 @@ def test_oracle_ld_flow_b_matches_reference():
     _ld_check(G, "g4_adj.mbim", "g4_ldB.ld.gz")
 
 
+def _ld_G(flow):
+    if flow == "A":
+        U = O.read_usv(os.path.join(GOLDEN, "ref", "g4_pcs.eigvecs"))
+        return O.ld_flow_a(g("g4"), U)
+    if flow == "A0":  # clumping on PLINK input: the centred genotypes, not projected off U
+        return O.ld_flow_a(g("g4"), None)
+    return O.read_residuals(os.path.join(GOLDEN, "ref", "g4_adj.residuals"))
+
+
+def _r2_of(G):
+    nrm = (G * G).sum(axis=0)
+    return lambda a, b: float((G[:, a] @ G[:, b]) ** 2 / (nrm[a] * nrm[b]))
+
+
+@pytest.mark.parametrize("name,flow,bim", [("g4_pruneA", "A", "ref/g4_pcs.mbim"), ("g4_pruneA_bim", "A", "g4.bim"),
+                                           ("g4_pruneB", "B", "ref/g4_adj.mbim")])
+def test_oracle_ld_prune_matches_reference(name, flow, bim):
+    G = _ld_G(flow)
+    filebim = os.path.join(GOLDEN, bim)
+    snp = O.read_snp_pos(filebim)
+    O.divide_pos_by_window(snp, 5000)
+    i, k, r = O.ld_pairs(G, snp)
+    r2 = {(int(a), int(b)): float(x * x) for a, b, x in zip(i, k, r)}
+    keep = O.ld_prune(snp, r2, 0.05, O.read_bim_af(filebim))
+    lines = open(filebim).read().splitlines()
+    assert [x for x, kk in zip(lines, keep) if kk] == open(os.path.join(GOLDEN, "ref", name + ".ld.prune.in")).read().splitlines()
+    assert [x for x, kk in zip(lines, keep) if not kk] == \
+        open(os.path.join(GOLDEN, "ref", name + ".ld.prune.out")).read().splitlines()
+    assert 0 < keep.sum() < len(keep)
+
+
+@pytest.mark.parametrize("name,flow,mbim,files,p1,p2,r2,bp", [
+    ("g4_clumpA", "A0", "ref/g4_pcs.mbim", ["g4_a.assoc", "g4_b.assoc"], 0.01, 0.2, 0.05, 5000),
+    ("g4_clumpB", "B", "ref/g4_adj.mbim", ["g4_a.assoc"], 0.05, 0.5, 0.03, 3000),
+])
+def test_oracle_ld_clump_matches_reference(name, flow, mbim, files, p1, p2, r2, bp):
+    G = _ld_G(flow)
+    snp = O.read_snp_pos(os.path.join(GOLDEN, mbim))
+    r2_of = _r2_of(G)
+    clumped = 0
+    for t, fname in enumerate(files):
+        head, idx, snp_t, lines = O.read_assoc(os.path.join(GOLDEN, fname))
+        pv = O.assoc_pvals(lines, idx, p2)
+        ipc, bpc = O.target_snp_idx(snp_t, snp)
+        out = O.ld_clump(head, bp, r2, p1, r2_of, ipc, bpc, pv)
+        ref = open(os.path.join(GOLDEN, "ref", f"{name}.p{t}.clump")).read().splitlines()
+        assert out == ref
+        clumped += sum(not x.endswith("NONE") for x in out[1:])
+    assert clumped > 0
+
+
 @pytest.mark.parametrize("name,shuffle", [("g3_pcangsd", False), ("g3_pcangsd_shuf", True)])
 def test_oracle_pcangsd_matches_reference(name, shuffle):
     eig, S, U, V, F, it, C, Dc = O.run_pcangsd(os.path.join(GOLDEN, "g3.beagle.gz"), k=3,

@@ -68,17 +68,26 @@ CONFIGS = {
                n=5000, m=200000, sim=["--pops", "3", "--fst-lo", "0.05", "--fst-hi", "0.1", "--pmin", "0.05",
                                       "--pmax", "0.5", "--beagle", "4,0.01", "--seed", "4"],
                k=6, svd=2, bands=64, maxp=20, tol=1e-4, maxiter=100, tolem=1e-5, cpu_fit_snps=(4096, 8192)),
+    "c5": dict(kind="ld", workload="LD r2 of every pair in 1 Mb windows (flow A: genotypes projected off the top 10 "
+                                    "PCs), 10000 samples x 300000 SNPs, about 100-1900 SNPs per window, Markov "
+                                    "haplotype LD (switch 0.01)",
+               n=10000, m=300000, sim=["--pops", "3", "--fst-lo", "0.05", "--fst-hi", "0.1", "--pmin", "0.05",
+                                       "--pmax", "0.5", "--miss", "0.01", "--bp-spacing", "1000",
+                                       "--ld-switch", "0.01", "--seed", "5"],
+               k=10, ld_bp=1000000, svd=1, maxp=7, tol=0.0, bands=64, cpu_fit_snps=(3000, 6000)),
 }
 
 METRIC = ("top-k PCA bed GB/s (packed .bed bytes x epochs / s), int8/BF16 tensor-core vs FP32 GPU "
           "path at matched eigval error")
 METRIC_GL = "PCAngsd GL GB/s (FP32 likelihood-pair bytes x likelihood passes / s)"
+METRIC_LD = "LD r2 pairs per second (every SNP pair of the --ld-bp windows, genotypes projected off the top k PCs)"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "PCAone")
 SIM = os.path.join(ROOT, "pcaone_b200", "bin", "pcaone-sim")
 DTYPE = {"mixed": "int8 (3-piece fixed-point sketch, int32 accumulation)",
-         "bf16": "bf16 (split hi+lo sketch, fp32 accumulation)"}
+         "bf16": "bf16 (split hi+lo sketch, fp32 accumulation)",
+         "int8": "int8 (exact integer genotype Gram, int32 accumulation; FP64 projection and normalisation)"}
 
 _T0 = time.time()
 
@@ -151,6 +160,13 @@ def reference_run(cfg, prefix, wd, nsnps):
         N = cfg["n"]
         args = [REF_BIN, "-G", sp + ".beagle.gz", "-k", str(cfg["k"]), "-S", "-w", str(cfg["bands"]),
                 "--maxiter", str(cfg["maxiter"]), "--tol-em", str(cfg["tolem"])]
+    elif kind == "ld":
+        N, nsnps = write_sample(prefix, sp, nsnps)
+        # the projection factors come from the reference's own PCA of the slice (not timed)
+        subprocess.run([REF_BIN, "-b", sp, "-k", str(cfg["k"]), "-d", "1", "-p", "3", "-n", str(cores), "-o",
+                        sp + "_pcs", "-v", "0"], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(cores)))
+        args = [REF_BIN, "-b", sp, "--read-U", sp + "_pcs.eigvecs", "--ld-bp", str(cfg["ld_bp"]), "-R"]
     else:
         N, nsnps = write_sample(prefix, sp, nsnps)
         args = [REF_BIN, "-b", sp, "-k", str(cfg["k"])]
@@ -184,8 +200,15 @@ def reference_run(cfg, prefix, wd, nsnps):
         raise RuntimeError("reference run failed: " + "".join(lines[-5:])[-300:])
     if kind == "rsvd" and epochs == 0:
         epochs = cfg["maxp"] + 1
+    pairs = 0
+    if kind == "ld":
+        import pcaone_b200 as pb
+
+        pos, ends = pb.read_bim_positions(sp + ".bim")
+        pairs = int((pb.ld_windows(pos, ends, cfg["ld_bp"])[1] - 1).sum())
     # likelihood passes of PCAngsd: the initial posterior and one per EM iteration
-    return {"seconds": wall, "epochs": epochs, "sweeps": sweeps + 1, "snps": nsnps, "samples": N, "cores": cores}
+    return {"seconds": wall, "epochs": epochs, "sweeps": sweeps + 1, "snps": nsnps, "samples": N, "cores": cores,
+            "pairs": pairs}
 
 
 def unit_bytes(cfg, nsnps):
@@ -197,6 +220,32 @@ def unit_bytes(cfg, nsnps):
 
 def passes_of(cfg, r):
     return r["sweeps"] if cfg["kind"] == "pcangsd" else r["epochs"]
+
+
+def fitted_rate_ld(cfg, runs, full_pairs):
+    """LD pairs per second of the reference from its runs on SNP slices: wall time fitted as
+    a + b * pairs over the slices and evaluated at the full workload's pairs (one slice: its
+    own rate)."""
+    x = np.array([r["pairs"] for r in runs], dtype=float)
+    y = np.array([r["seconds"] for r in runs])
+    desc = "; ".join(f"{r['samples']} x {r['snps']}: {r['pairs']} pairs in {r['seconds']:.2f} s" for r in runs)
+    if len(set(x)) > 1:
+        b, a = np.polyfit(x, y, 1)
+        value = full_pairs / (a + b * full_pairs)
+        sample = (f"wall time (text .ld.gz output included) fitted as a + b * pairs over [{desc}] "
+                  f"(a = {a:.4g} s, b = {b:.4g} s/pair) and evaluated at {full_pairs} pairs")
+    else:
+        value = float(np.mean(x / y))
+        sample = desc + " (a slice of the workload)"
+    return value, sample
+
+
+def full_ld_pairs(cfg, prefix):
+    import pcaone_b200 as pb
+
+    pos, ends = pb.read_bim_positions(prefix + ".bim")
+    ws, we = pb.ld_windows(pos, ends, cfg["ld_bp"])
+    return ws, we, int((we - 1).sum())
 
 
 def fitted_rate(cfg, runs):
@@ -613,13 +662,125 @@ def run_pcangsd_cfg(args, cfg, run):
           "timing": "host clock around the EM loop (every library call synchronises)"}, metric=METRIC_GL)
 
 
+def ld_dense_check(packed, N, U, ws, we, r2, nwin=3):
+    """Largest |r2 - r2_dense| over a few windows (first, middle, last long one), r2_dense
+    from a dense FP64 evaluation in numpy: centred genotypes (missing 0), projected off U,
+    Pearson r of every pair of the window."""
+    off = np.concatenate([[0], np.cumsum(np.maximum(we.astype(np.int64) - 1, 0))])
+    long_ = np.nonzero(we > 1)[0]
+    picks = sorted({int(long_[0]), int(long_[len(long_) // 2]), int(long_[-1])})[:nwin]
+    worst = 0.0
+    lut = np.array([2.0, 0.0, 1.0, 0.0])  # A1 count per code (missing -> 0)
+    for w in picks:
+        i0, n = int(ws[w]), int(we[w])
+        codes = np.unpackbits(packed[i0:i0 + n][:, :, None], axis=2, bitorder="little")
+        codes = (codes[:, :, 0::2] + 2 * codes[:, :, 1::2]).reshape(n, -1)[:, :N]
+        x = lut[codes] / 2.0
+        nm = codes != 1
+        F = (x * nm).sum(1) / np.maximum(nm.sum(1), 1)
+        G = np.where(nm, x - F[:, None], 0.0).T  # N x n
+        G = G - U @ (U.T @ G)
+        r = (G[:, 1:].T @ G[:, 0]) / np.sqrt((G[:, 1:] ** 2).sum(0) * (G[:, 0] ** 2).sum())
+        worst = max(worst, float(np.abs(r2[off[w]:off[w + 1]] - r * r).max()))
+    return {"max_abs_r2_err_vs_dense_fp64": worst, "windows_checked": picks}
+
+
+def run_ld_cfg(args, cfg, run):
+    """LD r2 of every window pair through the C ABI (pcaone_gpu_ld_r2): the band Gram of the
+    windows on the tensor cores. value = pairs / device time of the LD work (CUDA events on the
+    library's stream around the diagonal, tiling and band-Gram launches; the packed genotypes
+    and the projection factors resident); e2e = pairs / wall time of load + LD call with host
+    buffers (packed genotypes in, r2 of every pair out)."""
+    import pcaone_b200 as pb
+
+    wd, prefix = prepare(cfg, args.config, run)
+    packed, N, M = pb.read_bed(prefix)
+    ws, we, pairs = full_ld_pairs(cfg, prefix)
+    log(f"{len(ws)} windows, {pairs} pairs, window SNPs {int(we.min())}..{int(we.max())}")
+    ctx = pb.GpuContext(run.local)
+    ctx.load_bed(packed, N)
+    pcs = ctx.rsvd(k=cfg["k"], svd=1, maxp=cfg["maxp"], tol=cfg["tol"], precision="mixed")
+    U = pcs.U
+    for _ in range(args.warmup):
+        t0 = time.perf_counter()
+        ctx.ld_r2(ws, we, U)
+        log(f"warm-up LD: {time.perf_counter() - t0:.2f} s wall, device {ctx.ld_timing()}")
+    run.barrier()
+    dev, gram = [], []
+    with ClockSampler(run.local) as clk:
+        run.barrier()
+        for _ in range(args.steps):
+            ctx.ld_r2(ws, we, U)
+            d, g = ctx.ld_timing()
+            dev.append(d)
+            gram.append(g)
+        run.barrier()
+    clocks = clk.summary()
+    log(f"timed LD device ms: {[round(x, 2) for x in dev]}, band Gram ms: {[round(x, 2) for x in gram]}")
+    ms = run.max_over_ranks(float(np.mean(dev)))
+    value = pairs / (ms / 1e3) * run.world
+    # tensor roofline of the band Gram: 4 integer Grams (RR, RN, NR, NN), 2 ops per product
+    alg = 8.0 * pairs * N
+    g_ms = float(np.mean(gram))
+    pk, pk_kind = peaks()
+    peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+    # issued: per (128 x 128) tile of SNP pairs two M = 128, N = 256 int8 MMAs per sample
+    T = 128
+    reach = {}
+    for s, w in zip(ws, we):
+        if w >= 2:
+            b = int(s) // T
+            reach[b] = max(reach.get(b, -1), int(s) + int(w) - 1)
+    ntile = sum(v // T - b + 1 for b, v in reach.items())
+    issued = ntile * 2.0 * 2 * T * 256 * ((N + 127) // 128 * 128)
+    achieved = alg / (g_ms / 1e3) / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak, "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": f"{pk_kind} bf16_tflops_sustained",
+                "kernel": "k_ld_gram_i8", "launches": 1, "avg_launch_ms": round(g_ms, 4),
+                "algorithmic_ops_per_launch": alg, "issued_ops_factor": round(issued / alg, 4),
+                "ceiling_frac_of_bf16_peak": round(2.0 / (issued / alg), 4), "band_tiles": ntile,
+                "gram_share_of_device_ms": round(g_ms / ms, 4)}
+    pinned, keep = pinned_copy(packed)
+    e2e_t = []
+    for i in range(2):
+        t0 = time.perf_counter()
+        ctx.load_bed(pinned, N)
+        out = ctx.ld_r2(ws, we, U)
+        if i > 0:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_s = run.max_over_ranks(e2e_t[0])
+    e2e = {"value": round(pairs / e2e_s * run.world, 1), "unit": "pairs/s",
+           "h2d_bytes_per_step": int(packed.nbytes + U.nbytes + ws.nbytes + we.nbytes),
+           "d2h_bytes_per_step": int(out.nbytes), "seconds_per_call": round(e2e_s, 3),
+           "includes": "genotype upload, projection factors W = Gc^T U (FP64 product) and Y, r2 of every pair "
+                       "copied back"}
+    acc = {}
+    if not args.skip_compare:
+        acc = ld_dense_check(packed, N, U, ws, we, out)
+    ctx.close()
+    cpu = cpu_baseline(args, cfg, prefix, wd, run)
+    run.close()
+    if run.rank != 0:
+        return
+    emit(args, cfg, run, value, "pairs/s", ms, "int8", clocks, roofline, e2e, cpu, None,
+         {"samples": N, "snps": M, "k": cfg["k"], "ld_bp": cfg["ld_bp"], "windows": int(len(ws)), "pairs": pairs,
+          "window_snps": [int(we.min()), int(we.max())]},
+         {"accuracy": acc, "timing": "CUDA events on the library stream (pcaone_gpu_ld_timing)"}, metric=METRIC_LD)
+
+
 def cpu_baseline(args, cfg, prefix, wd, run):
     if run.rank != 0 or run.world != 1 or args.skip_cpu:
         return None
     try:
         runs = [reference_run(cfg, prefix, wd, s) for s in cfg["cpu_fit_snps"]]
-    except RuntimeError as e:
+    except (RuntimeError, subprocess.CalledProcessError) as e:
         return {"value": None, "unavailable": str(e)}
+    if cfg["kind"] == "ld":
+        value, sample = fitted_rate_ld(cfg, runs, full_ld_pairs(cfg, prefix)[2])
+        cpu = {"value": round(value, 1), "unit": "pairs/s", "cores": runs[0]["cores"], "kind": "reference",
+               "sample": sample}
+        log(f"cpu baseline: {cpu}")
+        return cpu
     value, sample = fitted_rate(cfg, runs)
     cpu = {"value": round(value, 6), "unit": "GL GB/s" if cfg["kind"] == "pcangsd" else "bed GB/s",
            "cores": runs[0]["cores"], "kind": "reference", "sample": sample}
@@ -661,17 +822,22 @@ def run_reference_arm(args, cfg):
     for i in range(args.warmup + args.steps):
         try:
             r = reference_run(cfg, prefix, wd, sizes[i % len(sizes)])
-        except RuntimeError as e:
+        except (RuntimeError, subprocess.CalledProcessError) as e:
             print(json.dumps({"impl": "reference", "unavailable": str(e)}))
             return
         if i >= args.warmup:
             runs.append(r)
         if time.perf_counter() - t_start > 240 and len(runs) >= len(sizes):
             break  # keep the arm within a few minutes
-    v, sample = fitted_rate(cfg, runs)
-    unit = "GL GB/s" if cfg["kind"] == "pcangsd" else "bed GB/s"
+    if cfg["kind"] == "ld":
+        v, sample = fitted_rate_ld(cfg, runs, full_ld_pairs(cfg, prefix)[2])
+        unit, metric = "pairs/s", METRIC_LD
+    else:
+        v, sample = fitted_rate(cfg, runs)
+        unit = "GL GB/s" if cfg["kind"] == "pcangsd" else "bed GB/s"
+        metric = METRIC_GL if cfg["kind"] == "pcangsd" else METRIC
     print(json.dumps({
-        "impl": "reference", "metric": METRIC_GL if cfg["kind"] == "pcangsd" else METRIC, "value": round(v, 6),
+        "impl": "reference", "metric": metric, "value": round(v, 6),
         "unit": unit, "n_gpus": world, "steps": len(runs), "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "dtype": "f64", "data": "synthetic (seeded simulator: " + " ".join(cfg["sim"]) + ")",
         "config": {"workload": cfg["workload"], "sample": f"{len(runs)} timed runs; " + sample},
@@ -743,7 +909,8 @@ def main():
         run_reference_arm(args, cfg)
     else:
         run = Run()
-        {"rsvd": run_rsvd_cfg, "emu": run_emu_cfg, "pcangsd": run_pcangsd_cfg}[cfg["kind"]](args, cfg, run)
+        {"rsvd": run_rsvd_cfg, "emu": run_emu_cfg, "pcangsd": run_pcangsd_cfg,
+         "ld": run_ld_cfg}[cfg["kind"]](args, cfg, run)
 
 
 if __name__ == "__main__":

@@ -187,6 +187,12 @@ int pcaone_gpu_ld_r2(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t
 int pcaone_gpu_ld_r2_f64(pcaone_ctx* ctx, const double* U, uint32_t k, const int64_t* ws,
                          const int32_t* we, uint64_t nwin, double* r2);
 
+/* Device time (CUDA events on the context's stream) of the last pcaone_gpu_ld_r2 /
+ * pcaone_gpu_ld_r2_f64 call on packed genotypes through the tensor-core band Gram: all its
+ * device work after the projection factors are in place (diagonal, code tiling, band Gram)
+ * and the band-Gram launch alone, in ms; -1 when that call took another path. */
+int pcaone_gpu_ld_timing(pcaone_ctx* ctx, double* device_ms, double* gram_ms);
+
 /* LD flow B, first half: the residual matrix of Data::write_residuals (src/Data.cpp:196-245)
  * for the SNPs snp0 .. snp0 + nsnp - 1 of the current order. R_ij = Gc_ij - sum_t U_it S_t
  * V_jt with Gc the centred genotypes (BED2GENO - F_j, missing -> 0; not standardised), or Gc

@@ -32,7 +32,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
            "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
            "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm",
-           "pcaone_gpu_ld_r2_f64"]
+           "pcaone_gpu_ld_r2_f64", "pcaone_gpu_ld_timing"]
 
 
 class PcaoneError(RuntimeError):
@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_clear_imputed.argtypes = [vp]
         L.pcaone_gpu_ld_r2.argtypes = [vp, vp, u32, vp, vp, u64, vp]
         L.pcaone_gpu_ld_r2_f64.argtypes = [vp, vp, u32, vp, vp, u64, vp]
+        L.pcaone_gpu_ld_timing.argtypes = [vp, vp, vp]
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
@@ -343,6 +344,54 @@ def _ld_r2(self, ws, we, U=None, f64=False):
 
 
 GpuContext.ld_r2 = _ld_r2
+
+
+def _ld_timing(self):
+    """(device ms, band-Gram ms) of the last LD r2 call (see pcaone_gpu_ld_timing)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    self._check(lib().pcaone_gpu_ld_timing(self._h, ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
+
+
+GpuContext.ld_timing = _ld_timing
+
+
+def read_bim_positions(path: str):
+    """Chromosome runs and positions of a .bim (get_snp_pos_bim, src/LD.cpp:51-77): returns
+    (positions int64, last index of each chromosome run)."""
+    pos, ends, prev = [], [], None
+    with open(path) as f:
+        for i, line in enumerate(f):
+            tok = line.split()
+            if prev is not None and tok[0] != prev:
+                ends.append(i - 1)
+            prev = tok[0]
+            pos.append(int(tok[3]))
+    ends.append(len(pos) - 1)
+    return np.array(pos, dtype=np.int64), ends
+
+
+def ld_windows(pos, ends, bp: int):
+    """divide_pos_by_window (src/LD.cpp:125-139): (ws, we) of the windows of SNPs within bp
+    of each lead SNP on its chromosome (none for a SNP at its chromosome's last position)."""
+    pos = np.asarray(pos, dtype=np.int64)
+    ws, we = [], []
+    c = 0
+    starts = [0] + [e + 1 for e in ends[:-1]]
+    ordered = all(np.all(np.diff(pos[s:e + 1]) >= 0) for s, e in zip(starts, ends))
+    for i in range(len(pos)):
+        e = ends[c]
+        if pos[i] == pos[e]:
+            c += 1
+            continue
+        if ordered:  # the first SNP past bp, by bisection
+            j = int(np.searchsorted(pos[i:e + 1], pos[i] + bp, side="right")) + i
+        else:
+            far = np.nonzero(pos[i:e + 1] - pos[i] > bp)[0]
+            j = i + int(far[0]) if len(far) else e + 1
+        ws.append(i)
+        we.append(j - i)
+    return np.array(ws, dtype=np.int64), np.array(we, dtype=np.int32)
 
 
 def _load_gl(self, P: np.ndarray):

@@ -340,6 +340,7 @@ void ld_r2_impl(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, c
                 void* r2, bool f64) {
   {
     const size_t esz = f64 ? 8 : 4;
+    c->ld_device_ms = c->ld_gram_ms = -1.0;
     PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
     PG_REQUIRE(ws && we && (r2 || nwin == 0), PCAONE_EBADARG, "null window arrays");
     PG_REQUIRE(!U || (k >= 1 && k <= (uint32_t)kLmax), PCAONE_EBADARG, "bad U width");
@@ -415,7 +416,18 @@ void ld_r2_impl(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, c
       PG_CUDA(cudaMemcpyAsync(d_we, we, nwin * 4, cudaMemcpyHostToDevice, c->stream));
       PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (nwin + 1) * 8, cudaMemcpyHostToDevice, c->stream));
     }
-    ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2, f64);
+    if (ld_tc_usable(c, U ? (int)k : 0)) {
+      // band Gram on the tensor cores: windows located by their lead SNP
+      std::vector<int64_t> win_of(c->M, -1);
+      for (uint64_t w = 0; w < nwin; ++w) win_of[ws[w]] = (int64_t)w;
+      int64_t* d_win_of = (int64_t*)scratch(c, "ld_win_of", c->M * 8);
+      PG_CUDA(cudaMemcpyAsync(d_win_of, win_of.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
+      tc_clear_error(c);
+      ld_r2_tc(c, dW, dY, U ? (int)k : 0, ws, we, nwin, d_win_of, d_we, d_off, d_r2, f64);
+      tc_check_error(c);
+    } else {
+      ld_r2(c, dW, dY, U ? (int)k : 0, d_ws, d_we, d_off, (int64_t)nwin, d_r2, f64);
+    }
     if (off[nwin] > 0)
       PG_CUDA(cudaMemcpyAsync(r2, d_r2, off[nwin] * esz, cudaMemcpyDeviceToHost, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
@@ -433,6 +445,14 @@ int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* 
 int pcaone_gpu_ld_r2_f64(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
                          uint64_t nwin, double* r2) {
   return guarded(c, [&] { ld_r2_impl(c, U, k, ws, we, nwin, r2, true); });
+}
+
+int pcaone_gpu_ld_timing(pcaone_ctx* c, double* device_ms, double* gram_ms) {
+  return guarded(c, [&] {
+    PG_REQUIRE(device_ms && gram_ms, PCAONE_EBADARG, "null timing outputs");
+    *device_ms = c->ld_device_ms;
+    *gram_ms = c->ld_gram_ms;
+  });
 }
 
 

@@ -68,6 +68,10 @@ struct pcaone_ctx {
   std::string err;
   int sm_count = 0;
   int cc_major = 0, cc_minor = 0;
+  // device time of the last LD r2 call (CUDA events on the stream): all of its device work
+  // (diagonal, tiling, band Gram) and the band-Gram launch alone; pairs it produced
+  double ld_device_ms = 0.0, ld_gram_ms = 0.0;
+  int64_t ld_pairs = 0;
 
   // genotypes
   bool loaded = false;
@@ -179,6 +183,12 @@ void compute_imputed_ws(pcaone_ctx* c);
 // d_r2 holds float values, or double with f64.
 void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,
            const int32_t* d_we, const int64_t* d_off, int64_t nwin, void* d_r2, bool f64);
+// The same on the tcgen05 tensor cores (kernels_ld_tc.cu): the band Gram of the windows as
+// exact int8 products, one persistent launch; usable for projections of at most 16 columns.
+// ws, we: host window arrays; d_win_of (M: window led by SNP i or -1), d_we, d_off: device.
+bool ld_tc_usable(pcaone_ctx* c, int k);
+void ld_r2_tc(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* ws, const int32_t* we,
+              uint64_t nwin, const int64_t* d_win_of, const int32_t* d_we, const int64_t* d_off, void* d_r2, bool f64);
 // LD flow B (kernels_ld.cu): residual rows of snp0..snp0+nsnp (US N x k, V nsnp x k
 // row-major device arrays, or null for the centred genotypes), the in-place centring of the
 // dense matrix with its squared column norms d, and r2 of the window pairs on it.

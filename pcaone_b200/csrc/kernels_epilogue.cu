@@ -142,7 +142,7 @@ __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* 
 // Omega when p.omega_f is set (half the L2 bytes of the FP64 rows); without imputed values
 // its weight is F_j for every entry, so it sums the rows unweighted (sum_rows, l % 4 == 0).
 template <typename T, int CPL>
-__global__ void __launch_bounds__(256, 3) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
+__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
   extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __res
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse, the sparse term over the sample's
 // missing entries in the windows [b0, b1).
 template <typename T, int CPL>
-__global__ void __launch_bounds__(256, 3) k_accum(EpiP2 p, const T* __restrict__ D2) {
+__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const T* __restrict__ D2) {
   extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = ssm + warp * p.l;

@@ -42,6 +42,36 @@ def test_ld_matches_oracle(gpu, N, M, with_u):
     assert np.abs(r2 - r * r).max() <= 1e-6
 
 
+@pytest.mark.parametrize("N,M,k,bp,chroms", [
+    (1001, 700, 5, 4000, 1),     # tensor-core band Gram, windows across several 128-SNP tiles
+    (130, 2000, 0, 60000, 2),    # unprojected, long windows (up to ~1000 SNPs), two chromosomes
+    (2049, 515, 16, 9000, 1),    # widest projection of the tensor-core path
+    (777, 600, 20, 5000, 1),     # projection wider than 16: the bit-plane kernel
+])
+def test_ld_band_gram_matches_oracle_f64(gpu, N, M, k, bp, chroms):
+    """FP64 r2 of every window pair (the pruning/clumping values) against the oracle's
+    dense FP64 correlations, on shapes that are not multiples of the 128-SNP and 128-sample
+    tiles."""
+    bed = random_bed(N, M, seed=3 * N + M, miss=0.05)
+    rng = np.random.default_rng(N)
+    U = np.linalg.qr(rng.standard_normal((N, k)))[0] if k else None
+    gpu.load_bed(bed.packed, N)
+    pos = np.concatenate([np.cumsum(rng.integers(1, 120, M // chroms + (c < M % chroms))) for c in range(chroms)])
+    ends, acc = [], 0
+    for c in range(chroms):
+        acc += M // chroms + (c < M % chroms)
+        ends.append(acc - 1)
+    snp = O.SnpLD([str(c + 1) for c in range(chroms)], pos, ends, [""] * M)
+    O.divide_pos_by_window(snp, bp)
+    r2 = gpu.ld_r2(snp.ws, snp.we, U, f64=True)
+    G = O.centered_matrix(O.decode_codes(bed), O.allele_freq(O.decode_codes(bed)))
+    if k:
+        G = G - U @ (U.T @ G)
+    i, kk, r = O.ld_pairs(G, snp)
+    assert len(r2) == len(r) and int(np.max(snp.we)) > 60  # windows cross 128-SNP tile edges
+    np.testing.assert_allclose(r2, r * r, rtol=1e-9, atol=1e-12)
+
+
 def test_ld_flow_b_matches_reference(gpu):
     """Flow B: r2 on the reference's own .residuals matrix (loaded and re-centred on the
     device) against the reference's .ld.gz of -B g4_adj.residuals -f g4_adj.mbim."""

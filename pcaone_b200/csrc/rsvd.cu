@@ -10,6 +10,7 @@
 //  * B = R^-T H^T is never formed: its SVD comes from CholeskyQR2 of B^T = H R^-1 and a
 //    one-sided Jacobi SVD of the l x l triangular factor on the host.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <random>
@@ -384,6 +385,78 @@ struct Engine {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
+    if (steady_exec) cudaGraphExecDestroy(steady_exec);
+  }
+
+  // Steady epochs as one CUDA graph. Once the schedule stops depending on the epoch (the
+  // winSVD from 2^pi >= bands on: every window run and every Omega update the same; Halko from
+  // its second update on), the epoch body is launched as a graph: run once directly (buffers
+  // sized), captured on the next epoch, replayed after it. The epoch tail, with its host round
+  // trip, stays outside. Used by the tensor-core back ends when no per-launch profile is asked.
+  cudaGraphExec_t steady_exec = nullptr;
+  int steady_seen = 0, steady_updates = 0;
+  uint64_t steady_launches = 0, steady_gemm_launches = 0;
+  bool graphs_failed = false;
+  bool graphs_on() const {
+    static const bool disabled = std::getenv("PCAONE_NO_GRAPHS") != nullptr;
+    return !disabled && !graphs_failed && !o.profile &&
+           (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) && !c->dense;
+  }
+  bool steady_epoch(int pi) const {
+    return o.svd == 1 ? pi >= 2 : (std::pow(2.0, pi) >= o.bands && o.block_snps == 0);
+  }
+  void run_epoch(int pi) {
+    auto body = [&] {
+      if (o.svd == 1)
+        epoch_halko(pi);
+      else
+        epoch_winsvd(pi);
+    };
+    if (!graphs_on() || !steady_epoch(pi)) {
+      body();
+      return;
+    }
+    if (steady_exec) {  // replay, with the host-side counters the body would have advanced
+      PG_CUDA(cudaGraphLaunch(steady_exec, c->stream));
+      updates += steady_updates;
+      c->launches += steady_launches;
+      c->gemm_launches += steady_gemm_launches;
+      return;
+    }
+    if (steady_seen++ == 0) {  // first steady epoch: direct, sizes every buffer it touches
+      body();
+      return;
+    }
+    const int u0 = updates;
+    const int64_t l0 = c->launches, g0 = c->gemm_launches;
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        body();
+      } catch (...) {
+        ok = false;
+      }
+      cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+      ok = ok && e == cudaSuccess && graph;
+      if (ok) ok = cudaGraphInstantiate(&steady_exec, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    if (!ok) {  // capture refused: run this epoch and the rest directly (nothing was executed)
+      (void)cudaGetLastError();
+      if (steady_exec) cudaGraphExecDestroy(steady_exec);
+      steady_exec = nullptr;
+      graphs_failed = true;
+      updates = u0;
+      c->launches = l0;
+      c->gemm_launches = g0;
+      body();
+      return;
+    }
+    steady_updates = updates - u0;
+    steady_launches = c->launches - l0;
+    steady_gemm_launches = c->gemm_launches - g0;
+    PG_CUDA(cudaGraphLaunch(steady_exec, c->stream));
   }
 
   void epoch_halko(int pi) {
@@ -466,10 +539,7 @@ struct Engine {
     int epochs = 0;
     bool done = false;
     for (int pi = 0; pi <= p && !done; ++pi) {
-      if (o.svd == 1)
-        epoch_halko(pi);
-      else
-        epoch_winsvd(pi);
+      run_epoch(pi);
       // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B)
       timed([&] {
         cholqr2(c, G, l, M, G, Rg, d_status);

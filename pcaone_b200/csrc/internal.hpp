@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <array>
 #include <map>
 #include <set>
 #include <stdexcept>
@@ -72,6 +73,9 @@ struct pcaone_ctx {
   // (diagonal, tiling, band Gram) and the band-Gram launch alone; pairs it produced
   double ld_device_ms = 0.0, ld_gram_ms = 0.0;
   int64_t ld_pairs = 0;
+  // int8 decode-GEMM autotuner: pipeline variant per product shape (NP, rows, K, K chunks per
+  // window, bytes per window)
+  std::map<std::array<int64_t, 5>, int> i8_tune;
 
   // genotypes
   bool loaded = false;

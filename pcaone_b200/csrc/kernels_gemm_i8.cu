@@ -44,6 +44,7 @@
 // an error flag, stops issuing work, waits (bounded) for its copies and MMAs in flight, frees
 // its tensor memory and returns, and the host reports PCAONE_ETIMEOUT.
 #include <algorithm>
+#include <array>
 
 #include "internal.hpp"
 #include "rsvd.hpp"
@@ -75,12 +76,16 @@ constexpr int kMinUnitsPerCta = 2;
 __host__ __device__ constexpr int lp_of(int l) { return (l + 7) / 8 * 8; }
 __host__ __device__ constexpr int np_of(int l) { return (3 * lp_of(l) + 15) / 16 * 16; }
 
-template <int NP>
+// Pipeline shape of variant V (chosen per product shape by the autotuner in run_i8):
+// V = 0: units of two K chunks, two units in flight in tensor memory per tile; V = 1: units
+// of one chunk, four in flight (finer stream-K split, half the MMAs per commit). Wide
+// sketches (NP > 128) have room for one variant only.
+template <int NP, int V = 0>
 struct Cfg {
-  static constexpr int UC = NP <= 128 ? 2 : 1;  // K chunks per unit
-  static constexpr int RA = NP <= 128 ? 4 : 2;  // A slots per tile (one chunk each)
-  static constexpr int NU = RA / UC;            // units in flight in tensor memory per tile
-  static constexpr int SB = NP * 128;           // B bytes per chunk
+  static constexpr int UC = (NP <= 128 && V == 0) ? 2 : 1;  // K chunks per unit
+  static constexpr int RA = NP <= 128 ? 4 : 2;              // A slots per tile (one chunk each)
+  static constexpr int NU = RA / UC;                        // units in flight in tensor memory per tile
+  static constexpr int SB = NP * 128;                       // B bytes per chunk
   static constexpr int STAGE = UC * (kPairChunkBytes + SB);
   static constexpr int S = (192 * 1024) / STAGE < 8 ? (192 * 1024) / STAGE : 8;
   static constexpr int ACOL = 2 * NP;
@@ -122,9 +127,9 @@ __device__ __forceinline__ int64_t cta_of_unit(int64_t x, const I8Args& a) {
   return ((x + 1) * a.grid + a.units - 1) / a.units - 1;
 }
 
-template <int NP>
+template <int NP, int V>
 __global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_constant__ I8Args args) {
-  using C = Cfg<NP>;
+  using C = Cfg<NP, V>;
   constexpr int S = C::S, UC = C::UC, RA = C::RA, NU = C::NU;
   constexpr uint32_t kStageA = UC * kPairChunkBytes, kStageB = UC * C::SB;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -441,13 +446,14 @@ __global__ void __launch_bounds__(256) k_quant(const T* __restrict__ X, int64_t 
 }
 
 // ------------------------------------------------------------------ host side
-template <int NP>
+template <int NP, int V>
 constexpr size_t smem_of() {
-  using C = Cfg<NP>;
+  using C = Cfg<NP, V>;
   return (size_t)1024 + (size_t)C::S * C::STAGE + (size_t)(2 * C::S + 2 * C::NU + 8) * 8 + (3 * 64 + 4 * 32 * 9) * 4;
 }
 
-int uc_of(int np) { return np <= 128 ? 2 : 1; }
+int uc_of(int np, int v) { return (np <= 128 && v == 0) ? 2 : 1; }
+int variants_of(int np) { return np <= 128 ? 2 : 1; }
 
 struct I8Plan {
   int64_t tiles = 0, pairs = 0, chunks = 0, upp = 0, units = 0;
@@ -456,12 +462,12 @@ struct I8Plan {
 
 int64_t plan_cta_of_unit(int64_t x, int64_t units, int grid) { return ((x + 1) * grid + units - 1) / units - 1; }
 
-I8Plan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K, int np) {
+I8Plan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K, int np, int v) {
   I8Plan p;
   p.tiles = (rows + kRows - 1) / kRows;
   p.pairs = (p.tiles + 1) / 2;
   p.chunks = (K + kChunk - 1) / kChunk;
-  p.upp = (p.chunks + uc_of(np) - 1) / uc_of(np);
+  p.upp = (p.chunks + uc_of(np, v) - 1) / uc_of(np, v);
   p.units = p.pairs * p.upp;
   if (p.units == 0) return p;
   p.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->sm_count, p.units / kMinUnitsPerCta));
@@ -475,14 +481,67 @@ I8Plan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K, int np) {
   return p;
 }
 
-template <int NP>
+// Output slots every variant can fill: the largest split count over the variants (a variant
+// that uses fewer zero-fills the rest).
+int ks_all(const pcaone_ctx* c, int64_t rows, int64_t K, int np) {
+  int ks = 1;
+  for (int v = 0; v < variants_of(np); ++v) ks = std::max(ks, make_plan(c, rows, K, np, v).ks);
+  return ks;
+}
+
+template <int NP, int V>
 void launch_np(pcaone_ctx* c, const I8Args& a) {
-  constexpr size_t smem = smem_of<NP>();
+  constexpr size_t smem = smem_of<NP, V>();
   static_assert(smem <= 227 * 1024, "shared memory above the per-CTA limit");
-  if (c->smem_attr_set.insert((const void*)k_decode_gemm_i8<NP>).second)
-    PG_CUDA(cudaFuncSetAttribute(k_decode_gemm_i8<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_decode_gemm_i8<NP><<<a.grid, kThreads, smem, c->stream>>>(a);
+  if (c->smem_attr_set.insert((const void*)k_decode_gemm_i8<NP, V>).second)
+    PG_CUDA(cudaFuncSetAttribute(k_decode_gemm_i8<NP, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_decode_gemm_i8<NP, V><<<a.grid, kThreads, smem, c->stream>>>(a);
   PG_CHECK_LAUNCH();
+}
+
+template <int NP>
+void launch_v(pcaone_ctx* c, const I8Args& a, int v) {
+  if constexpr (NP <= 128) {
+    if (v == 1) return launch_np<NP, 1>(c, a);
+  }
+  launch_np<NP, 0>(c, a);
+}
+
+// The autotuner: the first product of a given shape (NP, rows, K and window layout of K)
+// times each pipeline variant once, after a warm-up launch, with CUDA events on the
+// library's stream and keeps the fastest for every later product of that shape. Every
+// variant writes the same product (to the rounding of the partial sums), so the launches
+// that time them are the product itself. While the stream is being captured into a graph
+// an unknown shape runs variant 0 untimed.
+template <typename F>
+int tune_variant(pcaone_ctx* c, const std::array<int64_t, 5>& key, int nvar, F&& launch) {
+  auto it = c->i8_tune.find(key);
+  if (it != c->i8_tune.end()) return it->second;
+  if (nvar <= 1) return c->i8_tune[key] = 0;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PG_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return 0;
+  cudaEvent_t e0, e1;
+  PG_CUDA(cudaEventCreate(&e0));
+  PG_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 0.f;
+  for (int v = 0; v < nvar; ++v) {
+    launch(v);  // warm-up (first use of the variant)
+    PG_CUDA(cudaEventRecord(e0, c->stream));
+    launch(v);
+    PG_CUDA(cudaEventRecord(e1, c->stream));
+    PG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (v == 0 || ms < best_ms) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return c->i8_tune[key] = best;
 }
 
 // One product over tiled codes (a_stride chunks per pair row, rows valid, K codes) and the
@@ -493,51 +552,55 @@ void run_i8(pcaone_ctx* c, const uint8_t* a_tiles, int64_t a_stride, int64_t row
             const float* sig, int64_t kpad, int l, int ks, float* out, int64_t cpw = 0, int64_t win_bytes = 0) {
   const int np = np_of(l);
   PG_REQUIRE(np <= 192, PCAONE_EBADARG, "sketch width too large for the int8 tensor-core path");
-  const I8Plan p = make_plan(c, rows, K, np);
-  PG_REQUIRE(ks == p.ks, PCAONE_EBADARG, "output slot count does not match the product plan");
-  if (p.units == 0) {
+  PG_REQUIRE(ks == ks_all(c, rows, K, np), PCAONE_EBADARG, "output slot count does not match the product plan");
+  const I8Plan p0 = make_plan(c, rows, K, np, 0);
+  if (p0.units == 0) {
     PG_CUDA(cudaMemsetAsync(out, 0, (size_t)ks * rows * l * sizeof(float), c->stream));
     return;
   }
   if (cpw <= 0) {
-    cpw = p.chunks;
+    cpw = p0.chunks;
     win_bytes = 0;
   }
-  PG_REQUIRE(cpw <= a_stride && p.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
+  PG_REQUIRE(cpw <= a_stride && p0.chunks * kChunk <= kpad, PCAONE_EBADARG, "K padding too small");
   PG_REQUIRE(((uintptr_t)a_tiles & 15) == 0 && ((uintptr_t)bq & 15) == 0, PCAONE_EBADARG,
              "operands not 16-byte aligned");
-  I8Args a;
-  a.a_tiles = a_tiles;
-  a.bq = bq;
-  a.sig = sig;
-  a.a_stride = a_stride;
-  a.cpw = cpw;
-  a.win_bytes = win_bytes;
-  a.rows = rows;
-  a.chunks = p.chunks;
-  a.upp = p.upp;
-  a.units = p.units;
-  a.grid = p.grid;
-  a.ks = p.ks;
-  a.l = l;
-  a.lp = lp_of(l);
-  a.out = out;
-  a.err = (int*)scratch(c, "tc_err", sizeof(int));
-  switch (np) {
-    case 32: launch_np<32>(c, a); break;
-    case 48: launch_np<48>(c, a); break;
-    case 64: launch_np<64>(c, a); break;
-    case 80: launch_np<80>(c, a); break;
-    case 96: launch_np<96>(c, a); break;
-    case 112: launch_np<112>(c, a); break;
-    case 128: launch_np<128>(c, a); break;
-    case 144: launch_np<144>(c, a); break;
-    case 160: launch_np<160>(c, a); break;
-    case 176: launch_np<176>(c, a); break;
-    default: launch_np<192>(c, a); break;
-  }
-  c->launches++;
-  c->gemm_launches++;
+  auto launch = [&](int v) {
+    const I8Plan p = make_plan(c, rows, K, np, v);
+    I8Args a;
+    a.a_tiles = a_tiles;
+    a.bq = bq;
+    a.sig = sig;
+    a.a_stride = a_stride;
+    a.cpw = cpw;
+    a.win_bytes = win_bytes;
+    a.rows = rows;
+    a.chunks = p.chunks;
+    a.upp = p.upp;
+    a.units = p.units;
+    a.grid = p.grid;
+    a.ks = ks;
+    a.l = l;
+    a.lp = lp_of(l);
+    a.out = out;
+    a.err = (int*)scratch(c, "tc_err", sizeof(int));
+    switch (np) {
+      case 32: launch_v<32>(c, a, v); break;
+      case 48: launch_v<48>(c, a, v); break;
+      case 64: launch_v<64>(c, a, v); break;
+      case 80: launch_v<80>(c, a, v); break;
+      case 96: launch_v<96>(c, a, v); break;
+      case 112: launch_v<112>(c, a, v); break;
+      case 128: launch_v<128>(c, a, v); break;
+      case 144: launch_v<144>(c, a, v); break;
+      case 160: launch_v<160>(c, a, v); break;
+      case 176: launch_v<176>(c, a, v); break;
+      default: launch_v<192>(c, a, v); break;
+    }
+    c->launches++;
+    c->gemm_launches++;
+  };
+  launch(tune_variant(c, {np, rows, K, cpw, win_bytes}, variants_of(np), launch));
 }
 
 // Tiled copies of the codes for the current window layout: "i8_tile1" (per window: SNP
@@ -607,7 +670,7 @@ void quantize(pcaone_ctx* c, const T* X, int64_t K, int l, int64_t kpad, const c
   c->launches++;
 }
 
-int i8_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int l) { return make_plan(c, rows, K, np_of(l)).ks; }
+int i8_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int l) { return ks_all(c, rows, K, np_of(l)); }
 
 void i8_omega(pcaone_ctx* c, const double* omega, int l, int64_t npad) {
   quantize<double>(c, omega, (int64_t)c->N, l, npad, "1", false);
@@ -661,8 +724,8 @@ int64_t i8_seg_k2(pcaone_ctx* c) { return tile_geom(c).c2 * kChunk; }
 
 int i8_ksplit_seg(pcaone_ctx* c, int which, int nw, int l) {
   const TileGeom g = tile_geom(c);
-  return which == 1 ? make_plan(c, (int64_t)nw * g.p1 * 2 * kRows, (int64_t)c->N, np_of(l)).ks
-                    : make_plan(c, (int64_t)c->N, (int64_t)nw * g.c2 * kChunk, np_of(l)).ks;
+  return which == 1 ? ks_all(c, (int64_t)nw * g.p1 * 2 * kRows, (int64_t)c->N, np_of(l))
+                    : ks_all(c, (int64_t)c->N, (int64_t)nw * g.c2 * kChunk, np_of(l));
 }
 
 void i8_p1_seg(pcaone_ctx* c, int b0, int b1, int l, int ks, float* out) {

@@ -855,6 +855,19 @@ def run_profile_kernel(args, cfg):
     prefix = os.path.join(workdir(), args.config)
     make_data(cfg, prefix)
     packed, N, M = pb.read_bed(prefix)
+    if cfg["kind"] == "ld":  # one band-Gram launch over the first 60000 SNPs (150 MB packed)
+        m = min(M, 60000)
+        pos, ends = pb.read_bim_positions(prefix + ".bim")
+        ws, we = pb.ld_windows(pos[:m], [e for e in ends if e < m - 1] + [m - 1], cfg["ld_bp"])
+        U = np.linalg.qr(np.random.default_rng(1).standard_normal((N, cfg["k"])))[0]
+        with pb.GpuContext(0) as ctx:
+            ctx.load_bed(np.ascontiguousarray(packed[:m]), N)
+            for _ in range(args.steps):
+                r2 = ctx.ld_r2(ws, we, U)
+            t = ctx.ld_timing()
+        print(json.dumps({"profile_kernel": "ld", "samples": N, "snps": m, "pairs": int(r2.size),
+                          "device_ms": t[0], "gram_ms": t[1], "checksum": float(r2.sum())}))
+        return
     l = cfg["k"] + max(10, cfg["k"])
     B = pb.omega(101, N, l)
     with pb.GpuContext(0) as ctx:

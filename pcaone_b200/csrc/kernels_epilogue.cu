@@ -89,31 +89,50 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
 // them. FP64 sums; the row groups are combined in a fixed order (deterministic) into out
 // (shared memory of this warp). The batch is sized so that the kernels keep three CTAs of
 // 256 threads per SM (registers) with 16 rows in flight per warp.
+// With kWeighted, entry e's row is scaled by weight(e, idx_e) (computed by the lane that loads
+// the index and passed along with it).
 constexpr int kSumBatch = 16;
-template <int G>
+template <int G, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
 __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
-                                          const float* __restrict__ rows, int64_t row0, double* out) {
-  constexpr int R = 32 / G, T = (kSumBatch + R - 1) / R;
+                                          const float* __restrict__ rows, int64_t row0, double* out,
+                                          Wt weight = nullptr) {
+  // rows of 36-64 values: batches of 12 rows (4 per lane), which keeps the kernels in budget
+  constexpr int B = G >= 9 ? 12 : kSumBatch, R = 32 / G, T = (B + R - 1) / R;
   const int lane = threadIdx.x & 31, grp = lane / G, cg = lane - grp * G;
   const bool active = grp < R;
   const float4* rows4 = reinterpret_cast<const float4*>(rows);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t base = e0; base < e1; base += kSumBatch) {
-    const int cnt = (int)(e1 - base < kSumBatch ? e1 - base : kSumBatch);
-    const int64_t my = lane < cnt ? (int64_t)idx[base + lane] - row0 : 0;
+  for (int64_t base = e0; base < e1; base += B) {
+    const int cnt = (int)(e1 - base < B ? e1 - base : B);
+    int32_t myi = 0;
+    double myw = 0.0;
+    if (lane < cnt) {
+      myi = idx[base + lane];
+      if constexpr (kWeighted) myw = weight(base + lane, myi);
+    }
+    const int64_t my = (int64_t)myi - row0;
     float4 v[T];
+    double w[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) {
       const int src = grp + R * t;
       const int64_t ii = __shfl_sync(0xffffffffu, my, src & 31);
+      if constexpr (kWeighted) w[t] = __shfl_sync(0xffffffffu, myw, src & 31);
       v[t] = (active && src < cnt) ? __ldg(rows4 + ii * G + cg) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-      acc[0] += (double)v[t].x;
-      acc[1] += (double)v[t].y;
-      acc[2] += (double)v[t].z;
-      acc[3] += (double)v[t].w;
+      if constexpr (kWeighted) {
+        acc[0] = fma(w[t], (double)v[t].x, acc[0]);
+        acc[1] = fma(w[t], (double)v[t].y, acc[1]);
+        acc[2] = fma(w[t], (double)v[t].z, acc[2]);
+        acc[3] = fma(w[t], (double)v[t].w, acc[3]);
+      } else {
+        acc[0] += (double)v[t].x;
+        acc[1] += (double)v[t].y;
+        acc[2] += (double)v[t].z;
+        acc[3] += (double)v[t].w;
+      }
     }
   }
   for (int g = 0; g < R; ++g) {
@@ -126,13 +145,14 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
 
 // out = sum of the rows for l % 4 == 0 and ceil(l / 8) = CPL, i.e. G = l / 4 = 2 CPL - 1 or
 // 2 CPL (the two instantiations a kernel of that CPL can meet).
-template <int CPL>
+template <int CPL, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
 __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
-                                         const float* __restrict__ rows, int64_t row0, int l, double* out) {
+                                         const float* __restrict__ rows, int64_t row0, int l, double* out,
+                                         Wt weight = nullptr) {
   if ((l >> 2) == 2 * CPL)
-    sum_rows4<2 * CPL>(e0, e1, idx, rows, row0, out);
+    sum_rows4<2 * CPL, kWeighted>(e0, e1, idx, rows, row0, out, weight);
   else
-    sum_rows4<(2 * CPL - 1 > 0 ? 2 * CPL - 1 : 1)>(e0, e1, idx, rows, row0, out);
+    sum_rows4<(2 * CPL - 1 > 0 ? 2 * CPL - 1 : 1), kWeighted>(e0, e1, idx, rows, row0, out, weight);
 }
 
 // Warp per SNP of the window. Writes G (global rows), B2 (window-local rows, type T) and
@@ -141,8 +161,12 @@ __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* 
 // column maxima of |B2| the int8 quantiser needs. The sparse gather reads the FP32 copy of
 // Omega when p.omega_f is set (half the L2 bytes of the FP64 rows); without imputed values
 // its weight is F_j for every entry, so it sums the rows unweighted (sum_rows, l % 4 == 0).
-template <typename T, int CPL>
-__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
+// kMode picks the sparse gather at compile time, so that each form keeps its own register
+// budget: 0 = the generic 8-lane-group gather (any l, FP64 or FP32 rows; weighted when
+// imputed values are set), 1 = unweighted float4 row sums (no imputed values, FP32 rows,
+// l % 4 == 0), 2 = weighted float4 row sums (imputed values, FP32 rows, l % 4 == 0).
+template <typename T, int CPL, int kMode>
+__global__ void __launch_bounds__(256, (CPL <= 5 && kMode != 2) || CPL <= 3 ? 3 : 2) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
   extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -163,9 +187,11 @@ __global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_prep(EpiP1 p, const T
     const int64_t e0 = p.miss_ptr[j], e1 = p.miss_ptr[j + 1];
     const double* mv = p.miss_val;
     auto w = [&](int64_t e, int) { return (mv ? mv[e] : 0.0) + F; };
-    const bool plain = !mv && p.omega_f && (p.l & 3) == 0;
-    if (plain)
+    constexpr bool plain = kMode == 1;
+    if constexpr (kMode == 1)
       sum_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp);
+    else if constexpr (kMode == 2)
+      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp, w);
     else if (p.omega_f)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, w, ssp);
     else
@@ -265,8 +291,8 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __res
 
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse, the sparse term over the sample's
 // missing entries in the windows [b0, b1).
-template <typename T, int CPL>
-__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const T* __restrict__ D2) {
+template <typename T, int CPL, int kMode>
+__global__ void __launch_bounds__(256, (CPL <= 5 && kMode != 2) || CPL <= 3 ? 3 : 2) k_accum(EpiP2 p, const T* __restrict__ D2) {
   extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = ssm + warp * p.l;
@@ -275,8 +301,10 @@ __global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const 
     const double* mv = p.miss_val;
     const double *sc = p.scale, *F = p.F;
     auto w = [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); };
-    if (p.Gf && !mv && (p.l & 3) == 0)  // Gf holds s F G: the sparse term is a plain row sum
+    if constexpr (kMode == 1)  // Gf holds s F G: the sparse term is a plain row sum
       sum_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp);
+    else if constexpr (kMode == 2)
+      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp, w);
     else if (p.Gf && !mv)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, [](int64_t, int) { return 1.0; }, ssp);
     else if (p.Gf)
@@ -310,6 +338,7 @@ template <typename T>
 void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) {
   const int threads = 256, nwarps = threads / 32;
   const size_t smem = (size_t)2 * nwarps * p.l * 8 + (size_t)p.l * 8;
+  const int mode = (p.omega_f && (p.l & 3) == 0) ? (p.miss_val ? 2 : 1) : 0;
   auto go = [&](auto kern) {
     const int per_sm = resident_ctas((const void*)kern, threads, smem);
     const int nblk = (int)std::min<int64_t>((int64_t)per_sm * c->sm_count,
@@ -320,14 +349,14 @@ void launch_prep(pcaone_ctx* c, const EpiP1& p, const T* D1, T* B2, double* h0) 
     k_reduce_cols<<<p.l, kRedThreads, 0, c->stream>>>(part, nblk, p.l, h0);
   };
   switch ((p.l + 7) / 8) {
-    case 1: go(k_prep<T, 1>); break;
-    case 2: go(k_prep<T, 2>); break;
-    case 3: go(k_prep<T, 3>); break;
-    case 4: go(k_prep<T, 4>); break;
-    case 5: go(k_prep<T, 5>); break;
-    case 6: go(k_prep<T, 6>); break;
-    case 7: go(k_prep<T, 7>); break;
-    default: go(k_prep<T, 8>); break;
+    case 1: mode == 1 ? go(k_prep<T, 1, 1>) : mode == 2 ? go(k_prep<T, 1, 2>) : go(k_prep<T, 1, 0>); break;
+    case 2: mode == 1 ? go(k_prep<T, 2, 1>) : mode == 2 ? go(k_prep<T, 2, 2>) : go(k_prep<T, 2, 0>); break;
+    case 3: mode == 1 ? go(k_prep<T, 3, 1>) : mode == 2 ? go(k_prep<T, 3, 2>) : go(k_prep<T, 3, 0>); break;
+    case 4: mode == 1 ? go(k_prep<T, 4, 1>) : mode == 2 ? go(k_prep<T, 4, 2>) : go(k_prep<T, 4, 0>); break;
+    case 5: mode == 1 ? go(k_prep<T, 5, 1>) : mode == 2 ? go(k_prep<T, 5, 2>) : go(k_prep<T, 5, 0>); break;
+    case 6: mode == 1 ? go(k_prep<T, 6, 1>) : mode == 2 ? go(k_prep<T, 6, 2>) : go(k_prep<T, 6, 0>); break;
+    case 7: mode == 1 ? go(k_prep<T, 7, 1>) : mode == 2 ? go(k_prep<T, 7, 2>) : go(k_prep<T, 7, 0>); break;
+    default: mode == 1 ? go(k_prep<T, 8, 1>) : mode == 2 ? go(k_prep<T, 8, 2>) : go(k_prep<T, 8, 0>); break;
   }
   PG_CHECK_LAUNCH();
   c->launches += 2;
@@ -337,20 +366,21 @@ template <typename T>
 void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
   const int threads = 256, nwarps = threads / 32;
   const size_t smem = (size_t)nwarps * p.l * 8;
+  const int mode = (p.Gf && (p.l & 3) == 0) ? (p.miss_val ? 2 : 1) : 0;
   auto go = [&](auto kern) {
     const int per_sm = resident_ctas((const void*)kern, threads, smem);
     const int nblk = (int)std::min<int64_t>((int64_t)per_sm * c->sm_count, (p.n + nwarps - 1) / nwarps);
     kern<<<nblk, threads, smem, c->stream>>>(p, D2);
   };
   switch ((p.l + 7) / 8) {
-    case 1: go(k_accum<T, 1>); break;
-    case 2: go(k_accum<T, 2>); break;
-    case 3: go(k_accum<T, 3>); break;
-    case 4: go(k_accum<T, 4>); break;
-    case 5: go(k_accum<T, 5>); break;
-    case 6: go(k_accum<T, 6>); break;
-    case 7: go(k_accum<T, 7>); break;
-    default: go(k_accum<T, 8>); break;
+    case 1: mode == 1 ? go(k_accum<T, 1, 1>) : mode == 2 ? go(k_accum<T, 1, 2>) : go(k_accum<T, 1, 0>); break;
+    case 2: mode == 1 ? go(k_accum<T, 2, 1>) : mode == 2 ? go(k_accum<T, 2, 2>) : go(k_accum<T, 2, 0>); break;
+    case 3: mode == 1 ? go(k_accum<T, 3, 1>) : mode == 2 ? go(k_accum<T, 3, 2>) : go(k_accum<T, 3, 0>); break;
+    case 4: mode == 1 ? go(k_accum<T, 4, 1>) : mode == 2 ? go(k_accum<T, 4, 2>) : go(k_accum<T, 4, 0>); break;
+    case 5: mode == 1 ? go(k_accum<T, 5, 1>) : mode == 2 ? go(k_accum<T, 5, 2>) : go(k_accum<T, 5, 0>); break;
+    case 6: mode == 1 ? go(k_accum<T, 6, 1>) : mode == 2 ? go(k_accum<T, 6, 2>) : go(k_accum<T, 6, 0>); break;
+    case 7: mode == 1 ? go(k_accum<T, 7, 1>) : mode == 2 ? go(k_accum<T, 7, 2>) : go(k_accum<T, 7, 0>); break;
+    default: mode == 1 ? go(k_accum<T, 8, 1>) : mode == 2 ? go(k_accum<T, 8, 2>) : go(k_accum<T, 8, 0>); break;
   }
   PG_CHECK_LAUNCH();
   c->launches++;

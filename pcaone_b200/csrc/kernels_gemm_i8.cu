@@ -728,7 +728,7 @@ int i8_ksplit_seg(pcaone_ctx* c, int which, int nw, int l) {
                     : ks_all(c, (int64_t)c->N, (int64_t)nw * g.c2 * kChunk, np_of(l));
 }
 
-void i8_p1_seg(pcaone_ctx* c, int b0, int b1, int l, int ks, float* out) {
+void i8_p1_seg(pcaone_ctx* c, int b0, int b1, const float*, int l, int ks, float* out) {
   ensure_tiles(c);
   const TileGeom g = tile_geom(c);
   PG_REQUIRE(b0 >= 0 && b0 < b1 && b1 <= c->win.bands, PCAONE_EBADARG, "bad window run");
@@ -748,7 +748,7 @@ void i8_b2_seg(pcaone_ctx* c, const float* B2, int l, int b0, int b1) {
   c->i8_b2_max_ready = false;
 }
 
-void i8_p2_seg(pcaone_ctx* c, int b0, int b1, int l, int ks, float* out) {
+void i8_p2_seg(pcaone_ctx* c, int b0, int b1, const float*, int l, int ks, float* out) {
   ensure_tiles(c);
   const TileGeom g = tile_geom(c);
   PG_REQUIRE(b0 >= 0 && b0 < b1 && b1 <= c->win.bands, PCAONE_EBADARG, "bad window run");

@@ -228,6 +228,22 @@ void dense_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t r
               int l, int ks, float* out) {
   launch_dense<true>(c, c->d_E + c->win.start[window] * (uint64_t)c->Npad, c->Npad, rows, K, B, l, ks, out);
 }
+// Window runs on the dense matrix: a run's windows are contiguous rows of E (blocksize each,
+// the last one shorter), so both products are plain products over the run's rows.
+int64_t dense_seg_rows(pcaone_ctx* c) { return (int64_t)c->win.blocksize; }
+int dense_ksplit_seg(pcaone_ctx* c, int which, int nw, int l) {
+  const int64_t m = (int64_t)nw * (int64_t)c->win.blocksize;
+  return which == 1 ? dense_ksplit(c, m, (int64_t)c->N, l) : dense_ksplit(c, (int64_t)c->N, m, l);
+}
+void dense_p1_seg(pcaone_ctx* c, int b0, int b1, const float* B, int l, int ks, float* out) {
+  const int64_t s = (int64_t)c->win.start[b0], m = (int64_t)c->win.stop[b1 - 1] - s;
+  launch_dense<false>(c, c->d_E + (uint64_t)s * c->Npad, c->Npad, m, (int64_t)c->N, B, l, ks, out);
+}
+void dense_p2_seg(pcaone_ctx* c, int b0, int b1, const float* B2, int l, int ks, float* out) {
+  const int64_t s = (int64_t)c->win.start[b0], m = (int64_t)c->win.stop[b1 - 1] - s;
+  launch_dense<true>(c, c->d_E + (uint64_t)s * c->Npad, c->Npad, (int64_t)c->N, m, B2, l, ks, out);
+}
+void dense_seg_b2(pcaone_ctx*, const float*, int, int, int) {}
 void dense_none_omega(pcaone_ctx*, const double*, int, int64_t) {}
 void dense_none_b2(pcaone_ctx*, const float*, int, int64_t) {}
 
@@ -294,7 +310,14 @@ __global__ void k_grm_finish(const double* __restrict__ L, const double* __restr
 }  // namespace
 
 GemmFnT<float> gemm_dense_float() {
-  return GemmFnT<float>{dense_ksplit, dense_p1, dense_p2, dense_none_omega, dense_none_b2};
+  GemmFnT<float> f{dense_ksplit, dense_p1, dense_p2, dense_none_omega, dense_none_b2};
+  f.seg_rows1 = dense_seg_rows;
+  f.seg_k2 = dense_seg_rows;
+  f.ksplit_seg = dense_ksplit_seg;
+  f.p1_seg = dense_p1_seg;
+  f.b2_seg = dense_seg_b2;
+  f.p2_seg = dense_p2_seg;
+  return f;
 }
 
 void gl_from_bed(pcaone_ctx* c) {

@@ -276,8 +276,11 @@ struct Engine {
     const int nw = b1 - b0;
     const int64_t rows1 = gemm.seg_rows1(c), k2 = gemm.seg_k2(c);
     const int ks1 = gemm.ksplit_seg(c, 1, nw, l);
-    T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * nw * rows1 * l * sizeof(T));
-    timed([&] { gemm.p1_seg(c, b0, b1, l, ks1, D1); });
+    // D1 rows per split: the padded windows of the back end, or exactly the run's SNPs for the
+    // dense matrix (whose windows are contiguous rows without padding)
+    const int64_t d1rows = c->dense ? m : nw * rows1;
+    T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * std::max<int64_t>(d1rows, nw * rows1) * l * sizeof(T));
+    timed([&] { gemm.p1_seg(c, b0, b1, OmgT, l, ks1, D1); });
     EpiP1 p1;
     p1.start = s;
     p1.m = m;
@@ -286,7 +289,7 @@ struct Engine {
     p1.wlen = (int64_t)c->win.blocksize;
     p1.d1_ws = rows1;
     p1.b2_ws = k2;
-    p1.d1_rows = nw * rows1;
+    p1.d1_rows = d1rows;
     p1.F = Fcent;
     p1.scale = c->d_scale;
     p1.wsum = wsum;
@@ -298,7 +301,7 @@ struct Engine {
     p1.G = G;
     T* B2 = (T*)scratch(c, "r_B2", (size_t)nw * k2 * l * sizeof(T));
     double* h0 = (double*)scratch(c, "r_h0", l * 8);
-    p1.qmax = gemm.b2_qmax(c, l);
+    p1.qmax = gemm.b2_qmax ? gemm.b2_qmax(c, l) : nullptr;
     float* Gf = (float*)scratch(c, "r_Gf", (size_t)round_up(m, 256) * l * sizeof(float));
     p1.Gf = Gf;
     timed([&] {
@@ -307,7 +310,7 @@ struct Engine {
     }, 1);
     const int ks2 = gemm.ksplit_seg(c, 2, nw, l);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
-    timed([&] { gemm.p2_seg(c, b0, b1, l, ks2, D2); });
+    timed([&] { gemm.p2_seg(c, b0, b1, B2, l, ks2, D2); });
     EpiP2 p2;
     p2.b0 = b0;
     p2.b1 = b1;
@@ -333,7 +336,7 @@ struct Engine {
   // when the back end batches windows, else one window at a time.
   static constexpr int64_t kRunRows = int64_t(1) << 22;
   void process_windows(int b0, int b1, double* Ht) {
-    if (!gemm.p1_seg || c->dense) {
+    if (!gemm.p1_seg) {
       for (int b = b0; b < b1; ++b) process_window(b, Ht);
       return;
     }

@@ -35,9 +35,11 @@ struct GemmFnT {
   int64_t (*seg_rows1)(pcaone_ctx* c) = nullptr;
   int64_t (*seg_k2)(pcaone_ctx* c) = nullptr;
   int (*ksplit_seg)(pcaone_ctx* c, int which, int nw, int l) = nullptr;
-  void (*p1_seg)(pcaone_ctx* c, int b0, int b1, int l, int ks, T* out) = nullptr;
+  // B: the first product's operand (Omega, engine layout) / the run's B2 (seg_k2 rows per
+  // window); back ends that keep their own packed copy ignore it.
+  void (*p1_seg)(pcaone_ctx* c, int b0, int b1, const T* B, int l, int ks, T* out) = nullptr;
   void (*b2_seg)(pcaone_ctx* c, const T* B2, int l, int b0, int b1) = nullptr;
-  void (*p2_seg)(pcaone_ctx* c, int b0, int b1, int l, int ks, T* out) = nullptr;
+  void (*p2_seg)(pcaone_ctx* c, int b0, int b1, const T* B2, int l, int ks, T* out) = nullptr;
 };
 
 GemmFnT<float> gemm_simt_float();

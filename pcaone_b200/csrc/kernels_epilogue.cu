@@ -96,8 +96,11 @@ template <int G, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
 __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                           const float* __restrict__ rows, int64_t row0, double* out,
                                           Wt weight = nullptr) {
-  // rows of 36-64 values: batches of 12 rows (4 per lane), which keeps the kernels in budget
-  constexpr int B = G >= 9 ? 12 : kSumBatch, R = 32 / G, T = (B + R - 1) / R;
+  // batch size by row width, so that the kernels stay within three CTAs an SM without
+  // spilling: rows of up to 20 values take 24 entries a batch (18 weighted), 24-32 values 16
+  // (12), 36-64 values 12 (9)
+  constexpr int B = G >= 9 ? (kWeighted ? 9 : 12) : G >= 6 ? (kWeighted ? 12 : kSumBatch) : (kWeighted ? 18 : 24),
+                R = 32 / G, T = (B + R - 1) / R;
   const int lane = threadIdx.x & 31, grp = lane / G, cg = lane - grp * G;
   const bool active = grp < R;
   const float4* rows4 = reinterpret_cast<const float4*>(rows);
@@ -114,11 +117,14 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
     float4 v[T];
     double w[T];
 #pragma unroll
-    for (int t = 0; t < T; ++t) {
+    for (int t = 0; t < T; ++t) {  // every row load of the batch first
       const int src = grp + R * t;
       const int64_t ii = __shfl_sync(0xffffffffu, my, src & 31);
-      if constexpr (kWeighted) w[t] = __shfl_sync(0xffffffffu, myw, src & 31);
       v[t] = (active && src < cnt) ? __ldg(rows4 + ii * G + cg) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if constexpr (kWeighted) {  // then the weights (their loads overlap the rows')
+#pragma unroll
+      for (int t = 0; t < T; ++t) w[t] = __shfl_sync(0xffffffffu, myw, (grp + R * t) & 31);
     }
 #pragma unroll
     for (int t = 0; t < T; ++t) {
@@ -166,7 +172,7 @@ __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* 
 // imputed values are set), 1 = unweighted float4 row sums (no imputed values, FP32 rows,
 // l % 4 == 0), 2 = weighted float4 row sums (imputed values, FP32 rows, l % 4 == 0).
 template <typename T, int CPL, int kMode>
-__global__ void __launch_bounds__(256, (CPL <= 5 && kMode != 2) || CPL <= 3 ? 3 : 2) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
+__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_prep(EpiP1 p, const T* __restrict__ D1, T* __restrict__ B2,
                        double* __restrict__ h0_part) {
   extern __shared__ double sh0[];  // warps x l partial h0, then warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_cols(const double* __res
 // Warp per sample: H[i] += sum_split D2 - h0 + sparse, the sparse term over the sample's
 // missing entries in the windows [b0, b1).
 template <typename T, int CPL, int kMode>
-__global__ void __launch_bounds__(256, (CPL <= 5 && kMode != 2) || CPL <= 3 ? 3 : 2) k_accum(EpiP2 p, const T* __restrict__ D2) {
+__global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const T* __restrict__ D2) {
   extern __shared__ double ssm[];  // warps x l sparse sums
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double* ssp = ssm + warp * p.l;

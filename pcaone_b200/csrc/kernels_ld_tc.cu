@@ -56,8 +56,8 @@ constexpr int kTile = 128;                     // SNPs per tile
 constexpr int kChunk = 128;                    // samples per K chunk
 constexpr int kRawTile = kTile * kChunk / 4;   // packed bytes of one tile chunk: 4096
 constexpr int kImg = kTile * kChunk;           // one decoded operand image (r or n): 16384
-constexpr int kRS = 4;                         // raw stages (codes of both tiles)
-constexpr int kDS = 2;                         // decoded stages (r_I, n_I, r_K, n_K)
+constexpr int kRS = 2;                         // raw stages (codes of both tiles)
+constexpr int kDS = 3;                         // decoded stages (r_I, n_I, r_K, n_K)
 constexpr int kStageD = 4 * kImg;              // 65536
 constexpr int kThreads = 448;
 constexpr int kTmemCols = 512;
@@ -90,7 +90,7 @@ struct LdArgs {
   int ntiles, nchunks;
   uint64_t M;
   const double* F;         // M
-  const double* d;         // M, |G_i|^2 of the residualised columns
+  const double* isd;       // M, 1 / |G_i| of the residualised columns (inf / NaN kept: r is NaN then)
   const double* W;         // M x k row-major, or null
   const double* Y;         // M x k row-major, or null
   int k;
@@ -234,14 +234,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_ld_gram_i8(const __grid_constan
       const int2 tk = a.list[(int)blockIdx.x + tt * (int)gridDim.x];
       const uint64_t i = (uint64_t)tk.x * kTile + rw, k0 = (uint64_t)tk.y * kTile;
       int64_t w = -1;
-      double Fi = 0.0, di = 1.0;
+      double Fi = 0.0, isdi = 1.0;
       double wi[kMaxProj];
 #pragma unroll
       for (int t = 0; t < kMaxProj; ++t) wi[t] = 0.0;
       if (i < a.M) {
         w = a.win_of[i];
         Fi = a.F[i];
-        di = a.d[i];
+        isdi = a.isd[i];
         if (a.W)
 #pragma unroll
           for (int t = 0; t < kMaxProj; ++t)
@@ -268,13 +268,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_ld_gram_i8(const __grid_constan
         tc::tmem_ld8(tmem + lane_base + 256 + c0, nr);
         tc::tmem_ld8(tmem + lane_base + 384 + c0, nn);
         tc::tmem_wait_ld();
+        // the chunk's partner values, the same for every lane (broadcast loads)
+        double Fk8[8], isk8[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const uint64_t kk = k0 + c0 + j;
+          Fk8[j] = kk < a.M ? __ldg(a.F + kk) : 0.0;
+          isk8[j] = kk < a.M ? __ldg(a.isd + kk) : 0.0;
+        }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int col = c0 + j;
           if (col < clo || col > chi) continue;
           const uint64_t kk = k0 + col;
           if (kk >= a.M) continue;
-          const double Fk = a.F[kk];
+          const double Fk = Fk8[j];
           double num = 0.25 * ((double)(int)rr[j] - 2.0 * Fk * (double)(int)rn[j] - 2.0 * Fi * (double)(int)nr[j]) +
                        Fi * Fk * (double)(int)nn[j];
           if (a.W) {  // the lanes of a warp read the same partner row: broadcast loads
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_ld_gram_i8(const __grid_constan
             for (int t = 0; t < kMaxProj; ++t)
               if (t < k) num -= wi[t] * __ldg(yk + t);
           }
-          const double rv = num / sqrt(di * a.d[kk]);
+          const double rv = num * isdi * isk8[j];
           const int64_t o = base_out + (int64_t)(kk - i) - 1;
           if (a.f64)
             ((double*)a.r2)[o] = rv * rv;
@@ -341,11 +349,12 @@ __global__ void k_ld_tile_codes(const uint8_t* __restrict__ bed, uint32_t pitch,
 
 constexpr size_t ld_smem_bytes() { return 1024 + (size_t)kDS * kStageD + (size_t)kRS * 2 * kRawTile + 16 * 8; }
 
-// Warp per SNP: d_i = |G_i|^2 of the residualised column from the code counts of its first
-// N samples (RR = 4 n00 + n10, RN = NR = 2 n00 + n10, NN = non-missing) minus W_i . Y_i.
+// Warp per SNP: 1 / |G_i| with |G_i|^2 = d_i of the residualised column from the code counts
+// of its first N samples (RR = 4 n00 + n10, RN = NR = 2 n00 + n10, NN = non-missing) minus
+// W_i . Y_i; a zero or negative d_i gives inf or NaN, so r is NaN as the reference's 0 / 0.
 __global__ void k_ld_diag_codes(const uint8_t* __restrict__ bed, uint32_t pitch, uint64_t M, uint32_t N,
                                 const double* __restrict__ F, const double* __restrict__ W,
-                                const double* __restrict__ Y, int k, double* __restrict__ d) {
+                                const double* __restrict__ Y, int k, double* __restrict__ isd) {
   const uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (i >= M) return;
@@ -372,7 +381,8 @@ __global__ void k_ld_diag_codes(const uint8_t* __restrict__ bed, uint32_t pitch,
   }
   if (lane == 0) {
     const double f = F[i], rr = (double)(4 * n00 + n10), rn = (double)(2 * n00 + n10);
-    d[i] = 0.25 * (rr - 4.0 * f * rn) + f * f * (double)nm - wy;
+    const double d = 0.25 * (rr - 4.0 * f * rn) + f * f * (double)nm - wy;
+    isd[i] = 1.0 / sqrt(d);
   }
 }
 
@@ -393,9 +403,9 @@ void ld_r2_tc(pcaone_ctx* c, const double* W, const double* Y, int k, const int6
     }
   } guard{ev};
   PG_CUDA(cudaEventRecord(ev[0], c->stream));
-  double* d = (double*)scratch(c, "ld_diag", M * 8);
+  double* isd = (double*)scratch(c, "ld_isd", M * 8);
   k_ld_diag_codes<<<(unsigned)((M * 32 + 255) / 256), 256, 0, c->stream>>>(c->d_bed, c->pitch, M, c->N, c->d_F,
-                                                                           k > 0 ? W : nullptr, Y, k, d);
+                                                                           k > 0 ? W : nullptr, Y, k, isd);
   PG_CHECK_LAUNCH();
   c->launches++;
   const int64_t ntile = (int64_t)((M + kTile - 1) / kTile);
@@ -433,7 +443,7 @@ void ld_r2_tc(pcaone_ctx* c, const double* W, const double* Y, int k, const int6
   a.nchunks = nchunks;
   a.M = M;
   a.F = c->d_F;
-  a.d = d;
+  a.isd = isd;
   a.W = k > 0 ? W : nullptr;
   a.Y = k > 0 ? Y : nullptr;
   a.k = k;

@@ -364,7 +364,7 @@ def tensor_roofline(prec, l, alg_flops, prof):
             "gemm_share_of_step": round(prof.gemm_ms / prof.gpu_ms, 4),
             "step_breakdown_ms": {"gemm": round(prof.gemm_ms, 2), "epilogues": round(prof.epilogue_ms, 2),
                                   "omega_updates": round(prof.update_ms, 2), "epoch_tail": round(prof.tail_ms, 2),
-                                  "total": round(prof.gpu_ms, 2)}}
+                                  "waiting_for_host": round(prof.host_ms, 2), "total": round(prof.gpu_ms, 2)}}
 
 
 def subspace_err(Ua, Sa, Ub, Sb, k=None):

@@ -127,6 +127,8 @@ typedef struct {
   double epilogue_ms;    /* with opts.profile: centring/sparse epilogues and B-operand packing */
   double update_ms;      /* with opts.profile: Omega re-orthonormalisations (QR, signs, flip) */
   double tail_ms;        /* with opts.profile: per-epoch QR of G, B, small SVD, mev */
+  double host_ms;        /* with opts.profile: device idle while the host runs the epoch tail's
+                            small SVD and convergence test */
 } pcaone_rsvd_report;
 
 /* Run Halko (svd=1) or window-based (svd=2) RSVD on the loaded genotypes: the epoch loop of

@@ -56,7 +56,8 @@ class RsvdReport(ctypes.Structure):
                 ("last_diff", ctypes.c_double), ("gpu_ms", ctypes.c_double),
                 ("gemm_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64),
                 ("gemm_launches", ctypes.c_int64), ("epilogue_ms", ctypes.c_double),
-                ("update_ms", ctypes.c_double), ("tail_ms", ctypes.c_double)]
+                ("update_ms", ctypes.c_double), ("tail_ms", ctypes.c_double),
+                ("host_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -166,6 +167,7 @@ class RsvdResult:
     epilogue_ms: float = 0.0
     update_ms: float = 0.0
     tail_ms: float = 0.0
+    host_ms: float = 0.0
 
 
 class GpuContext:
@@ -244,7 +246,7 @@ class GpuContext:
         return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
                           rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
                           rep.kernel_launches, rep.gemm_launches, rep.epilogue_ms,
-                          rep.update_ms, rep.tail_ms)
+                          rep.update_ms, rep.tail_ms, rep.host_ms)
 
 
 def _product(ctx: "GpuContext", B: np.ndarray, transpose: int, precision, standardize, ploidy):

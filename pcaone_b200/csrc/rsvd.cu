@@ -541,7 +541,20 @@ struct Engine {
     double diff = 0.0;
     int epochs = 0;
     bool done = false;
+    // with opts.profile: event pairs around the stretches in which the device waits for the
+    // host (the small SVD, and the convergence test up to the next epoch's first launch)
+    std::vector<cudaEvent_t> gap_ev;
+    bool gap_open = false;
+    auto gap_mark = [&](bool begin) {
+      if (!o.profile || gap_open == begin) return;
+      cudaEvent_t e;
+      PG_CUDA(cudaEventCreate(&e));
+      PG_CUDA(cudaEventRecord(e, c->stream));
+      gap_ev.push_back(e);
+      gap_open = begin;
+    };
     for (int pi = 0; pi <= p && !done; ++pi) {
+      gap_mark(false);  // the previous epoch's host decisions end here
       run_epoch(pi);
       // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B)
       timed([&] {
@@ -549,16 +562,19 @@ struct Engine {
         trsm_right_upper(c, H, Rg, l, N, Tb);
         cholqr2(c, Tb, l, N, Tb, Rb, d_status);
       }, 3);
+      gap_mark(true);
       PG_CUDA(cudaMemcpyAsync(rb.data(), Rb, rb.size() * 8, cudaMemcpyDeviceToHost, c->stream));
       check_status();
       collect_times();
       jacobi_svd(l, rb.data(), ur.data(), sv.data(), vr.data());
+      gap_mark(false);
       // Ucur = Qb Ur[:, :k]
       PG_CUDA(cudaMemcpyAsync(Ck, ur.data(), ur.size() * 8, cudaMemcpyHostToDevice, c->stream));
       rowmat(c, Tb, l, Ck, l, k, N, Ucur);
       epochs = pi + 1;
       if (pi > 0) {
         cross(c, Ucur, k, Upre, k, N, Ck);
+        gap_mark(true);
         PG_CUDA(cudaMemcpyAsync(ck.data(), Ck, ck.size() * 8, cudaMemcpyDeviceToHost, c->stream));
         PG_CUDA(cudaStreamSynchronize(c->stream));
         double acc = 0.0;  // mev (src/Utils.cpp:192-198)
@@ -610,7 +626,18 @@ struct Engine {
       rep->epilogue_ms = cat_ms[1];
       rep->update_ms = cat_ms[2];
       rep->tail_ms = cat_ms[3];
+      rep->host_ms = 0.0;
+      gap_mark(false);
+      if (!gap_ev.empty()) {
+        PG_CUDA(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i + 1 < gap_ev.size(); i += 2) {  // (begin, end) pairs
+          float ms = 0.f;
+          PG_CUDA(cudaEventElapsedTime(&ms, gap_ev[i], gap_ev[i + 1]));
+          rep->host_ms += ms;
+        }
+      }
     }
+    for (auto e : gap_ev) cudaEventDestroy(e);
   }
 };
 

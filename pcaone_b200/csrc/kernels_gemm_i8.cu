@@ -77,16 +77,19 @@ __host__ __device__ constexpr int lp_of(int l) { return (l + 7) / 8 * 8; }
 __host__ __device__ constexpr int np_of(int l) { return (3 * lp_of(l) + 15) / 16 * 16; }
 
 // Pipeline shape of variant V (chosen per product shape by the autotuner in run_i8):
-// V = 0: units of two K chunks, two units in flight in tensor memory per tile; V = 1: units
-// of one chunk, four in flight (finer stream-K split, half the MMAs per commit). Wide
-// sketches (NP > 128) have room for one variant only.
+// bit 0 clear: units of two K chunks, two units in flight in tensor memory per tile; set:
+// units of one chunk, four in flight (finer stream-K split, half the MMAs per commit). Wide
+// sketches (NP > 128) take one-chunk units only. Bit 1 (AG): the decoders load the packed
+// codes straight from global memory, one unit ahead in registers, instead of through the
+// shared-memory ring, which then carries B alone (less shared-memory traffic per MMA).
 template <int NP, int V = 0>
 struct Cfg {
-  static constexpr int UC = (NP <= 128 && V == 0) ? 2 : 1;  // K chunks per unit
-  static constexpr int RA = NP <= 128 ? 4 : 2;              // A slots per tile (one chunk each)
-  static constexpr int NU = RA / UC;                        // units in flight in tensor memory per tile
-  static constexpr int SB = NP * 128;                       // B bytes per chunk
-  static constexpr int STAGE = UC * (kPairChunkBytes + SB);
+  static constexpr bool AG = (V & 2) != 0;
+  static constexpr int UC = (NP <= 128 && (V & 1) == 0) ? 2 : 1;  // K chunks per unit
+  static constexpr int RA = NP <= 128 ? 4 : 2;                    // A slots per tile (one chunk each)
+  static constexpr int NU = RA / UC;  // units in flight in tensor memory per tile
+  static constexpr int SB = NP * 128;  // B bytes per chunk
+  static constexpr int STAGE = UC * ((AG ? 0 : kPairChunkBytes) + SB);
   static constexpr int S = (192 * 1024) / STAGE < 8 ? (192 * 1024) / STAGE : 8;
   static constexpr int ACOL = 2 * NP;
   static_assert(2 * NP + 2 * RA * 32 <= kTmemCols, "tensor memory over-subscribed");
@@ -131,7 +134,7 @@ template <int NP, int V>
 __global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_constant__ I8Args args) {
   using C = Cfg<NP, V>;
   constexpr int S = C::S, UC = C::UC, RA = C::RA, NU = C::NU;
-  constexpr uint32_t kStageA = UC * kPairChunkBytes, kStageB = UC * C::SB;
+  constexpr uint32_t kStageA = C::AG ? 0 : UC * kPairChunkBytes, kStageB = UC * C::SB;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sB = smem;                      // S x kStageB (1024-byte aligned swizzle atoms)
@@ -179,6 +182,60 @@ __global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_con
     const int t = warp >> 2, q = warp & 3, r = q * 32 + lane;
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     int64_t p = u0 % P;
+    if constexpr (C::AG) {
+      // this row's 32 code bytes of every chunk of unit i, read from global memory
+      auto load = [&](int i, uint4 (&dst)[UC][2]) {
+        const int64_t u = u0 + i, pair = u / P, kc = (u - pair * P) * UC;
+#pragma unroll
+        for (int ch = 0; ch < UC; ++ch) {
+          const int64_t g = kc + ch;
+          if (g < Cn) {
+            const int64_t w = g / args.cpw;
+            const uint8_t* base = args.a_tiles + w * args.win_bytes +
+                                  (pair * args.a_stride + (g - w * args.cpw)) * kPairChunkBytes +
+                                  t * (2 * kHalfBytes) + r * 16;
+            dst[ch][0] = __ldg(reinterpret_cast<const uint4*>(base));
+            dst[ch][1] = __ldg(reinterpret_cast<const uint4*>(base + kHalfBytes));
+          }
+        }
+      };
+      uint4 cur[UC][2], nxt[UC][2];
+      if (n > 0) load(0, cur);
+      for (int i = 0; i < n; ++i) {
+        const int ua = i % NU;
+        const int nch = (int)(Cn - p * UC < UC ? Cn - p * UC : UC);
+        if (i + 1 < n) load(i + 1, nxt);  // in flight while this unit is decoded
+        if (i >= NU) {  // the MMAs of unit i - NU have released this tile's A slots
+          const int j = i - NU;
+          if (!mbar_wait(smem_u32(&empty[j % S]), (j / S) & 1, abort_flag, args.err, 8)) break;
+        }
+        tc::fence_after();
+#pragma unroll
+        for (int ch = 0; ch < UC; ++ch) {
+          if (ch >= nch) break;
+          uint32_t v[32];
+          decode_word_i8(cur[ch][0].x, v + 0);
+          decode_word_i8(cur[ch][0].y, v + 4);
+          decode_word_i8(cur[ch][0].z, v + 8);
+          decode_word_i8(cur[ch][0].w, v + 12);
+          decode_word_i8(cur[ch][1].x, v + 16);
+          decode_word_i8(cur[ch][1].y, v + 20);
+          decode_word_i8(cur[ch][1].z, v + 24);
+          decode_word_i8(cur[ch][1].w, v + 28);
+          tc::tmem_st32(tmem + lane_base + C::ACOL + t * (RA * 32) + (ua * UC + ch) * 32, v);
+        }
+        tc::tmem_wait_st();
+        tc::fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&dec_full[t * NU + ua]));
+#pragma unroll
+        for (int ch = 0; ch < UC; ++ch) {
+          cur[ch][0] = nxt[ch][0];
+          cur[ch][1] = nxt[ch][1];
+        }
+        if (++p == P) p = 0;
+      }
+    } else
     for (int i = 0; i < n; ++i) {
       const int s = i % S, ua = i % NU;
       const int nch = (int)(Cn - p * UC < UC ? Cn - p * UC : UC);
@@ -224,14 +281,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_decode_gemm_i8(const __grid_con
         const uint32_t nch = (uint32_t)(Cn - kc < UC ? Cn - kc : UC);
         const uint32_t bar = smem_u32(&full[s]);
         if (lane == 0) {
-          mbar_arrive_tx(bar, nch * (kPairChunkBytes + C::SB));
-          for (uint32_t ch = 0; ch < nch; ++ch) {  // chunk by chunk: a unit may straddle two windows
-            const int64_t g = kc + ch, w = g / args.cpw;
-            bulk_load(smem_u32(sA + s * kStageA + ch * kPairChunkBytes),
-                      args.a_tiles + w * args.win_bytes + (pair * args.a_stride + (g - w * args.cpw)) * kPairChunkBytes,
-                      kPairChunkBytes, bar);
+          if constexpr (C::AG) {  // B alone: the decoders read the codes from global memory
+            mbar_arrive_tx(bar, nch * C::SB);
+            bulk_load(smem_u32(sB + s * kStageB), args.bq + kc * C::SB, nch * C::SB, bar);
+          } else {
+            mbar_arrive_tx(bar, nch * (kPairChunkBytes + C::SB));
+            for (uint32_t ch = 0; ch < nch; ++ch) {  // chunk by chunk: a unit may straddle two windows
+              const int64_t g = kc + ch, w = g / args.cpw;
+              bulk_load(smem_u32(sA + s * kStageA + ch * kPairChunkBytes),
+                        args.a_tiles + w * args.win_bytes +
+                            (pair * args.a_stride + (g - w * args.cpw)) * kPairChunkBytes,
+                        kPairChunkBytes, bar);
+            }
           }
-        } else {
+        } else if (!C::AG) {
           bulk_load(smem_u32(sB + s * kStageB), args.bq + kc * C::SB, nch * C::SB, bar);
         }
         issued = i + 1;
@@ -452,8 +515,11 @@ constexpr size_t smem_of() {
   return (size_t)1024 + (size_t)C::S * C::STAGE + (size_t)(2 * C::S + 2 * C::NU + 8) * 8 + (3 * 64 + 4 * 32 * 9) * 4;
 }
 
-int uc_of(int np, int v) { return (np <= 128 && v == 0) ? 2 : 1; }
-int variants_of(int np) { return np <= 128 ? 2 : 1; }
+int uc_of(int np, int v) { return (np <= 128 && (v & 1) == 0) ? 2 : 1; }
+// the distinct variants of a sketch width: {0, 1, 2, 3}, or {0, 2} when NP > 128 (one-chunk
+// units only)
+int variants_of(int np) { return np <= 128 ? 4 : 2; }
+int variant_id(int np, int idx) { return np <= 128 ? idx : 2 * idx; }
 
 struct I8Plan {
   int64_t tiles = 0, pairs = 0, chunks = 0, upp = 0, units = 0;
@@ -485,7 +551,7 @@ I8Plan make_plan(const pcaone_ctx* c, int64_t rows, int64_t K, int np, int v) {
 // that uses fewer zero-fills the rest).
 int ks_all(const pcaone_ctx* c, int64_t rows, int64_t K, int np) {
   int ks = 1;
-  for (int v = 0; v < variants_of(np); ++v) ks = std::max(ks, make_plan(c, rows, K, np, v).ks);
+  for (int v = 0; v < variants_of(np); ++v) ks = std::max(ks, make_plan(c, rows, K, np, variant_id(np, v)).ks);
   return ks;
 }
 
@@ -503,7 +569,9 @@ template <int NP>
 void launch_v(pcaone_ctx* c, const I8Args& a, int v) {
   if constexpr (NP <= 128) {
     if (v == 1) return launch_np<NP, 1>(c, a);
+    if (v == 3) return launch_np<NP, 3>(c, a);
   }
+  if (v == 2) return launch_np<NP, 2>(c, a);
   launch_np<NP, 0>(c, a);
 }
 
@@ -526,7 +594,8 @@ int tune_variant(pcaone_ctx* c, const std::array<int64_t, 5>& key, int nvar, F&&
   PG_CUDA(cudaEventCreate(&e1));
   int best = 0;
   float best_ms = 0.f;
-  for (int v = 0; v < nvar; ++v) {
+  for (int idx = 0; idx < nvar; ++idx) {
+    const int v = variant_id((int)key[0], idx);
     launch(v);  // warm-up (first use of the variant)
     float vbest = 0.f;
     for (int rep = 0; rep < 3; ++rep) {  // the fastest of three timed launches
@@ -538,7 +607,7 @@ int tune_variant(pcaone_ctx* c, const std::array<int64_t, 5>& key, int nvar, F&&
       PG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       if (rep == 0 || ms < vbest) vbest = ms;
     }
-    if (v == 0 || vbest < best_ms) {
+    if (idx == 0 || vbest < best_ms) {
       best = v;
       best_ms = vbest;
     }

@@ -45,6 +45,7 @@
 // its tensor memory and returns, and the host reports PCAONE_ETIMEOUT.
 #include <algorithm>
 #include <array>
+#include <cstdlib>
 
 #include "internal.hpp"
 #include "rsvd.hpp"
@@ -581,8 +582,14 @@ void launch_v(pcaone_ctx* c, const I8Args& a, int v) {
 // shape. Every variant writes the same product (to the rounding of the partial sums), so the
 // launches that time them are the product itself. While the stream is being captured into a
 // graph an unknown shape runs variant 0 untimed.
+// PCAONE_I8_VARIANT=v pins variant v (when the sketch width has it) instead, for tests.
 template <typename F>
 int tune_variant(pcaone_ctx* c, const std::array<int64_t, 5>& key, int nvar, F&& launch) {
+  if (const char* pin = std::getenv("PCAONE_I8_VARIANT")) {
+    const int v = std::atoi(pin);
+    for (int idx = 0; idx < nvar; ++idx)
+      if (variant_id((int)key[0], idx) == v) return v;
+  }
   auto it = c->i8_tune.find(key);
   if (it != c->i8_tune.end()) return it->second;
   if (nvar <= 1) return c->i8_tune[key] = 0;

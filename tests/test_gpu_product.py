@@ -34,6 +34,23 @@ def test_products_match_dense(gpu, prec, N, M, l):
     assert rel_col_err(got2, Z @ B2) <= TOL[prec]
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("N,M,l", [(1003, 2500, 40), (2048, 1300, 7), (300, 4100, 64)])
+def test_int8_pipeline_variants_match_dense(gpu, monkeypatch, variant, N, M, l):
+    """Every pipeline variant of the int8 decode-GEMM (the autotuner's choices), pinned one at
+    a time: codes through shared memory or from global memory, one- or two-chunk units (wide
+    sketches, l = 64, have the one-chunk forms 0 and 2 only)."""
+    monkeypatch.setenv("PCAONE_I8_VARIANT", str(variant))
+    bed = random_bed(N, M, seed=N * 3 + l + variant, miss=0.02)
+    Z, F = O.standardized_from_bed(bed)
+    gpu.load_bed(bed.packed, N)
+    rng = np.random.default_rng(l + variant)
+    B1 = rng.standard_normal((N, l))
+    assert rel_col_err(gpu.product_t(B1, precision="mixed"), Z.T @ B1) <= TOL["mixed"]
+    B2 = rng.standard_normal((M, l))
+    assert rel_col_err(gpu.product(B2, precision="mixed"), Z @ B2) <= TOL["mixed"]
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed", "bf16"])
 def test_products_unstandardised_haploid(gpu, prec):
     bed = random_bed(640, 900, seed=3, miss=0.05)

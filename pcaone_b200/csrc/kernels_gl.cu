@@ -57,27 +57,35 @@ __global__ void k_em_maf(const float* __restrict__ P, uint64_t M, uint32_t N, ui
 }
 
 // E_ij = E[g | likelihoods, pt_ij] - 2 F_j for SNP rows (fit_with_pi, src/Data.cpp:249-270);
-// warp per SNP. The standardised E of the GRM stage is k_grm_e.
-// US: N x k (U diag S) row-major, V: M x k row-major (row j = the loading used for SNP j).
-__global__ void k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
-                              const double* __restrict__ F, const double* __restrict__ US,
-                              const double* __restrict__ V, int k, float* __restrict__ E, uint32_t lde) {
+// warp per SNP, lanes over samples (the likelihood pair of a sample read as one float2). The
+// standardised E of the GRM stage is k_grm_e. US: N x k (U diag S) row-major, V: M x k
+// row-major (row j = the loading used for SNP j); KM >= k is a compile-time bound, so the
+// loading stays in registers.
+template <int KM>
+__global__ void __launch_bounds__(256) k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+                                                     const double* __restrict__ F, const double* __restrict__ US,
+                                                     const double* __restrict__ V, int k, float* __restrict__ E,
+                                                     uint32_t lde) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
     const double f = F[j];
-    double v[kLmax];
-    if (V)
-      for (int t = 0; t < k; ++t) v[t] = V[j * k + t];
-    const float* row = P + j * ldp;
+    double v[KM];
+#pragma unroll
+    for (int t = 0; t < KM; ++t) v[t] = (V && t < k) ? V[j * k + t] : 0.0;
+    const float2* row = reinterpret_cast<const float2*>(P + j * ldp);
     for (uint32_t i = lane; i < N; i += 32) {
       double pt = f;
       if (V) {
         double pred = 0.0;
-        for (int t = 0; t < k; ++t) pred += US[(uint64_t)i * k + t] * v[t];
+        const double* us = US + (uint64_t)i * k;
+#pragma unroll
+        for (int t = 0; t < KM; ++t)
+          if (t < k) pred += __ldg(us + t) * v[t];
         pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
       }
+      const float2 gl = __ldg(row + i);
       double p0, p1, p2;
-      posterior(row[2 * i], row[2 * i + 1], pt, p0, p1, p2);
+      posterior(gl.x, gl.y, pt, p0, p1, p2);
       const double s = p0 + p1 + p2;
       E[j * lde + i] = (float)((p1 + 2.0 * p2) / s - 2.0 * f);
     }
@@ -186,6 +194,137 @@ k_dense_gemm(const float* __restrict__ A, uint64_t lda, int64_t rows, int64_t K,
   }
 }
 
+// Register-tiled form for sketch widths l <= 48 (the PCAngsd RSVD: l = k + max(10, k)):
+// CTA = 128 rows x CN columns (CN = l rounded up to 16), 256 threads; thread (ty, tx) owns
+// rows 4 ty .. 4 ty + 3 and columns tx CN/8 .. (tx + 1) CN/8 - 1. K runs in chunks of 32
+// through two shared-memory buffers (k-major A tile, so one 16-byte load gives the thread's
+// four rows); the next chunk's global loads are issued (16 bytes per thread and load) before
+// the current chunk is multiplied. The product is bound by reading A once from HBM.
+template <bool AT, int CN>
+__global__ void __launch_bounds__(256)
+k_dense_gemm2(const float* __restrict__ A, uint64_t lda, int64_t rows, int64_t K, const float* __restrict__ B,
+              int l, int64_t kchunks_per_split, float* __restrict__ out) {
+  constexpr int TR = 128, KC = 32, CW = CN / 8;
+  __shared__ __align__(16) float as[2][KC][TR + 4];
+  __shared__ __align__(16) float bs[2][KC][CN];
+  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+  const int64_t r0 = (int64_t)blockIdx.x * TR;
+  const int64_t kc_total = (K + KC - 1) / KC;
+  const int64_t kc0 = (int64_t)blockIdx.y * kchunks_per_split;
+  const int64_t kc1 = min(kc0 + kchunks_per_split, kc_total);
+  float acc[4][CW];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < CW; ++c) acc[q][c] = 0.f;
+  // global -> registers: A is 4096 floats a chunk (four float4 per thread), B KC x CN
+  float4 ra[4];
+  float rb[(KC * CN + 255) / 256];
+  auto load = [&](int64_t kc) {
+    const int64_t k0 = kc * KC;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + 256 * u;  // float4 index within the tile
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (AT) {  // A[k][r]: 32 k-rows of 128 r, 32 float4 per k-row
+        const int kk = e >> 5, r4 = (e & 31) * 4;
+        const int64_t k = k0 + kk, r = r0 + r4;
+        if (k < K) {
+          const float* src = A + (uint64_t)k * lda + r;
+          if (r + 3 < rows && ((uintptr_t)src & 15) == 0)
+            v = *reinterpret_cast<const float4*>(src);
+          else {
+            v.x = r < rows ? src[0] : 0.f;
+            v.y = r + 1 < rows ? src[1] : 0.f;
+            v.z = r + 2 < rows ? src[2] : 0.f;
+            v.w = r + 3 < rows ? src[3] : 0.f;
+          }
+        }
+      } else {  // A[r][k]: 128 rows of 32 k, 8 float4 per row
+        const int rr = e >> 3, k4 = (e & 7) * 4;
+        const int64_t r = r0 + rr, k = k0 + k4;
+        if (r < rows) {
+          const float* src = A + (uint64_t)r * lda + k;
+          if (k + 3 < K && ((uintptr_t)src & 15) == 0)
+            v = *reinterpret_cast<const float4*>(src);
+          else {
+            v.x = k < K ? src[0] : 0.f;
+            v.y = k + 1 < K ? src[1] : 0.f;
+            v.z = k + 2 < K ? src[2] : 0.f;
+            v.w = k + 3 < K ? src[3] : 0.f;
+          }
+        }
+      }
+      ra[u] = v;
+    }
+#pragma unroll
+    for (int u = 0; u < (KC * CN + 255) / 256; ++u) {
+      const int e = tid + 256 * u, kk = e / CN, cc = e - kk * CN;
+      const int64_t k = k0 + kk;
+      rb[u] = (e < KC * CN && cc < l && k < K) ? B[k * l + cc] : 0.f;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + 256 * u;
+      if (AT) {
+        const int kk = e >> 5, r4 = (e & 31) * 4;
+        *reinterpret_cast<float4*>(&as[buf][kk][r4]) = ra[u];
+      } else {
+        const int rr = e >> 3, k4 = (e & 7) * 4;
+        as[buf][k4][rr] = ra[u].x;
+        as[buf][k4 + 1][rr] = ra[u].y;
+        as[buf][k4 + 2][rr] = ra[u].z;
+        as[buf][k4 + 3][rr] = ra[u].w;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < (KC * CN + 255) / 256; ++u) {
+      const int e = tid + 256 * u;
+      if (e < KC * CN) (&bs[buf][0][0])[e] = rb[u];
+    }
+  };
+  if (kc0 < kc1) {
+    load(kc0);
+    store(0);
+  }
+  __syncthreads();
+  int buf = 0;
+  for (int64_t kc = kc0; kc < kc1; ++kc) {
+    const bool more = kc + 1 < kc1;
+    if (more) load(kc + 1);  // in flight during this chunk's products
+#pragma unroll 8
+    for (int kk = 0; kk < KC; ++kk) {
+      const float4 a = *reinterpret_cast<const float4*>(&as[buf][kk][4 * ty]);
+      float b[CW];
+#pragma unroll
+      for (int c = 0; c < CW; ++c) b[c] = bs[buf][kk][tx * CW + c];
+#pragma unroll
+      for (int c = 0; c < CW; ++c) {
+        acc[0][c] = fmaf(a.x, b[c], acc[0][c]);
+        acc[1][c] = fmaf(a.y, b[c], acc[1][c]);
+        acc[2][c] = fmaf(a.z, b[c], acc[2][c]);
+        acc[3][c] = fmaf(a.w, b[c], acc[3][c]);
+      }
+    }
+    if (more) store(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+  float* o = out + (int64_t)blockIdx.y * rows * l;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int64_t r = r0 + 4 * ty + q;
+    if (r >= rows) continue;
+#pragma unroll
+    for (int c = 0; c < CW; ++c) {
+      const int col = tx * CW + c;
+      if (col < l) o[r * l + col] = acc[q][c];
+    }
+  }
+}
+
 template <bool AT, int G>
 void launch_dense_g(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int64_t K, const float* B, int l,
                     int ks, float* out) {
@@ -196,9 +335,29 @@ void launch_dense_g(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, i
   PG_CHECK_LAUNCH();
 }
 
+template <bool AT, int CN>
+void launch_dense2(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int64_t K, const float* B, int l,
+                   int ks, float* out) {
+  const int64_t kct = (K + 31) / 32;
+  const int64_t per = (kct + ks - 1) / ks;
+  dim3 grid((unsigned)((rows + 127) / 128), (unsigned)ks);
+  k_dense_gemm2<AT, CN><<<grid, 256, 0, c->stream>>>(A, lda, rows, K, B, l, per, out);
+  PG_CHECK_LAUNCH();
+}
+
 template <bool AT>
 void launch_dense(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int64_t K, const float* B, int l,
                   int ks, float* out) {
+  if (l <= 48) {
+    switch ((l + 15) / 16) {
+      case 1: launch_dense2<AT, 16>(c, A, lda, rows, K, B, l, ks, out); break;
+      case 2: launch_dense2<AT, 32>(c, A, lda, rows, K, B, l, ks, out); break;
+      default: launch_dense2<AT, 48>(c, A, lda, rows, K, B, l, ks, out); break;
+    }
+    c->launches++;
+    c->gemm_launches++;
+    return;
+  }
   switch ((l + 7) / 8) {
     case 1: launch_dense_g<AT, 1>(c, A, lda, rows, K, B, l, ks, out); break;
     case 2: launch_dense_g<AT, 2>(c, A, lda, rows, K, B, l, ks, out); break;
@@ -216,8 +375,9 @@ void launch_dense(pcaone_ctx* c, const float* A, uint64_t lda, int64_t rows, int
 // Back end for the RSVD engine: "codes" are the float rows of E (the engine passes the row
 // offset through the pointer), "pitch" is unused.
 int dense_ksplit(pcaone_ctx* c, int64_t rows, int64_t K, int) {
+  // enough CTAs for four a SM, each split at least four K chunks long
   int64_t tiles = (rows + 127) / 128, chunks = (K + 31) / 32;
-  int64_t want = (2 * (int64_t)c->sm_count + tiles - 1) / tiles;
+  int64_t want = (4 * (int64_t)c->sm_count + tiles - 1) / tiles;
   return (int)std::max<int64_t>(1, std::min<int64_t>({want, chunks / 4, 64}));
 }
 void dense_p1(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t row0, int64_t rows, int64_t K, const float* B,
@@ -366,7 +526,15 @@ void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {
 void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
   const int threads = 256, nwarps = threads / 32;
   int nblk = (int)std::min<uint64_t>(8 * c->sm_count, (c->M + nwarps - 1) / nwarps);
-  k_posterior_e<<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+  PG_REQUIRE(k <= kLmax, PCAONE_EBADARG, "too many factors for the posterior");
+  if (k <= 8)
+    k_posterior_e<8><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+  else if (k <= 16)
+    k_posterior_e<16><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+  else if (k <= 32)
+    k_posterior_e<32><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+  else
+    k_posterior_e<64><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   PG_CHECK_LAUNCH();
   c->launches++;
 }

@@ -162,8 +162,10 @@ def test_oracle_pcangsd_matches_reference(name, shuffle):
     assert_cols_close(U, ref_table(name, ".eigvecs"), 2e-6)
     if not shuffle:
         assert_cols_close(V, ref_table(name, ".loadings"), 2e-6)
-        Cr = O.read_eigen_matrix(os.path.join(GOLDEN, "ref", name + ".cov"))
-        np.testing.assert_allclose(C, Cr, atol=1e-5)
+    # the GRM pairs each site's likelihoods with the loading row the EM updates use (with the
+    # shuffle: the permuted index), which the shuffled run's .cov pins
+    Cr = O.read_eigen_matrix(os.path.join(GOLDEN, "ref", name + ".cov"))
+    np.testing.assert_allclose(C, Cr, atol=1e-5)
 
 
 def test_eigen_aligned_format_reproduces_reference_cov():

@@ -205,85 +205,91 @@ __device__ __forceinline__ bool last_cta(unsigned* counter) {
   return last;
 }
 
-// One elimination step on the l x l matrix s (shared memory, row-major, l <= 64) by one warp:
-// for the columns b > j and the rows a = j + 1, ... (up to b in the upper form)
-//   s[a][b] -= (s[j][a] (upper) or s[a][j] (lower)) * inv * s[j][b];
-// lane b owns columns b and b + 32 and runs down their rows. Step j reads row j (upper) or
-// column j (lower), which it does not write; a __syncwarp ends the step. One warp with no CTA
-// barrier per step: the serial l-step factorisations are bound by the step latency.
+// One elimination step on the l x l matrix s (shared memory, row-major): for the rows
+// a = j + 1, ..., l - 1 (a warp per row, eight rows a warp in flight) and the columns b > j
+// (b >= a when upper; lanes over columns, two a lane for l <= 64),
+//   s[a][b] -= (s[a][j] or s[j][a]) * inv * s[j][b],
+// with the multiplier from column j (lu) or row j (upper). All loads of a batch of rows are
+// issued before its stores, so the step costs about one shared-memory round trip.
 template <bool kUpper>
-__device__ __forceinline__ void elim_warp(double* s, int l, int j, double inv) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void elim_step(double* s, int l, int j, double inv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int b0 = lane, b1 = lane + 32;
+  const double rj0 = (b0 > j && b0 < l) ? s[j * l + b0] : 0.0;
+  const double rj1 = (b1 > j && b1 < l) ? s[j * l + b1] : 0.0;
+  for (int a0 = j + 1 + warp; a0 < l; a0 += 8 * nw) {
+    double f[8], v0[8], v1[8];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int b = lane + 32 * h;
-    if (b <= j || b >= l) continue;
-    const double rj = s[j * l + b];
-    const int ahi = kUpper ? b : l - 1;
-    for (int a = j + 1; a <= ahi; ++a) {
-      const double f = (kUpper ? s[j * l + a] : s[a * l + j]) * inv;
-      s[a * l + b] = s[a * l + b] - f * rj;
+    for (int k = 0; k < 8; ++k) {
+      const int a = a0 + k * nw;
+      const bool ok = a < l;
+      const int lo = kUpper ? a : j + 1;  // first column updated in row a
+      f[k] = ok ? (kUpper ? s[j * l + a] : s[a * l + j]) * inv : 0.0;
+      v0[k] = (ok && b0 >= lo && b0 < l) ? s[a * l + b0] : 0.0;
+      v1[k] = (ok && b1 >= lo && b1 < l) ? s[a * l + b1] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int a = a0 + k * nw;
+      if (a >= l) break;
+      const int lo = kUpper ? a : j + 1;
+      if (b0 >= lo && b0 < l) s[a * l + b0] = v0[k] - f[k] * rj0;
+      if (b1 >= lo && b1 < l) s[a * l + b1] = v1[k] - f[k] * rj1;
     }
   }
-  __syncwarp();
 }
 
 // In-place Cholesky of the SPD l x l matrix in s (shared memory, row-major; the upper triangle
-// is read; l <= 64) by warp 0; every thread of the CTA must call it. On return s holds the
-// upper factor R (W = R^T R) with zeros below the diagonal. Right-looking with the row scaling
-// deferred: step j subtracts s[j][a] s[j][b] / s[j][j] from the trailing upper triangle (one
-// reciprocal of the pivot a step); row j is divided by sqrt(s[j][j]) at the end. A pivot that
-// is not positive and finite is replaced by 1. Returns 1 + the first such column, else 0 (in
-// every thread).
-__device__ __forceinline__ int chol_upper_warp(double* s, int l) {
-  __shared__ int bad_s;
+// is read; l <= 64): on return s holds the upper factor R (W = R^T R) with zeros below the
+// diagonal. Right-looking with the row scaling deferred: step j subtracts
+// s[j][a] s[j][b] / s[j][j] from the trailing upper triangle (elim_step; one reciprocal of the
+// pivot a step), one barrier a step; row j is divided by sqrt(s[j][j]) at the end. A pivot
+// that is not positive and finite is replaced by 1. Returns 1 + the first such column, else 0
+// (the same in every thread).
+__device__ __forceinline__ int chol_upper_smem(double* s, int l) {
+  int bad = 0;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    int bad = 0;
-    for (int j = 0; j < l; ++j) {
-      double p = s[j * l + j];
-      if (!(p > 0.0) || !isfinite(p)) {
-        if (!bad) bad = j + 1;
-        p = 1.0;
-      }
-      elim_warp<true>(s, l, j, __drcp_rn(p));
+  for (int j = 0; j < l; ++j) {
+    double p = s[j * l + j];
+    if (!(p > 0.0) || !isfinite(p)) {
+      if (!bad) bad = j + 1;
+      p = 1.0;
     }
-    for (int t = threadIdx.x; t < l * l; t += 32) {  // off-diagonal first: diagonals still pivots
-      const int i = t / l, jj = t - i * l;
-      if (jj > i) {
-        const double p = s[i * l + i];
-        s[t] /= (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
-      } else if (jj < i) {
-        s[t] = 0.0;
-      }
-    }
-    __syncwarp();
-    for (int i = threadIdx.x; i < l; i += 32) {
+    elim_step<true>(s, l, j, __drcp_rn(p));
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < l * l; t += blockDim.x) {  // off-diagonal first: diagonals still pivots
+    const int i = t / l, j = t - i * l;
+    if (j > i) {
       const double p = s[i * l + i];
-      s[i * l + i] = (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
+      s[t] /= (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
+    } else if (j < i) {
+      s[t] = 0.0;
     }
-    if (threadIdx.x == 0) bad_s = bad;
   }
   __syncthreads();
-  return bad_s;
+  for (int i = threadIdx.x; i < l; i += blockDim.x) {
+    const double p = s[i * l + i];
+    s[i * l + i] = (p > 0.0 && isfinite(p)) ? sqrt(p) : 1.0;
+  }
+  __syncthreads();
+  return bad;
 }
 
 // Householder column signs D (l) from the modified LU of the l x l block T (shared memory,
 // overwritten; l <= 64): step i takes the pivot s = T[i][i], D_i = -sign(s) with
 // sign(0) = +, and eliminates below it with the shifted pivot s - D_i (Ballard et al. 2015);
-// the multipliers T[r][i] / (s - D_i) are used, not stored. Run by warp 0, every thread of
-// the CTA must call it; D is written by thread 0 and visible to the CTA on return.
-__device__ __forceinline__ void householder_signs_warp(double* T, int l, double* D) {
+// the multipliers T[r][i] / (s - D_i) are used, not stored. One barrier a step. D is
+// written by thread 0 and visible to the CTA on return.
+__device__ __forceinline__ void householder_signs_smem(double* T, int l, double* D) {
   __syncthreads();
-  if (threadIdx.x < 32) {
-    for (int i = 0; i < l; ++i) {
-      const double piv = T[i * l + i];
-      const double di = piv >= 0.0 ? -1.0 : 1.0;
-      if (threadIdx.x == 0) D[i] = di;
-      elim_warp<false>(T, l, i, __drcp_rn(piv - di));
-    }
+  for (int i = 0; i < l; ++i) {
+    const double piv = T[i * l + i];
+    const double di = piv >= 0.0 ? -1.0 : 1.0;
+    if (threadIdx.x == 0) D[i] = di;
+    elim_step<false>(T, l, i, __drcp_rn(piv - di));
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 // Clusters of kGramCluster CTAs of kernel (threads, smem bytes) that fit on the device at

@@ -92,7 +92,7 @@ __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restri
                            int* __restrict__ status) {
   extern __shared__ double s[];  // l x l
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) s[t] = W[t];
-  const int bad = chol_upper_warp(s, l);
+  const int bad = chol_upper_smem(s, l);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) R[t] = s[t];
   __syncthreads();
   if (Rprev) {

@@ -85,7 +85,7 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   cluster_sum(cpart, g.ntiles * 16, a.part);
   if (!last_cta(&a.counters[0])) return;
   gram_final(g, a.part, gridDim.x / kGramCluster, l, l, stage);
-  const int bad = chol_upper_warp(stage, l);
+  const int bad = chol_upper_smem(stage, l);
   if (bad && threadIdx.x == 0) atomicMax(a.status, bad);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R1[t] = stage[t];
   if (threadIdx.x == 0) a.counters[0] = 0;
@@ -144,7 +144,7 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   if (!last_cta(&a.counters[1])) return;
   double* Rn = stage;  // W2, then R2 (row stride l)
   gram_final(g, a.part, gridDim.x / kGramCluster, l, l, Rn);
-  const int bad = chol_upper_warp(Rn, l);
+  const int bad = chol_upper_smem(Rn, l);
   if (bad && threadIdx.x == 0) atomicMax(a.status, bad);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) a.R2[t] = Rn[t];
   if (threadIdx.x == 0) a.counters[1] = 0;
@@ -202,7 +202,7 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kThreads)
   if (!last_cta(&a.counters[2])) return;
   double* top = R;  // the top l x l block of Q, written by this kernel's CTAs
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) top[t] = a.Q[t];
-  householder_signs_warp(top, l, a.D);
+  householder_signs_smem(top, l, a.D);
   const int ncl = gridDim.x / kGramCluster;
   for (int j = threadIdx.x; j < l; j += blockDim.x) {
     const double A = sum_all<kGramMaxParts>(a.part + j, ncl, 2 * l);

@@ -126,6 +126,9 @@ struct Engine {
   GemmFnT<T> gemm;
 
   double *Omg, *Omg2, *wsum, *G, *H, *H1, *H2, *Tb, *Rg, *Rb, *Dsig, *Ucur, *Upre, *Ck;
+  // epoch tail outputs kept apart from the epoch body's buffers (so the next body may run
+  // while the host finishes the tail): Q of the sketch B^T, Q of G, and Q_B^T U_pre (l x k)
+  double *Tq, *Gq, *Xk;
   T* OmgT;   // Omega as the B operand of the first product (alias of Omg for FP64)
   int* d_status;
   unsigned* upd_cnt;
@@ -147,6 +150,9 @@ struct Engine {
     H1 = d("r_H1", Npad * l);
     H2 = d("r_H2", Npad * l);
     Tb = d("r_Tb", Npad * l);
+    Tq = d("r_Tq", Npad * l);
+    Gq = d("r_Gq", (size_t)c->Mpad * l);
+    Xk = d("r_Xk", (size_t)kLmax * kLmax);
     Rg = d("r_Rg", l * l);
     Rb = d("r_Rb", l * l);
     Dsig = d("r_D", l);
@@ -513,15 +519,6 @@ struct Engine {
     if (run0 < nwin) process_windows(run0, nwin, run_target);
   }
 
-  void check_status() {
-    if (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) tc_check_error(c);
-    int st = 0;
-    PG_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    PG_CUDA(cudaStreamSynchronize(c->stream));
-    PG_REQUIRE(st == 0, PCAONE_ENUMERIC,
-               "Cholesky factorisation of a sketch Gram matrix failed at column " + std::to_string(st - 1));
-  }
-
   void run(double* U, double* S, double* V, pcaone_rsvd_report* rep) {
     // zero the FP64 work buffers once so padded rows stay zero; the winSVD window sums are
     // kept from the previous call when asked to and still valid for this shape and data
@@ -537,10 +534,39 @@ struct Engine {
     zero(c, Ucur, Npad * k);
     zero(c, Upre, Npad * k);
     int p = o.maxp;
-    std::vector<double> rb((size_t)l * l), ur((size_t)l * l), vr((size_t)l * l), sv(l), ck((size_t)k * k);
+    std::vector<double> ur((size_t)l * l), vr((size_t)l * l), sv(l), ck((size_t)k * k);
+    // pinned host copies of the tail's small results (read while the next body may run)
+    struct Pinned {
+      double* rb = nullptr;
+      double* xk = nullptr;
+      int* st = nullptr;
+      ~Pinned() {
+        if (rb) cudaFreeHost(rb);
+        if (xk) cudaFreeHost(xk);
+        if (st) cudaFreeHost(st);
+      }
+    } pin;
+    PG_CUDA(cudaMallocHost(&pin.rb, (size_t)l * l * 8));
+    PG_CUDA(cudaMallocHost(&pin.xk, (size_t)l * k * 8));
+    PG_CUDA(cudaMallocHost(&pin.st, 2 * sizeof(int)));
+    cudaEvent_t ev_tail;
+    PG_CUDA(cudaEventCreateWithFlags(&ev_tail, cudaEventDisableTiming));
+    struct EvFree {
+      cudaEvent_t e;
+      ~EvFree() { cudaEventDestroy(e); }
+    } ev_free{ev_tail};
     double diff = 0.0;
     int epochs = 0;
     bool done = false;
+    // Overlap of the epoch tail with the next epoch body. The body of epoch pi + 1 does not
+    // read the tail's results (they only decide whether to stop), so once the tail of epoch pi
+    // and the read-back of its small results are queued, the body of epoch pi + 1 is queued
+    // too and the host runs the l x l SVD and the convergence test meanwhile. If the run stops
+    // at pi that body is discarded: the outputs come from the tail's own buffers (Tq, Gq),
+    // which no body writes. Not with opts.profile (the breakdown measures the waits), nor when
+    // the winSVD sums are carried to the next call (the discarded body would change them).
+    const bool overlap = !o.profile && !(o.svd == 2 && o.carry_window_state);
+    bool ran_ahead = false;
     // with opts.profile: event pairs around the stretches in which the device waits for the
     // host (the small SVD, and the convergence test up to the next epoch's first launch)
     std::vector<cudaEvent_t> gap_ev;
@@ -555,29 +581,55 @@ struct Engine {
     };
     for (int pi = 0; pi <= p && !done; ++pi) {
       gap_mark(false);  // the previous epoch's host decisions end here
-      run_epoch(pi);
-      // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B)
+      if (!ran_ahead) run_epoch(pi);
+      ran_ahead = false;
+      // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B); Q_B^T U_pre for the test
       timed([&] {
-        cholqr2(c, G, l, M, G, Rg, d_status);
-        trsm_right_upper(c, H, Rg, l, N, Tb);
-        cholqr2(c, Tb, l, N, Tb, Rb, d_status);
+        cholqr2(c, G, l, M, Gq, Rg, d_status);
+        trsm_right_upper(c, H, Rg, l, N, Tq);
+        cholqr2(c, Tq, l, N, Tq, Rb, d_status);
+        if (pi > 0) cross(c, Tq, l, Upre, k, N, Xk);
       }, 3);
       gap_mark(true);
-      PG_CUDA(cudaMemcpyAsync(rb.data(), Rb, rb.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-      check_status();
+      const bool tc = o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16;
+      PG_CUDA(cudaMemcpyAsync(pin.rb, Rb, (size_t)l * l * 8, cudaMemcpyDeviceToHost, c->stream));
+      if (pi > 0) PG_CUDA(cudaMemcpyAsync(pin.xk, Xk, (size_t)l * k * 8, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaMemcpyAsync(pin.st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      pin.st[1] = 0;
+      if (tc)  // the tensor-core kernels' bounded-wait flag
+        PG_CUDA(cudaMemcpyAsync(pin.st + 1, scratch(c, "tc_err", sizeof(int)), sizeof(int), cudaMemcpyDeviceToHost,
+                                c->stream));
+      PG_CUDA(cudaEventRecord(ev_tail, c->stream));
+      const int updates_before = updates;
+      const int64_t launches_before = c->launches, gemm_launches_before = c->gemm_launches;
+      const bool may_continue = pi < p || (o.svd == 2 && std::pow(2.0, pi) < o.bands);
+      if (overlap && may_continue) {
+        run_epoch(pi + 1);
+        ran_ahead = true;
+      }
+      PG_CUDA(cudaEventSynchronize(ev_tail));
       collect_times();
-      jacobi_svd(l, rb.data(), ur.data(), sv.data(), vr.data());
+      PG_REQUIRE(pin.st[1] == 0, PCAONE_ETIMEOUT,
+                 "tensor-core decode-GEMM: bounded wait expired (code " + std::to_string(pin.st[1]) + ")");
+      PG_REQUIRE(*pin.st == 0, PCAONE_ENUMERIC,
+                 "Cholesky factorisation of a sketch Gram matrix failed at column " + std::to_string(*pin.st - 1));
+      jacobi_svd(l, pin.rb, ur.data(), sv.data(), vr.data());
       gap_mark(false);
-      // Ucur = Qb Ur[:, :k]
+      // Ucur = Q_B Ur[:, :k] (queued after the body that ran ahead; Tq is not one of its buffers)
       PG_CUDA(cudaMemcpyAsync(Ck, ur.data(), ur.size() * 8, cudaMemcpyHostToDevice, c->stream));
-      rowmat(c, Tb, l, Ck, l, k, N, Ucur);
+      rowmat(c, Tq, l, Ck, l, k, N, Ucur);
       epochs = pi + 1;
+      bool keep_going = true;
       if (pi > 0) {
-        cross(c, Ucur, k, Upre, k, N, Ck);
-        gap_mark(true);
-        PG_CUDA(cudaMemcpyAsync(ck.data(), Ck, ck.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-        PG_CUDA(cudaStreamSynchronize(c->stream));
-        double acc = 0.0;  // mev (src/Utils.cpp:192-198)
+        // mev (src/Utils.cpp:192-198) of U = Q_B Ur_k against U_pre: U^T U_pre = Ur_k^T (Q_B^T U_pre)
+        // ck (k x k, row-major) = U^T U_pre: ck[i][j] = sum_t Ur[t][i] X[t][j], X = Q_B^T U_pre
+        for (int i = 0; i < k; ++i)
+          for (int j = 0; j < k; ++j) {
+            double acc = 0.0;
+            for (int t = 0; t < l; ++t) acc += ur[(size_t)t * l + i] * pin.xk[(size_t)t * k + j];
+            ck[(size_t)i * k + j] = acc;
+          }
+        double acc = 0.0;
         for (int j = 0; j < k; ++j) {
           double nrm = 0.0;
           for (int i = 0; i < k; ++i) nrm += ck[(size_t)i * k + j] * ck[(size_t)i * k + j];
@@ -586,18 +638,22 @@ struct Engine {
         diff = 1.0 - acc / k;
         if (o.verbose) printf("running of epoch = %d, diff = %g\n", pi, diff);
         if (diff < o.tol || pi == p) {
-          if (o.svd == 2 && std::pow(2.0, pi) < o.bands) {
+          if (o.svd == 2 && std::pow(2.0, pi) < o.bands)
             p = (int)std::log2((double)o.bands);
-          } else {
-            done = true;
-            break;
-          }
-        } else {
-          PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
+          else
+            keep_going = false;
         }
-      } else {
-        PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
       }
+      if (!keep_going) {
+        done = true;
+        if (ran_ahead) {  // the body queued ahead is discarded: count only the kept epochs
+          updates = updates_before;
+          c->launches = launches_before;
+          c->gemm_launches = gemm_launches_before;
+        }
+        break;
+      }
+      PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
     }
     // outputs: U = Ucur, S = sigma[:k], V = Q_G Vr[:, :k]
     if (S)
@@ -613,7 +669,7 @@ struct Engine {
     if (V) {
       double* Vd = (double*)scratch(c, "r_V", (size_t)c->Mpad * k * 8);
       PG_CUDA(cudaMemcpyAsync(Ck, vr.data(), vr.size() * 8, cudaMemcpyHostToDevice, c->stream));
-      rowmat(c, G, l, Ck, l, k, M, Vd);
+      rowmat(c, Gq, l, Ck, l, k, M, Vd);
       k_to_colmajor<<<(unsigned)((M * k + 255) / 256), 256, 0, c->stream>>>(Vd, M, k, k, cmaj);
       PG_CHECK_LAUNCH();
       PG_CUDA(cudaMemcpyAsync(V, cmaj, (size_t)M * k * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -864,6 +920,7 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
     tc_clear_error(c);
     Engine<float> e(c, o, o.precision == PCAONE_PREC_MIXED ? gemm_i8() : gemm_tc());
     e.run(U, S, V, rep);
+    tc_check_error(c);  // also covers an epoch body queued ahead and discarded
   } else {
     throw Error(PCAONE_EBADARG, "unknown precision");
   }

@@ -619,7 +619,7 @@ struct Engine {
       PG_CUDA(cudaMemcpyAsync(Ck, ur.data(), ur.size() * 8, cudaMemcpyHostToDevice, c->stream));
       rowmat(c, Tq, l, Ck, l, k, N, Ucur);
       epochs = pi + 1;
-      bool keep_going = true;
+      bool keep_going = true, new_pre = true;  // U_pre is kept when the winSVD runs on past convergence
       if (pi > 0) {
         // mev (src/Utils.cpp:192-198) of U = Q_B Ur_k against U_pre: U^T U_pre = Ur_k^T (Q_B^T U_pre)
         // ck (k x k, row-major) = U^T U_pre: ck[i][j] = sum_t Ur[t][i] X[t][j], X = Q_B^T U_pre
@@ -638,6 +638,7 @@ struct Engine {
         diff = 1.0 - acc / k;
         if (o.verbose) printf("running of epoch = %d, diff = %g\n", pi, diff);
         if (diff < o.tol || pi == p) {
+          new_pre = false;
           if (o.svd == 2 && std::pow(2.0, pi) < o.bands)
             p = (int)std::log2((double)o.bands);
           else
@@ -653,7 +654,8 @@ struct Engine {
         }
         break;
       }
-      PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
+      if (new_pre)
+        PG_CUDA(cudaMemcpyAsync(Upre, Ucur, (size_t)Npad * k * 8, cudaMemcpyDeviceToDevice, c->stream));
     }
     // outputs: U = Ucur, S = sigma[:k], V = Q_G Vr[:, :k]
     if (S)

@@ -139,6 +139,8 @@ int pcaone_gpu_destroy(pcaone_ctx* c) {
   free_all(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_tail) cudaEventDestroy(c->ev_tail);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return PCAONE_OK;

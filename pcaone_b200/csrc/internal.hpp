@@ -158,6 +158,10 @@ struct pcaone_ctx {
 
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // pinned host buffer and event of the epoch tail's small read-backs (kept between calls)
+  void* h_pin = nullptr;
+  size_t h_pin_bytes = 0;
+  cudaEvent_t ev_tail = nullptr;
   double gemm_ms_accum = 0.0;
   int64_t launches = 0, gemm_launches = 0;
 };

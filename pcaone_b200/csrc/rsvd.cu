@@ -535,26 +535,26 @@ struct Engine {
     zero(c, Upre, Npad * k);
     int p = o.maxp;
     std::vector<double> ur((size_t)l * l), vr((size_t)l * l), sv(l), ck((size_t)k * k);
-    // pinned host copies of the tail's small results (read while the next body may run)
-    struct Pinned {
-      double* rb = nullptr;
-      double* xk = nullptr;
-      int* st = nullptr;
-      ~Pinned() {
-        if (rb) cudaFreeHost(rb);
-        if (xk) cudaFreeHost(xk);
-        if (st) cudaFreeHost(st);
-      }
+    // pinned host copies of the tail's small results (read while the next body may run),
+    // kept on the context with their event
+    struct {
+      double* rb;
+      double* xk;
+      int* st;
     } pin;
-    PG_CUDA(cudaMallocHost(&pin.rb, (size_t)l * l * 8));
-    PG_CUDA(cudaMallocHost(&pin.xk, (size_t)l * k * 8));
-    PG_CUDA(cudaMallocHost(&pin.st, 2 * sizeof(int)));
-    cudaEvent_t ev_tail;
-    PG_CUDA(cudaEventCreateWithFlags(&ev_tail, cudaEventDisableTiming));
-    struct EvFree {
-      cudaEvent_t e;
-      ~EvFree() { cudaEventDestroy(e); }
-    } ev_free{ev_tail};
+    const size_t pin_bytes = ((size_t)l * l + (size_t)l * k) * 8 + 16;
+    if (c->h_pin_bytes < pin_bytes) {
+      if (c->h_pin) PG_CUDA(cudaFreeHost(c->h_pin));
+      c->h_pin = nullptr;
+      c->h_pin_bytes = 0;
+      PG_CUDA(cudaMallocHost(&c->h_pin, pin_bytes));
+      c->h_pin_bytes = pin_bytes;
+    }
+    pin.rb = (double*)c->h_pin;
+    pin.xk = pin.rb + (size_t)l * l;
+    pin.st = (int*)(pin.xk + (size_t)l * k);
+    if (!c->ev_tail) PG_CUDA(cudaEventCreateWithFlags(&c->ev_tail, cudaEventDisableTiming));
+    cudaEvent_t ev_tail = c->ev_tail;
     double diff = 0.0;
     int epochs = 0;
     bool done = false;

@@ -563,10 +563,14 @@ struct Engine {
     // and the read-back of its small results are queued, the body of epoch pi + 1 is queued
     // too and the host runs the l x l SVD and the convergence test meanwhile. If the run stops
     // at pi that body is discarded: the outputs come from the tail's own buffers (Tq, Gq),
-    // which no body writes. Not with opts.profile (the breakdown measures the waits), nor when
-    // the winSVD sums are carried to the next call (the discarded body would change them).
-    const bool overlap = !o.profile && !(o.svd == 2 && o.carry_window_state);
+    // which no body writes. The winSVD window sums H1 / H2, which a later call may carry on
+    // from, are saved before the body runs ahead and put back when it is discarded. Not with
+    // opts.profile (the breakdown measures the waits).
+    const bool overlap = !o.profile;
     bool ran_ahead = false;
+    const size_t hbytes = (size_t)Npad * l * 8;
+    double* H1s = o.svd == 2 && overlap ? (double*)scratch(c, "r_H1s", hbytes) : nullptr;
+    double* H2s = o.svd == 2 && overlap ? (double*)scratch(c, "r_H2s", hbytes) : nullptr;
     // with opts.profile: event pairs around the stretches in which the device waits for the
     // host (the small SVD, and the convergence test up to the next epoch's first launch)
     std::vector<cudaEvent_t> gap_ev;
@@ -604,6 +608,10 @@ struct Engine {
       const int64_t launches_before = c->launches, gemm_launches_before = c->gemm_launches;
       const bool may_continue = pi < p || (o.svd == 2 && std::pow(2.0, pi) < o.bands);
       if (overlap && may_continue) {
+        if (H1s) {
+          PG_CUDA(cudaMemcpyAsync(H1s, H1, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+          PG_CUDA(cudaMemcpyAsync(H2s, H2, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+        }
         run_epoch(pi + 1);
         ran_ahead = true;
       }
@@ -651,6 +659,10 @@ struct Engine {
           updates = updates_before;
           c->launches = launches_before;
           c->gemm_launches = gemm_launches_before;
+          if (H1s) {
+            PG_CUDA(cudaMemcpyAsync(H1, H1s, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+            PG_CUDA(cudaMemcpyAsync(H2, H2s, hbytes, cudaMemcpyDeviceToDevice, c->stream));
+          }
         }
         break;
       }

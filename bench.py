@@ -629,14 +629,15 @@ def run_pcangsd_cfg(args, cfg, run):
     # per EM iteration (the allele-frequency EM sweeps are timed but not counted)
     passes = 1 + out[4]
     value = gl_bytes * passes / sec / 1e9 * run.world
-    # HBM roofline of the posterior kernel: P read (8 N bytes a site) + E write (4 Npad bytes)
+    # HBM roofline of the posterior kernel: P read (FP64 pairs, 16 N bytes a site) + E write
+    # (4 Npad bytes)
     reps = 5
     t0 = time.perf_counter()
     for _ in range(reps):
         ctx.gl_update(out[2], out[1], out[3])
     upd_s = (time.perf_counter() - t0) / reps
     npad = (N + 255) // 256 * 256
-    alg = M * (8 * N + 4 * npad)
+    alg = M * (16 * N + 4 * npad)
     pk, pk_kind = peaks()
     roofline = {"bound": "hbm", "achieved": round(alg / upd_s / 1e9, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(alg / upd_s / 1e9 / pk["hbm_gbs"], 4), "traffic": None,

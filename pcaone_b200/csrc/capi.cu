@@ -461,7 +461,7 @@ int pcaone_gpu_ld_timing(pcaone_ctx* c, double* device_ms, double* gram_ms) {
 }  // extern "C"
 
 namespace {
-// Likelihood pairs (FP64 or FP32 host, 2N x M column-major) -> the context's FP32 device copy.
+// Likelihood pairs (FP64 or FP32 host, 2N x M column-major) -> the context's FP64 device copy.
 template <typename T>
 void load_gl_impl(pcaone_ctx* c, const T* P, uint64_t nsnps, uint32_t nsamples) {
   PG_REQUIRE(P && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty likelihood matrix");
@@ -475,15 +475,13 @@ void load_gl_impl(pcaone_ctx* c, const T* P, uint64_t nsnps, uint32_t nsamples) 
   c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
   c->pitch = 1;
   const size_t np = (size_t)nsnps * 2 * nsamples;
-  c->d_P = (float*)scratch(c, "d_P", np * 4);
-  if (std::is_same<T, float>::value) {
-    PG_CUDA(cudaMemcpyAsync(c->d_P, P, np * 4, cudaMemcpyHostToDevice, c->stream));
-  } else {
-    std::vector<float> pf(np);
-    for (size_t t = 0; t < np; ++t) pf[t] = (float)P[t];
-    PG_CUDA(cudaMemcpyAsync(c->d_P, pf.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
-    PG_CUDA(cudaStreamSynchronize(c->stream));  // pf goes out of scope
-  }
+  // kept in FP64 as the reference keeps it: under the shuffle's index semantics the EM
+  // updates amplify FP32 rounding of the likelihoods to about 1e-6 of the singular values
+  c->d_P = (double*)scratch(c, "d_P", np * 8);
+  if (std::is_same<T, double>::value)
+    PG_CUDA(cudaMemcpyAsync(c->d_P, P, np * 8, cudaMemcpyHostToDevice, c->stream));
+  else
+    gl_widen_f32(c, reinterpret_cast<const float*>(P), np, c->d_P);
   c->d_E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
   PG_CUDA(cudaMemsetAsync(c->d_E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
   c->d_F = (double*)scratch(c, "d_F", c->M * 8);

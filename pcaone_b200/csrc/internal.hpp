@@ -96,7 +96,7 @@ struct pcaone_ctx {
   // posterior matrix E (SNP-major, Npad floats per SNP), rebuilt from the GL pairs P.
   bool dense = false;
   double* d_dense_norm = nullptr;  // pcaone_gpu_load_dense: squared norms of the centred rows
-  float* d_P = nullptr;       // M x 2N floats (P0, P1 per sample)
+  double* d_P = nullptr;      // M x 2N doubles (P0, P1 per sample)
   float* d_E = nullptr;       // M x Npad floats
   double* d_zero = nullptr;   // M zeros (centring frequencies of E, already centred)
 

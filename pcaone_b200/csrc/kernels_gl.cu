@@ -35,17 +35,18 @@ __device__ __forceinline__ void posterior(double P0, double P1, double pt, doubl
 }
 
 // One EM sweep of the allele frequencies: warp per SNP. diff2[j] = (F_new - F_old)^2.
-__global__ void k_em_maf(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+__global__ void k_em_maf(const double* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
                          double* __restrict__ F, double* __restrict__ diff2) {
   const uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (j >= M) return;
   const double f = F[j];
-  const float* row = P + j * ldp;
+  const double2* row = reinterpret_cast<const double2*>(P + j * ldp);
   double acc = 0.0;
   for (uint32_t i = lane; i < N; i += 32) {
+    const double2 gl = __ldg(row + i);
     double p0, p1, p2;
-    posterior(row[2 * i], row[2 * i + 1], f, p0, p1, p2);
+    posterior(gl.x, gl.y, f, p0, p1, p2);
     acc += (p1 + 2.0 * p2) / (p0 + p1 + p2);
   }
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -57,12 +58,12 @@ __global__ void k_em_maf(const float* __restrict__ P, uint64_t M, uint32_t N, ui
 }
 
 // E_ij = E[g | likelihoods, pt_ij] - 2 F_j for SNP rows (fit_with_pi, src/Data.cpp:249-270);
-// warp per SNP, lanes over samples (the likelihood pair of a sample read as one float2). The
+// warp per SNP, lanes over samples (the likelihood pair of a sample read as one double2). The
 // standardised E of the GRM stage is k_grm_e. US: N x k (U diag S) row-major, V: M x k
 // row-major (row j = the loading used for SNP j); KM >= k is a compile-time bound, so the
 // loading stays in registers.
 template <int KM>
-__global__ void __launch_bounds__(256) k_posterior_e(const float* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+__global__ void __launch_bounds__(256) k_posterior_e(const double* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
                                                      const double* __restrict__ F, const double* __restrict__ US,
                                                      const double* __restrict__ V, int k, float* __restrict__ E,
                                                      uint32_t lde) {
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(256) k_posterior_e(const float* __restrict__ P
     double v[KM];
 #pragma unroll
     for (int t = 0; t < KM; ++t) v[t] = (V && t < k) ? V[j * k + t] : 0.0;
-    const float2* row = reinterpret_cast<const float2*>(P + j * ldp);
+    const double2* row = reinterpret_cast<const double2*>(P + j * ldp);
     for (uint32_t i = lane; i < N; i += 32) {
       double pt = f;
       if (V) {
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(256) k_posterior_e(const float* __restrict__ P
           if (t < k) pred += __ldg(us + t) * v[t];
         pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
       }
-      const float2 gl = __ldg(row + i);
+      const double2 gl = __ldg(row + i);
       double p0, p1, p2;
       posterior(gl.x, gl.y, pt, p0, p1, p2);
       const double s = p0 + p1 + p2;
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(256) k_posterior_e(const float* __restrict__ P
 // 01 (missing) -> (0.333333, 0.333333), and the initial matrix E = BED2GENO - F_j with
 // BED2GENO = {1, -, 0.5, 0} and missing -> 0. Warp per SNP row of the packed codes.
 __global__ void k_bed_pseudo_gl(const uint8_t* __restrict__ bed, uint32_t pitch, uint64_t M, uint32_t N,
-                                const double* __restrict__ F, float* __restrict__ P, uint32_t ldp,
+                                const double* __restrict__ F, double* __restrict__ P, uint32_t ldp,
                                 float* __restrict__ E, uint32_t lde) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
@@ -105,17 +106,18 @@ __global__ void k_bed_pseudo_gl(const uint8_t* __restrict__ bed, uint32_t pitch,
     const uint8_t* rec = bed + j * pitch;
     for (uint32_t i = lane; i < N; i += 32) {
       const int code = (rec[i >> 2] >> (2 * (i & 3))) & 3;
-      float p0 = 0.0f, p1 = 0.0f, e = 0.0f;
+      double p0 = 0.0, p1 = 0.0;
+      float e = 0.0f;
       if (code == 3) {
-        p0 = 1.0f;
+        p0 = 1.0;
         e = (float)(0.0 - f);
       } else if (code == 0) {
         e = (float)(1.0 - f);
       } else if (code == 2) {
-        p1 = 1.0f;
+        p1 = 1.0;
         e = (float)(0.5 - f);
       } else {
-        p0 = p1 = (float)0.333333;
+        p0 = p1 = 0.333333;
       }
       P[j * ldp + 2 * i] = p0;
       P[j * ldp + 2 * i + 1] = p1;
@@ -413,7 +415,7 @@ void dense_none_b2(pcaone_ctx*, const float*, int, int64_t) {}
 // and the slice's diagonal sum is added to dpart[slice * N + i] (each entry has one owner and
 // the chunks run in stream order, so the sums are deterministic). US: N x k (U diag S) and
 // V: M x k row-major as in k_posterior_e; V null: pt = F_j.
-__global__ void __launch_bounds__(128) k_grm_e(const float* __restrict__ P, uint32_t N, uint32_t ldp,
+__global__ void __launch_bounds__(128) k_grm_e(const double* __restrict__ P, uint32_t N, uint32_t ldp,
                                                const double* __restrict__ F, const double* __restrict__ US,
                                                const double* __restrict__ V, int k, uint64_t j0, uint64_t mc,
                                                double* __restrict__ E, uint32_t lde, double* __restrict__ dpart) {
@@ -431,7 +433,7 @@ __global__ void __launch_bounds__(128) k_grm_e(const float* __restrict__ P, uint
       for (int t = 0; t < k; ++t) pred += US[(uint64_t)i * k + t] * V[j * k + t];
       pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
     }
-    const float2 pp = *reinterpret_cast<const float2*>(P + j * ldp + 2 * i);
+    const double2 pp = *reinterpret_cast<const double2*>(P + j * ldp + 2 * i);
     double p0, p1, p2;
     posterior(pp.x, pp.y, pt, p0, p1, p2);
     const double sum = p0 + p1 + p2;
@@ -480,10 +482,28 @@ GemmFnT<float> gemm_dense_float() {
   return f;
 }
 
+__global__ void k_widen(const float* __restrict__ in, size_t n, double* __restrict__ out) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    out[t] = in[t];
+}
+
+void gl_widen_f32(pcaone_ctx* c, const float* P, size_t n, double* dP) {
+  const size_t chunk = size_t(16) << 20;  // floats per staging pass (64 MB)
+  float* stage = (float*)scratch(c, "gl_stage", std::min(n, chunk) * 4);
+  for (size_t a = 0; a < n; a += chunk) {
+    const size_t m = std::min(chunk, n - a);
+    PG_CUDA(cudaMemcpyAsync(stage, P + a, m * 4, cudaMemcpyHostToDevice, c->stream));
+    const unsigned nblk = (unsigned)std::min<size_t>(4 * (size_t)c->sm_count, (m + 255) / 256);
+    k_widen<<<nblk, 256, 0, c->stream>>>(stage, m, dP + a);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+  }
+}
+
 void gl_from_bed(pcaone_ctx* c) {
   PG_REQUIRE(c->loaded && !c->dense && c->d_bed, PCAONE_ESTATE, "no packed genotypes loaded");
   const size_t np = (size_t)c->M * 2 * c->N;
-  float* P = (float*)scratch(c, "d_P", np * 4);
+  double* P = (double*)scratch(c, "d_P", np * 8);
   float* E = (float*)scratch(c, "d_E", (size_t)c->Mpad * c->Npad * 4);
   PG_CUDA(cudaMemsetAsync(E, 0, (size_t)c->Mpad * c->Npad * 4, c->stream));
   const int threads = 256, nwarps = threads / 32;

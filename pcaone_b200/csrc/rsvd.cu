@@ -565,8 +565,9 @@ struct Engine {
     // at pi that body is discarded: the outputs come from the tail's own buffers (Tq, Gq),
     // which no body writes. The winSVD window sums H1 / H2, which a later call may carry on
     // from, are saved before the body runs ahead and put back when it is discarded. Not with
-    // opts.profile (the breakdown measures the waits).
-    const bool overlap = !o.profile;
+    // opts.profile (the breakdown measures the waits); PCAONE_NO_OVERLAP turns it off.
+    static const bool no_overlap = std::getenv("PCAONE_NO_OVERLAP") != nullptr;
+    const bool overlap = !o.profile && !no_overlap;
     bool ran_ahead = false;
     const size_t hbytes = (size_t)Npad * l * 8;
     double* H1s = o.svd == 2 && overlap ? (double*)scratch(c, "r_H1s", hbytes) : nullptr;

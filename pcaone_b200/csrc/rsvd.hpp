@@ -53,6 +53,8 @@ void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters);
 // The loaded packed genotypes (current SNP order) -> likelihood mode: pseudo-likelihoods, the
 // initial centred matrix E and F = the genotype allele frequencies (pcaone_gpu_bed_to_gl).
 void gl_from_bed(pcaone_ctx* c);
+// FP32 likelihoods on the host -> FP64 on the device, through a bounded staging buffer
+void gl_widen_f32(pcaone_ctx* c, const float* P, size_t n, double* dP);
 void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k);
 // PCAngsd GRM (pcaone_gpu_gl_grm): C (host N x N, or null), its singular vectors (host N x N
 // column-major, or null) and values (host N, or null); US, V as for gl_posterior.

@@ -16,10 +16,9 @@ BEAGLE = os.path.join(GOLDEN, "g3.beagle.gz")
 
 
 def grm_oracle(P, F, U, S, V):
-    """C = E E^T / M with diag Dc / M from the oracle's pcangsd_standardize. The device keeps
-    the likelihoods in FP32, so the oracle gets them rounded the same way."""
-    Pf = P.astype(np.float32).astype(np.float64)
-    Es, Dc = O.pcangsd_standardize(Pf, F, (U * S) @ V.T)
+    """C = E E^T / M with diag Dc / M from the oracle's pcangsd_standardize (the device keeps
+    the likelihoods in FP64, as the reference does)."""
+    Es, Dc = O.pcangsd_standardize(P, F, (U * S) @ V.T)
     C = Es @ Es.T / P.shape[1]
     C[np.diag_indices(len(Dc))] = Dc / P.shape[1]
     return C

@@ -26,10 +26,6 @@ __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
-__device__ __forceinline__ void cp_async16(double* sdst, const double* gsrc) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
-}
 
 template <bool SYM>
 __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThreads)
@@ -49,23 +45,8 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThr
   }
   int64_t r0, r1;
   row_range(n, r0, r1);
-  // even widths with 16-byte aligned matrices: 16-byte copies, a warp per row (row starts stay
-  // 16-byte aligned in both places, la4 and lb4 being multiples of 4)
-  const bool vec = (la & 1) == 0 && (SYM || (lb & 1) == 0) &&
-                   ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(Bm)) & 15) == 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   auto issue = [&](int64_t b, double* dst) {
     const int nr = (int)(r1 - b < rows ? r1 - b : rows);
-    if (vec) {
-      for (int r = warp; r < nr; r += nwarps) {
-        for (int cc = 2 * lane; cc < la; cc += 64) cp_async16(dst + r * g.la4 + cc, A + (b + r) * la + cc);
-        if (!SYM)
-          for (int cc = 2 * lane; cc < lb; cc += 64)
-            cp_async16(dst + rows * g.la4 + r * g.lb4 + cc, Bm + (b + r) * lb + cc);
-      }
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      return;
-    }
     for (int t = threadIdx.x; t < nr * la; t += blockDim.x) {
       const int r = t / la;
       cp_async8(dst + r * g.la4 + (t - r * la), A + b * la + t);
@@ -125,34 +106,17 @@ __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restri
   if (threadIdx.x == 0 && bad && status) atomicMax(status, bad);
 }
 
-// Q = A R^{-1} (row-wise forward substitution x R = a), R upper l x l. CTAs stride over
-// tiles of kTrsmRows rows: a tile is read with coalesced row loads (a warp per row) into
-// shared memory (row stride l | 1, so the per-thread row reads below spread over the banks),
-// each thread then solves one row with its unknowns in registers (LMAX >= l, loops unrolled
-// over LMAX), and the tile is written back with coalesced row stores. A may alias Q: every
-// tile is read completely before any of it is written.
-constexpr int kTrsmRows = 128;
+// Q = A R^{-1} (row-wise forward substitution x R = a), R upper l x l. One thread per row;
+// the row's unknowns stay in registers (LMAX >= l, loops unrolled over LMAX).
 template <int LMAX>
-__global__ void __launch_bounds__(kTrsmRows) k_trsm_right_upper(const double* A, const double* __restrict__ R, int l,
-                                                                int64_t n, double* Q) {
-  extern __shared__ double sr[];  // LMAX x LMAX, then the tile
-  double* st = sr + LMAX * LMAX;
-  const int sp = l | 1;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+__global__ void __launch_bounds__(128) k_trsm_right_upper(const double* A, const double* __restrict__ R, int l,
+                                                          int64_t n, double* Q) {  // A may alias Q
+  extern __shared__ double sr[];  // LMAX x LMAX
   stage_r<LMAX>(R, l, sr);
-  const int64_t ntiles = (n + kTrsmRows - 1) / kTrsmRows;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t r0 = t * kTrsmRows;
-    const int nr = (int)(n - r0 < kTrsmRows ? n - r0 : kTrsmRows);
-    __syncthreads();  // R staged; the previous tile's stores have read the tile
-    for (int r = warp; r < nr; r += nwarps)
-      for (int c = lane; c < l; c += 32) st[r * sp + c] = A[(r0 + r) * l + c];
-    __syncthreads();
-    if ((int)threadIdx.x < nr) solve_row_upper<LMAX>(st + threadIdx.x * sp, sr, l, st + threadIdx.x * sp);
-    __syncthreads();
-    for (int r = warp; r < nr; r += nwarps)
-      for (int c = lane; c < l; c += 32) Q[(r0 + r) * l + c] = st[r * sp + c];
-  }
+  __syncthreads();
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  solve_row_upper<LMAX>(A + r * l, sr, l, Q + r * l);
 }
 
 // Column sums of A (n x l) into partials (grid.y = column).
@@ -241,32 +205,15 @@ void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rp
 }
 
 void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q) {
-  const int64_t ntiles = (n + kTrsmRows - 1) / kTrsmRows;
-  auto go = [&](auto kern, int lmax) {
-    const size_t smem = ((size_t)lmax * lmax + (size_t)kTrsmRows * (l | 1)) * 8;
-    static int set_for[4] = {0, 0, 0, 0};  // dynamic shared-memory limit raised once per instance
-    int& done = set_for[lmax / 16 - 1];
-    if (!done) {
-      PG_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(((size_t)64 * 64 + (size_t)kTrsmRows * 65) * 8)));
-      done = 1;
-    }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, kTrsmRows, smem) != cudaSuccess) {
-      (void)cudaGetLastError();
-      per_sm = 1;
-    }
-    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)std::max(1, per_sm) * c->sm_count);
-    kern<<<(unsigned)grid, kTrsmRows, smem, c->stream>>>(A, R, l, n, Q);
-  };
+  const dim3 grid((unsigned)((n + 127) / 128));
   if (l <= 16)
-    go(k_trsm_right_upper<16>, 16);
+    k_trsm_right_upper<16><<<grid, 128, 16 * 16 * 8, c->stream>>>(A, R, l, n, Q);
   else if (l <= 32)
-    go(k_trsm_right_upper<32>, 32);
+    k_trsm_right_upper<32><<<grid, 128, 32 * 32 * 8, c->stream>>>(A, R, l, n, Q);
   else if (l <= 48)
-    go(k_trsm_right_upper<48>, 48);
+    k_trsm_right_upper<48><<<grid, 128, 48 * 48 * 8, c->stream>>>(A, R, l, n, Q);
   else
-    go(k_trsm_right_upper<64>, 64);
+    k_trsm_right_upper<64><<<grid, 128, 64 * 64 * 8, c->stream>>>(A, R, l, n, Q);
   PG_CHECK_LAUNCH();
   c->launches++;
 }

@@ -46,6 +46,8 @@ struct EpiP2 {          // after the Z * G product of one window or of a run of 
   const int64_t* miss_ptr = nullptr; // (window, sample) CSR, row i * nwin + b
   const int32_t* miss_idx = nullptr;
   const double* miss_val = nullptr;
+  const double* miss_w = nullptr;    // when set: per-entry weights s_j (e_ij + F_j) (replaces the
+                                     // per-entry gathers of s and F)
   double* H = nullptr;               // Npad x l accumulator
 };
 

@@ -187,6 +187,8 @@ void build_missing_by_window_sample(pcaone_ctx* c);
 // semantics, else the current F (Data::fit_with_pi EMU branch, src/Data.cpp:272-287).
 void compute_imputed_snp(pcaone_ctx* c);
 void compute_imputed_ws(pcaone_ctx* c);
+// w[e] = scale_j (val[e] + F_j) for every entry e of the (window, sample) list (j its SNP)
+void compute_ws_weights(pcaone_ctx* c, const double* F, double* w);
 // LD r2 of every window pair (kernels_ld.cu). W, Y: M x k row-major device arrays (or null).
 // d_r2 holds float values, or double with f64.
 void ld_r2(pcaone_ctx* c, const double* W, const double* Y, int k, const int64_t* d_ws,

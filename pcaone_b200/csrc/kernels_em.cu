@@ -57,7 +57,26 @@ __global__ void k_impute_ws(const int64_t* __restrict__ ptr, const int32_t* __re
   }
 }
 
+// entry weights of the (window, sample) list: the SNP of entry e is idx[e]
+__global__ void k_ws_weights(const int32_t* __restrict__ idx, int64_t n, const double* __restrict__ val,
+                             const double* __restrict__ scale, const double* __restrict__ F,
+                             double* __restrict__ w) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t j = idx[e];
+    w[e] = scale[j] * (val[e] + F[j]);
+  }
+}
+
 }  // namespace
+
+void compute_ws_weights(pcaone_ctx* c, const double* F, double* w) {
+  PG_REQUIRE(c->miss_ws_valid && c->miss_ws_val_valid, PCAONE_ESTATE, "imputed values not set");
+  if (c->n_missing == 0) return;
+  const unsigned nblk = (unsigned)std::min<int64_t>(8 * (int64_t)c->sm_count, (c->n_missing + 255) / 256);
+  k_ws_weights<<<nblk, 256, 0, c->stream>>>(c->d_miss_ws_idx, c->n_missing, c->d_miss_ws_val, c->d_scale, F, w);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
 
 void compute_scale(pcaone_ctx* c, int standardize, int ploidy) {
   const double* Fs = (c->imputed && c->imputed_compat) ? c->d_F_load : c->d_F;

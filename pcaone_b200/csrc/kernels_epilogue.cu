@@ -305,8 +305,8 @@ __global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const 
   for (int64_t i = (int64_t)blockIdx.x * nwarps + warp; i < p.n; i += (int64_t)gridDim.x * nwarps) {
     const int64_t e0 = p.miss_ptr[i * p.nwin + p.b0], e1 = p.miss_ptr[i * p.nwin + p.b1];
     const double* mv = p.miss_val;
-    const double *sc = p.scale, *F = p.F;
-    auto w = [&](int64_t e, int j) { return sc[j] * ((mv ? mv[e] : 0.0) + F[j]); };
+    const double *sc = p.scale, *F = p.F, *mw = p.miss_w;
+    auto w = [&](int64_t e, int j) { return mw ? mw[e] : sc[j] * ((mv ? mv[e] : 0.0) + F[j]); };
     if constexpr (kMode == 1)  // Gf holds s F G: the sparse term is a plain row sum
       sum_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp);
     else if constexpr (kMode == 2)

@@ -269,6 +269,7 @@ struct Engine {
     p2.miss_ptr = c->d_miss_ws_ptr;
     p2.miss_idx = c->d_miss_ws_idx;
     p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
+    p2.miss_w = ws_weights();
     p2.H = Ht;
     timed([&] { launch_accum<T>(c, p2, D2); }, 1);
   }
@@ -334,6 +335,7 @@ struct Engine {
     p2.miss_ptr = c->d_miss_ws_ptr;
     p2.miss_idx = c->d_miss_ws_idx;
     p2.miss_val = c->imputed ? c->d_miss_ws_val : nullptr;
+    p2.miss_w = ws_weights();
     p2.H = Ht;
     timed([&] { launch_accum<T>(c, p2, D2); }, 1);
   }
@@ -348,6 +350,18 @@ struct Engine {
     }
     const int per = (int)std::max<int64_t>(1, kRunRows / gemm.seg_rows1(c));
     for (int b = b0; b < b1; b += per) process_run(b, std::min(b1, b + per), Ht);
+  }
+
+  // Weights s_j (e_ij + F_j) of the (window, sample) missing entries for the accumulation
+  // gather, built once a run when imputed values are set (scale and F are fixed within it).
+  double* ws_w = nullptr;
+  const double* ws_weights() {
+    if (!c->imputed || !c->miss_ws_val_valid || c->n_missing == 0) return nullptr;
+    if (!ws_w) {
+      ws_w = (double*)scratch(c, "r_ws_w", (size_t)c->n_missing * 8);
+      compute_ws_weights(c, Fcent, ws_w);
+    }
+    return ws_w;
   }
 
   int bandsize = 1;

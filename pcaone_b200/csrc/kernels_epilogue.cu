@@ -90,7 +90,8 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
 // (shared memory of this warp). The batch is sized so that the kernels keep three CTAs of
 // 256 threads per SM (registers) with 16 rows in flight per warp.
 // With kWeighted, entry e's row is scaled by weight(e, idx_e) (computed by the lane that loads
-// the index and passed along with it).
+// the index and passed along with it). The indices of the next batch are loaded while the
+// current batch's rows are in flight, so a batch waits for one load latency, not two.
 constexpr int kSumBatch = 16;
 template <int G, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
 __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
@@ -105,14 +106,10 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
   const bool active = grp < R;
   const float4* rows4 = reinterpret_cast<const float4*>(rows);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  int32_t nxt = (e0 + lane < e1) ? idx[e0 + lane] : 0;
   for (int64_t base = e0; base < e1; base += B) {
     const int cnt = (int)(e1 - base < B ? e1 - base : B);
-    int32_t myi = 0;
-    double myw = 0.0;
-    if (lane < cnt) {
-      myi = idx[base + lane];
-      if constexpr (kWeighted) myw = weight(base + lane, myi);
-    }
+    const int32_t myi = nxt;
     const int64_t my = (int64_t)myi - row0;
     float4 v[T];
     double w[T];
@@ -122,6 +119,10 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
       const int64_t ii = __shfl_sync(0xffffffffu, my, src & 31);
       v[t] = (active && src < cnt) ? __ldg(rows4 + ii * G + cg) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
+    double myw = 0.0;
+    if constexpr (kWeighted)
+      if (lane < cnt) myw = weight(base + lane, myi);
+    nxt = (base + B + lane < e1) ? idx[base + B + lane] : 0;
     if constexpr (kWeighted) {  // then the weights (their loads overlap the rows')
 #pragma unroll
       for (int t = 0; t < T; ++t) w[t] = __shfl_sync(0xffffffffu, myw, (grp + R * t) & 31);

@@ -89,11 +89,12 @@ __device__ __forceinline__ void gather_rows(int64_t e0, int64_t e1, const int32_
 // them. FP64 sums; the row groups are combined in a fixed order (deterministic) into out
 // (shared memory of this warp). The batch is sized so that the kernels keep three CTAs of
 // 256 threads per SM (registers) with 16 rows in flight per warp.
-// With kWeighted, entry e's row is scaled by weight(e, idx_e) (computed by the lane that loads
-// the index and passed along with it). The indices of the next batch are loaded while the
-// current batch's rows are in flight, so a batch waits for one load latency, not two.
+// With kWeighted, entry e's row is scaled by weight(e), a per-entry value loaded by the lane
+// that loads the index and passed along with it. The indices and weights of the next batch
+// are loaded while the current batch's rows are in flight, so a batch waits for one load
+// latency, not two.
 constexpr int kSumBatch = 16;
-template <int G, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
+template <int G, bool kWeighted = false, typename Wt = double (*)(int64_t)>
 __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                           const float* __restrict__ rows, int64_t row0, double* out,
                                           Wt weight = nullptr) {
@@ -106,11 +107,16 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
   const bool active = grp < R;
   const float4* rows4 = reinterpret_cast<const float4*>(rows);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  int32_t nxt = (e0 + lane < e1) ? idx[e0 + lane] : 0;
+  int32_t nxt = 0;
+  double nxtw = 0.0;
+  if (e0 + lane < e1) {
+    nxt = idx[e0 + lane];
+    if constexpr (kWeighted) nxtw = weight(e0 + lane);
+  }
   for (int64_t base = e0; base < e1; base += B) {
     const int cnt = (int)(e1 - base < B ? e1 - base : B);
-    const int32_t myi = nxt;
-    const int64_t my = (int64_t)myi - row0;
+    const int64_t my = (int64_t)nxt - row0;
+    const double myw = nxtw;
     float4 v[T];
     double w[T];
 #pragma unroll
@@ -119,11 +125,13 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
       const int64_t ii = __shfl_sync(0xffffffffu, my, src & 31);
       v[t] = (active && src < cnt) ? __ldg(rows4 + ii * G + cg) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    double myw = 0.0;
-    if constexpr (kWeighted)
-      if (lane < cnt) myw = weight(base + lane, myi);
-    nxt = (base + B + lane < e1) ? idx[base + B + lane] : 0;
-    if constexpr (kWeighted) {  // then the weights (their loads overlap the rows')
+    nxt = 0;
+    nxtw = 0.0;
+    if (base + B + lane < e1) {  // the next batch's index and weight, in flight with the rows
+      nxt = idx[base + B + lane];
+      if constexpr (kWeighted) nxtw = weight(base + B + lane);
+    }
+    if constexpr (kWeighted) {
 #pragma unroll
       for (int t = 0; t < T; ++t) w[t] = __shfl_sync(0xffffffffu, myw, (grp + R * t) & 31);
     }
@@ -152,7 +160,7 @@ __device__ __forceinline__ void sum_rows4(int64_t e0, int64_t e1, const int32_t*
 
 // out = sum of the rows for l % 4 == 0 and ceil(l / 8) = CPL, i.e. G = l / 4 = 2 CPL - 1 or
 // 2 CPL (the two instantiations a kernel of that CPL can meet).
-template <int CPL, bool kWeighted = false, typename Wt = double (*)(int64_t, int)>
+template <int CPL, bool kWeighted = false, typename Wt = double (*)(int64_t)>
 __device__ __forceinline__ void sum_rows(int64_t e0, int64_t e1, const int32_t* __restrict__ idx,
                                          const float* __restrict__ rows, int64_t row0, int l, double* out,
                                          Wt weight = nullptr) {
@@ -198,7 +206,7 @@ __global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_prep(EpiP1 p, const T
     if constexpr (kMode == 1)
       sum_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp);
     else if constexpr (kMode == 2)
-      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp, w);
+      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, ssp, [&](int64_t e) { return mv[e] + F; });
     else if (p.omega_f)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.omega_f, 0, p.l, w, ssp);
     else
@@ -311,7 +319,7 @@ __global__ void __launch_bounds__(256, CPL <= 5 ? 3 : 2) k_accum(EpiP2 p, const 
     if constexpr (kMode == 1)  // Gf holds s F G: the sparse term is a plain row sum
       sum_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp);
     else if constexpr (kMode == 2)
-      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp, w);
+      sum_rows<CPL, true>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, ssp, [&](int64_t e) { return mw[e]; });
     else if (p.Gf && !mv)
       gather_rows<CPL>(e0, e1, p.miss_idx, p.Gf, p.g_start, p.l, [](int64_t, int) { return 1.0; }, ssp);
     else if (p.Gf)
@@ -373,7 +381,8 @@ template <typename T>
 void launch_accum(pcaone_ctx* c, const EpiP2& p, const T* D2) {
   const int threads = 256, nwarps = threads / 32;
   const size_t smem = (size_t)nwarps * p.l * 8;
-  const int mode = (p.Gf && (p.l & 3) == 0) ? (p.miss_val ? 2 : 1) : 0;
+  // the weighted row sums read the per-entry weights p.miss_w; without them the generic gather
+  const int mode = (p.Gf && (p.l & 3) == 0) ? (p.miss_val ? (p.miss_w ? 2 : 0) : 1) : 0;
   auto go = [&](auto kern) {
     const int per_sm = resident_ctas((const void*)kern, threads, smem);
     const int nblk = (int)std::min<int64_t>((int64_t)per_sm * c->sm_count, (p.n + nwarps - 1) / nwarps);

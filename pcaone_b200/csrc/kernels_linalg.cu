@@ -80,6 +80,61 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThr
   cluster_sum(cpart, g.ntiles * 16, gpart);
 }
 
+// Gram of Q1 = A R^{-1} without writing Q1 (the second pass of CholeskyQR2 when only its R
+// is needed): k_cross<true> with a solve step. Each staged batch of rows (row stride
+// la4 + 2, which keeps the 16-byte alignment of the tile reads and spreads the rows of
+// neighbouring threads over the banks) is solved in place, a thread per row
+// (solve_row_upper with R staged, reciprocal diagonal), before it is summed into the tiles.
+template <int LMAX>
+__global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThreads)
+    k_cross_solved(const double* __restrict__ A, const double* __restrict__ R, int l, int64_t n, int rows,
+                   double* __restrict__ gpart) {
+  extern __shared__ double sm[];
+  const GramTiling g = gram_tiling(l, l, true, blockDim.x);
+  GramTiling gs = g;  // the tile reads with the staged row stride
+  gs.la4 = gs.lb4 = g.la4 + 2;
+  const int w = gs.la4;
+  double* Rs = sm;  // LMAX x LMAX
+  double* st = Rs + LMAX * LMAX;
+  double* red = st + 2 * rows * w;
+  double* cpart = red + g.ngrp * g.ntiles * 16;
+  stage_r<LMAX>(R, l, Rs);
+  for (int t = threadIdx.x; t < 2 * rows; t += blockDim.x)  // padding columns, never copied or solved
+    for (int cc = l; cc < w; ++cc) st[t * w + cc] = 0.0;
+  int64_t r0, r1;
+  row_range(n, r0, r1);
+  auto issue = [&](int64_t b, double* dst) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    for (int t = threadIdx.x; t < nr * l; t += blockDim.x) {
+      const int r = t / l;
+      cp_async8(dst + r * w + (t - r * l), A + b * l + t);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  GramThread gt;
+  gt.init(g);
+  int s = 0;
+  if (r0 < r1) issue(r0, st);
+  for (int64_t b = r0; b < r1; b += rows) {
+    const int nr = (int)(r1 - b < rows ? r1 - b : rows);
+    if (b + rows < r1) {
+      issue(b + rows, st + (s ^ 1) * rows * w);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();  // stage s complete, R staged, padding zeroed
+    double* sa = st + s * rows * w;
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) solve_row_upper<LMAX>(sa + r * w, Rs, l, sa + r * w);
+    __syncthreads();
+    gt.add_rows(sa, sa, nr, gs);
+    __syncthreads();  // stage s is consumed before it is refilled
+    s ^= 1;
+  }
+  gt.finish(g, red, cpart);
+  cluster_sum(cpart, g.ntiles * 16, gpart);
+}
+
 // out (la x lb, global) = sum of the nparts cluster sums of k_cross.
 __global__ void __launch_bounds__(kCrossThreads) k_cross_final(const double* __restrict__ gpart, int nparts, int la,
                                                                int lb, int sym, double* __restrict__ out) {
@@ -195,6 +250,48 @@ void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int6
   k_cross_final<<<1, kCrossThreads, 0, c->stream>>>(gpart, ncl, la, lb, sym ? 1 : 0, out);
   PG_CHECK_LAUNCH();
   c->launches += 2;
+}
+
+void cross_solved(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* out) {
+  PG_REQUIRE(l >= 1 && l <= kLmax, PCAONE_EBADARG, "cross product too wide");
+  const GramTiling g = gram_tiling(l, l, true, kCrossThreads);
+  const int lmax = l <= 16 ? 16 : l <= 32 ? 32 : l <= 48 ? 48 : 64;
+  const int w = g.la4 + 2;
+  const int fixed = (gram_smem_doubles(g) + lmax * lmax) * 8;
+  const int rows = std::max(8, std::min(128, (kCrossSmemBudget - fixed) / (2 * w * 8)));
+  const size_t smem = (size_t)fixed + (size_t)2 * rows * w * 8;
+  const int64_t want = (n + (int64_t)kGramCluster * 4 * rows - 1) / ((int64_t)kGramCluster * 4 * rows);
+  int cap = std::max(1, std::min(kCrossMaxClusters, 2 * c->sm_count / kGramCluster));
+  auto go = [&](auto kern) {
+    PG_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int resident = resident_clusters(c, (const void*)kern, ((uint64_t)l << 32) | 0x5u, kCrossThreads, smem);
+    if (resident > 0) cap = std::min(cap, resident);
+    const int ncl = (int)std::max<int64_t>(1, std::min<int64_t>(cap, want));
+    double* gpart = (double*)scratch(c, "cross_part", (size_t)ncl * g.ntiles * 16 * 8);
+    kern<<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, R, l, n, rows, gpart);
+    PG_CHECK_LAUNCH();
+    k_cross_final<<<1, kCrossThreads, 0, c->stream>>>(gpart, ncl, l, l, 1, out);
+    PG_CHECK_LAUNCH();
+  };
+  if (lmax == 16)
+    go(k_cross_solved<16>);
+  else if (lmax == 32)
+    go(k_cross_solved<32>);
+  else if (lmax == 48)
+    go(k_cross_solved<48>);
+  else
+    go(k_cross_solved<64>);
+  c->launches += 2;
+}
+
+void cholqr2_r(pcaone_ctx* c, const double* A, int l, int64_t n, double* R, int* d_status) {
+  double* W = (double*)scratch(c, "cq_W", (size_t)l * l * 8);
+  double* R1 = (double*)scratch(c, "cq_R1", (size_t)l * l * 8);
+  double* R2 = (double*)scratch(c, "cq_R2", (size_t)l * l * 8);
+  cross(c, A, l, A, l, n, W);
+  cholesky(c, W, l, R1, nullptr, nullptr, d_status);
+  cross_solved(c, A, R1, l, n, W);
+  cholesky(c, W, l, R2, R1, R, d_status);
 }
 
 void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rprev, double* Racc,

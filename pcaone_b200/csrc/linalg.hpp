@@ -15,6 +15,10 @@ void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rp
 void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q);
 // CholeskyQR2: A = Q R with Q orthonormal (Q may alias A).
 void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double* R, int* d_status);
+// out (l x l) = (A R^-1)^T (A R^-1), without writing A R^-1.
+void cross_solved(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* out);
+// The R factor of CholeskyQR2 of A (A = Q R), without Q: Q = A R^-1 when needed.
+void cholqr2_r(pcaone_ctx* c, const double* A, int l, int64_t n, double* R, int* d_status);
 void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);
 // Y (n x kc) = X (n x l) * C[:, :kc] with C l x ldc row-major.
 void rowmat(pcaone_ctx* c, const double* X, int l, const double* C, int ldc, int kc, int64_t n, double* Y);

@@ -127,8 +127,11 @@ struct Engine {
 
   double *Omg, *Omg2, *wsum, *G, *H, *H1, *H2, *Tb, *Rg, *Rb, *Dsig, *Ucur, *Upre, *Ck;
   // epoch tail outputs kept apart from the epoch body's buffers (so the next body may run
-  // while the host finishes the tail): Q of the sketch B^T, Q of G, and Q_B^T U_pre (l x k)
-  double *Tq, *Gq, *Xk;
+  // while the host finishes the tail): Q of the sketch B^T and Q_B^T U_pre (l x k)
+  double *Tq, *Xk;
+  // G of the even and the odd epochs: the epoch body writes G of its parity, so an epoch body
+  // queued ahead of the host's decision leaves the previous epoch's G (the output V needs it)
+  double* Gbuf[2];
   T* OmgT;   // Omega as the B operand of the first product (alias of Omg for FP64)
   int* d_status;
   unsigned* upd_cnt;
@@ -145,13 +148,13 @@ struct Engine {
     Omg = d("r_omg", Npad * l);
     Omg2 = d("r_omg2", Npad * l);
     wsum = d("r_wsum", l);
-    G = d("r_G", (size_t)c->Mpad * l);
+    Gbuf[0] = G = d("r_G", (size_t)c->Mpad * l);
+    Gbuf[1] = d("r_G1", (size_t)c->Mpad * l);
     H = d("r_H", Npad * l);
     H1 = d("r_H1", Npad * l);
     H2 = d("r_H2", Npad * l);
     Tb = d("r_Tb", Npad * l);
     Tq = d("r_Tq", Npad * l);
-    Gq = d("r_Gq", (size_t)c->Mpad * l);
     Xk = d("r_Xk", (size_t)kLmax * kLmax);
     Rg = d("r_Rg", l * l);
     Rb = d("r_Rb", l * l);
@@ -408,15 +411,17 @@ struct Engine {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
-    if (steady_exec) cudaGraphExecDestroy(steady_exec);
+    for (auto& e : steady_exec)
+      if (e) cudaGraphExecDestroy(e);
   }
 
   // Steady epochs as one CUDA graph. Once the schedule stops depending on the epoch (the
   // winSVD from 2^pi >= bands on: every window run and every Omega update the same; Halko from
   // its second update on), the epoch body is launched as a graph: run once directly (buffers
-  // sized), captured on the next epoch, replayed after it. The epoch tail, with its host round
+  // sized), then captured once for each epoch parity (each writes G of its parity) and
+  // replayed after that. The epoch tail, with its host round
   // trip, stays outside. Used by the tensor-core back ends when no per-launch profile is asked.
-  cudaGraphExec_t steady_exec = nullptr;
+  cudaGraphExec_t steady_exec[2] = {nullptr, nullptr};  // by epoch parity (G of that parity)
   int steady_seen = 0, steady_updates = 0;
   uint64_t steady_launches = 0, steady_gemm_launches = 0;
   bool graphs_failed = false;
@@ -435,12 +440,14 @@ struct Engine {
       else
         epoch_winsvd(pi);
     };
+    const int par = pi & 1;
+    G = Gbuf[par];
     if (!graphs_on() || !steady_epoch(pi)) {
       body();
       return;
     }
-    if (steady_exec) {  // replay, with the host-side counters the body would have advanced
-      PG_CUDA(cudaGraphLaunch(steady_exec, c->stream));
+    if (steady_exec[par]) {  // replay, with the host-side counters the body would have advanced
+      PG_CUDA(cudaGraphLaunch(steady_exec[par], c->stream));
       updates += steady_updates;
       c->launches += steady_launches;
       c->gemm_launches += steady_gemm_launches;
@@ -462,13 +469,15 @@ struct Engine {
       }
       cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
       ok = ok && e == cudaSuccess && graph;
-      if (ok) ok = cudaGraphInstantiate(&steady_exec, graph, 0) == cudaSuccess;
+      if (ok) ok = cudaGraphInstantiate(&steady_exec[par], graph, 0) == cudaSuccess;
       if (graph) cudaGraphDestroy(graph);
     }
     if (!ok) {  // capture refused: run this epoch and the rest directly (nothing was executed)
       (void)cudaGetLastError();
-      if (steady_exec) cudaGraphExecDestroy(steady_exec);
-      steady_exec = nullptr;
+      for (auto& ex : steady_exec) {
+        if (ex) cudaGraphExecDestroy(ex);
+        ex = nullptr;
+      }
       graphs_failed = true;
       updates = u0;
       c->launches = l0;
@@ -479,7 +488,7 @@ struct Engine {
     steady_updates = updates - u0;
     steady_launches = c->launches - l0;
     steady_gemm_launches = c->gemm_launches - g0;
-    PG_CUDA(cudaGraphLaunch(steady_exec, c->stream));
+    PG_CUDA(cudaGraphLaunch(steady_exec[par], c->stream));
   }
 
   void epoch_halko(int pi) {
@@ -576,8 +585,8 @@ struct Engine {
     // read the tail's results (they only decide whether to stop), so once the tail of epoch pi
     // and the read-back of its small results are queued, the body of epoch pi + 1 is queued
     // too and the host runs the l x l SVD and the convergence test meanwhile. If the run stops
-    // at pi that body is discarded: the outputs come from the tail's own buffers (Tq, Gq),
-    // which no body writes. The winSVD window sums H1 / H2, which a later call may carry on
+    // at pi that body is discarded: the outputs come from the tail's own buffers (Tq, R_G) and
+    // from G of epoch pi, which the body of epoch pi + 1 does not write (other parity). The winSVD window sums H1 / H2, which a later call may carry on
     // from, are saved before the body runs ahead and put back when it is discarded. Not with
     // opts.profile (the breakdown measures the waits); PCAONE_NO_OVERLAP turns it off.
     static const bool no_overlap = std::getenv("PCAONE_NO_OVERLAP") != nullptr;
@@ -604,7 +613,7 @@ struct Engine {
       ran_ahead = false;
       // tail of computeUSV: QR(G) twice, B = R^-T H^T, SVD(B); Q_B^T U_pre for the test
       timed([&] {
-        cholqr2(c, G, l, M, Gq, Rg, d_status);
+        cholqr2_r(c, G, l, M, Rg, d_status);  // Q_G itself only for the output V
         trsm_right_upper(c, H, Rg, l, N, Tq);
         cholqr2(c, Tq, l, N, Tq, Rb, d_status);
         if (pi > 0) cross(c, Tq, l, Upre, k, N, Xk);
@@ -698,7 +707,9 @@ struct Engine {
     if (V) {
       double* Vd = (double*)scratch(c, "r_V", (size_t)c->Mpad * k * 8);
       PG_CUDA(cudaMemcpyAsync(Ck, vr.data(), vr.size() * 8, cudaMemcpyHostToDevice, c->stream));
-      rowmat(c, Gq, l, Ck, l, k, M, Vd);
+      double* Gl = Gbuf[(epochs - 1) & 1];  // G of the last epoch kept; Q_G = G R_G^-1 in place
+      trsm_right_upper(c, Gl, Rg, l, M, Gl);
+      rowmat(c, Gl, l, Ck, l, k, M, Vd);
       k_to_colmajor<<<(unsigned)((M * k + 255) / 256), 256, 0, c->stream>>>(Vd, M, k, k, cmaj);
       PG_CHECK_LAUNCH();
       PG_CUDA(cudaMemcpyAsync(V, cmaj, (size_t)M * k * 8, cudaMemcpyDeviceToHost, c->stream));

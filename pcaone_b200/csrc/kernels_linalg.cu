@@ -81,13 +81,14 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThr
 }
 
 // Gram of Q1 = A R^{-1} without writing Q1 (the second pass of CholeskyQR2 when only its R
-// is needed): k_cross<true> with a solve step. Each staged batch of rows (row stride
-// la4 + 2, which keeps the 16-byte alignment of the tile reads and spreads the rows of
-// neighbouring threads over the banks) is solved in place, a thread per row
-// (solve_row_upper with R staged, reciprocal diagonal), before it is summed into the tiles.
+// is needed): k_cross<true> with a product step. Each staged batch of rows (row stride
+// la4 + 2, 16-byte aligned) is multiplied by Rinv = R^{-1} (upper, staged in shared memory
+// with row stride LMAX and zeros outside l x l) in 4 x 4 register tiles, a thread per tile
+// (the host sizes the batch so that one pass of the CTA covers it), written back in place
+// and then summed into the Gram tiles.
 template <int LMAX>
 __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThreads)
-    k_cross_solved(const double* __restrict__ A, const double* __restrict__ R, int l, int64_t n, int rows,
+    k_cross_solved(const double* __restrict__ A, const double* __restrict__ Rinv, int l, int64_t n, int rows,
                    double* __restrict__ gpart) {
   extern __shared__ double sm[];
   const GramTiling g = gram_tiling(l, l, true, blockDim.x);
@@ -98,8 +99,11 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThr
   double* st = Rs + LMAX * LMAX;
   double* red = st + 2 * rows * w;
   double* cpart = red + g.ngrp * g.ntiles * 16;
-  stage_r<LMAX>(R, l, Rs);
-  for (int t = threadIdx.x; t < 2 * rows; t += blockDim.x)  // padding columns, never copied or solved
+  for (int t = threadIdx.x; t < LMAX * LMAX; t += blockDim.x) {
+    const int i = t / LMAX, j = t - i * LMAX;
+    Rs[t] = (i < l && j < l) ? Rinv[i * l + j] : 0.0;
+  }
+  for (int t = threadIdx.x; t < 2 * rows; t += blockDim.x)  // padding columns, never copied or written
     for (int cc = l; cc < w; ++cc) st[t * w + cc] = 0.0;
   int64_t r0, r1;
   row_range(n, r0, r1);
@@ -125,7 +129,39 @@ __global__ void __cluster_dims__(kGramCluster, 1, 1) __launch_bounds__(kCrossThr
     }
     __syncthreads();  // stage s complete, R staged, padding zeroed
     double* sa = st + s * rows * w;
-    for (int r = threadIdx.x; r < nr; r += blockDim.x) solve_row_upper<LMAX>(sa + r * w, Rs, l, sa + r * w);
+    {
+      const int nbc = g.la4 >> 2, nbr = (nr + 3) >> 2;
+      const bool act = (int)threadIdx.x < nbr * nbc;
+      const int rb = act ? (int)threadIdx.x / nbc : 0, cb = act ? (int)threadIdx.x - rb * nbc : 0;
+      const int rr0 = 4 * rb, cc0 = 4 * cb;
+      double q[4][4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) q[x][y] = 0.0;
+      if (act) {
+        const int kend = l < cc0 + 4 ? l : cc0 + 4;  // Rinv is upper: rows past the tile's last column add 0
+        for (int kk = 0; kk < kend; ++kk) {
+          const double2 r01 = *reinterpret_cast<const double2*>(Rs + kk * LMAX + cc0);
+          const double2 r23 = *reinterpret_cast<const double2*>(Rs + kk * LMAX + cc0 + 2);
+          const double rv[4] = {r01.x, r01.y, r23.x, r23.y};
+          double av[4];
+#pragma unroll
+          for (int x = 0; x < 4; ++x) av[x] = rr0 + x < nr ? sa[(rr0 + x) * w + kk] : 0.0;
+#pragma unroll
+          for (int x = 0; x < 4; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) q[x][y] = fma(av[x], rv[y], q[x][y]);
+        }
+      }
+      __syncthreads();  // every row of the batch read before any is overwritten
+      if (act)
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+          for (int y = 0; y < 4; ++y)
+            if (rr0 + x < nr && cc0 + y < l) sa[(rr0 + x) * w + cc0 + y] = q[x][y];
+    }
     __syncthreads();
     gt.add_rows(sa, sa, nr, gs);
     __syncthreads();  // stage s is consumed before it is refilled
@@ -144,11 +180,25 @@ __global__ void __launch_bounds__(kCrossThreads) k_cross_final(const double* __r
 
 __global__ void k_cholesky(const double* __restrict__ W, int l, double* __restrict__ R,
                            const double* __restrict__ Rprev, double* __restrict__ Racc,
-                           int* __restrict__ status) {
-  extern __shared__ double s[];  // l x l
+                           double* __restrict__ Rinv, int* __restrict__ status) {
+  extern __shared__ double s[];  // l x l, then l x l for R^-1
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) s[t] = W[t];
   const int bad = chol_upper_smem(s, l);
   for (int t = threadIdx.x; t < l * l; t += blockDim.x) R[t] = s[t];
+  if (Rinv) {  // column j of R^-1 by back substitution (thread j), zeros below the diagonal
+    double* si = s + l * l;
+    for (int j = threadIdx.x; j < l; j += blockDim.x) {
+      for (int i = l - 1; i > j; --i) si[i * l + j] = 0.0;
+      si[j * l + j] = 1.0 / s[j * l + j];
+      for (int i = j - 1; i >= 0; --i) {
+        double acc = 0.0;
+        for (int m = i + 1; m <= j; ++m) acc = fma(s[i * l + m], si[m * l + j], acc);
+        si[i * l + j] = -acc / s[i * l + i];
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < l * l; t += blockDim.x) Rinv[t] = si[t];
+  }
   __syncthreads();
   if (Rprev) {
     for (int t = threadIdx.x; t < l * l; t += blockDim.x) {
@@ -252,13 +302,15 @@ void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int6
   c->launches += 2;
 }
 
-void cross_solved(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* out) {
+void cross_solved(pcaone_ctx* c, const double* A, const double* Rinv, int l, int64_t n, double* out) {
   PG_REQUIRE(l >= 1 && l <= kLmax, PCAONE_EBADARG, "cross product too wide");
   const GramTiling g = gram_tiling(l, l, true, kCrossThreads);
   const int lmax = l <= 16 ? 16 : l <= 32 ? 32 : l <= 48 ? 48 : 64;
   const int w = g.la4 + 2;
   const int fixed = (gram_smem_doubles(g) + lmax * lmax) * 8;
-  const int rows = std::max(8, std::min(128, (kCrossSmemBudget - fixed) / (2 * w * 8)));
+  // one 4 x 4 product tile per thread covers a batch of rows
+  const int rows_tiles = 4 * (kCrossThreads / (g.la4 / 4));
+  const int rows = std::max(4, std::min(std::min(128, rows_tiles), (kCrossSmemBudget - fixed) / (2 * w * 8)));
   const size_t smem = (size_t)fixed + (size_t)2 * rows * w * 8;
   const int64_t want = (n + (int64_t)kGramCluster * 4 * rows - 1) / ((int64_t)kGramCluster * 4 * rows);
   int cap = std::max(1, std::min(kCrossMaxClusters, 2 * c->sm_count / kGramCluster));
@@ -268,7 +320,7 @@ void cross_solved(pcaone_ctx* c, const double* A, const double* R, int l, int64_
     if (resident > 0) cap = std::min(cap, resident);
     const int ncl = (int)std::max<int64_t>(1, std::min<int64_t>(cap, want));
     double* gpart = (double*)scratch(c, "cross_part", (size_t)ncl * g.ntiles * 16 * 8);
-    kern<<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, R, l, n, rows, gpart);
+    kern<<<ncl * kGramCluster, kCrossThreads, smem, c->stream>>>(A, Rinv, l, n, rows, gpart);
     PG_CHECK_LAUNCH();
     k_cross_final<<<1, kCrossThreads, 0, c->stream>>>(gpart, ncl, l, l, 1, out);
     PG_CHECK_LAUNCH();
@@ -288,15 +340,16 @@ void cholqr2_r(pcaone_ctx* c, const double* A, int l, int64_t n, double* R, int*
   double* W = (double*)scratch(c, "cq_W", (size_t)l * l * 8);
   double* R1 = (double*)scratch(c, "cq_R1", (size_t)l * l * 8);
   double* R2 = (double*)scratch(c, "cq_R2", (size_t)l * l * 8);
+  double* R1i = (double*)scratch(c, "cq_R1i", (size_t)l * l * 8);
   cross(c, A, l, A, l, n, W);
-  cholesky(c, W, l, R1, nullptr, nullptr, d_status);
-  cross_solved(c, A, R1, l, n, W);
+  cholesky(c, W, l, R1, nullptr, nullptr, d_status, R1i);
+  cross_solved(c, A, R1i, l, n, W);
   cholesky(c, W, l, R2, R1, R, d_status);
 }
 
 void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rprev, double* Racc,
-              int* d_status) {
-  k_cholesky<<<1, 256, (size_t)l * l * 8, c->stream>>>(W, l, R, Rprev, Racc, d_status);
+              int* d_status, double* Rinv) {
+  k_cholesky<<<1, 256, (size_t)(Rinv ? 2 : 1) * l * l * 8, c->stream>>>(W, l, R, Rprev, Racc, Rinv, d_status);
   PG_CHECK_LAUNCH();
   c->launches++;
 }

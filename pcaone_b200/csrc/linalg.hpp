@@ -8,15 +8,16 @@ namespace pg {
 
 // out (la x lb, row-major) = A^T B for A: n x la, B: n x lb.
 void cross(pcaone_ctx* c, const double* A, int la, const double* B, int lb, int64_t n, double* out);
-// W = R^T R; R upper. When Rprev is given, Racc = R * Rprev. d_status gets 1+j on failure.
+// W = R^T R; R upper. When Rprev is given, Racc = R * Rprev; when Rinv is given, R^-1 (upper,
+// zeros below). d_status gets 1+j on failure.
 void cholesky(pcaone_ctx* c, const double* W, int l, double* R, const double* Rprev, double* Racc,
-              int* d_status);
+              int* d_status, double* Rinv = nullptr);
 // Q = A R^-1 (may alias A == Q).
 void trsm_right_upper(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* Q);
 // CholeskyQR2: A = Q R with Q orthonormal (Q may alias A).
 void cholqr2(pcaone_ctx* c, const double* A, int l, int64_t n, double* Q, double* R, int* d_status);
-// out (l x l) = (A R^-1)^T (A R^-1), without writing A R^-1.
-void cross_solved(pcaone_ctx* c, const double* A, const double* R, int l, int64_t n, double* out);
+// out (l x l) = (A Rinv)^T (A Rinv) for Rinv = R^-1 (upper), without writing A Rinv.
+void cross_solved(pcaone_ctx* c, const double* A, const double* Rinv, int l, int64_t n, double* out);
 // The R factor of CholeskyQR2 of A (A = Q R), without Q: Q = A R^-1 when needed.
 void cholqr2_r(pcaone_ctx* c, const double* A, int l, int64_t n, double* R, int* d_status);
 void colsum(pcaone_ctx* c, const double* A, int l, int64_t n, double* out);

@@ -63,6 +63,21 @@ const char* pcaone_gpu_last_error(const pcaone_ctx* ctx);
 int pcaone_gpu_load_bed(pcaone_ctx* ctx, const uint8_t* packed, uint64_t nsnps,
                         uint32_t nsamples);
 
+/* The same genotypes kept in host memory: the records are copied into a pinned host buffer
+ * owned by the context (the caller's array is not retained) and the counts are computed
+ * from them. pcaone_gpu_rsvd (Halko and winSVD at the FP32, FP64 and mixed precisions) then
+ * copies one run of windows at a time into one of two device slots of slot_bytes each
+ * (0: 1 GiB) on a copy stream, while the products of the other slot run; the missing-entry
+ * lists and per-SNP vectors stay on the device. For matrices beyond device memory.
+ * Replaces the out-of-core reader FileBed::read_block_initial / read_block_update
+ * (src/FilePlink.cpp:133-294) over the block plan of Data::prepare (src/Data.cpp:16-72); the
+ * winSVD windows are the plan's blocks when pcaone_rsvd_opts.block_snps is set, and Halko
+ * sums its products over blocks. pcaone_gpu_permute permutes the host records. The
+ * products, LD, residual and pseudo-likelihood calls need resident genotypes and return
+ * PCAONE_ESTATE on a streamed matrix. */
+int pcaone_gpu_load_bed_host(pcaone_ctx* ctx, const uint8_t* packed, uint64_t nsnps,
+                             uint32_t nsamples, uint64_t slot_bytes);
+
 /* Per-SNP integer counts in the current SNP order: a1x2[j] = 2*n(00) + n(10) (twice the sum
  * of BED2GENO over non-missing entries, src/FilePlink.cpp:36-57) and nonmiss[j] = number of
  * non-missing samples. Bit-exact. */
@@ -72,8 +87,9 @@ int pcaone_gpu_counts(pcaone_ctx* ctx, uint32_t* a1x2, uint32_t* nonmiss);
  * with the reference's accumulation. */
 int pcaone_gpu_allele_freq(pcaone_ctx* ctx, double* F);
 
-/* Permute SNP records on the device: new SNP j = old SNP perm[j] (src/RSVD.hpp:63-79 for
- * the in-core winSVD shuffle). perm is a host array of nsnps int32 indices. */
+/* Permute SNP records on the device (or in the host buffer of streamed genotypes): new SNP
+ * j = old SNP perm[j] (src/RSVD.hpp:63-79 for the in-core winSVD shuffle). perm is a host
+ * array of nsnps int32 indices. */
 int pcaone_gpu_permute(pcaone_ctx* ctx, const int32_t* perm);
 
 /* The reference's in-core SNP shuffle (std::shuffle of 0..n-1 with a default-seeded

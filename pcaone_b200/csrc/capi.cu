@@ -45,6 +45,13 @@ void free_data(pcaone_ctx* c) {
   c->d_miss_snp_ptr = c->d_miss_ws_ptr = nullptr;
   c->d_miss_snp_idx = c->d_miss_ws_idx = nullptr;
   c->loaded = c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
+  // streamed genotypes: the pinned host buffer and the slots are kept for reuse; their
+  // contents are forgotten (a copy still in flight completes first)
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+  c->streamed = false;
+  c->slot[0].key = c->slot[1].key = 0;
+  c->cur_slot = -1;
+  c->slot_windows = 0;
 }
 
 void free_all(pcaone_ctx* c) {
@@ -137,6 +144,7 @@ int pcaone_gpu_destroy(pcaone_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   pg::gl_release(c);
   free_all(c);
+  pg::stream_free(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_tail) cudaEventDestroy(c->ev_tail);
@@ -179,6 +187,33 @@ int pcaone_gpu_load_bed(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, ui
   });
 }
 
+int pcaone_gpu_load_bed_host(pcaone_ctx* c, const uint8_t* packed, uint64_t nsnps, uint32_t nsamples,
+                             uint64_t slot_bytes) {
+  return guarded(c, [&] {
+    PG_REQUIRE(packed && nsnps > 0 && nsamples > 0, PCAONE_EBADARG, "empty genotype matrix");
+    PG_REQUIRE(nsnps < (1ull << 31) && nsamples < (1u << 30), PCAONE_EBADARG, "genotype matrix too large");
+    free_data(c);
+    c->generation++;
+    c->N = nsamples;
+    c->M = nsnps;
+    c->bpr = (nsamples + 3) / 4;
+    c->Npad = (uint32_t)round_up(nsamples, kRowPad);
+    c->pitch = c->Npad / 4;
+    c->Mpad = round_up(nsnps, kRowPad) + kRowPad;
+    c->d_bed = nullptr;
+    c->d_a1x2 = (uint32_t*)scratch(c, "d_a1x2", c->M * 4);
+    c->d_nonmiss = (uint32_t*)scratch(c, "d_nonmiss", c->M * 4);
+    c->d_F = (double*)scratch(c, "d_F", c->M * 8);
+    c->d_F_load = (double*)scratch(c, "d_F_load", c->M * 8);
+    c->d_scale = (double*)scratch(c, "d_scale", c->M * 8);
+    stream_load(c, packed, (size_t)slot_bytes);
+    stream_counts(c);
+    PG_CUDA(cudaMemcpyAsync(c->d_F_load, c->d_F, c->M * 8, cudaMemcpyDeviceToDevice, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));
+    c->loaded = true;
+  });
+}
+
 int pcaone_gpu_counts(pcaone_ctx* c, uint32_t* a1x2, uint32_t* nonmiss) {
   return guarded(c, [&] {
     PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
@@ -208,18 +243,25 @@ int pcaone_gpu_permute(pcaone_ctx* c, const int32_t* perm) {
                  "perm is not a permutation of 0..nsnps-1");
       seen[perm[j]] = 1;
     }
-    int32_t* d_perm = (int32_t*)scratch(c, "perm", c->M * 4);
-    PG_CUDA(cudaMemcpyAsync(d_perm, perm, c->M * 4, cudaMemcpyHostToDevice, c->stream));
-    // permute into the other of the two packed-matrix slots, then swap
-    const size_t bytes = (size_t)c->Mpad * c->pitch;
-    uint8_t* out = (uint8_t*)scratch(c, c->bed_slot ? "d_bed_0" : "d_bed_1", bytes);
-    PG_CUDA(cudaMemsetAsync(out, 0xFF, bytes, c->stream));
-    launch_permute(c, d_perm, out);
-    PG_CUDA(cudaStreamSynchronize(c->stream));
-    c->d_bed = out;
-    c->bed_slot ^= 1;
-    launch_counts(c);
-    PG_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->streamed) {  // the host records are permuted, then counted again
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+      if (c->copy_stream) PG_CUDA(cudaStreamSynchronize(c->copy_stream));
+      stream_permute(c, perm);
+      stream_counts(c);
+    } else {
+      int32_t* d_perm = (int32_t*)scratch(c, "perm", c->M * 4);
+      PG_CUDA(cudaMemcpyAsync(d_perm, perm, c->M * 4, cudaMemcpyHostToDevice, c->stream));
+      // permute into the other of the two packed-matrix slots, then swap
+      const size_t bytes = (size_t)c->Mpad * c->pitch;
+      uint8_t* out = (uint8_t*)scratch(c, c->bed_slot ? "d_bed_0" : "d_bed_1", bytes);
+      PG_CUDA(cudaMemsetAsync(out, 0xFF, bytes, c->stream));
+      launch_permute(c, d_perm, out);
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+      c->d_bed = out;
+      c->bed_slot ^= 1;
+      launch_counts(c);
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+    }
     c->bedT_valid = c->miss_snp_valid = c->miss_ws_valid = false;
     c->generation++;
     c->imputed = false;  // imputed values are tied to the SNP order of the lists
@@ -296,12 +338,18 @@ int pcaone_gpu_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts* opts, double* U, doub
 
 int pcaone_gpu_gram_product(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X,
                             uint32_t ncols, double* Y) {
-  return guarded(c, [&] { run_gram(c, precision, standardize, ploidy, X, (int)ncols, Y); });
+  return guarded(c, [&] {
+    require_resident(c, "the Gram product");
+    run_gram(c, precision, standardize, ploidy, X, (int)ncols, Y);
+  });
 }
 
 int pcaone_gpu_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
                        const double* B, uint32_t ncols, double* out) {
-  return guarded(c, [&] { run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out); });
+  return guarded(c, [&] {
+    require_resident(c, "the product");
+    run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out);
+  });
 }
 
 int pcaone_gpu_fit_emu(pcaone_ctx* c, const double* U, const double* S, const double* V,
@@ -441,12 +489,18 @@ extern "C" {
 
 int pcaone_gpu_ld_r2(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
                      uint64_t nwin, float* r2) {
-  return guarded(c, [&] { ld_r2_impl(c, U, k, ws, we, nwin, r2, false); });
+  return guarded(c, [&] {
+    require_resident(c, "LD r2");
+    ld_r2_impl(c, U, k, ws, we, nwin, r2, false);
+  });
 }
 
 int pcaone_gpu_ld_r2_f64(pcaone_ctx* c, const double* U, uint32_t k, const int64_t* ws, const int32_t* we,
                          uint64_t nwin, double* r2) {
-  return guarded(c, [&] { ld_r2_impl(c, U, k, ws, we, nwin, r2, true); });
+  return guarded(c, [&] {
+    require_resident(c, "LD r2");
+    ld_r2_impl(c, U, k, ws, we, nwin, r2, true);
+  });
 }
 
 int pcaone_gpu_ld_timing(pcaone_ctx* c, double* device_ms, double* gram_ms) {
@@ -539,6 +593,7 @@ int pcaone_gpu_residuals(pcaone_ctx* c, const double* U, const double* S, const 
                          uint64_t snp0, uint64_t nsnp, float* out) {
   return guarded(c, [&] {
     PG_REQUIRE(c->loaded && !c->dense, PCAONE_ESTATE, "residuals need packed genotypes (load_bed)");
+    require_resident(c, "residuals");
     PG_REQUIRE(out && snp0 + nsnp <= c->M, PCAONE_EBADARG, "residual rows out of range");
     PG_REQUIRE(!U || (S && V && k >= 1 && k <= (uint32_t)kLmax), PCAONE_EBADARG, "bad factors");
     double *dUS = nullptr, *dV = nullptr;
@@ -561,7 +616,10 @@ int pcaone_gpu_residuals(pcaone_ctx* c, const double* U, const double* S, const 
 }
 
 int pcaone_gpu_bed_to_gl(pcaone_ctx* c) {
-  return guarded(c, [&] { gl_from_bed(c); });
+  return guarded(c, [&] {
+    require_resident(c, "pseudo-likelihoods");
+    gl_from_bed(c);
+  });
 }
 
 int pcaone_gpu_gl_freq(pcaone_ctx* c, int maxiter, double tolmaf, double* F, int* iters) {

@@ -92,6 +92,29 @@ struct pcaone_ctx {
   double* d_F_load = nullptr;  // F in the SNP order of load time (before any permutation)
   double* d_scale = nullptr;   // per-SNP multiplier of the centred genotypes (current order)
 
+  // Streamed genotypes (pcaone_gpu_load_bed_host): the SNP-major records (M x pitch, padding
+  // codes set) stay in a pinned host buffer and d_bed is null. The RSVD copies each run of
+  // windows into one of two device slots on the copy stream, builds the run's transposed copy
+  // (and the int8 back end's tiles) there, and the products read the slot; the other slot
+  // takes the next windows meanwhile. The missing-entry lists and per-SNP vectors stay
+  // resident (built by streaming passes).
+  bool streamed = false;
+  uint8_t* h_bed = nullptr;
+  size_t h_bed_bytes = 0;
+  cudaStream_t copy_stream = nullptr;
+  size_t slot_budget = 0;  // device bytes per slot (records, transposed copy, tiles)
+  struct StreamSlot {
+    int b0 = -1, b1 = -1;  // windows held, once `ready` has completed on the copy stream
+    uint64_t key = 0;      // data generation, window layout and tile kind of the contents
+    uint8_t *rec = nullptr, *recT = nullptr, *t1 = nullptr, *t2 = nullptr;
+    cudaEvent_t ready = nullptr;  // contents complete (copy stream)
+    cudaEvent_t idle = nullptr;   // last product reading the slot (main stream)
+  } slot[2];
+  int slot_windows = 0;   // windows a slot holds for the current layout
+  int cur_slot = -1;      // slot the products of the current run read
+  int last_slot = 1;      // slot staged most recently
+  uint64_t streamed_h2d = 0;  // bytes copied to the device by window staging (cumulative)
+
   // PCAngsd (genotype-likelihood) mode: no packed codes; the RSVD runs on the dense float
   // posterior matrix E (SNP-major, Npad floats per SNP), rebuilt from the GL pairs P.
   bool dense = false;
@@ -143,8 +166,7 @@ struct pcaone_ctx {
   void* tile82_ptr = nullptr;
   bool i8_b2_max_ready = false;  // the first epilogue filled the window operand's column maxima
 
-  // cuBLAS / cuSOLVER handles of the PCAngsd GRM (created on first use)
-  void* blas = nullptr;
+  // cuSOLVER handle of the PCAngsd GRM's N x N eigendecomposition (created on first use)
   void* solver = nullptr;
 
   // named scratch buffers (grown on demand, freed with the context)
@@ -208,6 +230,46 @@ void ld_r2_dense(pcaone_ctx* c, const double* d, const int64_t* d_win_of, const 
                  const int32_t* d_span, int max_span, void* d_r2, bool f64);
 // d_scale_j = 1/sqrt(ploidy Fs_j (1 - Fs_j)) (or 1 when not standardising / sd <= 1e-9).
 void compute_scale(pcaone_ctx* c, int standardize, int ploidy);
+
+// ---------------------------------------------------------------- streamed genotypes (stream.cu)
+// Counts and F of the host records (staged through the device), at load.
+void stream_counts(pcaone_ctx* c);
+// By-SNP missing-entry list from one staging pass.
+void stream_missing_snp(pcaone_ctx* c);
+// Window layout, and the two missing-entry lists built from two staging passes.
+void stream_prepare(pcaone_ctx* c, int bands, uint64_t blocksize, bool tiles);
+// Pinned host copy of the records at the device pitch (padding set), copy stream; counts at load.
+void stream_load(pcaone_ctx* c, const uint8_t* packed, size_t slot_bytes);
+// Host records in the order perm (row j = old row perm[j]).
+void stream_permute(pcaone_ctx* c, const int32_t* perm);
+// Make the slot holding window b current (staging [b, b + slot_windows) if no slot holds it;
+// the main stream waits for its contents); tiles: also the int8 back end's tiled copies.
+// Returns the last window + 1 the slot holds.
+int stream_acquire(pcaone_ctx* c, int b, bool tiles);
+// Stage the windows from b on into the slot that is not current, unless a slot holds b.
+void stream_prefetch(pcaone_ctx* c, int b, bool tiles);
+// The products of the current run are queued: the slot may be refilled after them.
+void stream_release(pcaone_ctx* c);
+// Packed rows of window b in the current slot: SNP-major records / sample-major copy.
+const uint8_t* stream_codes(const pcaone_ctx* c, int b);
+const uint8_t* stream_codesT(const pcaone_ctx* c, int b);
+void stream_free(pcaone_ctx* c);
+// Fails with PCAONE_ESTATE when the genotypes are streamed (calls that need them resident).
+void require_resident(const pcaone_ctx* c, const char* what);
+// Launchers used by the staging (kernels_bed.cu, kernels_gemm_i8.cu)
+void launch_counts_rows(pcaone_ctx* c, cudaStream_t st, const uint8_t* rows, uint64_t nrows, uint64_t row0);
+void launch_freq(pcaone_ctx* c);
+void launch_transpose_run(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, uint64_t nsnp, int nwin, uint8_t* recT);
+void launch_missing_snp_rows(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, uint64_t nrows, uint64_t row0);
+void launch_missing_ws_count(pcaone_ctx* c, cudaStream_t st, const uint8_t* recT, int b0, int nw, int64_t* cnt);
+void launch_missing_ws_fill(pcaone_ctx* c, cudaStream_t st, const uint8_t* recT, int b0, int nw,
+                            const uint64_t* d_base);
+int64_t missing_snp_scan(pcaone_ctx* c);  // by-SNP row pointers from the counts; total
+int64_t scan_counts(pcaone_ctx* c, const int64_t* cnt, uint64_t n, int64_t* ptr);
+// int8 back end: tile bytes per window (first, second product) and the tiling of one window
+void i8_tile_bytes(const pcaone_ctx* c, size_t* w1, size_t* w2);
+void i8_tile_window(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, int64_t m, const uint8_t* recT,
+                    uint8_t* t1, uint8_t* t2);
 
 // ---------------------------------------------------------------- SIMT decode-GEMM
 // out[s][r][c] = sum_{k in split s} val(code[r][k]) * B[k][c], val(00,01,10,11) = (2,0,1,0)

@@ -259,6 +259,62 @@ void launch_permute(pcaone_ctx* c, const int32_t* d_perm, uint8_t* d_out) {
   c->launches++;
 }
 
+// ---- launchers for streamed genotypes: the same kernels on rows staged in a device slot
+void launch_counts_rows(pcaone_ctx* c, cudaStream_t st, const uint8_t* rows, uint64_t nrows, uint64_t row0) {
+  const uint64_t threads = nrows * 32;
+  k_counts<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(rows, nrows, c->pitch, c->N, c->d_a1x2 + row0,
+                                                               c->d_nonmiss + row0);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void launch_freq(pcaone_ctx* c) {
+  k_freq<<<(unsigned)((c->M + 255) / 256), 256, 0, c->stream>>>(c->d_a1x2, c->d_nonmiss, c->M, c->d_F);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+// Sample-major copies of nwin consecutive windows of the current layout whose nsnp records
+// start at rec (the first window at rec); recT: nwin x Npad x win.pitch.
+void launch_transpose_run(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, uint64_t nsnp, int nwin,
+                          uint8_t* recT) {
+  PG_CUDA(cudaMemsetAsync(recT, 0xFF, (size_t)nwin * c->Npad * c->win.pitch, st));
+  dim3 grid((unsigned)((c->win.blocksize + 63) / 64), c->Npad / 64, (unsigned)nwin);
+  k_transpose<<<grid, 256, 0, st>>>(rec, c->pitch, nsnp, c->win.blocksize, recT, c->win.pitch, c->Npad);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+// By-SNP missing entries of the staged records of SNPs row0 .. row0 + nrows (row pointers set).
+void launch_missing_snp_rows(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, uint64_t nrows, uint64_t row0) {
+  const uint64_t threads = nrows * 32;
+  k_fill_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      rec, c->pitch, nrows, c->pitch / 4, c->d_miss_snp_ptr + row0, c->d_miss_snp_idx, nullptr, 1, 0);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+// (window, sample) missing counts / entries of the staged sample-major copies of the windows
+// b0 .. b0 + nw: row r of the copies is sample r % Npad of window b0 + r / Npad, whose CSR row
+// (i * bands + b) is reached by offsetting the count / pointer array by b0.
+void launch_missing_ws_count(pcaone_ctx* c, cudaStream_t st, const uint8_t* recT, int b0, int nw, int64_t* cnt) {
+  const uint64_t rows = (uint64_t)nw * c->Npad, threads = rows * 32;
+  k_count_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      recT, c->win.pitch, rows, c->win.pitch / 4, c->Npad, (uint32_t)c->win.bands, cnt + b0);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
+void launch_missing_ws_fill(pcaone_ctx* c, cudaStream_t st, const uint8_t* recT, int b0, int nw,
+                            const uint64_t* d_base) {
+  const uint64_t rows = (uint64_t)nw * c->Npad, threads = rows * 32;
+  k_fill_missing_rows<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+      recT, c->win.pitch, rows, c->win.pitch / 4, c->d_miss_ws_ptr + b0, c->d_miss_ws_idx, d_base + b0, c->Npad,
+      (uint32_t)c->win.bands);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+}
+
 // bands windows of blocksize SNPs; blocksize 0 = ceil(M / bands) (src/Halko.cpp:178), else the
 // blocks of the out-of-core plan (src/Data.cpp:56-71, bands = ceil(M / blocksize)).
 static WindowLayout make_layout(pcaone_ctx* c, int bands, uint64_t blocksize) {
@@ -336,8 +392,28 @@ static int64_t device_exclusive_scan(pcaone_ctx* c, const int64_t* cnt, uint64_t
   return total;
 }
 
+int64_t scan_counts(pcaone_ctx* c, const int64_t* cnt, uint64_t n, int64_t* ptr) {
+  return device_exclusive_scan(c, cnt, n, ptr);
+}
+
+// Row pointers of the by-SNP list from the non-missing counts, and its index array (sized).
+int64_t missing_snp_scan(pcaone_ctx* c) {
+  int64_t* d_cnt = (int64_t*)scratch(c, "miss_snp_cnt", c->M * 8);
+  k_missing_counts<<<(unsigned)((c->M + 255) / 256), 256, 0, c->stream>>>(c->d_nonmiss, c->M, c->N, d_cnt);
+  PG_CHECK_LAUNCH();
+  c->launches++;
+  c->d_miss_snp_ptr = (int64_t*)scratch(c, "d_miss_snp_ptr", (c->M + 1) * 8);
+  c->n_missing = device_exclusive_scan(c, d_cnt, c->M, c->d_miss_snp_ptr);
+  c->d_miss_snp_idx = (int32_t*)scratch(c, "d_miss_snp_idx", std::max<int64_t>(c->n_missing, 1) * 4);
+  return c->n_missing;
+}
+
 void build_missing_by_snp(pcaone_ctx* c) {
   if (c->miss_snp_valid) return;
+  if (c->streamed) {
+    stream_missing_snp(c);
+    return;
+  }
   int64_t* d_cnt = (int64_t*)scratch(c, "miss_snp_cnt", c->M * 8);
   k_missing_counts<<<(unsigned)((c->M + 255) / 256), 256, 0, c->stream>>>(c->d_nonmiss, c->M, c->N, d_cnt);
   PG_CHECK_LAUNCH();
@@ -354,6 +430,7 @@ void build_missing_by_snp(pcaone_ctx* c) {
 
 void build_missing_by_window_sample(pcaone_ctx* c) {
   if (c->miss_ws_valid) return;
+  require_resident(c, "the (window, sample) list outside an RSVD");
   PG_REQUIRE(c->bedT_valid, PCAONE_ESTATE, "transposed copy not built");
   const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
   int64_t* d_cnt = (int64_t*)scratch(c, "miss_ws_cnt", rows * 8);

@@ -696,6 +696,7 @@ TileGeom tile_geom(const pcaone_ctx* c) {
                   (bs + kChunk - 1) / kChunk};
 }
 void ensure_tiles(pcaone_ctx* c) {
+  if (c->streamed) return;  // the window run's tiles are built in its device slot
   PG_REQUIRE(c->bedT_valid, PCAONE_ESTATE, "transposed copy not built");
   const uint64_t key = (c->generation << 24) ^ ((uint64_t)c->win.bands << 44) ^ (uint64_t)c->win.blocksize;
   const TileGeom g = tile_geom(c);
@@ -719,6 +720,20 @@ void ensure_tiles(pcaone_ctx* c) {
   c->tiles8_valid = true;
   c->tile81_ptr = d1;
   c->tile82_ptr = d2;
+}
+
+// Tiles of windows [b0, b1) for the first (which = 1) or the second product: the resident
+// tiled copies, or the current slot of streamed genotypes (which must hold the windows).
+const uint8_t* tiles_of(pcaone_ctx* c, int which, int64_t b0, int64_t b1) {
+  const TileGeom g = tile_geom(c);
+  const size_t w = which == 1 ? (size_t)g.p1 * g.c1 * kPairChunkBytes : (size_t)g.p2 * g.c2 * kPairChunkBytes;
+  if (c->streamed) {
+    PG_REQUIRE(c->cur_slot >= 0, PCAONE_ESTATE, "no window slot staged");
+    const auto& S = c->slot[c->cur_slot];
+    PG_REQUIRE(S.t1 && b0 >= S.b0 && b1 <= S.b1, PCAONE_ESTATE, "windows not in the staged slot");
+    return (which == 1 ? S.t1 : S.t2) + (size_t)(b0 - S.b0) * w;
+  }
+  return (const uint8_t*)(which == 1 ? c->tile81_ptr : c->tile82_ptr) + (size_t)b0 * w;
 }
 
 // Quantise a row-major operand of kpad rows x l into the chunked piece layout (kpad / 128
@@ -778,7 +793,7 @@ void i8_p1(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t row_off, int64_t row
   const int np = np_of(l);
   auto* bq = (const int8_t*)scratch(c, "i8_bq1", (size_t)c->Npad * np);
   auto* sig = (const float*)scratch(c, "i8_sig1", 3 * 64 * sizeof(float));
-  run_i8(c, (const uint8_t*)c->tile81_ptr + (size_t)b * g.p1 * g.c1 * kPairChunkBytes, g.c1, rows, K, bq, sig,
+  run_i8(c, tiles_of(c, 1, b, b + 1), g.c1, rows, K, bq, sig,
          c->Npad, l, ks, out);
 }
 
@@ -791,7 +806,7 @@ void i8_p2(pcaone_ctx* c, const uint8_t*, uint32_t, int64_t window, int64_t rows
   const int np = np_of(l);
   auto* bq = (const int8_t*)scratch(c, "i8_bq2", (size_t)kpad * np);
   auto* sig = (const float*)scratch(c, "i8_sig2", 3 * 64 * sizeof(float));
-  run_i8(c, (const uint8_t*)c->tile82_ptr + (size_t)window * g.p2 * g.c2 * kPairChunkBytes, g.c2, rows, K, bq, sig,
+  run_i8(c, tiles_of(c, 2, window, window + 1), g.c2, rows, K, bq, sig,
          kpad, l, ks, out);
 }
 
@@ -815,7 +830,7 @@ void i8_p1_seg(pcaone_ctx* c, int b0, int b1, const float*, int l, int ks, float
   const int np = np_of(l);
   auto* bq = (const int8_t*)scratch(c, "i8_bq1", (size_t)c->Npad * np);
   auto* sig = (const float*)scratch(c, "i8_sig1", 3 * 64 * sizeof(float));
-  run_i8(c, (const uint8_t*)c->tile81_ptr + (size_t)b0 * g.p1 * g.c1 * kPairChunkBytes, g.c1,
+  run_i8(c, tiles_of(c, 1, b0, b1), g.c1,
          (int64_t)(b1 - b0) * g.p1 * 2 * kRows, (int64_t)c->N, bq, sig, c->Npad, l, ks, out);
 }
 
@@ -836,11 +851,28 @@ void i8_p2_seg(pcaone_ctx* c, int b0, int b1, const float*, int l, int ks, float
   const int np = np_of(l);
   auto* bq = (const int8_t*)scratch(c, "i8_bq2", (size_t)kpad * np);
   auto* sig = (const float*)scratch(c, "i8_sig2", 3 * 64 * sizeof(float));
-  run_i8(c, (const uint8_t*)c->tile82_ptr + (size_t)b0 * g.p2 * g.c2 * kPairChunkBytes, g.c2, (int64_t)c->N, kpad,
+  run_i8(c, tiles_of(c, 2, b0, b1), g.c2, (int64_t)c->N, kpad,
          bq, sig, kpad, l, ks, out, g.c2, g.p2 * g.c2 * kPairChunkBytes);
 }
 
 }  // namespace
+
+void i8_tile_bytes(const pcaone_ctx* c, size_t* w1, size_t* w2) {
+  const TileGeom g = tile_geom(c);
+  *w1 = (size_t)g.p1 * g.c1 * kPairChunkBytes;
+  *w2 = (size_t)g.p2 * g.c2 * kPairChunkBytes;
+}
+
+void i8_tile_window(pcaone_ctx* c, cudaStream_t st, const uint8_t* rec, int64_t m, const uint8_t* recT, uint8_t* t1,
+                    uint8_t* t2) {
+  const TileGeom g = tile_geom(c);
+  const int64_t n1 = g.p1 * 2 * kRows * 2 * g.c1, n2 = g.p2 * 2 * kRows * 2 * g.c2;
+  k_tile_codes_i8<<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(rec, c->pitch, m, g.p1, g.c1, t1);
+  PG_CHECK_LAUNCH();
+  k_tile_codes_i8<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(recT, c->win.pitch, (int64_t)c->N, g.p2, g.c2, t2);
+  PG_CHECK_LAUNCH();
+  c->launches += 2;
+}
 
 GemmFnT<float> gemm_i8() {
   GemmFnT<float> f{i8_ksplit, i8_p1, i8_p2, i8_omega, i8_b2, nullptr, nullptr, i8_b2_qmax};

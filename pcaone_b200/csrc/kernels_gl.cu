@@ -12,11 +12,11 @@
 // Layout: GL pairs are SNP-major floats, P[j][2i + {0,1}] (the reference's 2N x M column-major
 // P); E is SNP-major floats E[j][i] with rows padded to Npad samples (zeros beyond N).
 // Posterior arithmetic is FP64 in registers.
-#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -58,38 +58,62 @@ __global__ void k_em_maf(const double* __restrict__ P, uint64_t M, uint32_t N, u
 }
 
 // E_ij = E[g | likelihoods, pt_ij] - 2 F_j for SNP rows (fit_with_pi, src/Data.cpp:249-270);
-// warp per SNP, lanes over samples (the likelihood pair of a sample read as one double2). The
-// standardised E of the GRM stage is k_grm_e. US: N x k (U diag S) row-major, V: M x k
-// row-major (row j = the loading used for SNP j); KM >= k is a compile-time bound, so the
-// loading stays in registers.
+// the standardised E of the GRM stage is k_grm_e. Thread per sample: the sample's row of
+// US (U diag S, N x k row-major) stays in registers (KM >= k is a compile-time bound) and the
+// thread walks the sites of its CTA's slice; the loading row V[j] (M x k row-major) and F_j
+// are the same for every thread of the CTA (broadcast loads), the likelihood pair (one
+// double2) and the E entry are coalesced over the samples. Each sample-site is one 16-byte
+// read and one 4-byte write, four sites in flight per thread.
 template <int KM>
-__global__ void __launch_bounds__(256) k_posterior_e(const double* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
+__global__ void __launch_bounds__(128) k_posterior_e(const double* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
                                                      const double* __restrict__ F, const double* __restrict__ US,
                                                      const double* __restrict__ V, int k, float* __restrict__ E,
                                                      uint32_t lde) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (uint64_t j = (uint64_t)blockIdx.x * nwarps + warp; j < M; j += (uint64_t)gridDim.x * nwarps) {
-    const double f = F[j];
-    double v[KM];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint64_t per = (M + gridDim.y - 1) / gridDim.y;
+  const uint64_t ja = (uint64_t)blockIdx.y * per, jb = ja + per < M ? ja + per : M;
+  double us[KM];
 #pragma unroll
-    for (int t = 0; t < KM; ++t) v[t] = (V && t < k) ? V[j * k + t] : 0.0;
-    const double2* row = reinterpret_cast<const double2*>(P + j * ldp);
-    for (uint32_t i = lane; i < N; i += 32) {
+  for (int t = 0; t < KM; ++t) us[t] = (V && t < k) ? US[(uint64_t)i * k + t] : 0.0;
+  constexpr int U4 = 4;
+  uint64_t j = ja;
+  for (; j + U4 <= jb; j += U4) {
+    double2 gl[U4];
+#pragma unroll
+    for (int u = 0; u < U4; ++u) gl[u] = __ldcs(reinterpret_cast<const double2*>(P + (j + u) * ldp) + i);
+#pragma unroll
+    for (int u = 0; u < U4; ++u) {
+      const double f = __ldg(F + j + u);
       double pt = f;
       if (V) {
         double pred = 0.0;
-        const double* us = US + (uint64_t)i * k;
+        const double* v = V + (j + u) * k;
 #pragma unroll
         for (int t = 0; t < KM; ++t)
-          if (t < k) pred += __ldg(us + t) * v[t];
+          if (t < k) pred += us[t] * __ldg(v + t);
         pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
       }
-      const double2 gl = __ldg(row + i);
       double p0, p1, p2;
-      posterior(gl.x, gl.y, pt, p0, p1, p2);
-      const double s = p0 + p1 + p2;
-      E[j * lde + i] = (float)((p1 + 2.0 * p2) / s - 2.0 * f);
+      posterior(gl[u].x, gl[u].y, pt, p0, p1, p2);
+      __stcs(E + (j + u) * lde + i, (float)((p1 + 2.0 * p2) / (p0 + p1 + p2) - 2.0 * f));
     }
+  }
+  for (; j < jb; ++j) {
+    const double2 gl = __ldcs(reinterpret_cast<const double2*>(P + j * ldp) + i);
+    const double f = __ldg(F + j);
+    double pt = f;
+    if (V) {
+      double pred = 0.0;
+      const double* v = V + j * k;
+#pragma unroll
+      for (int t = 0; t < KM; ++t)
+        if (t < k) pred += us[t] * __ldg(v + t);
+      pt = fmin(fmax((pred + 2.0 * f) / 2.0, 1e-4), 1.0 - 1e-4);
+    }
+    double p0, p1, p2;
+    posterior(gl.x, gl.y, pt, p0, p1, p2);
+    __stcs(E + j * lde + i, (float)((p1 + 2.0 * p2) / (p0 + p1 + p2) - 2.0 * f));
   }
 }
 
@@ -469,6 +493,98 @@ __global__ void k_grm_finish(const double* __restrict__ L, const double* __restr
   }
 }
 
+// Lower-triangular tiles of L = E E^T (N x N, column-major, ld N) over the sites of one
+// chunk of the standardised posterior matrix (E: site-major, column j = site j, ld lde): the
+// O(N^2 M) product of the GRM (src/Halko.cpp:320, G G^T). One CTA per 128 x 128 tile (I, J)
+// with I >= J, 256 threads, each owning an 8 x 8 block (rows 4 ty + {0..3} and 64 + 4 ty +
+// {0..3}, columns likewise from tx) accumulated in FP64 registers, site by site in order, so
+// the result is deterministic. The two 128-row panels of 16 sites stream through a
+// three-stage ring of 16-byte asynchronous copies (zero-filled past N and past the chunk).
+// accumulate: add to L (later chunks) instead of overwriting it.
+constexpr int kSyrkT = 128, kSyrkKC = 16, kSyrkStages = 3;
+constexpr size_t kSyrkSmem = (size_t)kSyrkStages * 2 * kSyrkKC * kSyrkT * sizeof(double);
+
+__device__ __forceinline__ void cp_async16_zfill(double* sdst, const double* gsrc, int bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) k_syrk_lower(const double* __restrict__ E, uint32_t lde, uint32_t N,
+                                                       uint64_t mc, double* __restrict__ L, int accumulate) {
+  extern __shared__ __align__(16) double smem_syrk[];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const uint32_t t = blockIdx.x;
+  uint32_t I = (uint32_t)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((I + 1) * (I + 2) / 2 <= t) ++I;
+  while (I * (I + 1) / 2 > t) --I;
+  const uint32_t J = t - I * (I + 1) / 2;
+  const uint32_t r0 = I * kSyrkT, c0 = J * kSyrkT;
+  const int64_t nk = (int64_t)((mc + kSyrkKC - 1) / kSyrkKC);
+  auto issue = [&](int64_t kc, int stage) {
+    double* a = smem_syrk + (size_t)stage * 2 * kSyrkKC * kSyrkT;
+    double* b = a + kSyrkKC * kSyrkT;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + 256 * u;  // 1024 16-byte pieces per panel: site kk, rows p, p + 1
+      const int kk = e >> 6, p = (e & 63) * 2;
+      const uint64_t site = (uint64_t)kc * kSyrkKC + kk;
+      const bool in = site < mc;
+      const uint32_t ra = r0 + p, rb = c0 + p;
+      const int ba = in && ra < N ? (int)min(16u, (N - ra) * 8u) : 0;
+      const int bb = in && rb < N ? (int)min(16u, (N - rb) * 8u) : 0;
+      cp_async16_zfill(a + kk * kSyrkT + p, ba ? E + site * lde + ra : E, ba);
+      cp_async16_zfill(b + kk * kSyrkT + p, bb ? E + site * lde + rb : E, bb);
+    }
+  };
+  double acc[8][8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[q][c] = 0.0;
+#pragma unroll
+  for (int st = 0; st < kSyrkStages - 1; ++st) {
+    if (st < nk) issue(st, st);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int64_t kc = 0; kc < nk; ++kc) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kSyrkStages - 2) : "memory");
+    __syncthreads();  // stage kc landed for every thread; stage kc - 1 is no longer read
+    if (kc + kSyrkStages - 1 < nk) issue(kc + kSyrkStages - 1, (int)((kc + kSyrkStages - 1) % kSyrkStages));
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const double* a = smem_syrk + (size_t)(kc % kSyrkStages) * 2 * kSyrkKC * kSyrkT;
+    const double* b = a + kSyrkKC * kSyrkT;
+#pragma unroll 4
+    for (int kk = 0; kk < kSyrkKC; ++kk) {
+      double av[8], bv[8];
+      const double2* ap = reinterpret_cast<const double2*>(a + kk * kSyrkT);
+      const double2* bp = reinterpret_cast<const double2*>(b + kk * kSyrkT);
+      const double2 a0 = ap[2 * ty], a1 = ap[2 * ty + 1], a2 = ap[32 + 2 * ty], a3 = ap[33 + 2 * ty];
+      const double2 b0 = bp[2 * tx], b1 = bp[2 * tx + 1], b2 = bp[32 + 2 * tx], b3 = bp[33 + 2 * tx];
+      av[0] = a0.x; av[1] = a0.y; av[2] = a1.x; av[3] = a1.y;
+      av[4] = a2.x; av[5] = a2.y; av[6] = a3.x; av[7] = a3.y;
+      bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
+      bv[4] = b2.x; bv[5] = b2.y; bv[6] = b3.x; bv[7] = b3.y;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[q][c] = fma(av[q], bv[c], acc[q][c]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const uint32_t col = c0 + (c < 4 ? 4 * tx + c : 64 + 4 * tx + c - 4);
+    if (col >= N) continue;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t row = r0 + (q < 4 ? 4 * ty + q : 64 + 4 * ty + q - 4);
+      if (row >= N) continue;
+      double* dst = L + (uint64_t)col * N + row;
+      *dst = accumulate ? *dst + acc[q][c] : acc[q][c];
+    }
+  }
+}
+
 }  // namespace
 
 GemmFnT<float> gemm_dense_float() {
@@ -544,17 +660,20 @@ void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {
 }
 
 void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
-  const int threads = 256, nwarps = threads / 32;
-  int nblk = (int)std::min<uint64_t>(8 * c->sm_count, (c->M + nwarps - 1) / nwarps);
   PG_REQUIRE(k <= kLmax, PCAONE_EBADARG, "too many factors for the posterior");
+  // grid: sample blocks of 128 x site slices, about eight CTAs an SM
+  const unsigned bx = (c->N + 127) / 128;
+  const uint64_t want = (8ull * c->sm_count + bx - 1) / bx;
+  const unsigned by = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (c->M + 63) / 64));
+  const dim3 grid(bx, by);
   if (k <= 8)
-    k_posterior_e<8><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+    k_posterior_e<8><<<grid, 128, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   else if (k <= 16)
-    k_posterior_e<16><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+    k_posterior_e<16><<<grid, 128, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   else if (k <= 32)
-    k_posterior_e<32><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+    k_posterior_e<32><<<grid, 128, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   else
-    k_posterior_e<64><<<nblk, threads, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
+    k_posterior_e<64><<<grid, 128, 0, c->stream>>>(c->d_P, c->M, c->N, 2 * c->N, c->d_F, US, V, k, c->d_E, c->Npad);
   PG_CHECK_LAUNCH();
   c->launches++;
 }
@@ -568,16 +687,13 @@ void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
 void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, double* evecs, double* svals) {
   const uint32_t N = c->N;
   const uint64_t M = c->M;
-  if (!c->blas) {
-    cublasHandle_t h = nullptr;
-    PG_BLAS(cublasCreate(&h));
-    c->blas = h;
-  }
-  cublasHandle_t blas = (cublasHandle_t)c->blas;
-  PG_BLAS(cublasSetStream(blas, c->stream));
+  const uint32_t ntile = (N + kSyrkT - 1) / kSyrkT;
+  PG_CUDA(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkSmem));
   // E in chunks of sites: at most 2^27 doubles (1 GiB) a chunk
   const uint32_t lde = c->Npad;
-  const uint64_t mc_max = std::max<uint64_t>(1, std::min<uint64_t>(M, (1ull << 27) / lde));
+  uint64_t mc_max = std::max<uint64_t>(1, std::min<uint64_t>(M, (1ull << 27) / lde));
+  if (const char* pin = std::getenv("PCAONE_GRM_CHUNK_SITES"))  // smaller chunks, for tests
+    mc_max = std::max<uint64_t>(1, std::min<uint64_t>(mc_max, std::strtoull(pin, nullptr, 10)));
   const int nsl = (int)std::max<uint64_t>(1, std::min<uint64_t>(64, (4ull * c->sm_count * 128 + N - 1) / N));
   double* E = (double*)scratch(c, "grm_E", (size_t)mc_max * lde * 8);
   double* dpart = (double*)scratch(c, "grm_dpart", (size_t)nsl * N * 8);
@@ -590,9 +706,9 @@ void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, 
                                                               dpart);
     PG_CHECK_LAUNCH();
     c->launches++;
-    const double one = 1.0, beta = j0 == 0 ? 0.0 : 1.0;
-    PG_BLAS(cublasDsyrk(blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)N, (int)mc, &one, E, (int)lde, &beta, L,
-                        (int)N));
+    k_syrk_lower<<<ntile * (ntile + 1) / 2, 256, kSyrkSmem, c->stream>>>(E, lde, N, mc, L, j0 == 0 ? 0 : 1);
+    PG_CHECK_LAUNCH();
+    c->launches++;
   }
   const uint64_t n2 = (uint64_t)N * N;
   k_grm_finish<<<(unsigned)std::min<uint64_t>(8ull * c->sm_count, (n2 + 255) / 256), 256, 0, c->stream>>>(
@@ -638,9 +754,7 @@ void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, 
 }
 
 void gl_release(pcaone_ctx* c) {
-  if (c->blas) cublasDestroy((cublasHandle_t)c->blas);
   if (c->solver) cusolverDnDestroy((cusolverDnHandle_t)c->solver);
-  c->blas = nullptr;
   c->solver = nullptr;
 }
 

@@ -140,6 +140,7 @@ extern "C" int pcaone_gpu_product_t_noalloc(pcaone_ctx* c, int standardize, int 
   if (!c) return PCAONE_EBADARG;
   try {
     PG_CUDA(cudaSetDevice(c->device));
+    pg::require_resident(c, "the allocation-free product");
     pg::product_t_noalloc(c, standardize, ploidy, d_B, (int)ncols, d_out);
     c->err.clear();
     return PCAONE_OK;

@@ -221,7 +221,7 @@ struct Engine {
     // product 1: D1 = R_b^T Omega
     int ks1 = gemm.ksplit(c, m, N, l);
     T* D1 = (T*)scratch(c, "r_D1", (size_t)ks1 * m * l * sizeof(T));
-    const uint8_t* codes = c->dense ? nullptr : c->d_bed + s * (int64_t)c->pitch;
+    const uint8_t* codes = c->dense ? nullptr : c->streamed ? stream_codes(c, b) : c->d_bed + s * (int64_t)c->pitch;
     timed([&] { gemm.p1(c, codes, c->pitch, s, m, N, OmgT, l, ks1, D1); });
     EpiP1 p1;
     p1.start = s;
@@ -253,7 +253,9 @@ struct Engine {
     // product 2: D2 = R_b B2
     int ks2 = gemm.ksplit(c, N, m, l);
     T* D2 = (T*)scratch(c, "r_D2", (size_t)ks2 * N * l * sizeof(T));
-    const uint8_t* codesT = c->dense ? nullptr : c->d_bedT + (int64_t)b * Npad * c->win.pitch;
+    const uint8_t* codesT = c->dense      ? nullptr
+                            : c->streamed ? stream_codesT(c, b)
+                                          : c->d_bedT + (int64_t)b * Npad * c->win.pitch;
     timed([&] { gemm.p2(c, codesT, c->win.pitch, b, N, m, B2, l, ks2, D2); });
     EpiP2 p2;
     p2.b0 = b;
@@ -347,6 +349,22 @@ struct Engine {
   // when the back end batches windows, else one window at a time.
   static constexpr int64_t kRunRows = int64_t(1) << 22;
   void process_windows(int b0, int b1, double* Ht) {
+    if (c->streamed) {  // by device slots: the windows of one slot, while the next is filled
+      const bool tiles = o.precision == PCAONE_PREC_MIXED;
+      for (int b = b0; b < b1;) {
+        const int held = stream_acquire(c, b, tiles), e = std::min(b1, held);
+        stream_prefetch(c, held, tiles);
+        if (gemm.p1_seg) {
+          const int per = (int)std::max<int64_t>(1, kRunRows / gemm.seg_rows1(c));
+          for (int r = b; r < e; r += per) process_run(r, std::min(e, r + per), Ht);
+        } else {
+          for (int r = b; r < e; ++r) process_window(r, Ht);
+        }
+        stream_release(c);
+        b = e;
+      }
+      return;
+    }
     if (!gemm.p1_seg) {
       for (int b = b0; b < b1; ++b) process_window(b, Ht);
       return;
@@ -428,7 +446,7 @@ struct Engine {
   bool graphs_on() const {
     static const bool disabled = std::getenv("PCAONE_NO_GRAPHS") != nullptr;
     return !disabled && !graphs_failed && !o.profile &&
-           (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) && !c->dense;
+           (o.precision == PCAONE_PREC_MIXED || o.precision == PCAONE_PREC_BF16) && !c->dense && !c->streamed;
   }
   bool steady_epoch(int pi) const {
     return o.svd == 1 ? pi >= 2 : (std::pow(2.0, pi) >= o.bands && o.block_snps == 0);
@@ -499,7 +517,7 @@ struct Engine {
       updates++;
     }
     zero(c, H, Npad * l);
-    process_windows(0, 1, H);
+    process_windows(0, c->win.bands, H);  // one window, or the blocks of streamed genotypes
   }
 
   // The in-core schedule runs over the o.bands windows; with the out-of-core block plan the
@@ -925,8 +943,17 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
   // the out-of-core block plan changes only the winSVD windows; Halko's result does not depend
   // on the blocks
   const bool blocks = o.svd == 2 && o.block_snps > 0;
-  const int bands = o.svd == 1 ? 1 : (blocks ? (int)((c->M + o.block_snps - 1) / o.block_snps) : o.bands);
-  const uint64_t blocksize = blocks ? (uint64_t)o.block_snps : 0;
+  int bands = o.svd == 1 ? 1 : (blocks ? (int)((c->M + o.block_snps - 1) / o.block_snps) : o.bands);
+  uint64_t blocksize = blocks ? (uint64_t)o.block_snps : 0;
+  if (c->streamed && o.svd == 1) {
+    // Halko on streamed genotypes sums the product over blocks: those of the out-of-core plan
+    // when given, else blocks whose slot contents (records, transposed copy, tiles: about
+    // four bytes per SNP per packed byte) fit the slot budget
+    blocksize = o.block_snps > 0 ? (uint64_t)o.block_snps
+                                 : std::max<uint64_t>(kRowPad, c->slot_budget / (4ull * c->pitch) / kRowPad * kRowPad);
+    blocksize = std::min<uint64_t>(blocksize, c->M);
+    bands = (int)((c->M + blocksize - 1) / blocksize);
+  }
   if (c->dense) {
     // dense posterior matrix: already centred and not standardised in the EM steps; the
     // epilogues see F = 0 and s = 2 so that G = E^T Omega and B2 = G exactly
@@ -936,6 +963,12 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
     PG_CUDA(cudaMemcpyAsync(c->d_scale, two.data(), c->M * 8, cudaMemcpyHostToDevice, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
     PG_REQUIRE(o.precision != PCAONE_PREC_FP64, PCAONE_EBADARG, "the PCAngsd matrix is FP32");
+  } else if (c->streamed) {
+    PG_REQUIRE(o.precision != PCAONE_PREC_BF16, PCAONE_EBADARG,
+               "the split-BF16 back end needs the genotypes resident on the device");
+    stream_prepare(c, bands, blocksize, o.precision == PCAONE_PREC_MIXED);
+    if (c->imputed) compute_imputed_ws(c);
+    compute_scale(c, o.standardize, o.ploidy);
   } else {
     build_transposed(c, bands, blocksize);
     build_missing_by_snp(c);

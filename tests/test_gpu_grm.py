@@ -47,6 +47,29 @@ def test_gl_grm_matches_oracle_and_repeats(gpu):
     np.testing.assert_array_equal(sv, sv2)
 
 
+def test_gl_grm_multi_tile_and_chunks_match_oracle(gpu, monkeypatch):
+    """An odd sample count over several 128 x 128 tiles of the SYRK kernel (zero-filled past
+    N) and the sites in chunks with a ragged last chunk (accumulated into the same lower
+    triangle): synthetic normalised likelihoods, FP64 against the oracle."""
+    rng = np.random.default_rng(11)
+    N, M, k = 389, 1000, 4
+    g = rng.dirichlet(np.ones(3) * 0.7, size=(M, N))  # per sample-site likelihood triple
+    P = np.empty((2 * N, M))
+    P[0::2, :] = g[:, :, 0].T
+    P[1::2, :] = g[:, :, 1].T
+    monkeypatch.setenv("PCAONE_GRM_CHUNK_SITES", "333")
+    gpu.load_gl(P)
+    F, _ = gpu.gl_freq(30, 1e-6)
+    U = np.linalg.qr(rng.standard_normal((N, k)))[0]
+    V = np.linalg.qr(rng.standard_normal((M, k)))[0]
+    S = np.array([30.0, 20.0, 10.0, 5.0])
+    C, _, sv = gpu.gl_grm(U, S, V)
+    Co = grm_oracle(P, F, U, S, V)
+    np.testing.assert_allclose(C, Co, rtol=1e-10, atol=1e-13)
+    np.testing.assert_array_equal(C, C.T)
+    np.testing.assert_allclose(sv, np.sort(np.abs(np.linalg.eigvalsh(Co)))[::-1], rtol=1e-9, atol=1e-12)
+
+
 def test_gl_grm_rejects_missing_factors(gpu):
     P, N, M = O.parse_beagle(BEAGLE)
     gpu.load_gl(P)

@@ -503,6 +503,8 @@ def run_rsvd_cfg(args, cfg, run):
            "h2d_bytes_per_step": int(bed_bytes + (perm.nbytes if perm is not None else 0)),
            "d2h_bytes_per_step": int((N + M + 1) * cfg["k"] * 8), "seconds_per_pca": round(e2e_s, 4)}
     launches = int(res[-1].kernel_launches)
+    if cfg["svd"] == 2 and not args.skip_compare:
+        extra["streamed"] = streamed_rsvd(ctx, packed, N, perm, prec, rs_kw, bed_bytes, res[-1])
     ctx.close()
     cpu = cpu_baseline(args, cfg, prefix, wd, run)
     run.close()
@@ -512,6 +514,28 @@ def run_rsvd_cfg(args, cfg, run):
          {"samples": N, "snps": M, "k": cfg["k"], "oversamples": max(10, cfg["k"]),
           "windows": cfg["bands"] if cfg["svd"] == 2 else 1, "svd": cfg["svd"], "epochs": epochs},
          dict(extra, pca_seconds=round(ms_per_step / 1e3, 5), accuracy=acc))
+
+
+def streamed_rsvd(ctx, packed, N, perm, prec, rs_kw, bed_bytes, resident):
+    """The same PCA with the genotypes in pinned host memory (pcaone_gpu_load_bed_host, the
+    out-of-core mode): every epoch copies the windows into two 1 GiB device slots over PCIe
+    while the other slot's products run. Device time per PCA, the H2D bytes it moved and their
+    rate, and the eigenvalue difference to the resident run."""
+    ctx.load_bed_host(packed, N)
+    if perm is not None:
+        ctx.permute(perm)
+    for _ in range(2):
+        ctx.rsvd(precision=prec, **rs_kw)
+    rs = [ctx.rsvd(precision=prec, **rs_kw) for _ in range(3)]
+    ms = sum(r.gpu_ms for r in rs) / len(rs)
+    h2d = int(rs[-1].h2d_bytes)
+    out = {"ms_per_pca": round(ms, 2), "epochs": rs[-1].epochs, "h2d_bytes_per_pca": h2d,
+           "h2d_gbs": round(h2d / (ms / 1e3) / 1e9, 2),
+           "value_bed_gbs": round(bed_bytes * rs[-1].epochs / (ms / 1e3) / 1e9, 3),
+           "eig_rel_err_vs_resident": float(np.max(np.abs(rs[-1].S ** 2 / resident.S ** 2 - 1))),
+           "slots": "2 x 1 GiB (records, sample-major copy, int8 tiles of the windows they hold)"}
+    log(f"streamed: {out}")
+    return out
 
 
 def run_emu_cfg(args, cfg, run):

@@ -145,6 +145,8 @@ typedef struct {
   double tail_ms;        /* with opts.profile: per-epoch QR of G, B, small SVD, mev */
   double host_ms;        /* with opts.profile: device idle while the host runs the epoch tail's
                             small SVD and convergence test */
+  uint64_t h2d_bytes;    /* streamed genotypes (pcaone_gpu_load_bed_host): record bytes copied
+                            to the device slots by the call; 0 when resident */
 } pcaone_rsvd_report;
 
 /* Run Halko (svd=1) or window-based (svd=2) RSVD on the loaded genotypes: the epoch loop of

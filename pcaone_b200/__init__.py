@@ -32,7 +32,7 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
            "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
            "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm",
-           "pcaone_gpu_ld_r2_f64", "pcaone_gpu_ld_timing"]
+           "pcaone_gpu_ld_r2_f64", "pcaone_gpu_ld_timing", "pcaone_gpu_load_bed_host"]
 
 
 class PcaoneError(RuntimeError):
@@ -57,7 +57,7 @@ class RsvdReport(ctypes.Structure):
                 ("gemm_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64),
                 ("gemm_launches", ctypes.c_int64), ("epilogue_ms", ctypes.c_double),
                 ("update_ms", ctypes.c_double), ("tail_ms", ctypes.c_double),
-                ("host_ms", ctypes.c_double)]
+                ("host_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64)]
 
 
 _lib = None
@@ -91,6 +91,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_ld_r2_f64.argtypes = [vp, vp, u32, vp, vp, u64, vp]
         L.pcaone_gpu_ld_timing.argtypes = [vp, vp, vp]
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
+        L.pcaone_gpu_load_bed_host.argtypes = [vp, vp, u64, u32, u64]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
         L.pcaone_gpu_load_gl_f32.argtypes = [vp, vp, u64, u32]
@@ -168,6 +169,7 @@ class RsvdResult:
     update_ms: float = 0.0
     tail_ms: float = 0.0
     host_ms: float = 0.0
+    h2d_bytes: int = 0
 
 
 class GpuContext:
@@ -212,6 +214,17 @@ class GpuContext:
         self._check(lib().pcaone_gpu_load_bed(self._h, _ptr(packed), M, nsamples))
         self.N, self.M = nsamples, M
 
+    def load_bed_host(self, packed: np.ndarray, nsamples: int, slot_bytes: int = 0):
+        """The same records kept in (pinned) host memory and streamed to the device by runs of
+        windows during rsvd (pcaone_gpu_load_bed_host); slot_bytes: device bytes per slot
+        (0: 1 GiB)."""
+        packed = np.ascontiguousarray(packed, dtype=np.uint8)
+        M = packed.shape[0]
+        if packed.ndim != 2 or packed.shape[1] != (nsamples + 3) // 4:
+            raise ValueError("packed must be (nsnps, ceil(nsamples/4)) bytes")
+        self._check(lib().pcaone_gpu_load_bed_host(self._h, _ptr(packed), M, nsamples, int(slot_bytes)))
+        self.N, self.M = nsamples, M
+
     def counts(self):
         a = np.zeros(self.M, dtype=np.uint32)
         c = np.zeros(self.M, dtype=np.uint32)
@@ -246,7 +259,7 @@ class GpuContext:
         return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
                           rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
                           rep.kernel_launches, rep.gemm_launches, rep.epilogue_ms,
-                          rep.update_ms, rep.tail_ms, rep.host_ms)
+                          rep.update_ms, rep.tail_ms, rep.host_ms, rep.h2d_bytes)
 
 
 def _product(ctx: "GpuContext", B: np.ndarray, transpose: int, precision, standardize, ploidy):

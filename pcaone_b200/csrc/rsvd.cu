@@ -978,6 +978,7 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
   }
   c->gemm_ms_accum = 0.0;
   const int64_t l0 = c->launches, g0 = c->gemm_launches;
+  const uint64_t h2d0 = c->streamed_h2d;
   PG_CUDA(cudaEventRecord(c->ev0, c->stream));
   if (c->dense) {
     Engine<float> e(c, o, gemm_dense_float());
@@ -1006,6 +1007,7 @@ void run_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts& o, double* U, double* S, do
     rep->gemm_ms = c->gemm_ms_accum;
     rep->kernel_launches = c->launches - l0;
     rep->gemm_launches = c->gemm_launches - g0;
+    rep->h2d_bytes = c->streamed_h2d - h2d0;
   }
 }
 

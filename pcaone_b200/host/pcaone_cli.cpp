@@ -243,9 +243,10 @@ Params parse(int argc, char** argv) {
     p.maf = 1 - p.maf;
   }
   p.oversamples = std::max(p.oversamples, p.k);  // src/Cmd.cpp:190
-  // -m/--memory: the reference's out-of-core mode. The packed genotypes stay in device memory;
-  // what -m changes in the results (the permute_plink SNP order and the block-granular winSVD
-  // windows) is reproduced. The reference's own restrictions apply (src/Cmd.cpp:201-212).
+  // -m/--memory: the reference's out-of-core mode. The packed genotypes stay in host memory and
+  // the RSVD streams them to the device by blocks (pcaone_gpu_load_bed_host); what -m changes
+  // in the results (the permute_plink SNP order and the block-granular winSVD windows) is
+  // reproduced. The reference's own restrictions apply (src/Cmd.cpp:201-212).
   if (p.memory > 0 && p.maf > 0) fail("does not support --maf filters for out-of-core mode yet! ");
   if (p.memory > 0 && (p.emu || p.pcangsd || p.bfile.empty()))
     fail("-m/--memory applies to a plain PCA of PLINK input in this build");
@@ -966,7 +967,14 @@ int main(int argc, char** argv) {
 
   pcaone_ctx* ctx = nullptr;
   if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
-  check(ctx, pcaone_gpu_load_bed(ctx, packed.data(), M0, (uint32_t)N), "load_bed");
+  // out-of-core RSVD (-m with -d 1 or 2): the genotypes are streamed from host memory; the
+  // IRAM products, LD and the residual writer read them resident
+  const bool ld_mode = p.print_r2 || p.ld_r2 > 0 || !p.clump.empty();
+  const bool streamed = p.memory > 0 && p.svd != 0 && !p.ld_write && !ld_mode;
+  if (streamed)
+    check(ctx, pcaone_gpu_load_bed_host(ctx, packed.data(), M0, (uint32_t)N, 0), "load_bed_host");
+  else
+    check(ctx, pcaone_gpu_load_bed(ctx, packed.data(), M0, (uint32_t)N), "load_bed");
   std::vector<double> F(M0);
   check(ctx, pcaone_gpu_allele_freq(ctx, F.data()), "allele_freq");
   for (size_t j = 0; j < M0; ++j)
@@ -997,7 +1005,7 @@ int main(int argc, char** argv) {
   }
   g_log.print(date(), "done reading all data");
 
-  if (p.print_r2 || p.ld_r2 > 0 || !p.clump.empty()) {  // LD mode (src/Main.cpp:64-77)
+  if (ld_mode) {  // LD mode (src/Main.cpp:64-77)
     if (p.fileU.empty()) fail("LD from PLINK input needs --read-U (flow A)");
     g_log.print(date(), "run LD stuff");
     run_ld(p, ctx, N, M, false);
@@ -1068,8 +1076,8 @@ int main(int argc, char** argv) {
     check(ctx, pcaone_gpu_permute(ctx, perm.data()), "permute");
   }
   if (p.svd != 0)
-    g_log.print(date(), p.svd == 2 ? "initialize window-based RSVD (winSVD) with in-core"
-                                   : "initialize single-pass RSVD (sSVD) with in-core");
+    g_log.print(date(), p.svd == 2 ? "initialize window-based RSVD (winSVD) with" : "initialize single-pass RSVD (sSVD) with",
+                streamed ? "out-of-core" : "in-core");
   pcaone_rsvd_opts o{};
   o.k = (int)p.k;
   o.oversamples = (int)p.oversamples;

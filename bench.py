@@ -884,6 +884,22 @@ def run_profile_kernel(args, cfg):
 
     prefix = os.path.join(workdir(), args.config)
     make_data(cfg, prefix)
+    if cfg["kind"] == "pcangsd":  # posterior, dense products and GRM on the first 40000 sites
+        N, m, k = cfg["n"], 40000, cfg["k"]
+        P = np.fromfile(prefix + ".gl.f32", dtype=np.float32, count=m * 2 * N).reshape(m, 2 * N)
+        kw = dict(k=k, oversamples=10, maxp=cfg["maxp"], svd=2, bands=cfg["bands"], tol=cfg["tol"], seed=101,
+                  rand=1, precision=pb.PREC_FP32, standardize=False)
+        with pb.GpuContext(0) as ctx:
+            ctx.load_gl(P.T)
+            ctx.gl_freq(cfg["maxiter"], 1e-6)
+            ctx.gl_update()
+            r = ctx.rsvd(carry=False, **kw)
+            for _ in range(args.steps):
+                ctx.gl_update(r.U, r.S, r.V)
+            C, _, _ = ctx.gl_grm(r.U, r.S, r.V, vectors=False)
+        print(json.dumps({"profile_kernel": "pcangsd", "samples": N, "sites": m, "epochs": r.epochs,
+                          "checksum": float(np.trace(C))}))
+        return
     packed, N, M = pb.read_bed(prefix)
     if cfg["kind"] == "ld":  # one band-Gram launch over the first 60000 SNPs (150 MB packed)
         m = min(M, 60000)
@@ -897,6 +913,21 @@ def run_profile_kernel(args, cfg):
             t = ctx.ld_timing()
         print(json.dumps({"profile_kernel": "ld", "samples": N, "snps": m, "pairs": int(r2.size),
                           "device_ms": t[0], "gram_ms": t[1], "checksum": float(r2.sum())}))
+        return
+    if cfg["kind"] == "emu":  # the EMU imputation and the weighted epilogue gathers, 50000 SNPs
+        m = min(M, 50000)
+        kw = dict(k=cfg["k"], oversamples=10, maxp=cfg["maxp"], svd=2, bands=cfg["bands"], tol=cfg["tol"],
+                  seed=101, precision=args.precision)
+        with pb.GpuContext(0) as ctx:
+            ctx.load_bed(np.ascontiguousarray(packed[:m]), N)
+            ctx.permute(pb.shuffle_perm(m))
+            ctx.clear_imputed()
+            r = ctx.rsvd(standardize=False, **kw)
+            for _ in range(args.steps):
+                ctx.fit_emu(r.U, r.S, r.V, True)
+                r = ctx.rsvd(standardize=False, carry=True, **kw)
+        print(json.dumps({"profile_kernel": "emu", "samples": N, "snps": m, "epochs": r.epochs,
+                          "checksum": float(np.abs(r.S).sum())}))
         return
     l = cfg["k"] + max(10, cfg["k"])
     B = pb.omega(101, N, l)

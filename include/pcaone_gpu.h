@@ -261,6 +261,11 @@ int pcaone_gpu_gl_freq(pcaone_ctx* ctx, int maxiter, double tolmaf, double* F, i
 int pcaone_gpu_gl_update(pcaone_ctx* ctx, const double* U, const double* S, const double* V,
                          uint32_t k);
 
+/* Device time in ms of the posterior kernel of the last pcaone_gpu_gl_update call (CUDA
+ * events on the context's stream; the factor upload excluded). Measurement only; no
+ * reference counterpart. */
+int pcaone_gpu_gl_timing(pcaone_ctx* ctx, double* posterior_ms);
+
 /* PCAngsd genetic relationship matrix, the stage after the EM loop (src/Halko.cpp:317-331
  * with Data::pcangsd_standardize_E, src/Data.cpp:301-343). The posterior E is rebuilt in FP64
  * from U, S and V as pcaone_gpu_gl_update does (same arguments and index semantics), site j

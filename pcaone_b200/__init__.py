@@ -32,7 +32,8 @@ EXPORTS = ["pcaone_gpu_create", "pcaone_gpu_destroy", "pcaone_gpu_last_error",
            "pcaone_gpu_gl_update", "pcaone_gpu_gl_grm", "pcaone_gpu_product_t_noalloc",
            "pcaone_gpu_bed_to_gl", "pcaone_gpu_load_gl_f32", "pcaone_gpu_gram_product",
            "pcaone_gpu_residuals", "pcaone_gpu_load_dense", "pcaone_plink_perm",
-           "pcaone_gpu_ld_r2_f64", "pcaone_gpu_ld_timing", "pcaone_gpu_load_bed_host"]
+           "pcaone_gpu_ld_r2_f64", "pcaone_gpu_ld_timing", "pcaone_gpu_load_bed_host",
+           "pcaone_gpu_gl_timing"]
 
 
 class PcaoneError(RuntimeError):
@@ -92,6 +93,7 @@ def lib() -> ctypes.CDLL:
         L.pcaone_gpu_ld_timing.argtypes = [vp, vp, vp]
         L.pcaone_gpu_load_gl.argtypes = [vp, vp, u64, u32]
         L.pcaone_gpu_load_bed_host.argtypes = [vp, vp, u64, u32, u64]
+        L.pcaone_gpu_gl_timing.argtypes = [vp, vp]
         L.pcaone_gpu_gl_freq.argtypes = [vp, ctypes.c_int, ctypes.c_double, vp, vp]
         L.pcaone_gpu_bed_to_gl.argtypes = [vp]
         L.pcaone_gpu_load_gl_f32.argtypes = [vp, vp, u64, u32]
@@ -438,6 +440,13 @@ def _gl_update(self, U=None, S=None, V=None):
     self._check(lib().pcaone_gpu_gl_update(self._h, _ptr(Uf), _ptr(Sf), _ptr(Vf), len(S)))
 
 
+def _gl_timing(self) -> float:
+    """Device ms of the posterior kernel of the last gl_update (pcaone_gpu_gl_timing)."""
+    t = ctypes.c_double()
+    self._check(lib().pcaone_gpu_gl_timing(self._h, ctypes.byref(t)))
+    return t.value
+
+
 def _gl_grm(self, U, S, V, vectors=True):
     """PCAngsd GRM from the final factors (pcaone_gpu_gl_grm): returns (C, evecs, svals) with
     C nsamples x nsamples, evecs its singular vectors as columns (None unless vectors) and
@@ -469,6 +478,7 @@ def _bed_to_gl(self):
 GpuContext.product_t_noalloc = _product_t_noalloc
 GpuContext.bed_to_gl = _bed_to_gl
 GpuContext.load_gl = _load_gl
+GpuContext.gl_timing = _gl_timing
 GpuContext.gl_freq = _gl_freq
 GpuContext.gl_update = _gl_update
 GpuContext.gl_grm = _gl_grm

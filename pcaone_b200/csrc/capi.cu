@@ -98,10 +98,11 @@ void upload_factors(pcaone_ctx* c, const double* U, const double* S, const doubl
                     double** dV) {
   PG_REQUIRE(S && V && k >= 1 && k <= (uint32_t)pg::kLmax, PCAONE_EBADARG, "bad factors");
   std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
-  for (uint32_t i = 0; i < c->N; ++i)
-    for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
-  for (uint64_t j = 0; j < c->M; ++j)
-    for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
+  // column by column: sequential reads of the column-major inputs
+  for (uint32_t t = 0; t < k; ++t)
+    for (uint32_t i = 0; i < c->N; ++i) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+  for (uint32_t t = 0; t < k; ++t)
+    for (uint64_t j = 0; j < c->M; ++j) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
   *dUS = (double*)pg::scratch(c, "gl_US", us.size() * 8);
   *dV = (double*)pg::scratch(c, "gl_V", v.size() * 8);
   PG_CUDA(cudaMemcpyAsync(*dUS, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
@@ -360,10 +361,10 @@ int pcaone_gpu_fit_emu(pcaone_ctx* c, const double* U, const double* S, const do
     build_missing_by_snp(c);
     // US = U diag(S), row-major N x k; V row-major M x k
     std::vector<double> us((size_t)c->N * k), v((size_t)c->M * k);
-    for (uint32_t i = 0; i < c->N; ++i)
-      for (uint32_t t = 0; t < k; ++t) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
-    for (uint64_t j = 0; j < c->M; ++j)
-      for (uint32_t t = 0; t < k; ++t) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
+    for (uint32_t t = 0; t < k; ++t)  // column by column: sequential reads of the inputs
+      for (uint32_t i = 0; i < c->N; ++i) us[(size_t)i * k + t] = U[(size_t)t * c->N + i] * S[t];
+    for (uint32_t t = 0; t < k; ++t)
+      for (uint64_t j = 0; j < c->M; ++j) v[(size_t)j * k + t] = V[(size_t)t * c->M + j];
     c->d_imp_US = (double*)scratch(c, "d_imp_US", us.size() * 8);
     c->d_imp_V = (double*)scratch(c, "d_imp_V", v.size() * 8);
     PG_CUDA(cudaMemcpyAsync(c->d_imp_US, us.data(), us.size() * 8, cudaMemcpyHostToDevice, c->stream));
@@ -637,8 +638,20 @@ int pcaone_gpu_gl_update(pcaone_ctx* c, const double* U, const double* S, const 
     PG_REQUIRE(c->loaded && c->dense, PCAONE_ESTATE, "no likelihoods loaded");
     double *dUS = nullptr, *dV = nullptr;
     if (U) upload_factors(c, U, S, V, k, &dUS, &dV);
+    PG_CUDA(cudaEventRecord(c->ev0, c->stream));
     gl_posterior(c, dUS, dV, U ? (int)k : 0);
+    PG_CUDA(cudaEventRecord(c->ev1, c->stream));
     PG_CUDA(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    PG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->gl_post_ms = ms;
+  });
+}
+
+int pcaone_gpu_gl_timing(pcaone_ctx* c, double* posterior_ms) {
+  return guarded(c, [&] {
+    PG_REQUIRE(posterior_ms, PCAONE_EBADARG, "null timing output");
+    *posterior_ms = c->gl_post_ms;
   });
 }
 

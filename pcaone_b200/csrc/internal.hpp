@@ -72,6 +72,7 @@ struct pcaone_ctx {
   // device time of the last LD r2 call (CUDA events on the stream): all of its device work
   // (diagonal, tiling, band Gram) and the band-Gram launch alone; pairs it produced
   double ld_device_ms = 0.0, ld_gram_ms = 0.0;
+  double gl_post_ms = 0.0;  // device time of the last posterior kernel (pcaone_gpu_gl_update)
   int64_t ld_pairs = 0;
   // int8 decode-GEMM autotuner: pipeline variant per product shape (NP, rows, K, K chunks per
   // window, bytes per window)

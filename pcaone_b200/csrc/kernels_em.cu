@@ -25,35 +25,82 @@ __global__ void k_scale(const double* __restrict__ F, uint64_t M, int standardiz
   scale[j] = s;
 }
 
-__device__ __forceinline__ double imputed_value(const double* __restrict__ US, const double* __restrict__ V,
-                                                int k, int64_t i, int64_t j, double Fc) {
+// e = clip(sum_t US_it V_jt, -Fc, 1 - Fc) with one factor row in registers (`own`, the row
+// every entry of the thread's CSR row shares) and the other gathered (`row`, 16-byte loads
+// when k is even: the row then starts 16-byte aligned). KM >= k is a compile-time bound.
+template <int KM>
+__device__ __forceinline__ double imputed_dot(const double* own, const double* __restrict__ row, int k) {
   double g = 0.0;
-  for (int t = 0; t < k; ++t) g += US[i * k + t] * V[j * k + t];  // sum_k U S V^T
-  return fmin(fmax(g, -Fc), 1.0 - Fc);
+  if ((k & 1) == 0) {
+    const double2* r2 = reinterpret_cast<const double2*>(row);
+#pragma unroll
+    for (int t = 0; t < KM; t += 2)
+      if (t < k) {
+        const double2 v = __ldg(r2 + t / 2);
+        g += own[t] * v.x;  // sum_k U S V^T, in the order t = 0, 1, ...
+        g += own[t + 1] * v.y;
+      }
+  } else {
+#pragma unroll
+    for (int t = 0; t < KM; ++t)
+      if (t < k) g += own[t] * __ldg(row + t);
+  }
+  return g;
 }
 
-// by-SNP list: thread per entry, SNP found by the row of a grid-stride over rows (warp/row)
+// by-SNP list: warp per SNP row (V_j in registers), lanes over its entries (US_i gathered)
+template <int KM>
 __global__ void k_impute_snp(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, uint64_t M,
                              const double* __restrict__ US, const double* __restrict__ V, int k,
                              const double* __restrict__ Fc, double* __restrict__ val) {
   uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (j >= M) return;
-  for (int64_t e = ptr[j] + lane; e < ptr[j + 1]; e += 32)
-    val[e] = imputed_value(US, V, k, idx[e], (int64_t)j, Fc[j]);
+  double v[KM];
+#pragma unroll
+  for (int t = 0; t < KM; ++t) v[t] = t < k ? V[j * k + t] : 0.0;
+  const double fc = Fc[j];
+  for (int64_t e = ptr[j] + lane; e < ptr[j + 1]; e += 32) {
+    // same products and order as US_i . V_j
+    double g = 0.0;
+    const double* us = US + (int64_t)idx[e] * k;
+    if ((k & 1) == 0) {
+      const double2* u2 = reinterpret_cast<const double2*>(us);
+#pragma unroll
+      for (int t = 0; t < KM; t += 2)
+        if (t < k) {
+          const double2 u = __ldg(u2 + t / 2);
+          g += u.x * v[t];
+          g += u.y * v[t + 1];
+        }
+    } else {
+#pragma unroll
+      for (int t = 0; t < KM; ++t)
+        if (t < k) g += __ldg(us + t) * v[t];
+    }
+    val[e] = fmin(fmax(g, -fc), 1.0 - fc);
+  }
 }
 
-// (window, sample) list: CSR row r = i * nwin + b holds the SNPs of window b missing in sample i
+// (window, sample) list: CSR row r = i * nwin + b holds the SNPs of window b missing in sample
+// i; warp per row (US_i in registers), lanes over its entries (V_j gathered)
+template <int KM>
 __global__ void k_impute_ws(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, uint64_t rows,
                             uint32_t nwin, const double* __restrict__ US, const double* __restrict__ V,
                             int k, const double* __restrict__ Fc, double* __restrict__ val) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (r >= rows) return;
-  const int64_t i = (int64_t)(r / nwin);
-  for (int64_t e = ptr[r] + lane; e < ptr[r + 1]; e += 32) {
+  const int64_t i = (int64_t)(r / nwin), e0 = ptr[r], e1 = ptr[r + 1];
+  if (e0 == e1) return;
+  double us[KM];
+#pragma unroll
+  for (int t = 0; t < KM; ++t) us[t] = t < k ? US[i * k + t] : 0.0;
+  for (int64_t e = e0 + lane; e < e1; e += 32) {
     const int64_t j = idx[e];
-    val[e] = imputed_value(US, V, k, i, j, Fc[j]);
+    const double g = imputed_dot<KM>(us, V + j * k, k);
+    const double fc = Fc[j];
+    val[e] = fmin(fmax(g, -fc), 1.0 - fc);
   }
 }
 
@@ -91,9 +138,15 @@ void compute_imputed_snp(pcaone_ctx* c) {
   PG_REQUIRE(c->miss_snp_valid, PCAONE_ESTATE, "missing-entry list not built");
   c->d_miss_snp_val = (double*)scratch(c, "d_miss_snp_val", std::max<int64_t>(c->n_missing, 1) * 8);
   uint64_t threads = c->M * 32;
-  k_impute_snp<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-      c->d_miss_snp_ptr, c->d_miss_snp_idx, c->M, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
-      c->d_miss_snp_val);
+  auto go = [&](auto kern) {
+    kern<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(c->d_miss_snp_ptr, c->d_miss_snp_idx, c->M,
+                                                                   c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
+                                                                   c->d_miss_snp_val);
+  };
+  if (c->imp_k <= 8) go(k_impute_snp<8>);
+  else if (c->imp_k <= 16) go(k_impute_snp<16>);
+  else if (c->imp_k <= 32) go(k_impute_snp<32>);
+  else go(k_impute_snp<64>);
   PG_CHECK_LAUNCH();
   c->launches++;
 }
@@ -104,9 +157,15 @@ void compute_imputed_ws(pcaone_ctx* c) {
   c->d_miss_ws_val = (double*)scratch(c, "d_miss_ws_val", std::max<int64_t>(c->n_missing, 1) * 8);
   const uint64_t rows = (uint64_t)c->win.bands * c->Npad;
   uint64_t threads = rows * 32;
-  k_impute_ws<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-      c->d_miss_ws_ptr, c->d_miss_ws_idx, rows, (uint32_t)c->win.bands, c->d_imp_US, c->d_imp_V, c->imp_k, clip_freq(c),
-      c->d_miss_ws_val);
+  auto go = [&](auto kern) {
+    kern<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(c->d_miss_ws_ptr, c->d_miss_ws_idx, rows,
+                                                                   (uint32_t)c->win.bands, c->d_imp_US, c->d_imp_V,
+                                                                   c->imp_k, clip_freq(c), c->d_miss_ws_val);
+  };
+  if (c->imp_k <= 8) go(k_impute_ws<8>);
+  else if (c->imp_k <= 16) go(k_impute_ws<16>);
+  else if (c->imp_k <= 32) go(k_impute_ws<32>);
+  else go(k_impute_ws<64>);
   PG_CHECK_LAUNCH();
   c->launches++;
   c->miss_ws_val_valid = true;

@@ -63,7 +63,7 @@ __global__ void k_em_maf(const double* __restrict__ P, uint64_t M, uint32_t N, u
 // thread walks the sites of its CTA's slice; the loading row V[j] (M x k row-major) and F_j
 // are the same for every thread of the CTA (broadcast loads), the likelihood pair (one
 // double2) and the E entry are coalesced over the samples. Each sample-site is one 16-byte
-// read and one 4-byte write, four sites in flight per thread.
+// read and one 4-byte write, eight sites in flight per thread.
 template <int KM>
 __global__ void __launch_bounds__(128) k_posterior_e(const double* __restrict__ P, uint64_t M, uint32_t N, uint32_t ldp,
                                                      const double* __restrict__ F, const double* __restrict__ US,
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(128) k_posterior_e(const double* __restrict__ 
   double us[KM];
 #pragma unroll
   for (int t = 0; t < KM; ++t) us[t] = (V && t < k) ? US[(uint64_t)i * k + t] : 0.0;
-  constexpr int U4 = 4;
+  constexpr int U4 = 8;
   uint64_t j = ja;
   for (; j + U4 <= jb; j += U4) {
     double2 gl[U4];
@@ -661,9 +661,10 @@ void gl_em_maf(pcaone_ctx* c, int maxiter, double tolmaf, int* iters) {
 
 void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
   PG_REQUIRE(k <= kLmax, PCAONE_EBADARG, "too many factors for the posterior");
-  // grid: sample blocks of 128 x site slices, about eight CTAs an SM
+  // grid: sample blocks of 128 x site slices, about 16 CTAs an SM (two waves or more of the
+  // resident CTAs, so that the slices finish close together)
   const unsigned bx = (c->N + 127) / 128;
-  const uint64_t want = (8ull * c->sm_count + bx - 1) / bx;
+  const uint64_t want = (16ull * c->sm_count + bx - 1) / bx;
   const unsigned by = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (c->M + 63) / 64));
   const dim3 grid(bx, by);
   if (k <= 8)

@@ -342,6 +342,24 @@ def pinned_copy(arr):
         return np.ascontiguousarray(arr), None
 
 
+def capture_traffic(profile, alg_bytes_per_launch):
+    """DRAM traffic per launch scaled from a committed ncu summary of a smaller case of the same
+    kernel (its `traffic_bytes_per_launch` over its `algorithmic_bytes_per_launch`, both read
+    from the capture): the kernel's traffic grows with the packed bytes it streams."""
+    path = os.path.join(ROOT, "profiles", profile)
+    try:
+        vals = {}
+        for line in open(path):
+            for key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
+                if line.startswith(key + ":"):
+                    vals[key] = float(line.split(":")[1])
+        ratio = vals["traffic_bytes_per_launch"] / vals["algorithmic_bytes_per_launch"]
+    except (OSError, KeyError, ValueError):
+        return None, None
+    return int(alg_bytes_per_launch * ratio), f"profiles/{profile}: ncu capture of a smaller case, " \
+        f"traffic / algorithmic bytes = {ratio:.3f}, scaled to this launch size"
+
+
 def tensor_roofline(prec, l, alg_flops, prof):
     """Roofline of the dominant decode-GEMM from one profiled run (CUDA events around every
     decode-GEMM launch on the library's stream)."""
@@ -455,6 +473,10 @@ def run_rsvd_cfg(args, cfg, run):
         f"epilogue {prof.epilogue_ms:.1f}, updates {prof.update_ms:.1f}, epoch tail {prof.tail_ms:.1f}")
     l = cfg["k"] + max(10, cfg["k"])
     roofline = tensor_roofline(prec, l, 4.0 * M * N * l * prof.epochs, prof)
+    if prec == "mixed":  # each product streams the packed matrix once: 2 per epoch
+        alg_b = 2.0 * bed_bytes * prof.epochs / max(prof.gemm_launches, 1)
+        roofline["algorithmic_bytes_per_launch"] = int(alg_b)
+        roofline["traffic"], roofline["traffic_source"] = capture_traffic("k_decode_gemm_i8_c2s.md", alg_b)
 
     acc, extra = {}, {}
     if not args.skip_compare:

@@ -401,14 +401,19 @@ class Run:
     def __init__(self):
         self.rank, self.world, self.local = dist_env()
         self.dist = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            # NCCL between the GPUs; gloo on hosts without one (the CPU tests of this plumbing)
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = "cuda"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.dist = dist
 
     def barrier(self):
@@ -420,7 +425,7 @@ class Run:
             return x
         import torch
 
-        t = torch.tensor([x], device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 

@@ -252,13 +252,15 @@ class GpuContext:
         os_ = max(oversamples, k)  # src/Cmd.cpp:190
         o = RsvdOpts(k, os_, maxp, svd, bands, precision, int(standardize), ploidy, seed,
                      rand, tol, int(verbose), int(profile), int(carry), block_snps, band_factor)
-        U = np.zeros((k, self.N))
+        # column-major outputs (filled completely by the library): U and V are returned as
+        # Fortran-ordered (N x k, M x k) views, without a transposing copy
+        U = np.empty((k, self.N))
         S = np.zeros(k)
-        V = np.zeros((k, self.M)) if want_v else None
+        V = np.empty((k, self.M)) if want_v else None
         rep = RsvdReport()
         self._check(lib().pcaone_gpu_rsvd(self._h, ctypes.byref(o), _ptr(U), _ptr(S),
                                           _ptr(V), ctypes.byref(rep)))
-        return RsvdResult(U.T.copy(), S, V.T.copy() if V is not None else None, rep.epochs,
+        return RsvdResult(U.T, S, V.T if V is not None else None, rep.epochs,
                           rep.omega_updates, rep.last_diff, rep.gpu_ms, rep.gemm_ms,
                           rep.kernel_launches, rep.gemm_launches, rep.epilogue_ms,
                           rep.update_ms, rep.tail_ms, rep.host_ms, rep.h2d_bytes)

@@ -511,6 +511,9 @@ def run_rsvd_cfg(args, cfg, run):
                 extra[f"{p2}_path_ms"] = round(comp[p2].gpu_ms, 3)
         if "fp32" in comp:
             extra["speedup_vs_fp32_path"] = round(comp["fp32"].gpu_ms / ms_per_step, 3)
+            # the FP32 SIMT path's own rate: algorithmic flops of its products over its whole step
+            extra["fp32_path_tflops_algorithmic"] = round(
+                4.0 * M * N * l * comp["fp32"].epochs / (comp["fp32"].gpu_ms / 1e3) / 1e12, 2)
 
     # e2e: pinned host buffers -> device -> PCA -> host, through the C ABI
     pinned, keep = pinned_copy(packed)

@@ -113,7 +113,6 @@ struct pcaone_ctx {
   } slot[2];
   int slot_windows = 0;   // windows a slot holds for the current layout
   int cur_slot = -1;      // slot the products of the current run read
-  int last_slot = 1;      // slot staged most recently
   uint64_t streamed_h2d = 0;  // bytes copied to the device by window staging (cumulative)
 
   // PCAngsd (genotype-likelihood) mode: no packed codes; the RSVD runs on the dense float

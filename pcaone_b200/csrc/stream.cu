@@ -62,7 +62,6 @@ void stage(pcaone_ctx* c, int s, int b0, int b1, bool tiles) {
   S.b0 = b0;
   S.b1 = b1;
   S.key = slot_key(c, tiles);
-  c->last_slot = s;
   c->streamed_h2d += (s1 - s0) * c->pitch;
 }
 

@@ -339,18 +339,12 @@ int pcaone_gpu_rsvd(pcaone_ctx* c, const pcaone_rsvd_opts* opts, double* U, doub
 
 int pcaone_gpu_gram_product(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X,
                             uint32_t ncols, double* Y) {
-  return guarded(c, [&] {
-    require_resident(c, "the Gram product");
-    run_gram(c, precision, standardize, ploidy, X, (int)ncols, Y);
-  });
+  return guarded(c, [&] { run_gram(c, precision, standardize, ploidy, X, (int)ncols, Y); });
 }
 
 int pcaone_gpu_product(pcaone_ctx* c, int precision, int transpose, int standardize, int ploidy,
                        const double* B, uint32_t ncols, double* out) {
-  return guarded(c, [&] {
-    require_resident(c, "the product");
-    run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out);
-  });
+  return guarded(c, [&] { run_product(c, precision, transpose, standardize, ploidy, B, (int)ncols, out); });
 }
 
 int pcaone_gpu_fit_emu(pcaone_ctx* c, const double* U, const double* S, const double* V,

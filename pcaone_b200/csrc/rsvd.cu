@@ -188,6 +188,38 @@ struct Engine {
     gemm.omega_changed(c, Omg, l, Npad);
   }
 
+  // Y = Z (Z^T X) over the windows of the current layout (the Gram product of streamed
+  // genotypes, window run by window run): X (N x l, column-major host) takes Omega's place,
+  // the window sums go to H, and Y (column-major host) is read back.
+  void gram_windows(const double* X, double* Y, double* Gt = nullptr) {
+    std::vector<double> cm(X, X + (size_t)N * l);
+    double* d_cm = (double*)scratch(c, "r_omg_cm", cm.size() * 8);
+    PG_CUDA(cudaMemcpyAsync(d_cm, cm.data(), cm.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    const int64_t tot = Npad * l;
+    k_omega_layout<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(d_cm, N, l, Npad, Omg, Omg2, omg_float());
+    PG_CHECK_LAUNCH();
+    c->launches++;
+    colsum(c, Omg, l, N, wsum);
+    gemm.omega_changed(c, Omg, l, Npad);
+    G = Gbuf[0];
+    zero(c, H, Npad * l);
+    process_windows(0, c->win.bands, H);
+    double* cmaj = (double*)scratch(c, "r_out_cm", (size_t)Npad * l * 8);
+    k_to_colmajor<<<(unsigned)(((int64_t)N * l + 255) / 256), 256, 0, c->stream>>>(H, N, l, l, cmaj);
+    PG_CHECK_LAUNCH();
+    c->launches++;
+    if (Y) PG_CUDA(cudaMemcpyAsync(Y, cmaj, (size_t)N * l * 8, cudaMemcpyDeviceToHost, c->stream));
+    PG_CUDA(cudaStreamSynchronize(c->stream));  // cm (host) and Y complete
+    if (Gt) {  // Z^T X of every window (G rows, current SNP order), column-major
+      double* gm = (double*)scratch(c, "r_out_g", (size_t)M * l * 8);
+      k_to_colmajor<<<(unsigned)((M * l + 255) / 256), 256, 0, c->stream>>>(G, M, l, l, gm);
+      PG_CHECK_LAUNCH();
+      c->launches++;
+      PG_CUDA(cudaMemcpyAsync(Gt, gm, (size_t)M * l * 8, cudaMemcpyDeviceToHost, c->stream));
+      PG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+  }
+
   // Omega = flipOmg(Omega2, thinQ(Householder QR of H)); Omega2 = Omega. With H2, the sketch
   // is H = H1 + H2 (written to H); otherwise H1 is the sketch itself.
   void update_omega(double* H1in, const double* H2in) {
@@ -876,11 +908,55 @@ void gram_t(pcaone_ctx* c, GemmFnT<T> gemm, const double* X, int l, double* Y) {
     for (int j = 0; j < l; ++j) Y[(size_t)j * N + i] = rm[(size_t)i * l + j];
 }
 
+// The Gram product on streamed genotypes (the out-of-core matvec of ArnoldiOpData::perform_op,
+// src/Arnoldi.cpp:18-46, block by block): the blocks of the Halko plan on streamed data
+// (blocks whose slot contents fit the slot budget), each window run staged into a device slot.
+// Y = Z Z^T X (Y may be null) and, with Gt, Z^T X itself (the single product on streamed
+// genotypes comes out of the same pass over the windows).
+void run_gram_streamed(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X, int l,
+                       double* Y, double* Gt = nullptr) {
+  PG_REQUIRE(precision != PCAONE_PREC_BF16, PCAONE_EBADARG,
+             "the split-BF16 back end needs the genotypes resident on the device");
+  PG_REQUIRE((uint32_t)l <= c->N, PCAONE_EBADARG, "more columns than samples");
+  uint64_t blocksize = std::max<uint64_t>(kRowPad, c->slot_budget / (4ull * c->pitch) / kRowPad * kRowPad);
+  blocksize = std::min<uint64_t>(blocksize, c->M);
+  const int bands = (int)((c->M + blocksize - 1) / blocksize);
+  stream_prepare(c, bands, blocksize, precision == PCAONE_PREC_MIXED);
+  if (c->imputed) compute_imputed_ws(c);
+  compute_scale(c, standardize, ploidy);
+  pcaone_rsvd_opts o{};
+  o.k = l;
+  o.oversamples = 0;
+  o.svd = 1;
+  o.bands = bands;
+  o.precision = precision;
+  o.ploidy = ploidy;
+  if (precision == PCAONE_PREC_FP64) {
+    Engine<double> e(c, o, gemm_simt_double());
+    e.gram_windows(X, Y, Gt);
+  } else if (precision == PCAONE_PREC_FP32) {
+    Engine<float> e(c, o, gemm_simt_float());
+    e.gram_windows(X, Y, Gt);
+  } else if (precision == PCAONE_PREC_MIXED) {
+    PG_REQUIRE(tc_supported(c), PCAONE_ENODEV, "tcgen05 path needs an sm_100 device");
+    tc_clear_error(c);
+    Engine<float> e(c, o, gemm_i8());
+    e.gram_windows(X, Y, Gt);
+    tc_check_error(c);
+  } else {
+    throw Error(PCAONE_EBADARG, "unknown precision");
+  }
+}
+
 void run_gram(pcaone_ctx* c, int precision, int standardize, int ploidy, const double* X, int l, double* Y) {
   PG_REQUIRE(c->loaded, PCAONE_ESTATE, "no genotypes loaded");
   PG_REQUIRE(X && Y && l >= 1 && l <= kLmax, PCAONE_EBADARG, "bad gram-product operands");
   PG_REQUIRE(ploidy == 1 || ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
   PG_REQUIRE(!c->dense, PCAONE_ESTATE, "products need packed genotypes (load_bed)");
+  if (c->streamed) {
+    run_gram_streamed(c, precision, standardize, ploidy, X, l, Y);
+    return;
+  }
   build_transposed(c, 1);
   build_missing_by_snp(c);
   build_missing_by_window_sample(c);
@@ -907,6 +983,11 @@ void run_product(pcaone_ctx* c, int precision, int transpose, int standardize, i
   PG_REQUIRE(transpose == 0 || transpose == 1, PCAONE_EBADARG, "transpose must be 0 or 1");
   PG_REQUIRE(ploidy == 1 || ploidy == 2, PCAONE_EBADARG, "ploidy must be 1 or 2");
   PG_REQUIRE(!c->dense, PCAONE_ESTATE, "products need packed genotypes (load_bed)");
+  if (c->streamed) {  // Z^T B from a pass over the streamed windows; Z B needs them resident
+    if (transpose == 1) require_resident(c, "the product Z B");
+    run_gram_streamed(c, precision, standardize, ploidy, B, l, nullptr, out);
+    return;
+  }
   build_transposed(c, 1);
   build_missing_by_snp(c);
   build_missing_by_window_sample(c);

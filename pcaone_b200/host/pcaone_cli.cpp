@@ -967,10 +967,11 @@ int main(int argc, char** argv) {
 
   pcaone_ctx* ctx = nullptr;
   if (pcaone_gpu_create(p.device, &ctx) != PCAONE_OK) fail("no usable CUDA device");
-  // out-of-core RSVD (-m with -d 1 or 2): the genotypes are streamed from host memory; the
-  // IRAM products, LD and the residual writer read them resident
+  // out-of-core mode (-m): the genotypes are streamed from host memory for the RSVD (-d 1, 2)
+  // and for IRAM (-d 0) when its operator is Z Z^T (samples <= SNPs); LD and the residual
+  // writer read them resident
   const bool ld_mode = p.print_r2 || p.ld_r2 > 0 || !p.clump.empty();
-  const bool streamed = p.memory > 0 && p.svd != 0 && !p.ld_write && !ld_mode;
+  const bool streamed = p.memory > 0 && !p.ld_write && !ld_mode && (p.svd != 0 || N <= M0);
   if (streamed)
     check(ctx, pcaone_gpu_load_bed_host(ctx, packed.data(), M0, (uint32_t)N, 0), "load_bed_host");
   else
@@ -1103,7 +1104,7 @@ int main(int argc, char** argv) {
     // Z Z^T by restarted Lanczos, each operator application one device gram product; then
     // S = sqrt(eigenvalues), U = eigenvectors, V = Z^T U / S. FP64 products unless --precision
     // is given (the Lanczos residuals need the operator to full precision).
-    g_log.print(date(), "running IRAM SVD with in-core mode.");
+    g_log.print(date(), streamed ? "running IRAM SVD with out-of-core mode." : "running IRAM SVD with in-core mode.");
     const int prec = p.precision_set ? p.precision : PCAONE_PREC_FP64;
     const int stdz = (p.scale == 0 || p.ld_write) ? 0 : 1, ploidy = p.haploid ? 1 : 2;
     auto op = [&](const double* x, double* y) {

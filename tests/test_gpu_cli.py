@@ -92,6 +92,18 @@ def test_cli_iram_matches_reference_outputs(tmp_path):
 
 
 @pytest.mark.gpu
+def test_cli_iram_out_of_core_matches_reference_outputs(tmp_path):
+    """--svd 0 with -m: the same Lanczos on the Gram product of streamed genotypes (blocks
+    staged into device slots) gives the reference's IRAM outputs."""
+    r = run_cli(golden_args("g1_iram", tmp_path) + ["-m", "0.0001"], tmp_path)
+    assert "out-of-core" in r.stdout
+    out = str(tmp_path / "g1_iram")
+    assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table("g1_iram", ".eigvals")[:, 0], 1e-5)
+    assert_cols_close(O.read_table(out + ".eigvecs"), ref_table("g1_iram", ".eigvecs"), 5e-4)
+    assert_cols_close(O.read_table(out + ".loadings"), ref_table("g1_iram", ".loadings"), 5e-4)
+
+
+@pytest.mark.gpu
 def test_cli_emu_matches_reference_outputs(tmp_path):
     run_cli(golden_args("g2_emu", tmp_path), tmp_path)
     out = str(tmp_path / "g2_emu")

@@ -110,11 +110,28 @@ def test_streamed_emu_matches_resident(gpu):
     assert_eig_close(eig2, ref_eigvals("g2_emu"), 1e-5)
 
 
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 2e-6), ("mixed", 5e-6)])
+def test_streamed_gram_and_product_match_resident(gpu, prec, tol):
+    """The IRAM operator Z (Z^T X) and the product Z^T B over streamed blocks (one window per
+    slot) against the resident whole-matrix products, at the product tolerances."""
+    bed = random_bed(777, 3001, seed=21, miss=0.02)
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((bed.N, 5))
+    B = rng.standard_normal((bed.N, 6))
+    gpu.load_bed(bed.packed, bed.N)
+    y_res, g_res = gpu.gram_product(X, precision=prec), gpu.product_t(B, precision=prec)
+    gpu.load_bed_host(bed.packed, bed.N, ONE_WINDOW)
+    y_str, g_str = gpu.gram_product(X, precision=prec), gpu.product_t(B, precision=prec)
+    rel = lambda a, b: float((np.abs(a - b).max(axis=0) / np.abs(b).max(axis=0)).max())
+    assert rel(y_str, y_res) <= 2 * tol
+    assert rel(g_str, g_res) <= 2 * tol
+
+
 def test_streamed_rejects_resident_only_calls(gpu):
     bed = random_bed(300, 1200, seed=2)
     gpu.load_bed_host(bed.packed, bed.N)
     with pytest.raises(pb.PcaoneError) as e:
-        gpu.product_t(np.zeros((bed.N, 4)), precision="fp32")
+        gpu.product(np.zeros((bed.M, 4)), precision="fp32")
     assert e.value.status == 6 and "streamed" in str(e.value)
     with pytest.raises(pb.PcaoneError) as e:
         gpu.rsvd(k=4, svd=2, bands=8, precision="bf16")

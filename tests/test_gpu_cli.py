@@ -95,9 +95,9 @@ def test_cli_iram_matches_reference_outputs(tmp_path):
 def test_cli_iram_out_of_core_matches_reference_outputs(tmp_path):
     """--svd 0 with -m: the same Lanczos on the Gram product of streamed genotypes (blocks
     staged into device slots) gives the reference's IRAM outputs."""
-    r = run_cli(golden_args("g1_iram", tmp_path) + ["-m", "0.0001"], tmp_path)
-    assert "out-of-core" in r.stdout
+    run_cli(golden_args("g1_iram", tmp_path) + ["-m", "0.0001"], tmp_path)
     out = str(tmp_path / "g1_iram")
+    assert "running IRAM SVD with out-of-core mode." in open(out + ".log").read()
     assert_eig_close(O.read_table(out + ".eigvals")[:, 0], ref_table("g1_iram", ".eigvals")[:, 0], 1e-5)
     assert_cols_close(O.read_table(out + ".eigvecs"), ref_table("g1_iram", ".eigvecs"), 5e-4)
     assert_cols_close(O.read_table(out + ".loadings"), ref_table("g1_iram", ".loadings"), 5e-4)

@@ -72,9 +72,12 @@ int pcaone_gpu_load_bed(pcaone_ctx* ctx, const uint8_t* packed, uint64_t nsnps,
  * Replaces the out-of-core reader FileBed::read_block_initial / read_block_update
  * (src/FilePlink.cpp:133-294) over the block plan of Data::prepare (src/Data.cpp:16-72); the
  * winSVD windows are the plan's blocks when pcaone_rsvd_opts.block_snps is set, and Halko
- * sums its products over blocks. pcaone_gpu_permute permutes the host records. The
- * products, LD, residual and pseudo-likelihood calls need resident genotypes and return
- * PCAONE_ESTATE on a streamed matrix. */
+ * sums its products over blocks. pcaone_gpu_permute permutes the host records.
+ * pcaone_gpu_gram_product and pcaone_gpu_product with transpose = 0 (Z^T B) also run over
+ * the streamed blocks (FP32, FP64, mixed; the IRAM operator of the out-of-core Arnoldi,
+ * src/Arnoldi.cpp:18-46). Z B (transpose = 1), LD, residual, pseudo-likelihood and the
+ * allocation-free product need resident genotypes and return PCAONE_ESTATE on a streamed
+ * matrix. */
 int pcaone_gpu_load_bed_host(pcaone_ctx* ctx, const uint8_t* packed, uint64_t nsnps,
                              uint32_t nsamples, uint64_t slot_bytes);
 

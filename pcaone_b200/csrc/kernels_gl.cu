@@ -679,7 +679,7 @@ void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k) {
   c->launches++;
 }
 
-#define PG_BLAS(call)                                                                          \
+#define PG_SOLVER(call)                                                                          \
   do {                                                                                         \
     const int st_ = (int)(call);                                                               \
     PG_REQUIRE(st_ == 0, PCAONE_ECUDA, std::string(#call) + " failed with status " + std::to_string(st_)); \
@@ -722,18 +722,18 @@ void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, 
     // eigenvectors ordered by decreasing |eigenvalue|
     if (!c->solver) {
       cusolverDnHandle_t h = nullptr;
-      PG_BLAS(cusolverDnCreate(&h));
+      PG_SOLVER(cusolverDnCreate(&h));
       c->solver = h;
     }
     cusolverDnHandle_t sol = (cusolverDnHandle_t)c->solver;
-    PG_BLAS(cusolverDnSetStream(sol, c->stream));
+    PG_SOLVER(cusolverDnSetStream(sol, c->stream));
     double* W = (double*)scratch(c, "grm_W", (size_t)N * 8);
     int* info = (int*)scratch(c, "grm_info", sizeof(int));
     int lwork = 0;
-    PG_BLAS(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W,
+    PG_SOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W,
                                         &lwork));
     double* work = (double*)scratch(c, "grm_work", (size_t)std::max(lwork, 1) * 8);
-    PG_BLAS(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W, work,
+    PG_SOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)N, dC, (int)N, W, work,
                              lwork, info));
     std::vector<double> w(N), vec(evecs ? n2 : 0);
     int hinfo = 0;

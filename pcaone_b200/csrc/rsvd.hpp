@@ -59,7 +59,7 @@ void gl_posterior(pcaone_ctx* c, const double* US, const double* V, int k);
 // PCAngsd GRM (pcaone_gpu_gl_grm): C (host N x N, or null), its singular vectors (host N x N
 // column-major, or null) and values (host N, or null); US, V as for gl_posterior.
 void gl_grm(pcaone_ctx* c, const double* US, const double* V, int k, double* C, double* evecs, double* svals);
-// Frees the context's cuBLAS / cuSOLVER handles.
+// Frees the context's cuSOLVER handle.
 void gl_release(pcaone_ctx* c);
 
 void omega_host(int seed, int rand, uint64_t nrow, uint32_t ncol, double* out);

@@ -54,3 +54,36 @@ def test_create_without_device_fails_cleanly():
             "try:\n    pb.GpuContext(999)\nexcept pb.PcaoneError as e:\n    print('ERR', e.status)\n")
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT)
     assert "ERR 7" in out.stdout, out.stdout + out.stderr
+
+
+def test_ld_windows_match_oracle():
+    """The package's window helper (bisection on sorted positions, a scan otherwise) against
+    the oracle's restatement of divide_pos_by_window: the golden .bim, a synthetic three-
+    chromosome layout with repeated positions, and an unsorted chromosome."""
+    import os
+
+    import numpy as np
+
+    import pcaone_b200 as pb
+    from oracle import pcaone_oracle as O
+    from tests.helpers import GOLDEN
+
+    bim = os.path.join(GOLDEN, "g4.bim")
+    pos, ends = pb.read_bim_positions(bim)
+    for bp in (1, 500, 5000, 10 ** 9):
+        ws, we = pb.ld_windows(pos, ends, bp)
+        snp = O.read_snp_pos(bim)
+        O.divide_pos_by_window(snp, bp)
+        np.testing.assert_array_equal(ws, snp.ws)
+        np.testing.assert_array_equal(we, snp.we)
+    rng = np.random.default_rng(4)
+    chrom = [np.sort(rng.integers(0, 20000, 300)), np.sort(rng.integers(0, 5000, 120)),
+             rng.integers(0, 9000, 200)]  # the last one unsorted
+    pos = np.concatenate(chrom)
+    ends = list(np.cumsum([len(c) for c in chrom]) - 1)
+    for bp in (0, 37, 1000):
+        ws, we = pb.ld_windows(pos, ends, bp)
+        snp = O.SnpLD(["1", "2", "3"], pos.astype(np.int64), ends, [])
+        O.divide_pos_by_window(snp, bp)
+        np.testing.assert_array_equal(ws, snp.ws)
+        np.testing.assert_array_equal(we, snp.we)

@@ -239,3 +239,18 @@ def test_oracle_block_plan_windows():
     bed = g("g1")
     assert O.block_plan(bed.N, bed.M, 4, 10, 0.0001, 8) == (63, 3)
     assert O.block_plan(bed.N, bed.M, 4, 10, 0.0003, 8) == (188, 1)
+
+
+def test_reference_iram_out_of_core_equals_in_core(tmp_path):
+    """The reference's -d 0 with -m (its block-by-block Arnoldi operator) prints the same
+    outputs as its in-core IRAM golden, which the streamed IRAM CLI test compares against."""
+    ref = os.path.join(os.path.dirname(O._HERE), "oracle", "_ref", "PCAone")
+    if not os.path.exists(ref):
+        pytest.skip("reference binary not built")
+    out = str(tmp_path / "iram_m")
+    r = subprocess.run([ref, "-b", os.path.join(GOLDEN, "g1"), "-d", "0", "-k", "4", "-V", "-m", "0.0001",
+                        "-o", out], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "out-of-core" in open(out + ".log").read()
+    for ext in (".eigvals", ".eigvecs", ".loadings"):
+        assert_cols_close(O.read_table(out + ext), ref_table("g1_iram", ext), 1e-6)

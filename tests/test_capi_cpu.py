@@ -87,3 +87,28 @@ def test_ld_windows_match_oracle():
         O.divide_pos_by_window(snp, bp)
         np.testing.assert_array_equal(ws, snp.ws)
         np.testing.assert_array_equal(we, snp.we)
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/pcaone_gpu.h is a C header (the boundary a cgo / ctypes / C caller binds): it
+    compiles as C99 with -pedantic, and as C++11."""
+    import os
+    import shutil
+    import subprocess
+
+    import pytest
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "use.c"
+    src.write_text('#include <string.h>\n#include "pcaone_gpu.h"\nint main(void) {\n'
+                   '  pcaone_rsvd_opts o; pcaone_rsvd_report r;\n'
+                   '  memset(&o, 0, sizeof o); memset(&r, 0, sizeof r);\n'
+                   '  int (*fn)(pcaone_ctx*, const pcaone_rsvd_opts*, double*, double*, double*,\n'
+                   '            pcaone_rsvd_report*) = pcaone_gpu_rsvd;\n'
+                   '  (void)fn;\n  return o.k != 0 || r.epochs != 0;\n}\n')
+    for cc, std, lang in (("gcc", "-std=c99", "c"), ("g++", "-std=c++11", "c++")):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not available")
+        r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-x", lang,
+                            "-I", os.path.join(root, "include"), str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
